@@ -1,0 +1,324 @@
+#!/usr/bin/env python3
+"""Benchmark of the path-tracing hot path (one JSON line on rank 0).
+
+Workload ("large" configuration): ~1.15M triangles in 256 seeded instances,
+DSPBR materials over the whole feature set, 2048x1024 log-normal HDR
+environment with a 1e4 sun, 1920x1080, 12 bounces, MWC RNG of the reference.
+A step is one progressive frame: one sample per pixel, all bounces, NEE,
+accumulation.  Metric: Mrays/s (primary + extension + shadow rays).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the reference's own CPU implementation (its fragment
+shader compiled for the host, oracle/_ref) on a bounded pixel sample of the
+same workload with all host threads.  Under torchrun (N>1) every rank renders
+its own replica of the frame stream (weak scaling, no collective on the data
+path); the reported value is the sum of rays over ranks / max device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dspbr-pt_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if self.proc is None or not self.path:
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        return rank, ws, local, dist
+    return 0, 1, 0, None
+
+
+def reduce_max(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def make_workload():
+    from dspbr import synth
+    from dspbr.viewport import Bvh
+    sc = synth.make_large(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    return sc
+
+
+def config_of(sc):
+    return {"workload": "large: 256 seeded instances (displaced grids + icospheres), DSPBR feature-set materials, "
+                        "2048x1024 log-normal HDR env + 1e4 sun", "triangles": int(sc.num_triangles),
+            "bvh_nodes": int(sc.bvh.nodes.size // 16), "width": sc.width, "height": sc.height,
+            "max_bounces": sc.max_bounces, "spp_per_step": 1, "rng": "mwc (reference rng.glsl)",
+            "env_sampling": "alias", "l2": "inputs larger than L2 (BVH + triangles + vertices + env ~ 230 MB)",
+            "seed": sc.seed}
+
+
+def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0):
+    """Times oracle/_ref (the reference shader compiled for the host) on pixel
+    samples of the workload; returns (Mrays/s, cores, sample description, per-step values)."""
+    from oracle import ref_lib
+    kind = "reference"
+    if not ref_lib.available("f32"):
+        return None
+    ref = ref_lib.GlslReference("f32")
+    ref.set_scene(sc.vertices, sc.indices, sc.materials, sc.bvh.nodes, sc.bvh.indices)
+    ref.set_ibl(sc.env)
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    npx = 4096
+    vals = []
+    tot_rays, tot_t = 0, 0.0
+    step = 0
+    t_start = time.perf_counter()
+    while True:
+        xy = np.stack([rng.integers(0, sc.width, npx), rng.integers(0, sc.height, npx)], 1).astype(np.int32)
+        ref.set_uniforms(ref_lib.uniform_block(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, sc.width,
+                                               sc.height, step + 1, sc.max_bounces))
+        t0 = time.perf_counter()
+        _, rays = ref.render_pixels(xy, sc.width, sc.height, cores)
+        dt = time.perf_counter() - t0
+        if step >= warmup:
+            vals.append(rays / dt / 1e6)
+            tot_rays += rays
+            tot_t += dt
+        step += 1
+        if steps is not None and step >= steps + warmup:
+            break
+        if steps is None and time.perf_counter() - t_start > seconds:
+            break
+    sample = f"{npx} random pixels x 1 sample per step, {len(vals)} steps ({tot_t:.1f} s of CPU time), same scene/BVH/env"
+    return tot_rays / tot_t / 1e6, cores, sample, vals, kind
+
+
+def run_reference_arm(args):
+    rank, ws, local, dist = dist_setup()
+    if rank != 0:
+        return 0
+    sc = make_workload()
+    res = cpu_reference_sample(sc, steps=args.steps, warmup=args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference shaders compiled for the host) "
+                                                              "was not built"}))
+        return 0
+    value, cores, sample, vals, kind = res
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(sc), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_gpu_arm(args):
+    rank, ws, local, dist = dist_setup()
+    from dspbr import _lib
+    from dspbr.viewport import PathtracingViewport, PathtracingCamera
+
+    sc = make_workload()
+    v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
+                            settings={"maxBounces": sc.max_bounces})
+    v.setScene(sc)
+    v.setIBL(sc.env)
+    v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
+    lib, h = v.ctx.lib, v.ctx.h
+    # warm-up frames (untimed)
+    v.ctx.check(lib.dspbr_render(h, args.warmup))
+    # ---- device-timed region: K frames, events on the render stream ----
+    v.ctx.check(lib.dspbr_set_profiling(h, 1))
+    d0 = v.diagnostics
+    barrier(dist)
+    with ClockSampler(local) as clocks:
+        v.ctx.check(lib.dspbr_render(h, args.steps))
+    barrier(dist)
+    d1 = v.diagnostics
+    dev_ms = d1["last_render_ms"]
+    rays = (d1["rays_primary"] + d1["rays_extension"] + d1["rays_shadow"]) - \
+           (d0["rays_primary"] + d0["rays_extension"] + d0["rays_shadow"])
+    v.ctx.check(lib.dspbr_set_profiling(h, 0))
+    t_max = reduce_max(dist, dev_ms)
+    rays_all = reduce_sum(dist, float(rays))
+    value = rays_all / (t_max * 1e-3) / 1e6
+    extend_ms, extend_launches = d1["extend_ms"], d1["extend_launches"]
+    gpu_launches = int(d1["extend_launches"] + d1["connect_launches"] + d1["shade_launches"] + d1["other_launches"])
+
+    # ---- traversal work of one more frame (untimed), for the roofline ----
+    v.ctx.check(lib.dspbr_set_counting(h, 1))
+    v.ctx.check(lib.dspbr_set_profiling(h, 1))
+    v.ctx.check(lib.dspbr_render(h, 1))
+    d2 = v.diagnostics
+    v.ctx.check(lib.dspbr_set_counting(h, 0))
+    v.ctx.check(lib.dspbr_set_profiling(h, 0))
+    alg_bytes_frame = 64.0 * d2["nodes_closest"] + 40.0 * d2["tris_closest"]
+    rays_closest_frame = (d2["rays_primary"] + d2["rays_extension"]) - (d1["rays_primary"] + d1["rays_extension"])
+    peak, peak_kind = peaks()
+    ext_ms_frame = extend_ms / max(1, args.steps)
+    achieved = alg_bytes_frame / (ext_ms_frame * 1e-3) / 1e9 if ext_ms_frame > 0 else None
+
+    # ---- end to end through the public API: per step camera upload (H2D),
+    #      one frame, read back of the accumulation buffer (D2H) ----
+    cam = PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near)
+    v.resetAccumulation()
+    e2e_steps = max(1, min(args.steps, 5))
+    d3 = v.diagnostics
+    barrier(dist)
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        v.setCamera(cam)
+        v.start(1)
+        img = v.readAccumulation()
+    t1 = time.perf_counter()
+    d4 = v.diagnostics
+    rays_e2e = (d4["rays_primary"] + d4["rays_extension"] + d4["rays_shadow"]) - \
+               (d3["rays_primary"] + d3["rays_extension"] + d3["rays_shadow"])
+    e2e_t = reduce_max(dist, t1 - t0)
+    e2e_rays = reduce_sum(dist, float(rays_e2e))
+    e2e_value = e2e_rays / e2e_t / 1e6
+    cs = clocks.summary()
+
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            r = cpu_reference_sample(sc, seconds=12.0)
+            if r is not None:
+                cpu = {"value": r[0], "unit": "Mrays/s", "cores": r[1], "kind": r[4], "sample": r[2]}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene + env map, no assets)",
+            "config": config_of(sc),
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 + 8 + 4 * 52,
+                    "d2h_bytes_per_step": int(img.nbytes), "steps": e2e_steps},
+            "gpu_launches": gpu_launches,
+            "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": None,
+                         "bytes_per_frame": alg_bytes_frame, "closest_rays_per_frame": rays_closest_frame,
+                         "nodes_per_ray": d2["nodes_closest"] / max(1, rays_closest_frame),
+                         "tris_per_ray": d2["tris_closest"] / max(1, rays_closest_frame),
+                         "extend_ms_per_frame": ext_ms_frame,
+                         "connect_ms_per_frame": d1["connect_ms"] / max(1, args.steps),
+                         "shade_ms_per_frame": d1["shade_ms"] / max(1, args.steps)},
+            "cpu_baseline": cpu,
+            "clocks": cs,
+            "rays_per_step": rays / max(1, args.steps),
+            "traversal_aborted": d1["traversal_aborted"],
+        }
+        print(json.dumps(line))
+    v.dispose()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,873 @@
+// C ABI of libdspbr_cuda.so (include/dspbr.h): contexts, scenes, IBLs, the
+// progressive render loop and the kernel-level query entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dspbr.h"
+#include "kernels.h"
+
+using namespace dspbr;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    reset();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    else p = nullptr;
+    return e;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+struct Status {
+  std::string* err;
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (err) *err = buf;
+    return code;
+  }
+  int cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return DSPBR_OK;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? DSPBR_ERR_OOM : DSPBR_ERR_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+  }
+};
+
+#define TRY_CUDA(st, expr, what)                 \
+  do {                                           \
+    int rc_ = (st).cuda((expr), (what));         \
+    if (rc_ != DSPBR_OK) return rc_;             \
+  } while (0)
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+struct dspbr_scene {
+  dspbr_ctx* ctx = nullptr;
+  DevBuf<float4> nodes, tris, verts, materials;
+  DevBuf<uint32_t> indices;
+  uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
+  double bvh_build_ms = 0, upload_ms = 0;
+  DevScene view() const {
+    DevScene s;
+    s.nodes = nodes.p; s.tris = tris.p; s.verts = verts.p; s.indices = indices.p; s.materials = materials.p;
+    s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
+    s.num_materials = int(num_materials);
+    return s;
+  }
+  uint64_t bytes() const { return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes(); }
+};
+
+struct dspbr_ibl {
+  dspbr_ctx* ctx = nullptr;
+  DevBuf<float4> rgba;
+  DevBuf<float> pdf, cdf, ypdf, ycdf, alias_prob, lum, rowsum;
+  DevBuf<int> alias_idx;
+  DevBuf<double> total;
+  double total_sum = 0;
+  int w = 0, h = 0;
+  DevIbl view() const {
+    DevIbl e;
+    e.rgba = rgba.p; e.pdf = pdf.p; e.cdf = cdf.p; e.ypdf = ypdf.p; e.ycdf = ycdf.p;
+    e.alias_prob = alias_prob.p; e.alias_idx = alias_idx.p; e.w = w; e.h = h;
+    return e;
+  }
+};
+
+struct dspbr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  dspbr_params params{};
+  float matrix[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  float fov = 45.f, near_plane = 0.01f;
+  bool has_camera = false;
+  int width = 0, height = 0;
+  dspbr_scene* scene = nullptr;
+  dspbr_ibl* ibl = nullptr;
+  uint32_t wave_paths = 1u << 21;
+  // path state
+  uint32_t capacity = 0;
+  DevBuf<float4> org, dir, weight, rad, hit, sh_dir, sh_c, pl_dir, pl_c, result;
+  DevBuf<uint64_t> rng;
+  DevBuf<int> sh_flags;
+  DevBuf<uint32_t> q0, q1, qs, counts;
+  DevBuf<unsigned long long> stats;
+  DevBuf<double4> accum;
+  DevBuf<float4> mean;
+  uint64_t sample_count = 0;
+  uint64_t rays_primary = 0;
+  double last_render_ms = 0;
+  bool pending = false;
+  bool counting = false;
+  bool profiling = false;
+  // profiling: event pairs per launch, resolved at dspbr_wait
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_marks;  // (kind, first event index)
+  size_t ev_used = 0;
+  double kind_ms[3] = {0, 0, 0};
+  uint64_t kind_launches[4] = {0, 0, 0, 0};
+  Status st() { return Status{&err}; }
+  cudaEvent_t next_event() {
+    if (ev_used == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_used++];
+  }
+  void mark_begin(int kind) {
+    if (!profiling) return;
+    ev_marks.push_back({kind, int(ev_used)});
+    cudaEventRecord(next_event(), stream);
+  }
+  void mark_end() {
+    if (profiling) cudaEventRecord(next_event(), stream);
+  }
+  void resolve_marks() {
+    for (auto& m : ev_marks) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev_pool[m.second], ev_pool[m.second + 1]);
+      kind_ms[m.first] += ms;
+    }
+    ev_marks.clear();
+    ev_used = 0;
+  }
+  ~dspbr_ctx() {
+    for (auto e : ev_pool) cudaEventDestroy(e);
+  }
+};
+
+extern "C" {
+
+void dspbr_params_default(dspbr_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->max_bounces = 8;
+  p->use_ibl = 1;
+  p->ibl_rotation_deg = 0.f;
+  p->background_from_ibl = 1;
+  p->background_color[0] = 0.f; p->background_color[1] = 0.f; p->background_color[2] = 0.f;
+  p->background_color[3] = 1.f;
+  p->ray_eps = 0.0001f;
+  p->clamp_threshold = 3.0f;
+  p->rr_start_depth = 2;
+  p->rr_termination_prob = 0.1f;
+  p->profile = DSPBR_PROFILE_FULL;
+  p->rng = DSPBR_RNG_MWC;
+  p->seed = 0;
+  p->env_sampling = DSPBR_ENV_ALIAS;
+}
+
+int dspbr_device_count(int* count) {
+  if (!count) return DSPBR_ERR_INVALID;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) { cudaGetLastError(); *count = 0; return DSPBR_ERR_CUDA; }
+  *count = n;
+  return DSPBR_OK;
+}
+
+int dspbr_create(int device, dspbr_ctx** out) {
+  if (!out) return DSPBR_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return DSPBR_ERR_CUDA;
+  }
+  auto* c = new dspbr_ctx();
+  c->device = device;
+  dspbr_params_default(&c->params);
+  Status s = c->st();
+  if (s.cuda(cudaSetDevice(device), "cudaSetDevice") || s.cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
+      s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event") ||
+      s.cuda(c->counts.alloc(4), "counters") || s.cuda(c->stats.alloc(8), "stats") ||
+      s.cuda(cudaMemset(c->stats.p, 0, c->stats.bytes()), "stats")) {
+    delete c;
+    return DSPBR_ERR_CUDA;
+  }
+  *out = c;
+  return DSPBR_OK;
+}
+
+int dspbr_destroy(dspbr_ctx* c) {
+  if (!c) return DSPBR_ERR_INVALID;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return DSPBR_OK;
+}
+
+int dspbr_last_error(const dspbr_ctx* c, char* buf, size_t size) {
+  if (!c || !buf || size == 0) return DSPBR_ERR_INVALID;
+  std::snprintf(buf, size, "%s", c->err.c_str());
+  return DSPBR_OK;
+}
+
+// ---- scene -------------------------------------------------------------------------------------
+int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertices, const uint32_t* indices,
+                       uint32_t num_indices, const float* materials, uint32_t num_materials, const float* bvh_nodes,
+                       uint32_t num_bvh_nodes, const int32_t* bvh_indices, uint32_t num_bvh_indices,
+                       dspbr_scene** out) {
+  if (!c || !out) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  *out = nullptr;
+  if (!vertices || num_vertices == 0) return s.fail(DSPBR_ERR_INVALID, "scene: empty vertex buffer");
+  if (!indices || num_indices == 0 || num_indices % 3)
+    return s.fail(DSPBR_ERR_INVALID, "scene: index buffer does not describe whole triangles");
+  if (!materials || num_materials == 0) return s.fail(DSPBR_ERR_INVALID, "scene: no materials");
+  for (uint32_t i = 0; i < num_indices; ++i)
+    if (indices[i] >= num_vertices) return s.fail(DSPBR_ERR_INVALID, "scene: index %u out of range", i);
+  for (uint32_t v = 0; v < num_vertices; ++v) {
+    float m = vertices[size_t(v) * 20 + 3];
+    if (!(m >= 0.f) || uint32_t(m) >= num_materials)
+      return s.fail(DSPBR_ERR_INVALID, "scene: vertex %u references material %g of %u", v, m, num_materials);
+  }
+  // texture ids (material.ts: slots 39, 44-59, 63); textures are not supported yet
+  static const int kTexSlots[] = {39, 44, 45, 46, 47, 48, 49, 50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 63};
+  for (uint32_t m = 0; m < num_materials; ++m)
+    for (int k : kTexSlots)
+      if (materials[size_t(m) * 68 + k] >= 0.f)
+        return s.fail(DSPBR_ERR_INVALID, "scene: material %u uses a texture (record slot %d); textured materials are not supported", m, k);
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  auto* sc = new dspbr_scene();
+  sc->ctx = c;
+  std::vector<float> host_nodes;
+  std::vector<int32_t> host_remap;
+  double t0 = now_ms();
+  if (!bvh_nodes || !bvh_indices) {
+    dspbr_bvh* bvh = nullptr;
+    int rc = dspbr_bvh_build(vertices, num_vertices, 20, indices, num_indices, &bvh);
+    if (rc != DSPBR_OK) {
+      char msg[256] = {0};
+      if (bvh) dspbr_bvh_error(bvh, msg, sizeof msg);
+      dspbr_bvh_free(bvh);
+      delete sc;
+      return s.fail(DSPBR_ERR_INVALID, "bvh build failed: %s", msg);
+    }
+    uint32_t nn = 0, ni = 0;
+    dspbr_bvh_info(bvh, &nn, &ni, nullptr, nullptr);
+    host_nodes.resize(size_t(nn) * 16);
+    host_remap.resize(ni);
+    dspbr_bvh_copy(bvh, host_nodes.data(), host_remap.data());
+    dspbr_bvh_free(bvh);
+    bvh_nodes = host_nodes.data();
+    num_bvh_nodes = nn;
+    bvh_indices = host_remap.data();
+    num_bvh_indices = ni;
+  }
+  sc->bvh_build_ms = now_ms() - t0;
+  if (num_bvh_nodes == 0) { delete sc; return s.fail(DSPBR_ERR_INVALID, "scene: empty BVH"); }
+  t0 = now_ms();
+  // child index / count / first: the shader's int() of the stored floats
+  std::vector<float> conv(size_t(num_bvh_nodes) * 16);
+  for (size_t i = 0; i < size_t(num_bvh_nodes); ++i) {
+    const float* src = bvh_nodes + i * 16;
+    float* dst = conv.data() + i * 16;
+    std::memcpy(dst, src, 16 * sizeof(float));
+    for (int k = 3; k < 16; k += 4) {
+      float f = src[k];
+      int32_t v = (std::isfinite(f) && f > -2147483648.f && f < 2147483648.f) ? int32_t(f) : -1;
+      std::memcpy(dst + k, &v, 4);
+    }
+  }
+  sc->num_nodes = num_bvh_nodes;
+  sc->num_slots = num_bvh_indices;
+  sc->num_tris = num_indices / 3;
+  sc->num_verts = num_vertices;
+  sc->num_materials = num_materials;
+  DevBuf<int32_t> remap;
+  int rc = DSPBR_OK;
+  if ((rc = s.cuda(sc->nodes.alloc(size_t(num_bvh_nodes) * 4), "alloc nodes")) ||
+      (rc = s.cuda(sc->tris.alloc(size_t(std::max<uint32_t>(num_bvh_indices, 1)) * 3), "alloc tris")) ||
+      (rc = s.cuda(sc->verts.alloc(size_t(num_vertices) * 5), "alloc vertices")) ||
+      (rc = s.cuda(sc->indices.alloc(num_indices), "alloc indices")) ||
+      (rc = s.cuda(sc->materials.alloc(size_t(num_materials) * 17), "alloc materials")) ||
+      (rc = s.cuda(remap.alloc(std::max<uint32_t>(num_bvh_indices, 1)), "alloc remap")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->nodes.p, conv.data(), conv.size() * 4, cudaMemcpyHostToDevice, c->stream), "upload nodes")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->verts.p, vertices, size_t(num_vertices) * 80, cudaMemcpyHostToDevice, c->stream), "upload vertices")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->indices.p, indices, size_t(num_indices) * 4, cudaMemcpyHostToDevice, c->stream), "upload indices")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->materials.p, materials, size_t(num_materials) * 272, cudaMemcpyHostToDevice, c->stream), "upload materials")) ||
+      (rc = s.cuda(cudaMemcpyAsync(remap.p, bvh_indices, size_t(num_bvh_indices) * 4, cudaMemcpyHostToDevice, c->stream), "upload remap"))) {
+    delete sc;
+    return rc;
+  }
+  if (num_bvh_indices)
+    launch_gather_tris(sc->verts.p, sc->indices.p, remap.p, num_bvh_indices, sc->num_tris, sc->tris.p, c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) || (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload"))) {
+    delete sc;
+    return rc;
+  }
+  sc->upload_ms = now_ms() - t0;
+  *out = sc;
+  return DSPBR_OK;
+}
+
+int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32_t first, uint32_t count) {
+  if (!sc || !materials || first + count > sc->num_materials) return DSPBR_ERR_INVALID;
+  Status s = sc->ctx->st();
+  TRY_CUDA(s, cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaMemcpyAsync(sc->materials.p + size_t(first) * 17, materials, size_t(count) * 272,
+                              cudaMemcpyHostToDevice, sc->ctx->stream), "update materials");
+  TRY_CUDA(s, cudaStreamSynchronize(sc->ctx->stream), "update materials");
+  dspbr_reset(sc->ctx);
+  return DSPBR_OK;
+}
+
+int dspbr_scene_device_bytes(const dspbr_scene* sc, uint64_t* bytes) {
+  if (!sc || !bytes) return DSPBR_ERR_INVALID;
+  *bytes = sc->bytes();
+  return DSPBR_OK;
+}
+
+int dspbr_scene_destroy(dspbr_scene* sc) {
+  if (!sc) return DSPBR_ERR_INVALID;
+  cudaSetDevice(sc->ctx->device);
+  cudaStreamSynchronize(sc->ctx->stream);
+  if (sc->ctx->scene == sc) sc->ctx->scene = nullptr;
+  delete sc;
+  return DSPBR_OK;
+}
+
+// ---- IBL ---------------------------------------------------------------------------------------------
+// Vose's alias method in FP64 over p(x,y) = yPdf[y] * pdf[y][x], the pmf the
+// reference's two-level CDF inversion realises.
+static void build_alias(const std::vector<float>& pdf, const std::vector<float>& ypdf, int w, int h,
+                        std::vector<float>& prob, std::vector<int>& alias) {
+  size_t n = size_t(w) * h;
+  std::vector<double> q(n);
+  double tot = 0;
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      double v = double(ypdf[y]) * double(pdf[size_t(y) * w + x]);
+      q[size_t(y) * w + x] = v;
+      tot += v;
+    }
+  prob.assign(n, 1.f);
+  alias.resize(n);
+  for (size_t i = 0; i < n; ++i) alias[i] = int(i);
+  if (!(tot > 0)) return;
+  std::vector<size_t> small, large;
+  for (size_t i = 0; i < n; ++i) {
+    q[i] = q[i] * double(n) / tot;
+    (q[i] < 1.0 ? small : large).push_back(i);
+  }
+  while (!small.empty() && !large.empty()) {
+    size_t l = small.back(); small.pop_back();
+    size_t g = large.back();
+    prob[l] = float(q[l]);
+    alias[l] = int(g);
+    q[g] = (q[g] + q[l]) - 1.0;
+    if (q[g] < 1.0) { large.pop_back(); small.push_back(g); }
+  }
+  for (size_t g : large) prob[g] = 1.f;
+  for (size_t l : small) prob[l] = 1.f;
+}
+
+int dspbr_ibl_create(dspbr_ctx* c, const float* rgba, int w, int h, dspbr_ibl** out) {
+  if (!c || !out) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  *out = nullptr;
+  if (!rgba || w <= 0 || h <= 0) return s.fail(DSPBR_ERR_INVALID, "ibl: empty image");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  auto* e = new dspbr_ibl();
+  e->ctx = c;
+  e->w = w;
+  e->h = h;
+  size_t n = size_t(w) * h;
+  int rc;
+  if ((rc = s.cuda(e->rgba.alloc(n), "alloc env")) || (rc = s.cuda(e->pdf.alloc(n), "alloc pdf")) ||
+      (rc = s.cuda(e->cdf.alloc(n), "alloc cdf")) || (rc = s.cuda(e->lum.alloc(n), "alloc lum")) ||
+      (rc = s.cuda(e->ypdf.alloc(h), "alloc ypdf")) || (rc = s.cuda(e->ycdf.alloc(h), "alloc ycdf")) ||
+      (rc = s.cuda(e->rowsum.alloc(h), "alloc rowsum")) || (rc = s.cuda(e->total.alloc(1), "alloc total")) ||
+      (rc = s.cuda(e->alias_prob.alloc(n), "alloc alias")) || (rc = s.cuda(e->alias_idx.alloc(n), "alloc alias")) ||
+      (rc = s.cuda(cudaMemcpyAsync(e->rgba.p, rgba, n * 16, cudaMemcpyHostToDevice, c->stream), "upload env"))) {
+    delete e;
+    return rc;
+  }
+  launch_ibl_tables(e->rgba.p, w, h, e->lum.p, e->pdf.p, e->cdf.p, e->rowsum.p, e->ypdf.p, e->ycdf.p, e->total.p,
+                    c->stream);
+  std::vector<float> pdf(n), ypdf(h);
+  if ((rc = s.cuda(cudaGetLastError(), "ibl tables")) ||
+      (rc = s.cuda(cudaMemcpyAsync(pdf.data(), e->pdf.p, n * 4, cudaMemcpyDeviceToHost, c->stream), "read pdf")) ||
+      (rc = s.cuda(cudaMemcpyAsync(ypdf.data(), e->ypdf.p, size_t(h) * 4, cudaMemcpyDeviceToHost, c->stream), "read ypdf")) ||
+      (rc = s.cuda(cudaMemcpyAsync(&e->total_sum, e->total.p, 8, cudaMemcpyDeviceToHost, c->stream), "read total")) ||
+      (rc = s.cuda(cudaStreamSynchronize(c->stream), "ibl tables"))) {
+    delete e;
+    return rc;
+  }
+  e->lum.reset();
+  e->rowsum.reset();
+  std::vector<float> prob;
+  std::vector<int> alias;
+  build_alias(pdf, ypdf, w, h, prob, alias);
+  if ((rc = s.cuda(cudaMemcpyAsync(e->alias_prob.p, prob.data(), n * 4, cudaMemcpyHostToDevice, c->stream), "upload alias")) ||
+      (rc = s.cuda(cudaMemcpyAsync(e->alias_idx.p, alias.data(), n * 4, cudaMemcpyHostToDevice, c->stream), "upload alias")) ||
+      (rc = s.cuda(cudaStreamSynchronize(c->stream), "upload alias"))) {
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return DSPBR_OK;
+}
+
+int dspbr_ibl_tables(const dspbr_ibl* e, float* pdf, float* cdf, float* ypdf, float* ycdf, double* total) {
+  if (!e) return DSPBR_ERR_INVALID;
+  Status s = e->ctx->st();
+  size_t n = size_t(e->w) * e->h;
+  TRY_CUDA(s, cudaSetDevice(e->ctx->device), "cudaSetDevice");
+  if (pdf) TRY_CUDA(s, cudaMemcpy(pdf, e->pdf.p, n * 4, cudaMemcpyDeviceToHost), "read pdf");
+  if (cdf) TRY_CUDA(s, cudaMemcpy(cdf, e->cdf.p, n * 4, cudaMemcpyDeviceToHost), "read cdf");
+  if (ypdf) TRY_CUDA(s, cudaMemcpy(ypdf, e->ypdf.p, size_t(e->h) * 4, cudaMemcpyDeviceToHost), "read ypdf");
+  if (ycdf) TRY_CUDA(s, cudaMemcpy(ycdf, e->ycdf.p, size_t(e->h) * 4, cudaMemcpyDeviceToHost), "read ycdf");
+  if (total) *total = e->total_sum;
+  return DSPBR_OK;
+}
+
+int dspbr_ibl_alias_table(const dspbr_ibl* e, float* prob, int32_t* alias) {
+  if (!e) return DSPBR_ERR_INVALID;
+  Status s = e->ctx->st();
+  size_t n = size_t(e->w) * e->h;
+  TRY_CUDA(s, cudaSetDevice(e->ctx->device), "cudaSetDevice");
+  if (prob) TRY_CUDA(s, cudaMemcpy(prob, e->alias_prob.p, n * 4, cudaMemcpyDeviceToHost), "read alias prob");
+  if (alias) TRY_CUDA(s, cudaMemcpy(alias, e->alias_idx.p, n * 4, cudaMemcpyDeviceToHost), "read alias");
+  return DSPBR_OK;
+}
+
+int dspbr_ibl_destroy(dspbr_ibl* e) {
+  if (!e) return DSPBR_ERR_INVALID;
+  cudaSetDevice(e->ctx->device);
+  cudaStreamSynchronize(e->ctx->stream);
+  if (e->ctx->ibl == e) e->ctx->ibl = nullptr;
+  delete e;
+  return DSPBR_OK;
+}
+
+// ---- viewport state -------------------------------------------------------------------------------
+int dspbr_set_scene(dspbr_ctx* c, dspbr_scene* sc) {
+  if (!c || (sc && sc->ctx != c)) return DSPBR_ERR_INVALID;
+  c->scene = sc;
+  return dspbr_reset(c);
+}
+int dspbr_set_ibl(dspbr_ctx* c, dspbr_ibl* e) {
+  if (!c || (e && e->ctx != c)) return DSPBR_ERR_INVALID;
+  c->ibl = e;
+  return dspbr_reset(c);
+}
+int dspbr_set_camera(dspbr_ctx* c, const float m[16], float fov_deg, float near_plane) {
+  if (!c || !m || !(fov_deg > 0.f && fov_deg < 180.f) || !(near_plane > 0.f)) return DSPBR_ERR_INVALID;
+  std::memcpy(c->matrix, m, sizeof c->matrix);
+  c->fov = fov_deg;
+  c->near_plane = near_plane;
+  c->has_camera = true;
+  return dspbr_reset(c);
+}
+int dspbr_set_params(dspbr_ctx* c, const dspbr_params* p) {
+  if (!c || !p || p->max_bounces < 0 || p->max_bounces > 4096) return DSPBR_ERR_INVALID;
+  c->params = *p;
+  return dspbr_reset(c);
+}
+int dspbr_get_params(const dspbr_ctx* c, dspbr_params* p) {
+  if (!c || !p) return DSPBR_ERR_INVALID;
+  *p = c->params;
+  return DSPBR_OK;
+}
+int dspbr_set_wave_paths(dspbr_ctx* c, uint32_t paths) {
+  if (!c) return DSPBR_ERR_INVALID;
+  c->wave_paths = paths ? paths : (1u << 21);
+  return DSPBR_OK;
+}
+
+int dspbr_resize(dspbr_ctx* c, int w, int h) {
+  if (!c || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28)) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "resize");
+  size_t npix = size_t(w) * h;
+  TRY_CUDA(s, c->accum.alloc(npix), "alloc accumulation");
+  TRY_CUDA(s, c->mean.alloc(npix), "alloc readback");
+  c->width = w;
+  c->height = h;
+  return dspbr_reset(c);
+}
+
+int dspbr_reset(dspbr_ctx* c) {
+  if (!c) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  c->sample_count = 0;
+  if (c->accum.p) {
+    TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+    TRY_CUDA(s, cudaMemsetAsync(c->accum.p, 0, c->accum.bytes(), c->stream), "clear accumulation");
+  }
+  return DSPBR_OK;
+}
+
+static int ensure_paths(dspbr_ctx* c, uint32_t cap) {
+  Status s = c->st();
+  if (c->capacity >= cap) return DSPBR_OK;
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "sync");
+  int rc;
+  if ((rc = s.cuda(c->org.alloc(cap), "paths")) || (rc = s.cuda(c->dir.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->weight.alloc(cap), "paths")) || (rc = s.cuda(c->rad.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->hit.alloc(cap), "paths")) || (rc = s.cuda(c->sh_dir.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->sh_c.alloc(cap), "paths")) || (rc = s.cuda(c->pl_dir.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->pl_c.alloc(cap), "paths")) || (rc = s.cuda(c->result.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->rng.alloc(cap), "paths")) || (rc = s.cuda(c->sh_flags.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->q0.alloc(cap), "queues")) || (rc = s.cuda(c->q1.alloc(cap), "queues")) ||
+      (rc = s.cuda(c->qs.alloc(cap), "queues"))) {
+    c->capacity = 0;
+    return rc;
+  }
+  c->capacity = cap;
+  return DSPBR_OK;
+}
+
+static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int spp) {
+  WaveParams p{};
+  double film = std::tan(double(c->fov) * 0.5 * M_PI / 180.0) * double(c->near_plane);
+  for (int col = 0; col < 3; ++col)
+    for (int r = 0; r < 3; ++r) p.cam.m[col * 3 + r] = c->matrix[col * 4 + r];
+  p.cam.pos[0] = c->matrix[12]; p.cam.pos[1] = c->matrix[13]; p.cam.pos[2] = c->matrix[14];
+  p.cam.film_height = float(film);
+  p.cam.focal = c->near_plane;
+  p.cam.inv_res[0] = float(1.0 / c->width);
+  p.cam.inv_res[1] = float(1.0 / c->height);
+  p.cam.width = c->width;
+  p.cam.height = c->height;
+  p.npix = c->width * c->height;
+  p.spp = spp;
+  p.frame_base = frame_base;
+  const dspbr_params& q = c->params;
+  p.max_bounces = q.max_bounces;
+  p.rng_pcg = q.rng == DSPBR_RNG_PCG;
+  p.seed = q.seed;
+  p.use_ibl = q.use_ibl ? 1 : 0;
+  p.bg_from_ibl = q.background_from_ibl ? 1 : 0;
+  p.env_mode = q.env_sampling == DSPBR_ENV_CDF ? 1 : 0;
+  p.lean = q.profile == DSPBR_PROFILE_LEAN;
+  p.has_ibl = c->ibl != nullptr;
+  p.ibl_rot = float(double(q.ibl_rotation_deg) / 180.0 * M_PI);
+  p.bg_color = make_float4(q.background_color[0], q.background_color[1], q.background_color[2], q.background_color[3]);
+  p.ray_eps = q.ray_eps;
+  p.clamp_threshold = q.clamp_threshold;
+  p.rr_prob = q.rr_termination_prob;
+  p.rr_factor = 1.0f / (1.0f - q.rr_termination_prob);
+  p.rr_start = q.rr_start_depth;
+  p.pl_pos = make_float4(q.point_light_position[0], q.point_light_position[1], q.point_light_position[2],
+                         q.point_light_position[3]);
+  p.pl_emis = make_float4(q.point_light_emission[0], q.point_light_emission[1], q.point_light_emission[2],
+                          q.point_light_emission[3]);
+  return p;
+}
+
+static int enqueue_frames(dspbr_ctx* c, int frames) {
+  Status s = c->st();
+  if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
+  if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
+  if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
+  if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  uint32_t npix = uint32_t(c->width) * uint32_t(c->height);
+  int spp_max = int(std::max<uint32_t>(1u, c->wave_paths / npix));
+  int rc = ensure_paths(c, npix * uint32_t(std::min(spp_max, frames)));
+  if (rc) return rc;
+  DevScene sv = c->scene->view();
+  DevIbl ev{};
+  if (c->ibl) ev = c->ibl->view();
+  PathBuf b{};
+  b.org = c->org.p; b.dir = c->dir.p; b.weight = c->weight.p; b.rad = c->rad.p; b.rng = c->rng.p; b.hit = c->hit.p;
+  b.sh_dir = c->sh_dir.p; b.sh_c = c->sh_c.p; b.pl_dir = c->pl_dir.p; b.pl_c = c->pl_c.p; b.sh_flags = c->sh_flags.p;
+  b.result = c->result.p; b.q[0] = c->q0.p; b.q[1] = c->q1.p; b.qs = c->qs.p; b.counts = c->counts.p;
+  b.stats = c->stats.p; b.capacity = c->capacity;
+  LaunchCfg lc;
+  lc.trace_threads = 128;
+  lc.trace_blocks = 148 * 16;
+  lc.shade_threads = 128;
+  lc.shade_blocks = 148 * 8;
+  TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
+  int left = frames;
+  while (left > 0) {
+    int spp = std::min(left, spp_max);
+    WaveParams p = make_wave(c, uint32_t(c->sample_count + 1), spp);
+    p.count_traversal = c->counting ? 1 : 0;
+    launch_generate(p, b, c->stream);
+    int cur = 0;
+    for (int d = 0; d <= p.max_bounces; ++d) {
+      c->mark_begin(0);
+      launch_extend(sv, b, cur, c->counting, lc, c->stream);
+      c->mark_end();
+      if (d > 0) {
+        c->mark_begin(1);
+        launch_connect(sv, b, c->counting, lc, c->stream);
+        c->mark_end();
+      }
+      cudaMemsetAsync(c->counts.p + (cur ^ 1), 0, 4, c->stream);
+      cudaMemsetAsync(c->counts.p + 2, 0, 4, c->stream);
+      c->mark_begin(2);
+      launch_shade(sv, ev, p, b, cur, d, lc, c->stream);
+      c->mark_end();
+      cur ^= 1;
+    }
+    launch_accumulate(p, b, c->accum.p, c->stream);
+    c->kind_launches[0] += uint64_t(p.max_bounces + 1);
+    c->kind_launches[1] += uint64_t(p.max_bounces);
+    c->kind_launches[2] += uint64_t(p.max_bounces + 1);
+    c->kind_launches[3] += 2;  // generate + accumulate
+    TRY_CUDA(s, cudaGetLastError(), "render launch");
+    c->sample_count += uint64_t(spp);
+    c->rays_primary += uint64_t(npix) * uint64_t(spp);
+    left -= spp;
+  }
+  TRY_CUDA(s, cudaEventRecord(c->ev1, c->stream), "event");
+  c->pending = true;
+  return DSPBR_OK;
+}
+
+int dspbr_wait(dspbr_ctx* c) {
+  if (!c) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "render");
+  if (c->pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_render_ms = ms;
+    c->pending = false;
+  }
+  c->resolve_marks();
+  return DSPBR_OK;
+}
+
+int dspbr_set_counting(dspbr_ctx* c, int enable) {
+  if (!c) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaMemsetAsync(c->stats.p + 3, 0, 4 * sizeof(unsigned long long), c->stream), "counters");
+  c->counting = enable != 0;
+  return DSPBR_OK;
+}
+
+int dspbr_set_profiling(dspbr_ctx* c, int enable) {
+  if (!c) return DSPBR_ERR_INVALID;
+  int rc = dspbr_wait(c);
+  if (rc) return rc;
+  c->profiling = enable != 0;
+  for (double& v : c->kind_ms) v = 0;
+  for (uint64_t& v : c->kind_launches) v = 0;
+  return DSPBR_OK;
+}
+
+int dspbr_render(dspbr_ctx* c, int frames) {
+  int rc = enqueue_frames(c, frames);
+  if (rc) return rc;
+  return dspbr_wait(c);
+}
+
+int dspbr_render_async(dspbr_ctx* c, int frames) { return enqueue_frames(c, frames); }
+
+int dspbr_poll(dspbr_ctx* c, int* done) {
+  if (!c || !done) return DSPBR_ERR_INVALID;
+  cudaSetDevice(c->device);
+  cudaError_t e = cudaStreamQuery(c->stream);
+  if (e == cudaErrorNotReady) { cudaGetLastError(); *done = 0; return DSPBR_OK; }
+  *done = 1;
+  if (e != cudaSuccess) return c->st().cuda(e, "render");
+  return dspbr_wait(c);
+}
+
+int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
+  if (!c || !rgba) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  size_t npix = size_t(c->width) * c->height;
+  if (num_floats < npix * 4) return s.fail(DSPBR_ERR_INVALID, "read_accum: buffer holds %zu floats, need %zu", num_floats, npix * 4);
+  if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_accum: no image");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
+  launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
+  TRY_CUDA(s, cudaMemcpyAsync(rgba, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read accumulation");
+  return DSPBR_OK;
+}
+
+int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
+  if (!c || !d) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  std::memset(d, 0, sizeof *d);
+  unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaMemcpyAsync(st, c->stats.p, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read stats");
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read stats");
+  d->sample_count = c->sample_count;
+  d->width = c->width;
+  d->height = c->height;
+  d->rays_primary = c->rays_primary;
+  d->rays_extension = st[0] >= c->rays_primary ? st[0] - c->rays_primary : 0;
+  d->rays_shadow = st[1];
+  d->traversal_aborted = st[2];
+  if (c->scene) {
+    d->scene_triangles = c->scene->num_tris;
+    d->bvh_nodes = c->scene->num_nodes;
+    d->bvh_indices = c->scene->num_slots;
+    d->bvh_build_ms = c->scene->bvh_build_ms;
+    d->upload_ms = c->scene->upload_ms;
+  }
+  d->device_bytes = c->org.bytes() * 10 + c->rng.bytes() + c->sh_flags.bytes() + c->q0.bytes() * 3 + c->accum.bytes() +
+                    c->mean.bytes();
+  d->last_render_ms = c->last_render_ms;
+  d->nodes_closest = st[3];
+  d->tris_closest = st[4];
+  d->nodes_shadow = st[5];
+  d->tris_shadow = st[6];
+  d->extend_ms = c->kind_ms[0];
+  d->connect_ms = c->kind_ms[1];
+  d->shade_ms = c->kind_ms[2];
+  d->extend_launches = c->kind_launches[0];
+  d->connect_launches = c->kind_launches[1];
+  d->shade_launches = c->kind_launches[2];
+  d->other_launches = c->kind_launches[3];
+  return DSPBR_OK;
+}
+
+}  // extern "C"
+
+// ---- kernel-level queries -------------------------------------------------------------------------
+template <class T>
+static int up(Status& s, DevBuf<T>& d, const T* h, size_t n, cudaStream_t st) {
+  int rc = s.cuda(d.alloc(std::max<size_t>(n, 1)), "alloc");
+  if (rc) return rc;
+  return s.cuda(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, st), "upload");
+}
+template <class T>
+static int down(Status& s, T* h, const DevBuf<T>& d, size_t n, cudaStream_t st) {
+  return s.cuda(cudaMemcpyAsync(h, d.p, n * sizeof(T), cudaMemcpyDeviceToHost, st), "download");
+}
+
+extern "C" {
+
+int dspbr_trace_closest(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, uint32_t n, int32_t* tri, float* t,
+                        float* uv) {
+  if (!c || !sc || !rays || !tri || !t || !uv) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  DevBuf<float> r;
+  DevBuf<int32_t> dt;
+  DevBuf<float> dtt, duv;
+  int rc;
+  if ((rc = up(s, r, rays, size_t(n) * 8, c->stream)) || (rc = s.cuda(dt.alloc(std::max(n, 1u)), "alloc")) ||
+      (rc = s.cuda(dtt.alloc(std::max(n, 1u)), "alloc")) || (rc = s.cuda(duv.alloc(2 * size_t(std::max(n, 1u))), "alloc")))
+    return rc;
+  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 0, dt.p, dtt.p,
+                    reinterpret_cast<float2*>(duv.p), nullptr, c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "trace")) || (rc = down(s, tri, dt, n, c->stream)) ||
+      (rc = down(s, t, dtt, n, c->stream)) || (rc = down(s, uv, duv, 2 * size_t(n), c->stream)))
+    return rc;
+  return s.cuda(cudaStreamSynchronize(c->stream), "trace");
+}
+
+int dspbr_trace_occluded(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, uint32_t n, int32_t* occ) {
+  if (!c || !sc || !rays || !occ) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  DevBuf<float> r;
+  DevBuf<int32_t> o;
+  int rc;
+  if ((rc = up(s, r, rays, size_t(n) * 8, c->stream)) || (rc = s.cuda(o.alloc(std::max(n, 1u)), "alloc"))) return rc;
+  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 1, nullptr, nullptr, nullptr, o.p, c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "occluded")) || (rc = down(s, occ, o, n, c->stream))) return rc;
+  return s.cuda(cudaStreamSynchronize(c->stream), "occluded");
+}
+
+int dspbr_bsdf_query(dspbr_ctx* c, const dspbr_scene* sc, uint32_t n, const float* hit, const float* wo,
+                     const float* rnd, float* eval4, float* sample10, int32_t* flags) {
+  if (!c || !sc || !hit || !wo || !rnd || !eval4 || !sample10 || !flags) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  DevBuf<float> dh, dw, dr, de, ds;
+  DevBuf<int32_t> df;
+  int rc;
+  size_t m = std::max(n, 1u);
+  if ((rc = up(s, dh, hit, size_t(n) * 20, c->stream)) || (rc = up(s, dw, wo, size_t(n) * 3, c->stream)) ||
+      (rc = up(s, dr, rnd, size_t(n) * 4, c->stream)) || (rc = s.cuda(de.alloc(m * 4), "alloc")) ||
+      (rc = s.cuda(ds.alloc(m * 10), "alloc")) || (rc = s.cuda(df.alloc(m), "alloc")))
+    return rc;
+  launch_bsdf_query(sc->view(), n, dh.p, dw.p, dr.p, c->params.profile == DSPBR_PROFILE_LEAN, de.p, ds.p, df.p,
+                    c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "bsdf")) || (rc = down(s, eval4, de, size_t(n) * 4, c->stream)) ||
+      (rc = down(s, sample10, ds, size_t(n) * 10, c->stream)) || (rc = down(s, flags, df, n, c->stream)))
+    return rc;
+  return s.cuda(cudaStreamSynchronize(c->stream), "bsdf");
+}
+
+int dspbr_ibl_query(dspbr_ctx* c, const dspbr_ibl* e, uint32_t n, const float* r2, const float* dirs, float* sdp4,
+                    float* pdf, float* rgb) {
+  if (!c || !e || !r2 || !dirs || !sdp4 || !pdf || !rgb) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  DevBuf<float> dr, dd, ds, dp, dc;
+  size_t m = std::max(n, 1u);
+  int rc;
+  if ((rc = up(s, dr, r2, size_t(n) * 2, c->stream)) || (rc = up(s, dd, dirs, size_t(n) * 3, c->stream)) ||
+      (rc = s.cuda(ds.alloc(m * 4), "alloc")) || (rc = s.cuda(dp.alloc(m), "alloc")) ||
+      (rc = s.cuda(dc.alloc(m * 3), "alloc")))
+    return rc;
+  float rot = float(double(c->params.ibl_rotation_deg) / 180.0 * M_PI);
+  launch_ibl_query(e->view(), rot, c->params.env_sampling == DSPBR_ENV_CDF ? 1 : 0, n, dr.p, dd.p, ds.p, dp.p, dc.p,
+                   c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "ibl query")) || (rc = down(s, sdp4, ds, size_t(n) * 4, c->stream)) ||
+      (rc = down(s, pdf, dp, n, c->stream)) || (rc = down(s, rgb, dc, size_t(n) * 3, c->stream)))
+    return rc;
+  return s.cuda(cudaStreamSynchronize(c->stream), "ibl query");
+}
+
+int dspbr_camera_rays(dspbr_ctx* c, uint32_t n, const int32_t* xy, const float* r2, float* rays6) {
+  if (!c || !xy || !r2 || !rays6) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  if (!c->has_camera || c->width <= 0) return s.fail(DSPBR_ERR_STATE, "camera_rays: camera and size required");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  DevBuf<int32_t> dxy;
+  DevBuf<float> dr, dout;
+  int rc;
+  if ((rc = up(s, dxy, xy, size_t(n) * 2, c->stream)) || (rc = up(s, dr, r2, size_t(n) * 2, c->stream)) ||
+      (rc = s.cuda(dout.alloc(std::max(n, 1u) * size_t(6)), "alloc")))
+    return rc;
+  WaveParams p = make_wave(c, 1, 1);
+  launch_camera_rays(p.cam, n, dxy.p, dr.p, dout.p, c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "camera rays")) || (rc = down(s, rays6, dout, size_t(n) * 6, c->stream)))
+    return rc;
+  return s.cuda(cudaStreamSynchronize(c->stream), "camera rays");
+}
+
+}  // extern "C"

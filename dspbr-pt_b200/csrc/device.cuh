@@ -1,0 +1,413 @@
+// Device-side scene/IBL views, traversal, RNG, camera and hit set-up.
+#pragma once
+#include <stdint.h>
+
+#include "material.cuh"
+#include "vecmath.cuh"
+
+namespace dspbr {
+
+// reference constants (constants.glsl:12-21, bvh.glsl:8-10)
+constexpr float kGlslPi = 3.14159265358979323f;
+constexpr float kGlslTwoPi = 6.28318530717958648f;
+constexpr float kEps = 1e-8f;
+constexpr float kEpsCos = 0.001f;
+constexpr float kEpsPdf = 0.001f;
+constexpr float kTfarMax = 100000.0f;
+constexpr float kBvhFar = 1e30f;
+constexpr int kStackSize = 64;
+constexpr int kMaxSteps = 4096;
+constexpr int kMaxLeafTris = 64;
+
+// Device scene.  nodes: 4 float4 per node, child index / count / first are
+// stored as int bits in .w (converted once from the reference's floats with the
+// same truncating conversion the shader's int() performs).  tris: 3 float4 per
+// BVH leaf slot, pre-gathered in leaf order: (p0.xyz, mesh triangle id bits),
+// (p1 - p0, 0), (p2 - p0, 0); id -1 marks a remap entry the reference skips.
+struct DevScene {
+  const float4* __restrict__ nodes;
+  const float4* __restrict__ tris;
+  const float4* __restrict__ verts;      // 5 float4 per vertex (20-float record)
+  const uint32_t* __restrict__ indices;  // 3 per triangle
+  const float4* __restrict__ materials;  // 17 float4 per material (68 floats)
+  int num_nodes, num_slots, num_tris, num_materials;
+};
+
+struct DevIbl {
+  const float4* __restrict__ rgba;  // w*h, row 0 = v 0 (zenith)
+  const float* __restrict__ pdf;    // w*h  (renderer.ts:802-838 tables)
+  const float* __restrict__ cdf;
+  const float* __restrict__ ypdf;   // h
+  const float* __restrict__ ycdf;
+  const float* __restrict__ alias_prob;  // w*h
+  const int* __restrict__ alias_idx;
+  int w, h;
+};
+
+// ---- RNG ----------------------------------------------------------------------
+// George Marsaglia MWC of rng.glsl:5-29, seeded from the fragment coordinate.
+struct Mwc {
+  uint32_t x, y;
+};
+DEV Mwc mwc_init(int seed, int px, int py) {
+  float off = float(seed * 17);
+  float fx = __fadd_rn(float(px), 0.5f), fy = __fadd_rn(float(py), 0.5f);
+  Mwc s;
+  s.x = __float2uint_rz(__fmul_rn(397.6432f, __fadd_rn(fx, off)));
+  s.y = __float2uint_rz(__fmul_rn(397.6432f, __fadd_rn(fy, 0.0f)));
+  s.x ^= __float2uint_rz(__fmul_rn(32.9875f, __fadd_rn(fy, off)));
+  s.y ^= __float2uint_rz(__fmul_rn(32.9875f, __fadd_rn(fx, 0.0f)));
+  return s;
+}
+DEV float mwc_float(Mwc& s) {
+  s.x = 36969u * (s.x & 65535u) + (s.x >> 16u);
+  s.y = 18000u * (s.y & 65535u) + (s.y >> 16u);
+  uint32_t r = (s.x << 16u) + s.y;
+  return __fdiv_rn(__uint2float_rn(r), 4294967296.0f);
+}
+
+// PCG32 (O'Neill, XSH-RR output), one stream per pixel sample.  State is the
+// 64-bit LCG state; the stream increment is derived from the stream id.
+DEV uint64_t pcg_inc(uint64_t stream) { return (stream << 1u) | 1u; }
+DEV uint32_t pcg_next(uint64_t& state, uint64_t inc) {
+  uint64_t old = state;
+  state = old * 6364136223846793005ull + inc;
+  uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+  uint32_t rot = uint32_t(old >> 59u);
+  return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+DEV uint64_t pcg_init(uint64_t seed, uint64_t stream) {
+  uint64_t inc = pcg_inc(stream);
+  uint64_t st = 0;
+  pcg_next(st, inc);
+  st += seed;
+  pcg_next(st, inc);
+  return st;
+}
+DEV float pcg_float(uint64_t& state, uint64_t inc) { return float(pcg_next(state, inc) >> 8) * (1.0f / 16777216.0f); }
+
+struct Rng {
+  uint64_t state;
+  uint64_t inc;  // 0 selects MWC (state = x | y << 32)
+  DEV float next() {
+    if (inc == 0) {
+      Mwc m{uint32_t(state), uint32_t(state >> 32)};
+      float f = mwc_float(m);
+      state = uint64_t(m.x) | (uint64_t(m.y) << 32);
+      return f;
+    }
+    return pcg_float(state, inc);
+  }
+};
+
+// ---- traversal (bvh.glsl:31-62, 149-229) ------------------------------------------
+struct Hit {
+  int tri;
+  float t, u, v;
+};
+
+DEV float slab(float4 bmin, float4 bmax, v3 org, v3 inv, float tfar) {
+  float t0x = __fmul_rn(__fsub_rn(bmin.x, org.x), inv.x), t1x = __fmul_rn(__fsub_rn(bmax.x, org.x), inv.x);
+  float t0y = __fmul_rn(__fsub_rn(bmin.y, org.y), inv.y), t1y = __fmul_rn(__fsub_rn(bmax.y, org.y), inv.y);
+  float t0z = __fmul_rn(__fsub_rn(bmin.z, org.z), inv.z), t1z = __fmul_rn(__fsub_rn(bmax.z, org.z), inv.z);
+  float tmin = gmax(gmax(gmin(t0x, t1x), gmin(t0y, t1y)), gmin(t0z, t1z));
+  float tmax = gmin(gmin(gmax(t0x, t1x), gmax(t0y, t1y)), gmax(t0z, t1z));
+  if (isnan(tmin) || isnan(tmax) || tmin > tmax || tmax < 0.f || tmin >= tfar) return kBvhFar;
+  return tmin;
+}
+
+// Moller-Trumbore with the reference's rejection tests, every operation
+// rounded separately (identical to the IEEE host oracle).
+DEV bool intersect_tri(v3 org, v3 dir, float4 a, float4 b, float4 c, float tfar, float& t, float& u, float& v) {
+  v3 p0 = mk(a), e0 = mk(b), e1 = mk(c);
+  v3 pv = cross_rn(dir, e1);
+  float det = dot_rn(e0, pv);
+  if (fabsf(det) < kEps) return false;
+  float f = __fdiv_rn(1.0f, det);
+  v3 s = sub_rn(org, p0);
+  u = __fmul_rn(f, dot_rn(s, pv));
+  if (u < 0.f || u > 1.f) return false;
+  v3 q = cross_rn(s, e0);
+  v = __fmul_rn(f, dot_rn(dir, q));
+  if (v < 0.f || __fadd_rn(u, v) > 1.f) return false;
+  t = __fmul_rn(f, dot_rn(e1, q));
+  if (t < kEps || t >= tfar) return false;
+  return true;
+}
+
+DEV v3 inv_dir(v3 d) { return mk(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z)); }
+
+// Stack traversal with the reference's limits: 64-entry stack (pushes beyond
+// it are dropped), 4096 steps, 64 triangles per leaf, node-range and
+// self-reference checks.  kAny: stop at the first accepted triangle (same
+// boolean as the reference's closest-hit isOccluded).  Returns false and sets
+// `aborted` when the step cap ends the loop with work left.
+template <bool kAny>
+DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted, uint32_t* nodes_visited = nullptr,
+                  uint32_t* tris_tested = nullptr) {
+  v3 inv = inv_dir(dir);
+  hit.t = tfar;
+  hit.tri = -1;
+  hit.u = hit.v = 0.f;
+  int stack[kStackSize];
+  int top = 1;
+  stack[0] = 0;
+  int step = 0;
+  for (; step < kMaxSteps && top > 0; ++step) {
+    int ni = stack[--top];
+    if (ni < 0 || ni >= s.num_nodes) continue;
+    if (nodes_visited) ++*nodes_visited;
+    const float4* nd = s.nodes + 4 * size_t(ni);
+    float4 n0 = __ldg(nd), n1 = __ldg(nd + 1), n2 = __ldg(nd + 2), n3 = __ldg(nd + 3);
+    int cnt = __float_as_int(n2.w);
+    if (cnt > 0) {
+      int first = __float_as_int(n3.w);
+      int end = min(first + min(cnt, kMaxLeafTris), s.num_slots);
+      for (int i = max(first, 0); i < end; ++i) {
+        const float4* tp = s.tris + 3 * size_t(i);
+        float4 a = __ldg(tp);
+        int id = __float_as_int(a.w);
+        if (id < 0) continue;
+        if (tris_tested) ++*tris_tested;
+        float t, u, v;
+        if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
+          hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
+          if (kAny) { aborted = false; return true; }
+        }
+      }
+    } else {
+      int left = __float_as_int(n0.w), right = __float_as_int(n1.w);
+      float d0 = slab(n0, n1, org, inv, hit.t);
+      float d1 = slab(n2, n3, org, inv, hit.t);
+      // bvh_push_child (bvh.glsl:141-145): bounded stack, valid node, not self
+      auto push = [&](int c) {
+        if (top < kStackSize && c >= 0 && c < s.num_nodes && c != ni) stack[top++] = c;
+      };
+      if (d0 < kBvhFar && d1 < kBvhFar) {
+        if (d0 < d1) { push(right); push(left); }
+        else { push(left); push(right); }
+      } else if (d0 < kBvhFar) {
+        push(left);
+      } else if (d1 < kBvhFar) {
+        push(right);
+      }
+    }
+  }
+  aborted = (top > 0 && step >= kMaxSteps);
+  return hit.tri >= 0;
+}
+
+// ---- camera (renderer.frag:129-142, renderer.ts:399-404) -------------------------
+struct Camera {
+  float m[9];          // mat3(u_u_view_mat), column-major
+  float pos[3];
+  float film_height;   // u_camera_pos.w = tan(fov/2) * near
+  float focal;         // u_focal_length = near
+  float inv_res[2];
+  int width, height;
+};
+
+// v_uv of the pixel centre of the full-screen quad: (2x+1)/W - 1
+DEV void camera_ray(const Camera& c, int px, int py, float r0, float r1, v3& org, v3& dir) {
+  float vx = __fsub_rn(__fdiv_rn(float(2 * px + 1), float(c.width)), 1.f);
+  float vy = __fsub_rn(__fdiv_rn(float(2 * py + 1), float(c.height)), 1.f);
+  float ox = __fmul_rn(r0, c.inv_res[0]), oy = __fmul_rn(r1, c.inv_res[1]);
+  float aspect = __fdiv_rn(c.inv_res[1], c.inv_res[0]);
+  float ux = __fmul_rn(__fadd_rn(__fmul_rn(vx, aspect), ox), c.film_height);
+  float uy = __fmul_rn(__fadd_rn(__fmul_rn(vy, 1.f), oy), c.film_height);
+  v3 d = normalize_rn(mk(ux, uy, -c.focal));
+  v3 c0 = mk(c.m[0], c.m[1], c.m[2]), c1 = mk(c.m[3], c.m[4], c.m[5]), c2 = mk(c.m[6], c.m[7], c.m[8]);
+  dir = add_rn(add_rn(mul_rn(c0, d.x), mul_rn(c1, d.y)), mul_rn(c2, d.z));
+  org = mk(c.pos[0], c.pos[1], c.pos[2]);
+}
+
+// ---- environment (lighting.glsl:24-98, utils.glsl:125-154) ---------------------------
+DEV v3 rotate_phi(v3 d, float angle) {
+  float s, c;
+  sincosf(angle, &s, &c);
+  return mk(c * d.x - s * d.z, d.y, s * d.x + c * d.z);
+}
+DEV float sin_theta_pdf(float theta) { return 1.f / (2.f * kGlslPi * kGlslPi * fmaxf(kEpsCos, sinf(theta))); }
+DEV void dir_to_uv(v3 d, float& u, float& v, float& pdf) {
+  float theta = acosf(fmaxf(-1.f, fminf(1.f, d.y)));
+  float phi = atan2f(d.z, d.x);
+  if (phi < 0.f) phi = kGlslTwoPi + phi;
+  u = phi / kGlslTwoPi;
+  v = theta / kGlslPi;
+  pdf = sin_theta_pdf(theta);
+}
+DEV v3 uv_to_dir(float u, float v, float& pdf) {
+  float theta = v * kGlslPi, phi = u * kGlslTwoPi;
+  pdf = sin_theta_pdf(theta);
+  float st = sinf(theta);
+  return mk(st * cosf(phi), cosf(theta), st * sinf(phi));
+}
+DEV int wrap(int i, int n) {
+  int m = i % n;
+  return m < 0 ? m + n : m;
+}
+DEV float4 env_texel(const DevIbl& e, int x, int y) { return __ldg(e.rgba + size_t(y) * e.w + x); }
+// texture() with LINEAR filtering and REPEAT wrapping, level 0
+DEV v3 env_bilinear(const DevIbl& e, float u, float v) {
+  float fu = u * float(e.w) - 0.5f, fv = v * float(e.h) - 0.5f;
+  float u0 = floorf(fu), v0 = floorf(fv);
+  float a = fu - u0, b = fv - v0;
+  int i0 = wrap(int(u0), e.w), j0 = wrap(int(v0), e.h);
+  int i1 = wrap(int(u0) + 1, e.w), j1 = wrap(int(v0) + 1, e.h);
+  float4 t00 = env_texel(e, i0, j0), t10 = env_texel(e, i1, j0), t01 = env_texel(e, i0, j1), t11 = env_texel(e, i1, j1);
+  float w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+  return mk(w00 * t00.x + w10 * t10.x + w01 * t01.x + w11 * t11.x, w00 * t00.y + w10 * t10.y + w01 * t01.y + w11 * t11.y,
+            w00 * t00.z + w10 * t10.z + w01 * t01.z + w11 * t11.z);
+}
+DEV v3 ibl_eval(const DevIbl& e, float rot, v3 d) {
+  float u, v, pdf;
+  dir_to_uv(rotate_phi(d, rot), u, v, pdf);
+  return env_bilinear(e, u, v);
+}
+// lower_bound over a float CDF (utils.glsl:196-217)
+DEV int lower_bound(const float* data, int size, float value) {
+  int count = size, first = 0;
+  while (count > 0) {
+    int step = count / 2;
+    int idx = first + step;
+    if (__ldg(data + idx) < value) { first = idx + 1; count -= step + 1; }
+    else count = step;
+  }
+  return first;
+}
+// ibl_sample_direction (lighting.glsl:32-42, 74-84).  mode 1: the reference's
+// binary searches; mode 0: the alias table over the same pixel pmf.
+DEV v3 ibl_sample(const DevIbl& e, float rot, int mode, float r0, float r1, float& pdf_out) {
+  int x, y;
+  float pdf_y, pdf_x;
+  if (mode == 1) {
+    int yi = lower_bound(e.ycdf, e.h, r1);
+    pdf_y = yi < e.h ? __ldg(e.ypdf + yi) : 0.f;
+    y = yi >= e.h ? e.h - 1 : yi;
+    const float* row = e.cdf + size_t(y) * e.w;
+    int xi = lower_bound(row, e.w, r0);
+    pdf_x = xi < e.w ? __ldg(e.pdf + size_t(y) * e.w + xi) : 0.f;
+    x = xi >= e.w ? e.w - 1 : xi;
+  } else {
+    int n = e.w * e.h;
+    int i = min(int(r1 * float(n)), n - 1);
+    if (r0 >= __ldg(e.alias_prob + i)) i = __ldg(e.alias_idx + i);
+    y = i / e.w;
+    x = i - y * e.w;
+    pdf_y = __ldg(e.ypdf + y);
+    pdf_x = __ldg(e.pdf + i);
+  }
+  float spdf = float(e.w) * float(e.h) * pdf_y * pdf_x;
+  float pdf_w;
+  v3 d = uv_to_dir(float(x) / float(e.w), float(y) / float(e.h), pdf_w);
+  pdf_out = spdf * pdf_w;
+  return rotate_phi(d, -rot);
+}
+DEV float ibl_pdf(const DevIbl& e, float rot, v3 d) {
+  float u, v, pdf_w;
+  dir_to_uv(rotate_phi(d, rot), u, v, pdf_w);
+  float w = float(e.w), h = float(e.h);
+  float x = fminf(u * w, w - 1.f), y = fminf(v * h, h - 1.f);
+  int xi = int(x), yi = int(y);
+  float py = (yi >= 0 && yi < e.h) ? __ldg(e.ypdf + yi) : 0.f;
+  float px = (xi >= 0 && yi >= 0 && xi < e.w && yi < e.h) ? __ldg(e.pdf + size_t(yi) * e.w + xi) : 0.f;
+  return w * h * py * px * pdf_w;
+}
+
+// ---- hit set-up: fillRenderState + configure_gltf_material -------------------------
+struct Surface {
+  Closure c;
+  v3 n, ng;          // fixed to the incident side (fix_normals, utils.glsl:79-89)
+  v3 emissive;
+  v3 att_color;
+  float att_dist;
+  float cutout;
+  bool backside, thin_walled;
+  v3 pos;
+};
+
+DEV float4 vtx(const DevScene& s, uint32_t vi, int slot) { return __ldg(s.verts + 5 * size_t(vi) + slot); }
+
+// get_onb(n) (utils.glsl:97-102): Spencer & Jones basis, first column
+DEV v3 onb_tangent(v3 n) { return normalize(cross(n, mk(-n.z, n.x, -n.y))); }
+
+DEV Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
+  Surface S;
+  uint32_t i0 = __ldg(s.indices + 3 * size_t(tri)), i1 = __ldg(s.indices + 3 * size_t(tri) + 1),
+           i2 = __ldg(s.indices + 3 * size_t(tri) + 2);
+  float4 q0 = vtx(s, i0, 0), q1 = vtx(s, i1, 0), q2 = vtx(s, i2, 0);
+  v3 p0 = mk(q0), p1 = mk(q1), p2 = mk(q2);
+  float w0 = 1.f - bu - bv;
+  v3 ng = normalize(cross(p1 - p0, p2 - p0));
+  v3 n = normalize(w0 * mk(vtx(s, i0, 1)) + bu * mk(vtx(s, i1, 1)) + bv * mk(vtx(s, i2, 1)));
+  float4 t0 = vtx(s, i0, 3), t1 = vtx(s, i1, 3), t2 = vtx(s, i2, 3);
+  float hand = (t0.w == t1.w && t0.w == t2.w) ? t0.w : 0.f;
+  v3 tg = normalize(w0 * mk(t0) + bu * mk(t1) + bv * mk(t2));
+  float4 tangent;
+  if (length(tg) > 0.99f && fabsf(hand) > 0.99f) tangent = make_float4(tg.x, tg.y, tg.z, -hand);
+  else { v3 o = onb_tangent(n); tangent = make_float4(o.x, o.y, o.z, 1.f); }
+  float4 c0 = vtx(s, i0, 4), c1 = vtx(s, i1, 4), c2 = vtx(s, i2, 4);
+  float4 vcol = make_float4(w0 * c0.x + bu * c1.x + bv * c2.x, w0 * c0.y + bu * c1.y + bv * c2.y,
+                            w0 * c0.z + bu * c1.z + bv * c2.z, w0 * c0.w + bu * c1.w + bv * c2.w);
+  int mat = int(uint32_t(q0.w));
+  mat = min(max(mat, 0), s.num_materials - 1);
+  const float4* m = s.materials + 17 * size_t(mat);
+  float4 m0 = __ldg(m + 0), m1 = __ldg(m + 1), m2 = __ldg(m + 2), m3 = __ldg(m + 3), m4 = __ldg(m + 4),
+         m5 = __ldg(m + 5), m6 = __ldg(m + 6), m7 = __ldg(m + 7), m8 = __ldg(m + 8), m9 = __ldg(m + 9),
+         m10 = __ldg(m + 10), m15 = __ldg(m + 15), m16 = __ldg(m + 16);
+  GltfMaterial g;
+  g.base_color = mk(m0);
+  float opacity = 1.f;
+  if (sqrtf(vcol.x * vcol.x + vcol.y * vcol.y + vcol.z * vcol.z + vcol.w * vcol.w) > 0.f) {
+    g.base_color = g.base_color * mk(vcol);
+    opacity = opacity * vcol.w;
+  }
+  float cutout = m2.x * opacity;
+  if (m6.w > 0.f) cutout = cutout < m6.w ? 0.f : 1.f;
+  if (m6.w == 1.f) cutout = 1.f;
+  g.metallic = m0.w;
+  g.roughness = m1.x;
+  g.anisotropy = m1.y;
+  g.transmission = m1.w;
+  g.ior = m2.w;
+  g.specular_color = mk(m3);
+  g.specular = m3.w;
+  g.sheen_color = mk(m4);
+  g.sheen_roughness = m4.w;
+  g.clearcoat = m6.x;
+  g.clearcoat_roughness = m6.y;
+  g.diffuse_transmission = m6.z;
+  g.diffuse_transmission_color = mk(m15);
+  bool thin = m8.w > 0.5f;
+  g.thickness = thin ? 0.f : 1.f;
+  g.iridescence = m10.x;
+  g.iridescence_ior = m10.y;
+  g.iridescence_thickness = mixf(m10.z, m10.w, 1.f);
+  g.dispersion = m16.x;
+  // fix_normals
+  bool back = false;
+  if (dot(wi, ng) < 0.f) { ng = -ng; back = true; }
+  if (dot(ng, n) < 0.f) n = -n;
+  // anisotropy rotation -> tangent (material.glsl:84-93, utils.glsl:179-186)
+  float rot = atan2f(m9.y, m9.x) + kGlslPi;
+  v3 t3 = mk(tangent.x, tangent.y, tangent.z);
+  if (rot > 0.f) {
+    v3 b = cross(n, t3) * tangent.w;
+    float sr, cr;
+    sincosf(rot, &sr, &cr);
+    t3 = t3 * cr + b * sr;
+  }
+  S.c = build_closure(g, t3, lean);
+  S.n = n;
+  S.ng = ng;
+  S.emissive = mk(m5);
+  S.att_color = mk(m7);
+  S.att_dist = m7.w;
+  S.cutout = cutout;
+  S.backside = back;
+  S.thin_walled = thin;
+  S.pos = hit_pos;
+  return S;
+}
+
+}  // namespace dspbr

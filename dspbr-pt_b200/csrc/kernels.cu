@@ -1,0 +1,497 @@
+// Wavefront path tracer: generate / extend / connect / shade / accumulate.
+//
+// One wave traces `spp` samples of every pixel.  The reference evaluates a
+// whole path per fragment (renderer.frag:146-157 -> integrator/misptdl.glsl:
+// 34-93); here each bounce is split into
+//   extend   closest hit for every live path (bvh.glsl:149-216),
+//   connect  any-hit test of the NEE shadow rays emitted by the previous
+//            shade; visible contributions are added to the path radiance,
+//   shade    Russian roulette, absorption, emission, BSDF sampling, NEE
+//            sample generation (misptdl.glsl:54-90, renderer.frag:94-123),
+// and live paths are compacted into the next queue with one atomic per warp
+// (__ballot_sync / __popc).  The per-path arithmetic and RNG consumption order
+// follow the reference exactly; see DESIGN.md for the event_type note.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace dspbr {
+
+namespace {
+
+DEV void enqueue(uint32_t* q, uint32_t* counter, bool pred, uint32_t value) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, uint32_t(__popc(m)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (pred) q[base + __popc(m & ((1u << lane) - 1u))] = value;
+}
+
+DEV void count_warp(unsigned long long* ctr, bool pred) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(ctr, (unsigned long long)__popc(m));
+}
+
+DEV Rng load_rng(const WaveParams& p, const PathBuf& b, uint32_t path) {
+  Rng r;
+  r.state = b.rng[path];
+  if (p.rng_pcg) {
+    uint32_t pixel = path % uint32_t(p.npix), s = path / uint32_t(p.npix);
+    r.inc = pcg_inc(uint64_t(p.frame_base + s) * uint64_t(p.npix) + pixel);
+  } else {
+    r.inc = 0;
+  }
+  return r;
+}
+
+DEV float4 f4(v3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+}  // namespace
+
+// ---- generate: rng_init + calcuateViewRay (renderer.frag:146-150) ------------------
+__global__ void k_generate(WaveParams p, PathBuf b) {
+  uint32_t P = uint32_t(p.npix) * uint32_t(p.spp);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    b.counts[0] = P;
+    b.counts[1] = 0;
+    b.counts[2] = 0;
+  }
+  for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < P; path += gridDim.x * blockDim.x) {
+    uint32_t pixel = path % uint32_t(p.npix), s = path / uint32_t(p.npix);
+    int px = int(pixel % uint32_t(p.cam.width)), py = int(pixel / uint32_t(p.cam.width));
+    uint32_t frame = p.frame_base + s;
+    Rng r;
+    if (p.rng_pcg) {
+      uint64_t stream = uint64_t(frame) * uint64_t(p.npix) + pixel;
+      r.inc = pcg_inc(stream);
+      r.state = pcg_init(p.seed, stream);
+    } else {
+      Mwc m = mwc_init(int(frame) * p.max_bounces, px, py);
+      r.state = uint64_t(m.x) | (uint64_t(m.y) << 32);
+      r.inc = 0;
+    }
+    float r0 = r.next();
+    float r1 = r.next();
+    v3 org, dir;
+    camera_ray(p.cam, px, py, r0, r1, org, dir);
+    b.org[path] = f4(org, 0.f);
+    b.dir[path] = f4(dir, 0.f);
+    b.weight[path] = make_float4(1.f, 1.f, 1.f, 0.f);
+    b.rad[path] = make_float4(0.f, 0.f, 0.f, 0.f);
+    b.rng[path] = r.state;
+    b.q[0][path] = path;
+  }
+}
+
+// ---- extend: closest hit -----------------------------------------------------------------
+DEV void add_warp(unsigned long long* ctr, uint32_t v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, (unsigned long long)v);
+}
+
+template <bool kCount>
+__global__ void __launch_bounds__(128) k_extend(DevScene s, PathBuf b, int cur) {
+  const uint32_t count = b.counts[cur];
+  const uint32_t* q = b.q[cur];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool aborted = false;
+    uint32_t nodes = 0, tris = 0;
+    if (i < count) {
+      uint32_t path = q[i];
+      float4 o = b.org[path], d = b.dir[path];
+      Hit h;
+      traverse<false>(s, mk(o), mk(d), kTfarMax, h, aborted, kCount ? &nodes : nullptr, kCount ? &tris : nullptr);
+      b.hit[path] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+    }
+    count_warp(b.stats + 0, i < count);
+    count_warp(b.stats + 2, aborted);
+    if (kCount) {
+      add_warp(b.stats + 3, nodes);
+      add_warp(b.stats + 4, tris);
+    }
+  }
+}
+
+// ---- connect: shadow rays (bvh.glsl:218-229) ---------------------------------------------
+template <bool kCount>
+__global__ void __launch_bounds__(128) k_connect(DevScene s, PathBuf b) {
+  const uint32_t count = b.counts[2];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool aborted = false;
+    int nrays = 0;
+    uint32_t nodes = 0, tris = 0;
+    if (i < count) {
+      uint32_t path = b.qs[i];
+      int flags = b.sh_flags[path];
+      v3 org = mk(b.org[path]);
+      v3 add = mk(0.f);
+      if (flags & 1) {
+        float4 d = b.sh_dir[path];
+        Hit h;
+        bool ab = false;
+        // isOccluded normalises the light direction (bvh.glsl:225-229)
+        if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
+                            kCount ? &tris : nullptr))
+          add = mk(b.sh_c[path]);
+        aborted |= ab;
+        ++nrays;
+      }
+      if (flags & 2) {
+        float4 d = b.pl_dir[path];
+        Hit h;
+        bool ab = false;
+        if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
+                            kCount ? &tris : nullptr))
+          add = add + mk(b.pl_c[path]);
+        aborted |= ab;
+        ++nrays;
+      }
+      float4 L = b.rad[path];
+      b.rad[path] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+    }
+    unsigned m1 = __ballot_sync(0xffffffffu, nrays >= 1), m2 = __ballot_sync(0xffffffffu, nrays >= 2);
+    if ((threadIdx.x & 31) == 0 && (m1 | m2)) atomicAdd(b.stats + 1, (unsigned long long)(__popc(m1) + __popc(m2)));
+    count_warp(b.stats + 2, aborted);
+    if (kCount) {
+      add_warp(b.stats + 5, nodes);
+      add_warp(b.stats + 6, tris);
+    }
+  }
+}
+
+// ---- shade ------------------------------------------------------------------------------------
+DEV float mis_balance(float a, float c) { return a / (a + c); }
+
+DEV float4 clamp_result(const WaveParams& p, v3 L) {
+  if (p.clamp_threshold > 0.f)
+    return make_float4(clampf(L.x, 0.f, p.clamp_threshold), clampf(L.y, 0.f, p.clamp_threshold),
+                       clampf(L.z, 0.f, p.clamp_threshold), 1.f);
+  return f4(L, 1.f);
+}
+
+// Returns true if the path continues with an extension ray; sets `shadow`
+// when NEE shadow rays were emitted.
+DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t path,
+                    int depth, bool& shadow) {
+  shadow = false;
+  float4 hit = b.hit[path];
+  int tri = __float_as_int(hit.w);
+  float4 o4 = b.org[path], d4 = b.dir[path], w4 = b.weight[path], l4 = b.rad[path];
+  v3 dir = mk(d4);
+  v3 w = mk(w4);
+  float last_pdf = w4.w;
+  v3 L = mk(l4);
+  int bounce = depth;
+
+  if (tri < 0) {
+    if (depth == 0) {  // primary miss (misptdl.glsl:41-46)
+      if (p.bg_from_ibl > 0) {
+        v3 env = p.has_ibl ? ibl_eval(e, p.ibl_rot, dir) : mk(0.f);
+        b.result[path] = f4(env * w, 1.f);
+      } else {
+        b.result[path] = make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
+                                     p.bg_color.w);
+      }
+      return false;
+    }
+    // environment hit with MIS against the BSDF pdf (misptdl.glsl:84-88)
+    if (p.has_ibl) {
+      float ipdf = ibl_pdf(e, p.ibl_rot, dir);
+      float mis = mis_balance(last_pdf, ipdf);
+      L = L + ibl_eval(e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
+    }
+    b.result[path] = clamp_result(p, L);
+    return false;
+  }
+  if (!(bounce < p.max_bounces)) {  // loop condition (misptdl.glsl:54)
+    b.result[path] = clamp_result(p, L);
+    return false;
+  }
+  Rng rng = load_rng(p, b, path);
+  // Russian roulette (renderer.frag:119-123): weight boost every bounce
+  w = w * p.rr_factor;
+  if (bounce > p.rr_start && rng.next() <= p.rr_prob) {
+    b.result[path] = clamp_result(p, L);
+    return false;
+  }
+  v3 org = mk(o4);
+  v3 wi = -dir;
+  v3 pos = org + dir * hit.x;
+  Surface S = make_surface(s, tri, hit.y, hit.z, pos, wi, p.lean != 0);
+  if (S.backside && !S.thin_walled) {  // Beer-Lambert absorption (misptdl.glsl:60-63)
+    v3 sigma = -vlog(S.att_color) / S.att_dist;
+    w = w * vexp(-sigma * hit.x);
+  }
+  L = L + S.emissive * 1.0f * w;
+
+  // sample_bsdf_bounce (renderer.frag:94-116)
+  v3 wo;
+  v3 bw = mk(1.f);
+  float pdf = 1.f;
+  if (rng.next() > S.cutout) {
+    wo = -wi;
+  } else {
+    float u0 = rng.next(), u1 = rng.next(), u2 = rng.next();
+    float comp = rng.next();
+    BsdfSample bs = bsdf_sample(S.c, S.n, wi, comp, u0, u1, u2);
+    wo = bs.dir;
+    pdf = bs.pdf;
+    bw = bs.weight;
+    if (pdf < kEpsPdf) {  // absorbed: returns L without the clamp
+      b.result[path] = f4(L, 1.f);
+      return false;
+    }
+  }
+  pos = pos + (dot(S.ng, wo) < 0.f ? -S.ng : S.ng) * p.ray_eps;
+
+  // next-event estimation (misptdl.glsl:2-32, lighting.glsl:2-22)
+  float r0 = rng.next(), r1 = rng.next();
+  v3 n_nee = S.backside ? -S.n : S.n;
+  int flags = 0;
+  if (p.use_ibl > 0 && p.has_ibl) {
+    float ipdf;
+    v3 ld = ibl_sample(e, p.ibl_rot, p.env_mode, r0, r1, ipdf);
+    float cosnl = sat(dot(ld, n_nee));
+    if (cosnl > kEpsCos && ipdf > kEpsPdf) {
+      v3 f = bsdf_eval(S.c, S.n, wi, ld) / fmaxf(fabsf(dot(S.n, ld)), kEps);
+      float bpdf = bsdf_pdf(S.c, S.n, wi, ld);
+      v3 c = ibl_eval(e, p.ibl_rot, ld) * f * cosnl / ipdf;
+      if (bpdf > kEpsPdf) c = c * mis_balance(ipdf, bpdf);
+      b.sh_dir[path] = f4(ld, kTfarMax);
+      b.sh_c[path] = f4(c * w, 0.f);
+      flags |= 1;
+    }
+  }
+  if (p.pl_pos.w > 0.5f) {
+    v3 lp = mk(p.pl_pos.x, p.pl_pos.y, p.pl_pos.z);
+    v3 ld = lp - pos;
+    float dist2 = dot(ld, ld);
+    v3 ldn = normalize(ld);
+    float cosnl = sat(dot(ldn, n_nee));
+    if (cosnl > kEpsCos) {
+      v3 f = bsdf_eval(S.c, S.n, wi, ldn) / fmaxf(fabsf(dot(S.n, ldn)), kEps);
+      v3 c = f * (mk(p.pl_emis.x, p.pl_emis.y, p.pl_emis.z) / dist2) * cosnl;
+      b.pl_dir[path] = f4(ldn, sqrtf(dist2));
+      b.pl_c[path] = f4(c * w, 0.f);
+      flags |= 2;
+    }
+  }
+  b.sh_flags[path] = flags;
+  shadow = flags != 0;
+
+  w = w * bw;
+  b.org[path] = f4(pos, 0.f);
+  b.dir[path] = f4(wo, 0.f);
+  b.weight[path] = f4(w, pdf);
+  b.rad[path] = f4(L, 0.f);
+  b.rng[path] = rng.state;
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams p, PathBuf b, int cur, int depth) {
+  const uint32_t count = b.counts[cur];
+  const uint32_t* q = b.q[cur];
+  uint32_t* qn = b.q[cur ^ 1];
+  uint32_t* cn = b.counts + (cur ^ 1);
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    bool cont = false, shadow = false;
+    uint32_t path = 0;
+    if (i < count) {
+      path = q[i];
+      cont = shade_path(s, e, p, b, path, depth, shadow);
+    }
+    enqueue(qn, cn, cont, path);
+    enqueue(b.qs, b.counts + 2, shadow, path);
+  }
+}
+
+// ---- accumulate: running sum in FP64 per pixel -----------------------------------------
+__global__ void k_accumulate(WaveParams p, PathBuf b, double4* accum) {
+  for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < uint32_t(p.npix); px += gridDim.x * blockDim.x) {
+    double4 a = accum[px];
+    for (int s = 0; s < p.spp; ++s) {
+      float4 r = b.result[size_t(s) * p.npix + px];
+      a.x += double(r.x); a.y += double(r.y); a.z += double(r.z); a.w += double(r.w);
+    }
+    accum[px] = a;
+  }
+}
+
+__global__ void k_mean(const double4* accum, double inv, float4* out, int npix) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+    double4 a = accum[i];
+    out[i] = make_float4(float(a.x * inv), float(a.y * inv), float(a.z * inv), float(a.w * inv));
+  }
+}
+
+// ---- scene preparation: leaf-ordered triangle records ------------------------------------
+__global__ void k_gather_tris(const float4* verts, const uint32_t* indices, const int32_t* remap, uint32_t nslots,
+                              uint32_t ntris, float4* tris) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += gridDim.x * blockDim.x) {
+    int32_t t = remap[i];
+    if (t < 0 || uint32_t(t) >= ntris) {
+      tris[3 * size_t(i)] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+      tris[3 * size_t(i) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      tris[3 * size_t(i) + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
+    }
+    float4 a = verts[5 * size_t(indices[3 * size_t(t)])];
+    float4 b = verts[5 * size_t(indices[3 * size_t(t) + 1])];
+    float4 c = verts[5 * size_t(indices[3 * size_t(t) + 2])];
+    tris[3 * size_t(i)] = make_float4(a.x, a.y, a.z, __int_as_float(t));
+    tris[3 * size_t(i) + 1] = make_float4(__fsub_rn(b.x, a.x), __fsub_rn(b.y, a.y), __fsub_rn(b.z, a.z), 0.f);
+    tris[3 * size_t(i) + 2] = make_float4(__fsub_rn(c.x, a.x), __fsub_rn(c.y, a.y), __fsub_rn(c.z, a.z), 0.f);
+  }
+}
+
+// ---- kernel-level queries ----------------------------------------------------------------
+__global__ void k_trace_rays(DevScene s, const float4* rays, uint32_t n, int any, int32_t* tri, float* t, float2* uv,
+                             int32_t* occ) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 a = rays[2 * i], c = rays[2 * i + 1];
+    v3 org = mk(a.x, a.y, a.z), dir = mk(a.w, c.x, c.y);
+    Hit h;
+    bool ab = false;
+    if (any) {
+      // isOccluded (bvh.glsl:225-229) normalises the direction first
+      bool o = traverse<true>(s, org, normalize_rn(dir), c.z, h, ab);
+      occ[i] = o ? 1 : 0;
+    } else {
+      traverse<false>(s, org, dir, c.z, h, ab);
+      tri[i] = h.tri;
+      t[i] = h.t;
+      uv[i] = make_float2(h.u, h.v);
+    }
+  }
+}
+
+__global__ void k_bsdf_query(DevScene s, uint32_t n, const float* hit20, const float* wo3, const float* rnd4, int lean,
+                             float* eval4, float* sample10, int32_t* flags) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float* h = hit20 + 20 * size_t(i);
+    // Build the surface the way fillRenderState + configure_gltf_material do,
+    // from explicit shading inputs instead of a triangle fetch.
+    v3 n0 = mk(h[0], h[1], h[2]), ng = mk(h[3], h[4], h[5]);
+    float4 tangent = make_float4(h[6], h[7], h[8], h[9]);
+    v3 wi = mk(h[10], h[11], h[12]);
+    float4 vcol = make_float4(h[15], h[16], h[17], h[18]);
+    int mat = min(max(int(uint32_t(h[19])), 0), s.num_materials - 1);
+    const float4* m = s.materials + 17 * size_t(mat);
+    float4 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3], m4 = m[4], m6 = m[6], m8 = m[8], m9 = m[9], m10 = m[10],
+           m15 = m[15], m16 = m[16];
+    GltfMaterial g;
+    g.base_color = mk(m0);
+    if (sqrtf(vcol.x * vcol.x + vcol.y * vcol.y + vcol.z * vcol.z + vcol.w * vcol.w) > 0.f)
+      g.base_color = g.base_color * mk(vcol);
+    g.metallic = m0.w; g.roughness = m1.x; g.anisotropy = m1.y; g.transmission = m1.w; g.ior = m2.w;
+    g.specular_color = mk(m3); g.specular = m3.w; g.sheen_color = mk(m4); g.sheen_roughness = m4.w;
+    g.clearcoat = m6.x; g.clearcoat_roughness = m6.y; g.diffuse_transmission = m6.z;
+    g.diffuse_transmission_color = mk(m15);
+    g.thickness = m8.w > 0.5f ? 0.f : 1.f;
+    g.iridescence = m10.x; g.iridescence_ior = m10.y; g.iridescence_thickness = mixf(m10.z, m10.w, 1.f);
+    g.dispersion = m16.x;
+    bool back = false;
+    if (dot(wi, ng) < 0.f) { ng = -ng; back = true; }
+    if (dot(ng, n0) < 0.f) n0 = -n0;
+    float rot = atan2f(m9.y, m9.x) + kGlslPi;
+    v3 t3 = mk(tangent.x, tangent.y, tangent.z);
+    if (rot > 0.f) {
+      v3 bt = cross(n0, t3) * tangent.w;
+      float sr, cr;
+      sincosf(rot, &sr, &cr);
+      t3 = t3 * cr + bt * sr;
+    }
+    Closure c = build_closure(g, t3, lean != 0);
+    v3 wo = mk(wo3[3 * i], wo3[3 * i + 1], wo3[3 * i + 2]);
+    v3 ev = bsdf_eval(c, n0, wi, wo);
+    float pd = bsdf_pdf(c, n0, wi, wo);
+    eval4[4 * i] = ev.x; eval4[4 * i + 1] = ev.y; eval4[4 * i + 2] = ev.z; eval4[4 * i + 3] = pd;
+    const float* r = rnd4 + 4 * size_t(i);
+    BsdfSample bs = bsdf_sample(c, n0, wi, r[0], r[1], r[2], r[3]);
+    float* o = sample10 + 10 * size_t(i);
+    o[0] = bs.dir.x; o[1] = bs.dir.y; o[2] = bs.dir.z; o[3] = bs.pdf;
+    o[4] = bs.weight.x; o[5] = bs.weight.y; o[6] = bs.weight.z;
+    o[7] = bs.specular; o[8] = bs.crossed; o[9] = bs.next_ior;
+    flags[i] = back ? 1 : 0;
+  }
+}
+
+__global__ void k_ibl_query(DevIbl e, float rot, int mode, uint32_t n, const float* r2, const float* dirs, float* sdp4,
+                            float* pdf, float* rgb) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float sp;
+    v3 d = ibl_sample(e, rot, mode, r2[2 * i], r2[2 * i + 1], sp);
+    sdp4[4 * i] = d.x; sdp4[4 * i + 1] = d.y; sdp4[4 * i + 2] = d.z; sdp4[4 * i + 3] = sp;
+    v3 q = mk(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]);
+    pdf[i] = ibl_pdf(e, rot, q);
+    v3 c = ibl_eval(e, rot, q);
+    rgb[3 * i] = c.x; rgb[3 * i + 1] = c.y; rgb[3 * i + 2] = c.z;
+  }
+}
+
+__global__ void k_camera_rays(Camera c, uint32_t n, const int32_t* xy, const float* r2, float* rays6) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    v3 o, d;
+    camera_ray(c, xy[2 * i], xy[2 * i + 1], r2[2 * i], r2[2 * i + 1], o, d);
+    float* r = rays6 + 6 * size_t(i);
+    r[0] = o.x; r[1] = o.y; r[2] = o.z; r[3] = d.x; r[4] = d.y; r[5] = d.z;
+  }
+}
+
+// ---- launchers --------------------------------------------------------------------------------
+static int grid_for(uint64_t n, int threads, int cap) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return int(b < uint64_t(cap) ? b : uint64_t(cap));
+}
+
+void launch_generate(const WaveParams& p, const PathBuf& b, cudaStream_t st) {
+  uint64_t P = uint64_t(p.npix) * p.spp;
+  k_generate<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(p, b);
+}
+void launch_extend(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
+  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+}
+void launch_connect(const DevScene& s, const PathBuf& b, bool count, const LaunchCfg& lc, cudaStream_t st) {
+  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b);
+  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b);
+}
+void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int cur, int depth,
+                  const LaunchCfg& lc, cudaStream_t st) {
+  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(s, e, p, b, cur, depth);
+}
+void launch_accumulate(const WaveParams& p, const PathBuf& b, double4* accum, cudaStream_t st) {
+  k_accumulate<<<grid_for(p.npix, 256, 148 * 8), 256, 0, st>>>(p, b, accum);
+}
+void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st) {
+  k_mean<<<grid_for(npix, 256, 148 * 8), 256, 0, st>>>(accum, inv_count, out, npix);
+}
+void launch_gather_tris(const float4* verts, const uint32_t* indices, const int32_t* remap, uint32_t nslots,
+                        uint32_t ntris, float4* tris, cudaStream_t st) {
+  k_gather_tris<<<grid_for(nslots, 256, 148 * 16), 256, 0, st>>>(verts, indices, remap, nslots, ntris, tris);
+}
+void launch_trace_rays(const DevScene& s, const float4* rays, uint32_t n, int any, int32_t* tri, float* t, float2* uv,
+                       int32_t* occ, cudaStream_t st) {
+  k_trace_rays<<<grid_for(n, 128, 148 * 16), 128, 0, st>>>(s, rays, n, any, tri, t, uv, occ);
+}
+void launch_bsdf_query(const DevScene& s, uint32_t n, const float* hit20, const float* wo3, const float* rnd4,
+                       int lean, float* eval4, float* sample10, int32_t* flags, cudaStream_t st) {
+  k_bsdf_query<<<grid_for(n, 128, 148 * 16), 128, 0, st>>>(s, n, hit20, wo3, rnd4, lean, eval4, sample10, flags);
+}
+void launch_ibl_query(const DevIbl& e, float rot, int mode, uint32_t n, const float* r2, const float* dirs,
+                      float* sdp4, float* pdf, float* rgb, cudaStream_t st) {
+  k_ibl_query<<<grid_for(n, 128, 148 * 16), 128, 0, st>>>(e, rot, mode, n, r2, dirs, sdp4, pdf, rgb);
+}
+void launch_camera_rays(const Camera& c, uint32_t n, const int32_t* xy, const float* r2, float* rays6,
+                        cudaStream_t st) {
+  k_camera_rays<<<grid_for(n, 128, 148 * 16), 128, 0, st>>>(c, n, xy, r2, rays6);
+}
+
+}  // namespace dspbr

@@ -1,0 +1,83 @@
+// Host-visible interface of the wavefront kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device.cuh"
+
+namespace dspbr {
+
+// Per-wave constants of the reference's uniform block (renderer.frag:10-31).
+struct WaveParams {
+  Camera cam;
+  int npix;             // width * height
+  int spp;              // samples per pixel in this wave (path = s * npix + pixel)
+  uint32_t frame_base;  // 1-based progressive frame number of sample 0
+  int max_bounces;
+  int rng_pcg;          // 0: MWC of rng.glsl, 1: PCG32
+  uint64_t seed;
+  int use_ibl, bg_from_ibl, env_mode, lean, has_ibl;
+  float ibl_rot;        // radians
+  float4 bg_color;
+  float ray_eps, clamp_threshold;
+  float rr_prob, rr_factor;
+  int rr_start;
+  float4 pl_pos, pl_emis;
+  int count_traversal;  // accumulate node visits / triangle tests into stats[3..6]
+};
+
+// Structure-of-arrays path state, capacity = paths of one wave.
+struct PathBuf {
+  float4* org;      // ray origin (shadow rays of the same vertex share it)
+  float4* dir;
+  float4* weight;   // path_weight.xyz, last_bounce_pdf
+  float4* rad;      // L.xyz
+  uint64_t* rng;
+  float4* hit;      // t, u, v, triangle id bits
+  float4* sh_dir;   // IBL shadow ray dir.xyz, tfar
+  float4* sh_c;     // IBL NEE contribution * path weight
+  float4* pl_dir;   // point-light shadow ray dir.xyz, tfar
+  float4* pl_c;
+  int* sh_flags;    // bit0: IBL shadow ray, bit1: point-light shadow ray
+  float4* result;   // final RGBA of each path
+  uint32_t* q[2];   // extension ray queues (path ids)
+  uint32_t* qs;     // shadow queue (path ids)
+  uint32_t* counts; // [0],[1]: extension queue sizes, [2]: shadow queue size
+  // [0] closest-hit rays, [1] shadow rays, [2] aborted traversals,
+  // [3]/[4] nodes visited / triangles tested by closest-hit rays, [5]/[6] by shadow rays
+  unsigned long long* stats;
+  uint32_t capacity;
+};
+
+struct LaunchCfg {
+  int trace_blocks = 0, trace_threads = 128;
+  int shade_blocks = 0, shade_threads = 128;
+};
+
+void launch_generate(const WaveParams& p, const PathBuf& b, cudaStream_t st);
+void launch_extend(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
+void launch_connect(const DevScene& s, const PathBuf& b, bool count, const LaunchCfg& lc, cudaStream_t st);
+void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int cur, int depth,
+                  const LaunchCfg& lc, cudaStream_t st);
+void launch_accumulate(const WaveParams& p, const PathBuf& b, double4* accum, cudaStream_t st);
+void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
+
+// kernel-level queries (device buffers)
+void launch_trace_rays(const DevScene& s, const float4* rays, uint32_t n, int any, int32_t* tri, float* t, float2* uv,
+                       int32_t* occ, cudaStream_t st);
+void launch_bsdf_query(const DevScene& s, uint32_t n, const float* hit20, const float* wo3, const float* rnd4,
+                       int lean, float* eval4, float* sample10, int32_t* flags, cudaStream_t st);
+void launch_ibl_query(const DevIbl& e, float rot, int mode, uint32_t n, const float* r2, const float* dirs,
+                      float* sdp4, float* pdf, float* rgb, cudaStream_t st);
+void launch_camera_rays(const Camera& c, uint32_t n, const int32_t* xy, const float* r2, float* rays6,
+                        cudaStream_t st);
+
+// environment tables (ibl.cu)
+void launch_ibl_tables(const float4* rgba, int w, int h, float* lum, float* pdf, float* cdf, float* rowsum,
+                       float* ypdf, float* ycdf, double* total, cudaStream_t st);
+
+// scene preparation (kernels.cu)
+void launch_gather_tris(const float4* verts, const uint32_t* indices, const int32_t* remap, uint32_t nslots,
+                        uint32_t ntris, float4* tris, cudaStream_t st);
+
+}  // namespace dspbr

@@ -1,0 +1,13 @@
+"""B200 path-tracing hot path of dspbr-pt behind the reference's embedding API.
+
+Public surface: PathtracingViewport (viewport.py, mirror of
+packages/lib/pathtracing_viewport.ts), the lower-level Context / DeviceScene /
+DeviceIbl / Bvh wrappers of the C ABI (include/dspbr.h), and the seeded
+synthetic workloads (synth.py).
+"""
+from .viewport import (Bvh, Context, DeviceIbl, DeviceScene, PathtracingCamera, PathtracingViewport,
+                       createPathtracingViewport, look_at_matrix)
+from . import synth
+
+__all__ = ["Bvh", "Context", "DeviceIbl", "DeviceScene", "PathtracingCamera", "PathtracingViewport",
+           "createPathtracingViewport", "look_at_matrix", "synth"]

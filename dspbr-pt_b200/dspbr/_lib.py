@@ -1,0 +1,159 @@
+"""ctypes binding of libdspbr_cuda.so (include/dspbr.h).
+
+The library is the product: every call goes to the CUDA implementation.  If
+the shared object is missing the import fails loudly; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("DSPBR_LIB", os.path.join(HERE, "libdspbr_cuda.so"))
+
+OK = 0
+ERR = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4: "invalid state",
+       -5: "admission refused", -6: "not found", -7: "device fault"}
+PROFILE_FULL, PROFILE_LEAN = 0, 1
+RNG_MWC, RNG_PCG = 0, 1
+ENV_ALIAS, ENV_CDF = 0, 1
+
+
+class DspbrError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERR.get(code, code)}: {message}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("max_bounces", C.c_int32), ("use_ibl", C.c_int32), ("ibl_rotation_deg", C.c_float),
+        ("background_from_ibl", C.c_int32), ("background_color", C.c_float * 4), ("ray_eps", C.c_float),
+        ("clamp_threshold", C.c_float), ("point_light_position", C.c_float * 4),
+        ("point_light_emission", C.c_float * 4), ("rr_start_depth", C.c_int32), ("rr_termination_prob", C.c_float),
+        ("profile", C.c_int32), ("rng", C.c_int32), ("seed", C.c_uint64), ("env_sampling", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Diag(C.Structure):
+    _fields_ = [
+        ("sample_count", C.c_uint64), ("width", C.c_int32), ("height", C.c_int32),
+        ("rays_primary", C.c_uint64), ("rays_extension", C.c_uint64), ("rays_shadow", C.c_uint64),
+        ("traversal_aborted", C.c_uint64), ("scene_triangles", C.c_uint64), ("bvh_nodes", C.c_uint64),
+        ("bvh_indices", C.c_uint64), ("device_bytes", C.c_uint64), ("last_render_ms", C.c_double),
+        ("bvh_build_ms", C.c_double), ("upload_ms", C.c_double),
+        ("nodes_closest", C.c_uint64), ("tris_closest", C.c_uint64), ("nodes_shadow", C.c_uint64),
+        ("tris_shadow", C.c_uint64), ("extend_ms", C.c_double), ("connect_ms", C.c_double), ("shade_ms", C.c_double),
+        ("extend_launches", C.c_uint64), ("connect_launches", C.c_uint64), ("shade_launches", C.c_uint64),
+        ("other_launches", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_F = C.POINTER(C.c_float)
+_I = C.POINTER(C.c_int32)
+_U = C.POINTER(C.c_uint32)
+_D = C.POINTER(C.c_double)
+_V = C.c_void_p
+_PV = C.POINTER(C.c_void_p)
+
+SIGNATURES = {
+    "dspbr_params_default": (None, [C.POINTER(Params)]),
+    "dspbr_create": (C.c_int, [C.c_int, _PV]),
+    "dspbr_destroy": (C.c_int, [_V]),
+    "dspbr_last_error": (C.c_int, [_V, C.c_char_p, C.c_size_t]),
+    "dspbr_device_count": (C.c_int, [_I]),
+    "dspbr_bvh_build": (C.c_int, [_F, C.c_uint32, C.c_uint32, _U, C.c_uint32, _PV]),
+    "dspbr_bvh_info": (C.c_int, [_V, _U, _U, _U, _U]),
+    "dspbr_bvh_copy": (C.c_int, [_V, _F, _I]),
+    "dspbr_bvh_error": (C.c_int, [_V, C.c_char_p, C.c_size_t]),
+    "dspbr_bvh_free": (None, [_V]),
+    "dspbr_scene_create": (C.c_int, [_V, _F, C.c_uint32, _U, C.c_uint32, _F, C.c_uint32, _F, C.c_uint32, _I,
+                                      C.c_uint32, _PV]),
+    "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),
+    "dspbr_scene_device_bytes": (C.c_int, [_V, C.POINTER(C.c_uint64)]),
+    "dspbr_scene_destroy": (C.c_int, [_V]),
+    "dspbr_ibl_create": (C.c_int, [_V, _F, C.c_int, C.c_int, _PV]),
+    "dspbr_ibl_tables": (C.c_int, [_V, _F, _F, _F, _F, _D]),
+    "dspbr_ibl_alias_table": (C.c_int, [_V, _F, _I]),
+    "dspbr_ibl_destroy": (C.c_int, [_V]),
+    "dspbr_set_scene": (C.c_int, [_V, _V]),
+    "dspbr_set_ibl": (C.c_int, [_V, _V]),
+    "dspbr_set_camera": (C.c_int, [_V, _F, C.c_float, C.c_float]),
+    "dspbr_set_params": (C.c_int, [_V, C.POINTER(Params)]),
+    "dspbr_get_params": (C.c_int, [_V, C.POINTER(Params)]),
+    "dspbr_resize": (C.c_int, [_V, C.c_int, C.c_int]),
+    "dspbr_reset": (C.c_int, [_V]),
+    "dspbr_render": (C.c_int, [_V, C.c_int]),
+    "dspbr_render_async": (C.c_int, [_V, C.c_int]),
+    "dspbr_poll": (C.c_int, [_V, _I]),
+    "dspbr_wait": (C.c_int, [_V]),
+    "dspbr_read_accum": (C.c_int, [_V, _F, C.c_size_t]),
+    "dspbr_get_diagnostics": (C.c_int, [_V, C.POINTER(Diag)]),
+    "dspbr_set_wave_paths": (C.c_int, [_V, C.c_uint32]),
+    "dspbr_set_counting": (C.c_int, [_V, C.c_int]),
+    "dspbr_set_profiling": (C.c_int, [_V, C.c_int]),
+    "dspbr_trace_closest": (C.c_int, [_V, _V, _F, C.c_uint32, _I, _F, _F]),
+    "dspbr_trace_occluded": (C.c_int, [_V, _V, _F, C.c_uint32, _I]),
+    "dspbr_bsdf_query": (C.c_int, [_V, _V, C.c_uint32, _F, _F, _F, _F, _F, _I]),
+    "dspbr_ibl_query": (C.c_int, [_V, _V, C.c_uint32, _F, _F, _F, _F, _F]),
+    "dspbr_camera_rays": (C.c_int, [_V, C.c_uint32, _I, _F, _F]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libdspbr_cuda.so not found at {path}: build it with dspbr-pt_b200/build.py")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_F)
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_I)
+
+
+def uptr(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_U)
+
+
+def f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def check(rc: int, ctx=None) -> None:
+    if rc != OK:
+        msg = ""
+        if ctx is not None:
+            buf = C.create_string_buffer(512)
+            load().dspbr_last_error(ctx, buf, 512)
+            msg = buf.value.decode(errors="replace")
+        raise DspbrError(rc, msg)
+
+
+def default_params() -> Params:
+    p = Params()
+    load().dspbr_params_default(C.byref(p))
+    return p

@@ -1,0 +1,359 @@
+"""Host-side mirror of the reference's embedding API.
+
+`PathtracingViewport` keeps the method names, argument meaning and error
+behaviour of packages/lib/pathtracing_viewport.ts:100-342 (settings, setScene,
+setIBL, setCamera / setLookAtCamera, resize, start / stop, resetAccumulation,
+diagnostics, events).  Rendering goes through the C ABI of libdspbr_cuda.so;
+the WebGL canvas becomes a headless device buffer read back with
+readAccumulation().  Display-only settings (tone mapping, exposure, gamma,
+FXAA, pixel ratio, tiling) are accepted and stored: they act after the
+accumulation buffer, outside the path-tracing hot path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, f32, fptr, iptr, uptr
+from .synth import MATERIAL_STRIDE, VERTEX_STRIDE
+
+
+class Bvh:
+    """BVH in the reference's node layout (replaces buildIndexedBvh, tinybvh_builder.ts:142-215)."""
+
+    def __init__(self, nodes: np.ndarray, indices: np.ndarray, depth: int, triangles: int):
+        self.nodes = nodes
+        self.indices = indices
+        self.depth = depth
+        self.triangles = triangles
+
+    @staticmethod
+    def build(positions: np.ndarray, indices: np.ndarray, stride: int | None = None) -> "Bvh":
+        lib = _lib.load()
+        pos = f32(positions)
+        if stride is None:
+            stride = pos.shape[1] if pos.ndim == 2 else 3
+        idx = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        h = C.c_void_p()
+        rc = lib.dspbr_bvh_build(fptr(pos), pos.size // stride, stride, uptr(idx), idx.size, C.byref(h))
+        try:
+            if rc != 0:
+                buf = C.create_string_buffer(256)
+                if h:
+                    lib.dspbr_bvh_error(h, buf, 256)
+                raise _lib.DspbrError(rc, "BVH build failed: " + buf.value.decode())
+            nn, ni, dep, nt = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+            lib.dspbr_bvh_info(h, C.byref(nn), C.byref(ni), C.byref(dep), C.byref(nt))
+            nodes = np.zeros(nn.value * 16, np.float32)
+            remap = np.zeros(ni.value, np.int32)
+            check(lib.dspbr_bvh_copy(h, fptr(nodes), iptr(remap)))
+            return Bvh(nodes, remap, dep.value, nt.value)
+        finally:
+            lib.dspbr_bvh_free(h)
+
+
+class Context:
+    """One CUDA device + stream (the C ABI's dspbr_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.dspbr_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.dspbr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        check(rc, self.h)
+
+
+class DeviceScene:
+    """Scene resident on the device (dspbr_scene)."""
+
+    def __init__(self, ctx: Context, vertices, indices, materials, bvh: Bvh | None = None):
+        self.ctx = ctx
+        v = f32(vertices).reshape(-1, VERTEX_STRIDE)
+        i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        m = f32(materials).reshape(-1, MATERIAL_STRIDE)
+        h = C.c_void_p()
+        if bvh is None:
+            rc = ctx.lib.dspbr_scene_create(ctx.h, fptr(v), v.shape[0], uptr(i), i.size, fptr(m), m.shape[0],
+                                            None, 0, None, 0, C.byref(h))
+        else:
+            rc = ctx.lib.dspbr_scene_create(ctx.h, fptr(v), v.shape[0], uptr(i), i.size, fptr(m), m.shape[0],
+                                            fptr(bvh.nodes), bvh.nodes.size // 16, iptr(bvh.indices),
+                                            bvh.indices.size, C.byref(h))
+        ctx.check(rc)
+        self.h = h
+        self.num_triangles = i.size // 3
+
+    def update_materials(self, materials, first: int = 0):
+        m = f32(materials).reshape(-1, MATERIAL_STRIDE)
+        self.ctx.check(self.ctx.lib.dspbr_scene_update_materials(self.h, fptr(m), first, m.shape[0]))
+
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        self.ctx.check(self.ctx.lib.dspbr_scene_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.dspbr_scene_destroy(self.h)
+            self.h = None
+
+
+class DeviceIbl:
+    """Environment map + importance tables on the device (dspbr_ibl)."""
+
+    def __init__(self, ctx: Context, rgba: np.ndarray):
+        self.ctx = ctx
+        img = f32(rgba)
+        self.height, self.width = img.shape[0], img.shape[1]
+        h = C.c_void_p()
+        ctx.check(ctx.lib.dspbr_ibl_create(ctx.h, fptr(img), self.width, self.height, C.byref(h)))
+        self.h = h
+
+    def tables(self):
+        n = self.width * self.height
+        pdf, cdf = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        ypdf, ycdf = np.zeros(self.height, np.float32), np.zeros(self.height, np.float32)
+        tot = C.c_double()
+        self.ctx.check(self.ctx.lib.dspbr_ibl_tables(self.h, fptr(pdf), fptr(cdf), fptr(ypdf), fptr(ycdf),
+                                                     C.byref(tot)))
+        return {"pdf": pdf, "cdf": cdf, "yPdf": ypdf, "yCdf": ycdf, "totalSum": tot.value}
+
+    def alias_table(self):
+        n = self.width * self.height
+        prob, alias = np.zeros(n, np.float32), np.zeros(n, np.int32)
+        self.ctx.check(self.ctx.lib.dspbr_ibl_alias_table(self.h, fptr(prob), iptr(alias)))
+        return prob, alias
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.dspbr_ibl_destroy(self.h)
+            self.h = None
+
+
+@dataclass
+class PathtracingCamera:
+    """PathtracingCamera (renderer.ts:56-61): fov in degrees, near, matrixWorld."""
+    matrixWorld: np.ndarray
+    fov: float = 45.0
+    near: float = 0.01
+
+
+def look_at_matrix(position, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
+    """ViewportCamera.setLookAt (pathtracing_viewport.ts:82-97)."""
+    p, t, u = (np.asarray(x, np.float64) for x in (position, target, up))
+
+    def nrm(v, fb):
+        n = math.sqrt(float(v @ v))
+        return np.asarray(fb, np.float64) if n <= 1e-10 else v / n
+
+    fwd = nrm(t - p, (0, 0, -1))
+    right = nrm(np.cross(fwd, u), (1, 0, 0))
+    cam_up = nrm(np.cross(right, fwd), (0, 1, 0))
+    e = np.zeros(16, np.float32)
+    e[0:3], e[4:7], e[8:11], e[12:15], e[15] = right, cam_up, -fwd, p, 1.0
+    return e
+
+
+class PathtracingViewport:
+    """Drop-in for PathtracingViewport (pathtracing_viewport.ts:100-342) on a B200."""
+
+    EVENTS = ("sceneLoaded", "sceneLoadFailed", "iblLoaded", "iblLoadFailed", "diagnosticsChanged",
+              "frameRendered", "renderFinished")
+
+    def __init__(self, settings: dict | None = None, device: int = 0, width: int = 1, height: int = 1,
+                 materialProfile: str = "webgl-full"):
+        self.ctx = Context(device)
+        self.params = _lib.default_params()
+        self.params.profile = _lib.PROFILE_LEAN if materialProfile == "webgl-lean" else _lib.PROFILE_FULL
+        self._display = {"exposure": 1.0, "toneMapping": "None", "pixelRatio": 1.0, "interactionPixelRatio": 0.5,
+                         "enableGamma": True, "enableFxaa": False, "tileResolution": 4, "debugMode": "None"}
+        self._listeners: dict[str, set] = {e: set() for e in self.EVENTS}
+        self._scene: DeviceScene | None = None
+        self._ibl: DeviceIbl | None = None
+        self.camera = PathtracingCamera(look_at_matrix((0, 0, 6), (0, 0, 0)), 45.0, 0.01)
+        self.running = False
+        self.width, self.height = 0, 0
+        self._apply_params()
+        self.resize(width, height)
+        self._apply_camera()
+        if settings:
+            self.setSettings(settings)
+
+    # ---- events (pathtracing_viewport.ts:125-143) ----
+    def on(self, event: str, listener):
+        self._listeners[event].add(listener)
+        return lambda: self.off(event, listener)
+
+    def off(self, event: str, listener):
+        self._listeners[event].discard(listener)
+
+    def _emit(self, event, payload):
+        for fn in list(self._listeners[event]):
+            fn(payload)
+
+    # ---- settings (pathtracing_viewport.ts:147-170) ----
+    def setSettings(self, settings: dict) -> None:
+        p = self.params
+        for k, v in settings.items():
+            if k == "maxBounces":
+                p.max_bounces = int(v)
+            elif k == "useIBL":
+                p.use_ibl = int(bool(v))
+            elif k == "showBackground":
+                p.background_from_ibl = int(bool(v))
+            elif k == "iblRotationDegrees":
+                p.ibl_rotation_deg = float(v)
+            elif k == "backgroundColor":
+                for j in range(4):
+                    p.background_color[j] = float(v[j])
+            elif k == "rayEps":
+                p.ray_eps = float(v)
+            elif k == "clampThreshold":
+                p.clamp_threshold = float(v)
+            elif k in self._display:
+                self._display[k] = v
+            elif k == "rng":
+                p.rng = _lib.RNG_PCG if v == "pcg" else _lib.RNG_MWC
+            elif k == "seed":
+                p.seed = int(v)
+            elif k == "envSampling":
+                p.env_sampling = _lib.ENV_CDF if v == "cdf" else _lib.ENV_ALIAS
+            elif k == "russianRouletteStartDepth":
+                p.rr_start_depth = int(v)
+            else:
+                raise KeyError(f"unknown setting {k!r}")
+        self._apply_params()
+        self._emit_diag()
+
+    def _apply_params(self):
+        self.ctx.check(self.ctx.lib.dspbr_set_params(self.ctx.h, C.byref(self.params)))
+
+    # ---- scene / IBL ----
+    def setScene(self, scene) -> None:
+        """scene: a synth.Scene or any object with vertices / indices / materials arrays."""
+        try:
+            ds = DeviceScene(self.ctx, scene.vertices, scene.indices, scene.materials, getattr(scene, "bvh", None))
+        except Exception as e:
+            self._emit("sceneLoadFailed", {"error": e})
+            raise
+        if self._scene is not None:
+            self._scene.close()
+        self._scene = ds
+        self.ctx.check(self.ctx.lib.dspbr_set_scene(self.ctx.h, ds.h))
+        self._emit("sceneLoaded", {"scene": scene})
+        self._emit_diag()
+
+    def setIBL(self, ibl) -> None:
+        """ibl: IblTextureLike ({'image': {'data', 'width', 'height'}}) or an (H, W, 4) array."""
+        if isinstance(ibl, dict):
+            im = ibl["image"]
+            rgba = np.asarray(im["data"], np.float32).reshape(im["height"], im["width"], 4)
+        else:
+            rgba = np.asarray(ibl, np.float32)
+        try:
+            di = DeviceIbl(self.ctx, rgba)
+        except Exception as e:
+            self._emit("iblLoadFailed", {"error": e})
+            raise
+        if self._ibl is not None:
+            self._ibl.close()
+        self._ibl = di
+        self.ctx.check(self.ctx.lib.dspbr_set_ibl(self.ctx.h, di.h))
+        self._emit("iblLoaded", {"ibl": ibl})
+        self._emit_diag()
+
+    # ---- camera ----
+    def setCamera(self, camera) -> None:
+        self.camera = PathtracingCamera(f32(camera.matrixWorld).reshape(16), float(camera.fov), float(camera.near))
+        self._apply_camera()
+        self._emit_diag()
+
+    def setLookAtCamera(self, position, target, up=(0.0, 1.0, 0.0), fov=None, near=None) -> None:
+        self.camera = PathtracingCamera(look_at_matrix(position, target, up),
+                                        self.camera.fov if fov is None else float(fov),
+                                        self.camera.near if near is None else float(near))
+        self._apply_camera()
+        self._emit_diag()
+
+    def _apply_camera(self):
+        m = f32(self.camera.matrixWorld)
+        self.ctx.check(self.ctx.lib.dspbr_set_camera(self.ctx.h, fptr(m), self.camera.fov, self.camera.near))
+
+    # ---- size / progressive rendering ----
+    def resize(self, width: int, height: int) -> None:
+        self.width, self.height = max(1, int(width)), max(1, int(height))
+        self.ctx.check(self.ctx.lib.dspbr_resize(self.ctx.h, self.width, self.height))
+        self._emit_diag()
+
+    def start(self, sampleLimit: int = -1, frames_per_call: int | None = None) -> None:
+        """Renders progressive frames until `sampleLimit` (synchronous; -1 = one frame)."""
+        if self._scene is None:
+            raise RuntimeError("Cannot start rendering without a scene.")
+        self.running = True
+        target = 1 if sampleLimit < 0 else int(sampleLimit)
+        done = self.diagnostics["sample_count"]
+        while self.running and done < target:
+            n = target - done if frames_per_call is None else min(frames_per_call, target - done)
+            self.ctx.check(self.ctx.lib.dspbr_render(self.ctx.h, n))
+            done += n
+            self._emit("frameRendered", {"frameCount": done})
+        self.running = False
+        self._emit("renderFinished", {"frameCount": done})
+        self._emit_diag()
+
+    def stop(self) -> None:
+        self.running = False
+        self._emit_diag()
+
+    def resetAccumulation(self) -> None:
+        self.ctx.check(self.ctx.lib.dspbr_reset(self.ctx.h))
+        self._emit_diag()
+
+    def readAccumulation(self) -> np.ndarray:
+        """Running mean, (height, width, 4) float32, row 0 = bottom row."""
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        self.ctx.check(self.ctx.lib.dspbr_read_accum(self.ctx.h, fptr(out), out.size))
+        return out
+
+    @property
+    def diagnostics(self) -> dict:
+        d = _lib.Diag()
+        self.ctx.check(self.ctx.lib.dspbr_get_diagnostics(self.ctx.h, C.byref(d)))
+        out = d.as_dict()
+        out["display"] = dict(self._display)
+        return out
+
+    def _emit_diag(self):
+        if self._listeners["diagnosticsChanged"]:
+            self._emit("diagnosticsChanged", {"diagnostics": self.diagnostics})
+
+    def dispose(self) -> None:
+        self.stop()
+        for o in (self._scene, self._ibl):
+            if o is not None:
+                o.close()
+        self._scene = self._ibl = None
+        self.ctx.close()
+        for s in self._listeners.values():
+            s.clear()
+
+
+def createPathtracingViewport(**kw) -> PathtracingViewport:
+    return PathtracingViewport(**kw)

@@ -1,0 +1,188 @@
+/*
+ * dspbr.h — C ABI of the B200 path-tracing library (libdspbr_cuda.so).
+ *
+ * Drop-in boundary for the hot path of dspbr-pt's PathtracingViewport /
+ * PathtracingRenderer (packages/lib/pathtracing_viewport.ts:100-342,
+ * packages/lib/renderer.ts:116-1109).  Each entry point names the reference
+ * interface it replaces.  Conventions:
+ *   - every call returns an int status: DSPBR_OK (0) or a negative DSPBR_ERR_*;
+ *     dspbr_last_error() gives the message of the last failure on a context;
+ *   - handles are opaque; all host buffers passed in are copied (the caller
+ *     keeps ownership, like the reference's typed arrays -> GL textures);
+ *   - one context per host thread (a context is not internally locked);
+ *   - data formats are the reference's: 20-float vertex records
+ *     (scene_data.ts:21, scene_loader.ts:296-344), uint32 triangle indices,
+ *     68-float material records (material.ts:2-481), the binary BVH node
+ *     layout of bvh.glsl:1-6 (16 floats per node) and RGBA32F environment maps.
+ */
+#ifndef DSPBR_H
+#define DSPBR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DSPBR_OK = 0,
+  DSPBR_ERR_INVALID = -1,     /* bad argument or malformed input data */
+  DSPBR_ERR_CUDA = -2,        /* CUDA runtime error (message in dspbr_last_error) */
+  DSPBR_ERR_OOM = -3,         /* device allocation failed */
+  DSPBR_ERR_STATE = -4,       /* missing scene/IBL/camera, or a render in flight */
+  DSPBR_ERR_ADMISSION = -5,   /* serving: request refused by the HBM budget */
+  DSPBR_ERR_NOT_FOUND = -6,   /* serving: unknown request id */
+  DSPBR_ERR_DEVICE_FAULT = -7 /* a kernel reported a bounded-wait / traversal abort status */
+};
+
+enum { DSPBR_PROFILE_FULL = 0, DSPBR_PROFILE_LEAN = 1 };
+enum { DSPBR_RNG_MWC = 0, DSPBR_RNG_PCG = 1 };
+enum { DSPBR_ENV_ALIAS = 0, DSPBR_ENV_CDF = 1 };
+
+typedef struct dspbr_ctx dspbr_ctx;
+typedef struct dspbr_scene dspbr_scene;
+typedef struct dspbr_ibl dspbr_ibl;
+typedef struct dspbr_bvh dspbr_bvh;
+typedef struct dspbr_server dspbr_server;
+
+/* Renderer settings: the uniform block of renderer.frag:10-31 plus the setters
+ * of renderer.ts:172-306 (defaults in dspbr_params_default). */
+typedef struct dspbr_params {
+  int32_t max_bounces;            /* u_max_bounces, renderer.ts:229 (8) */
+  int32_t use_ibl;                /* u_use_ibl, renderer.ts:238 (1) */
+  float ibl_rotation_deg;         /* iblRotation, renderer.ts:265-271 (0) */
+  int32_t background_from_ibl;    /* showBackground -> u_background_from_ibl (1) */
+  float background_color[4];      /* u_background_color, renderer.ts:282 (0,0,0,1) */
+  float ray_eps;                  /* u_ray_eps, renderer.ts:290 (1e-4) */
+  float clamp_threshold;          /* u_clamp_threshold, renderer.ts:299 (3.0) */
+  float point_light_position[4];  /* u_point_light_position, w>0.5 enables (renderer.ts:422-424) */
+  float point_light_emission[4];  /* u_point_light_emission */
+  int32_t rr_start_depth;         /* RR_START_DEPTH, constants.glsl:19 (2) */
+  float rr_termination_prob;      /* RR_TERMINATION_PROB, constants.glsl:20 (0.1) */
+  int32_t profile;                /* DSPBR_PROFILE_*: material kernel profile (renderer.ts:154, 1078-1080) */
+  int32_t rng;                    /* DSPBR_RNG_MWC = rng.glsl sequence; DSPBR_RNG_PCG = PCG32 per pixel/sample */
+  uint64_t seed;                  /* PCG seed */
+  int32_t env_sampling;           /* DSPBR_ENV_ALIAS (O(1), same pmf) or DSPBR_ENV_CDF (reference's binary search) */
+  int32_t reserved[7];
+} dspbr_params;
+
+/* PathtracingRendererDiagnostics (renderer.ts:79-110) plus throughput counters. */
+typedef struct dspbr_diag {
+  uint64_t sample_count;          /* frames accumulated since the last reset */
+  int32_t width, height;
+  uint64_t rays_primary, rays_extension, rays_shadow; /* since context creation */
+  uint64_t traversal_aborted;     /* rays that hit MAX_BVH_TRAVERSAL_STEPS (bvh.glsl:9) */
+  uint64_t scene_triangles, bvh_nodes, bvh_indices;
+  uint64_t device_bytes;          /* device memory held by the context's own buffers */
+  double last_render_ms;          /* device time of the last dspbr_render call */
+  double bvh_build_ms, upload_ms; /* set-up profiling, renderer.ts:930-958 */
+  /* with dspbr_set_counting(ctx, 1): traversal work since counting was enabled */
+  uint64_t nodes_closest, tris_closest, nodes_shadow, tris_shadow;
+  /* with dspbr_set_profiling(ctx, 1): device time per kernel kind (CUDA events
+   * on the render stream) and launch counts since profiling was enabled */
+  double extend_ms, connect_ms, shade_ms;
+  uint64_t extend_launches, connect_launches, shade_launches, other_launches;
+} dspbr_diag;
+
+void dspbr_params_default(dspbr_params* p);
+
+/* ---- context: replaces new PathtracingRenderer (renderer.ts:309-325) ----- */
+int dspbr_create(int device, dspbr_ctx** out);
+int dspbr_destroy(dspbr_ctx* ctx);
+int dspbr_last_error(const dspbr_ctx* ctx, char* buf, size_t size);
+int dspbr_device_count(int* count);
+
+/* ---- BVH: replaces the TinyBVH module ABI (tinybvh_builder.ts:7-24) ------ */
+/* _build_bvh_indexed: positions = float records with `vertex_stride_floats`
+ * stride (3 for a packed float3 buffer, 20 for the reference vertex record). */
+int dspbr_bvh_build(const float* positions, uint32_t num_vertices, uint32_t vertex_stride_floats,
+                    const uint32_t* indices, uint32_t num_indices, dspbr_bvh** out);
+/* _get_bvh_node_count / _get_bvh_indices_len / _get_bvh_depth / _get_bvh_triangle_count */
+int dspbr_bvh_info(const dspbr_bvh* bvh, uint32_t* num_nodes, uint32_t* num_indices, uint32_t* depth,
+                   uint32_t* num_triangles);
+/* _get_bvh_nodes_ptr / _get_bvh_indices_ptr: copies 16*num_nodes floats and num_indices ints. */
+int dspbr_bvh_copy(const dspbr_bvh* bvh, float* nodes, int32_t* indices);
+/* _get_last_error_ptr / _get_last_error_len */
+int dspbr_bvh_error(const dspbr_bvh* bvh, char* buf, size_t size);
+void dspbr_bvh_free(dspbr_bvh* bvh);
+
+/* ---- scene: replaces PathtracingSceneDataWebGL2.init + initBvh
+ *      (scene_data_webgl2.ts:74-100, renderer.ts:872-912) ----------------- */
+/* bvh_nodes/bvh_indices may be NULL: the BVH is then built here. */
+int dspbr_scene_create(dspbr_ctx* ctx, const float* vertices, uint32_t num_vertices, const uint32_t* indices,
+                       uint32_t num_indices, const float* materials, uint32_t num_materials,
+                       const float* bvh_nodes, uint32_t num_bvh_nodes, const int32_t* bvh_indices,
+                       uint32_t num_bvh_indices, dspbr_scene** out);
+/* material edits (dirty materials re-uploaded, renderer.ts:440-448) */
+int dspbr_scene_update_materials(dspbr_scene* scene, const float* materials, uint32_t first, uint32_t count);
+int dspbr_scene_device_bytes(const dspbr_scene* scene, uint64_t* bytes);
+int dspbr_scene_destroy(dspbr_scene* scene);
+
+/* ---- IBL: replaces setIBL + precomputeIBLImportanceSamplingData
+ *      (renderer.ts:777-865).  Tables are built on the device: FP64 prefix
+ *      sums stored as float32 (the reference's Float32Array), plus an alias
+ *      table over the same pmf. ------------------------------------------- */
+int dspbr_ibl_create(dspbr_ctx* ctx, const float* rgba32f, int width, int height, dspbr_ibl** out);
+/* copies back pdf (w*h), cdf (w*h), yPdf (h), yCdf (h), totalSum */
+int dspbr_ibl_tables(const dspbr_ibl* ibl, float* pdf, float* cdf, float* ypdf, float* ycdf, double* total_sum);
+/* alias table: prob (w*h float) and alias (w*h int32) */
+int dspbr_ibl_alias_table(const dspbr_ibl* ibl, float* prob, int32_t* alias);
+int dspbr_ibl_destroy(dspbr_ibl* ibl);
+
+/* ---- viewport state (pathtracing_viewport.ts:147-291) -------------------- */
+int dspbr_set_scene(dspbr_ctx* ctx, dspbr_scene* scene);          /* setScene */
+int dspbr_set_ibl(dspbr_ctx* ctx, dspbr_ibl* ibl);                /* setIBL */
+/* setCamera: matrixWorld column-major 16 floats (camera-to-world), vertical fov
+ * in degrees, near plane (renderer.ts:399-404) */
+int dspbr_set_camera(dspbr_ctx* ctx, const float matrix_world[16], float fov_deg, float near_plane);
+int dspbr_set_params(dspbr_ctx* ctx, const dspbr_params* params); /* setSettings */
+int dspbr_get_params(const dspbr_ctx* ctx, dspbr_params* params);
+int dspbr_resize(dspbr_ctx* ctx, int width, int height);          /* resize */
+int dspbr_reset(dspbr_ctx* ctx);                                  /* resetAccumulation */
+/* start(sampleLimit) driven synchronously: renders `frames` progressive frames
+ * (1 sample per pixel each) and returns when they are on the device. */
+int dspbr_render(dspbr_ctx* ctx, int frames);
+/* asynchronous variant: enqueue and return; dspbr_poll reports completion */
+int dspbr_render_async(dspbr_ctx* ctx, int frames);
+int dspbr_poll(dspbr_ctx* ctx, int* done);
+int dspbr_wait(dspbr_ctx* ctx);
+/* readAccumulation (absent in the reference, which only displays): running
+ * mean RGBA32F, width*height*4 floats, row 0 = bottom row (gl_FragCoord.y 0.5). */
+int dspbr_read_accum(dspbr_ctx* ctx, float* rgba, size_t num_floats);
+int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
+/* paths per wave (0 = default 2^21); the wave covers min(frames, paths/pixels)
+ * samples of every pixel.  Set by the autotuner. */
+int dspbr_set_wave_paths(dspbr_ctx* ctx, uint32_t paths);
+/* count BVH node visits and triangle tests of every traced ray (diagnostics) */
+int dspbr_set_counting(dspbr_ctx* ctx, int enable);
+/* time every extend / connect / shade launch with CUDA events (diagnostics) */
+int dspbr_set_profiling(dspbr_ctx* ctx, int enable);
+
+/* ---- kernel-level entry points used by parity tests and embedders -------- */
+/* closest hit (bvh.glsl:149-216): rays n x 8 floats (org.xyz, dir.xyz, tfar, 0);
+ * outputs mesh triangle index (-1 = miss), t, barycentric u,v. */
+int dspbr_trace_closest(dspbr_ctx* ctx, const dspbr_scene* scene, const float* rays, uint32_t n, int32_t* tri,
+                        float* t, float* uv);
+/* isOccluded (bvh.glsl:225-229) with an any-hit traversal: rays n x 8 floats. */
+int dspbr_trace_occluded(dspbr_ctx* ctx, const dspbr_scene* scene, const float* rays, uint32_t n, int32_t* occluded);
+/* BSDF through configure_gltf_material + pbrEval/Pdf/SampleGltfState
+ * (material.glsl:5-110, material_kernel.glsl:4390-4425).  hit: n x 20 floats
+ * (n.xyz, ng.xyz, tangent.xyzw, wi.xyz, uv0.xy, vertex colour rgba, material
+ * index); wo: n x 3; rnd: n x 4 (component, lobe.x, lobe.y, boundary).
+ * eval4: bsdf*cos rgb + pdf; sample10: dir.xyz, pdf, bsdfOverPdf.rgb, specular,
+ * crossedBoundary, nextMediumIor; flags: bit0 = backside. */
+int dspbr_bsdf_query(dspbr_ctx* ctx, const dspbr_scene* scene, uint32_t n, const float* hit, const float* wo,
+                     const float* rnd, float* eval4, float* sample10, int32_t* flags);
+/* IBL (lighting.glsl:24-98): sample (r0,r1) -> dir.xyz + pdf with the
+ * context's env_sampling mode; pdf and radiance at given directions. */
+int dspbr_ibl_query(dspbr_ctx* ctx, const dspbr_ibl* ibl, uint32_t n, const float* r2, const float* dirs,
+                    float* sample_dir_pdf4, float* pdf, float* rgb);
+/* camera rays (renderer.frag:129-142) for pixels xy with jitter r2: n x 6 (org, dir) */
+int dspbr_camera_rays(dspbr_ctx* ctx, uint32_t n, const int32_t* xy, const float* r2, float* rays6);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DSPBR_H */
