@@ -71,3 +71,19 @@ def camera_rays_ref(ref, cam, width, height, n, seed=3):
     xy = np.stack([rng.integers(0, width, n), rng.integers(0, height, n)], 1).astype(np.int32)
     r2 = rng.uniform(size=(n, 2)).astype(np.float32)
     return xy, r2
+
+
+def load_golden():
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_small.npz")
+    return dict(np.load(path))
+
+
+def close_mask(a, b, rtol, atol):
+    """Element-wise |a-b| <= atol + rtol|b|, treating equal infinities and NaN pairs as equal."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    same = (a == b) | (np.isnan(a) & np.isnan(b))
+    with np.errstate(invalid="ignore"):
+        near = np.abs(a - b) <= atol + rtol * np.abs(b)
+    return same | near

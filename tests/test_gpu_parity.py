@@ -1,0 +1,362 @@
+"""GPU parity of the CUDA path (through the C ABI of libdspbr_cuda.so) against
+the reference: golden vectors produced by the reference's own shaders
+(tests/golden), and the CPU oracle (oracle/dspbr_oracle.cpp), which the CPU
+tests pin to the same golden vectors and to the compiled reference."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from dspbr import _lib, synth
+from dspbr.viewport import Bvh, Context, DeviceIbl, DeviceScene, PathtracingCamera, PathtracingViewport
+from oracle import oracle_lib, ref_lib
+from tests import helpers
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances (FP32 on both sides; the GPU contracts multiply-adds into FMA and
+# uses CUDA's libm, the host uses IEEE-separate operations and glibc):
+BSDF_RTOL = 1e-4        # eval / pdf element-wise relative tolerance ...
+BSDF_ATOL = 1e-6        # ... plus this absolute floor
+BSDF_MIN_FRACTION = 0.999   # fraction of queries whose 4 outputs all agree
+SAMPLE_MIN_FRACTION = 0.995  # lobe/branch choices may flip at FP32 thresholds
+
+
+@pytest.fixture(scope="module")
+def g():
+    return helpers.load_golden()
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return Context(0)
+
+
+@pytest.fixture(scope="module")
+def gscene(ctx, g):
+    bvh = Bvh(g["bvh_nodes"], g["bvh_indices"], 0, g["indices"].size // 3)
+    return DeviceScene(ctx, g["vertices"], g["indices"], g["materials"], bvh)
+
+
+def trace_gpu(ctx, ds, rays, any_hit=False):
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[0]
+    if any_hit:
+        occ = np.zeros(n, np.int32)
+        ctx.check(ctx.lib.dspbr_trace_occluded(ctx.h, ds.h, _lib.fptr(rays), n, _lib.iptr(occ)))
+        return occ
+    tri, t, uv = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros((n, 2), np.float32)
+    ctx.check(ctx.lib.dspbr_trace_closest(ctx.h, ds.h, _lib.fptr(rays), n, _lib.iptr(tri), _lib.fptr(t),
+                                          _lib.fptr(uv)))
+    return tri, t, uv
+
+
+def bsdf_gpu(ctx, ds, hit, wo, rnd):
+    n = hit.shape[0]
+    ev, sm, fl = np.zeros((n, 4), np.float32), np.zeros((n, 10), np.float32), np.zeros(n, np.int32)
+    ctx.check(ctx.lib.dspbr_bsdf_query(ctx.h, ds.h, n, _lib.fptr(hit), _lib.fptr(wo), _lib.fptr(rnd),
+                                       _lib.fptr(ev), _lib.fptr(sm), _lib.iptr(fl)))
+    return ev, sm, fl
+
+
+# ---- traversal: bit-exact ------------------------------------------------------------
+def test_closest_hit_bitexact_golden(ctx, g, gscene):
+    tri, t, uv = trace_gpu(ctx, gscene, g["rays"])
+    np.testing.assert_array_equal(tri, g["hit_tri"])
+    np.testing.assert_array_equal(t.view(np.uint32), g["hit_t"].view(np.uint32))
+    np.testing.assert_array_equal(uv.view(np.uint32), g["hit_uv"].view(np.uint32))
+    np.testing.assert_array_equal(trace_gpu(ctx, gscene, g["rays"], True), g["occluded"])
+
+
+@pytest.mark.parametrize("ntris", [200_000, 1_000_000])
+def test_closest_hit_bitexact_large_scene(ctx, ntris):
+    sc = synth.make_sized(17, ntris, env_size=(16, 8))
+    bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    ds = DeviceScene(ctx, sc.vertices, sc.indices, sc.materials, bvh)
+    o = oracle_lib.Oracle()
+    o.set_scene(sc.vertices, sc.indices, sc.materials, bvh.nodes, bvh.indices)
+    rays = helpers.random_rays(sc.vertices, 50_000, seed=21)
+    # rays from the camera too (coherent, long)
+    p = oracle_lib.make_params(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, 640, 360)
+    xy, r2 = helpers.camera_rays_ref(None, None, 640, 360, 50_000, seed=22)
+    cam = o.camera_rays(p, xy, r2)
+    crays = np.zeros((cam.shape[0], 8), np.float32)
+    crays[:, :6], crays[:, 6] = cam, 1e5
+    rays = np.concatenate([rays, crays])
+    tri, t, uv = trace_gpu(ctx, ds, rays)
+    otri, ot, ouv, _ = o.trace(rays)
+    assert (tri >= 0).mean() > 0.1
+    np.testing.assert_array_equal(tri, otri)
+    np.testing.assert_array_equal(t.view(np.uint32), ot.view(np.uint32))
+    np.testing.assert_array_equal(uv.view(np.uint32), ouv.view(np.uint32))
+    occ = trace_gpu(ctx, ds, rays, True)
+    np.testing.assert_array_equal(occ, (o.trace(rays, mode=2)[0] >= 0).astype(np.int32))
+
+
+def test_empty_and_degenerate_rays(ctx, gscene, g):
+    rays = np.zeros((6, 8), np.float32)
+    rays[:, 6] = 1e5
+    rays[0, 3:6] = [0, 0, 0]            # zero direction: NaN slabs, no hit
+    rays[1, 3:6] = [1, 0, 0]; rays[1, 6] = 0.0   # tfar 0
+    rays[2, 3:6] = [0, 1, 0]; rays[2, 0:3] = [1e30, 1e30, 1e30]
+    rays[3, 3:6] = [0, 0, 1]; rays[3, 0:3] = [np.nan, 0, 0]
+    rays[4, 3:6] = [0, -1, 0]; rays[4, 0:3] = [0.6, 1.5, -0.6]  # straight down onto the floor
+    rays[5, 3:6] = [1e-30, 1, 0]
+    tri, t, uv = trace_gpu(ctx, gscene, rays)
+    o = oracle_lib.Oracle()
+    o.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    otri, ot, _, _ = o.trace(rays)
+    np.testing.assert_array_equal(tri, otri)
+    assert tri[0] == -1 and tri[1] == -1 and tri[4] >= 0
+    # zero rays is a valid call
+    z = np.zeros((0, 8), np.float32)
+    trace_gpu(ctx, gscene, np.zeros((1, 8), np.float32))
+    assert z.shape[0] == 0
+
+
+def test_camera_rays_bitexact_golden(g):
+    fov, near, W, H = g["cam_fov_near_wh"]
+    v = PathtracingViewport(width=int(W), height=int(H))
+    v.setCamera(PathtracingCamera(g["cam_matrix"], float(fov), float(near)))
+    xy, r2 = g["cam_xy"], g["cam_r2"]
+    out = np.zeros((xy.shape[0], 6), np.float32)
+    v.ctx.check(v.ctx.lib.dspbr_camera_rays(v.ctx.h, xy.shape[0], _lib.iptr(xy), _lib.fptr(r2), _lib.fptr(out)))
+    np.testing.assert_array_equal(out.view(np.uint32), g["cam_rays"].view(np.uint32))
+    v.dispose()
+
+
+# ---- DSPBR material -------------------------------------------------------------------
+def _bsdf_agreement(ev, sm, rev, rsm):
+    ok_e = helpers.close_mask(ev, rev, BSDF_RTOL, BSDF_ATOL).all(axis=1)
+    same_dir = helpers.close_mask(sm[:, :3], rsm[:, :3], 1e-3, 1e-4).all(axis=1)
+    ok_s = same_dir & helpers.close_mask(sm, rsm, 1e-3, 1e-5).all(axis=1)
+    return ok_e.mean(), same_dir.mean(), ok_s.mean()
+
+
+def test_bsdf_matches_reference_golden(ctx, gscene, g):
+    ev, sm, fl = bsdf_gpu(ctx, gscene, g["bsdf_hit"], g["bsdf_wo"], g["bsdf_rnd"])
+    np.testing.assert_array_equal(fl, g["bsdf_flags"])
+    fe, fd, fs = _bsdf_agreement(ev, sm, g["bsdf_eval32"], g["bsdf_sample32"])
+    print(f"golden: eval/pdf {fe:.5f}  sample dir {fd:.5f}  sample all {fs:.5f}")
+    assert fe >= BSDF_MIN_FRACTION and fd >= SAMPLE_MIN_FRACTION and fs >= SAMPLE_MIN_FRACTION
+
+
+@pytest.mark.parametrize("lean", [0, 1])
+def test_bsdf_matches_oracle_many(ctx, gscene, g, lean):
+    hit, wo, rnd = helpers.bsdf_queries(100_000, g["materials"].shape[0], seed=31 + lean)
+    if lean:
+        p = _lib.default_params()
+        p.profile = _lib.PROFILE_LEAN
+        ctx.check(ctx.lib.dspbr_set_params(ctx.h, p))
+    try:
+        ev, sm, fl = bsdf_gpu(ctx, gscene, hit, wo, rnd)
+    finally:
+        ctx.check(ctx.lib.dspbr_set_params(ctx.h, _lib.default_params()))
+    o = oracle_lib.Oracle()
+    o.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    rev, rsm, rfl = o.bsdf(hit, wo, rnd, "f32", lean)
+    np.testing.assert_array_equal(fl, rfl)
+    fe, fd, fs = _bsdf_agreement(ev, sm, rev, rsm)
+    print(f"lean={lean}: eval/pdf {fe:.5f}  sample dir {fd:.5f}  sample all {fs:.5f}")
+    assert fe >= BSDF_MIN_FRACTION and fd >= SAMPLE_MIN_FRACTION and fs >= SAMPLE_MIN_FRACTION
+
+
+def test_bsdf_relative_error_vs_fp64(ctx, gscene, g):
+    """GPU FP32 against the FP64 port of the reference material model: the
+    fraction of eval/pdf values within 1e-5 relative must be as high as the
+    reference's own FP32 arithmetic achieves (the FP32 shader is itself not
+    within 1e-5 of FP64 everywhere: cancellations, thin-film phases)."""
+    hit, wo, rnd = helpers.bsdf_queries(50_000, g["materials"].shape[0], seed=41)
+    ev, _, _ = bsdf_gpu(ctx, gscene, hit, wo, rnd)
+    o = oracle_lib.Oracle()
+    o.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    r64, _, _ = o.bsdf(hit, wo, rnd, "f64")
+    r32, _, _ = o.bsdf(hit, wo, rnd, "f32")
+    gpu = helpers.close_mask(ev, r64, 1e-5, 1e-7).mean()
+    cpu = helpers.close_mask(r32, r64, 1e-5, 1e-7).mean()
+    print(f"within 1e-5 rel of FP64: GPU {gpu:.5f}, reference FP32 arithmetic {cpu:.5f}")
+    assert gpu >= cpu - 0.002
+    assert helpers.close_mask(ev, r64, 1e-3, 1e-6).mean() > 0.999
+
+
+# ---- IBL --------------------------------------------------------------------------------
+def test_ibl_tables_bitexact_golden(ctx, g):
+    ibl = DeviceIbl(ctx, g["env"])
+    t = ibl.tables()
+    for k in ("pdf", "cdf", "yPdf", "yCdf"):
+        np.testing.assert_array_equal(t[k].view(np.uint32), g["ibl_" + k].view(np.uint32), err_msg=k)
+    assert t["totalSum"] == g["ibl_totalSum"][0]
+    prob, alias = ibl.alias_table()
+    n = prob.size
+    mass = prob.astype(np.float64) / n
+    np.add.at(mass, alias, (1.0 - prob.astype(np.float64)) / n)
+    h = t["yPdf"].size
+    target = (t["yPdf"][:, None].astype(np.float64) * t["pdf"].reshape(h, -1)).reshape(-1)
+    target /= target.sum()
+    assert np.abs(mass - target).max() < 1e-6
+
+
+def test_ibl_tables_large_env_bitexact(ctx):
+    env = synth.env_lognormal(2048, 1024, np.random.default_rng(3))
+    t = DeviceIbl(ctx, env).tables()
+    o = oracle_lib.Oracle()
+    o.set_ibl(env)
+    ot = o.ibl_tables()
+    for k in ("pdf", "cdf", "yPdf", "yCdf"):
+        np.testing.assert_array_equal(t[k].view(np.uint32), ot[k].view(np.uint32), err_msg=k)
+    assert t["totalSum"] == ot["totalSum"]
+
+
+def _ibl_query(ctx, ibl, r2, dirs, mode):
+    p = _lib.default_params()
+    p.env_sampling = mode
+    ctx.check(ctx.lib.dspbr_set_params(ctx.h, p))
+    n = r2.shape[0]
+    sdp, pdf, rgb = np.zeros((n, 4), np.float32), np.zeros(n, np.float32), np.zeros((n, 3), np.float32)
+    ctx.check(ctx.lib.dspbr_ibl_query(ctx.h, ibl.h, n, _lib.fptr(r2), _lib.fptr(dirs), _lib.fptr(sdp),
+                                      _lib.fptr(pdf), _lib.fptr(rgb)))
+    ctx.check(ctx.lib.dspbr_set_params(ctx.h, _lib.default_params()))
+    return sdp, pdf, rgb
+
+
+def test_ibl_queries_golden(ctx, g):
+    ibl = DeviceIbl(ctx, g["env"])
+    sdp, pdf, rgb = _ibl_query(ctx, ibl, g["ibl_r2"], g["ibl_dirs"], _lib.ENV_CDF)
+    np.testing.assert_allclose(sdp, g["ibl_sample"], rtol=2e-5, atol=2e-6)
+    np.testing.assert_allclose(pdf, g["ibl_pdf_at"], rtol=2e-5, atol=1e-7)
+    np.testing.assert_allclose(rgb, g["ibl_rgb_at"], rtol=2e-5, atol=2e-6)
+
+
+def test_alias_sampling_distribution(ctx, g):
+    """The alias sampler draws pixels with the reference pmf: chi-square over
+    the 64x32 pixels, and every returned pdf equals the reference's ibl_pdf
+    formula for the returned pixel."""
+    ibl = DeviceIbl(ctx, g["env"])
+    rng = np.random.default_rng(5)
+    n = 400_000
+    r2 = rng.uniform(size=(n, 2)).astype(np.float32)
+    dirs = np.zeros((n, 3), np.float32)
+    sdp, _, _ = _ibl_query(ctx, ibl, r2, dirs, _lib.ENV_ALIAS)
+    w, h = g["env"].shape[1], g["env"].shape[0]
+    d = sdp[:, :3].astype(np.float64)
+    theta = np.arccos(np.clip(d[:, 1], -1, 1))
+    phi = np.mod(np.arctan2(d[:, 2], d[:, 0]), 2 * np.pi)
+    y = np.clip(np.rint(theta / np.pi * h).astype(int), 0, h - 1)
+    x = np.clip(np.rint(phi / (2 * np.pi) * w).astype(int) % w, 0, w - 1)
+    counts = np.bincount(y * w + x, minlength=w * h).astype(np.float64)
+    pmf = (g["ibl_yPdf"][:, None].astype(np.float64) * g["ibl_pdf"].reshape(h, w)).reshape(-1)
+    pmf /= pmf.sum()
+    expected = pmf * n
+    m = expected > 20
+    chi2 = ((counts[m] - expected[m]) ** 2 / expected[m]).sum()
+    dof = m.sum() - 1
+    assert chi2 < dof + 6 * np.sqrt(2 * dof), (chi2, dof)
+    assert counts[~m].sum() <= expected[~m].sum() * 2 + 50
+
+
+# ---- whole frames ---------------------------------------------------------------------------
+def _viewport(sc, W, H, settings):
+    v = PathtracingViewport(width=W, height=H, settings=settings)
+    v.setScene(sc)
+    v.setIBL(sc.env)
+    v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
+    return v
+
+
+def test_image_matches_golden_path_for_path(g):
+    sc = synth.Scene("golden", g["vertices"], g["indices"], g["image_scene_materials"],
+                     synth.Camera(g["cam_matrix"], float(g["cam_fov_near_wh"][0]), float(g["cam_fov_near_wh"][1])),
+                     env=g["image_env"])
+    sc.bvh = Bvh(g["bvh_nodes"], g["bvh_indices"], 0, 0)
+    W, H, F = (int(x) for x in g["image_whf"])
+    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf"})
+    v.start(F)
+    img = v.readAccumulation()
+    v.dispose()
+    close = helpers.close_mask(img[..., :3], g["image"][..., :3], 1e-3, 1e-4).all(-1)
+    print("pixels equal to the reference path for path:", close.mean())
+    assert close.mean() > 0.95
+    assert np.abs(img - g["image"]).mean() < 0.01 * g["image"][..., :3].mean()
+
+
+def test_image_mwc_matches_oracle_per_pixel():
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    W, H, F = 128, 128, 8
+    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf"})
+    v.start(F)
+    img = v.readAccumulation()
+    d = v.diagnostics
+    v.dispose()
+    assert d["sample_count"] == F and d["rays_primary"] == W * H * F and d["traversal_aborted"] == 0
+    o = oracle_lib.Oracle()
+    o.set_scene(sc.vertices, sc.indices, sc.materials, sc.bvh.nodes, sc.bvh.indices)
+    o.set_ibl(sc.env)
+    p = oracle_lib.make_params(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, W, H, max_bounces=8)
+    ref = o.render_image(p, F)
+    close = helpers.close_mask(img[..., :3], ref[..., :3], 1e-3, 1e-4).all(-1)
+    print("pixels equal path for path:", close.mean())
+    assert close.mean() > 0.95
+
+
+def test_converged_image_statistics_pcg_alias_vs_oracle():
+    """PCG streams + alias-table NEE against the oracle's reference RNG + CDF
+    sampler: different sample streams, same estimator; per-pixel z-test on
+    8x8 tiles and RMSE bound."""
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    W, H, F = 64, 64, 256
+    v = _viewport(sc, W, H, {"maxBounces": 8, "rng": "pcg", "seed": 7, "envSampling": "alias"})
+    v.start(F)
+    img = v.readAccumulation()[..., :3].astype(np.float64)
+    v.dispose()
+    o = oracle_lib.Oracle()
+    o.set_scene(sc.vertices, sc.indices, sc.materials, sc.bvh.nodes, sc.bvh.indices)
+    o.set_ibl(sc.env)
+    p = oracle_lib.make_params(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, W, H, max_bounces=8)
+    xy = oracle_lib.all_pixels(W, H)
+    s1 = np.zeros((H * W, 3))
+    s2 = np.zeros((H * W, 3))
+    for f in range(1, F + 1):
+        out, _ = o.render(p, xy, f)
+        s1 += out[:, :3]
+        s2 += out[:, :3].astype(np.float64) ** 2
+    mean = (s1 / F).reshape(H, W, 3)
+    var = (s2 / F - (s1 / F) ** 2).reshape(H, W, 3)
+    # tiles of 8x8 pixels: mean difference against the combined standard error
+    t = lambda a: a.reshape(H // 8, 8, W // 8, 8, 3).mean(axis=(1, 3))
+    se = np.sqrt(2 * t(var) / (64 * F)) + 1e-6
+    z = (t(img) - t(mean)) / se
+    print("tile z max", np.abs(z).max(), "rmse", np.sqrt(((img - mean) ** 2).mean()))
+    assert (np.abs(z) < 4.5).mean() > 0.99
+    assert np.sqrt(((img - mean) ** 2).mean()) < 0.05
+
+
+def test_progressive_accumulation_and_reset():
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    v = _viewport(sc, 48, 32, {"maxBounces": 4})
+    v.start(3)
+    a = v.readAccumulation()
+    v.start(5)  # continues to 5 samples
+    assert v.diagnostics["sample_count"] == 5
+    b = v.readAccumulation()
+    v.resetAccumulation()
+    assert v.diagnostics["sample_count"] == 0
+    v.start(3)
+    c = v.readAccumulation()
+    np.testing.assert_array_equal(a, c)  # same frames, same samples
+    assert not np.array_equal(a, b)
+    v.dispose()
+
+
+def test_reference_shader_direct_when_available(ctx, g, gscene):
+    if not ref_lib.available("f32"):
+        pytest.skip("oracle/_ref not built here")
+    ref = ref_lib.GlslReference("f32")
+    ref.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    rays = helpers.random_rays(g["vertices"], 20000, seed=51)
+    tri, t, uv = trace_gpu(ctx, gscene, rays)
+    rtri, rt, ruv = ref.trace(rays)
+    np.testing.assert_array_equal(tri, rtri)
+    np.testing.assert_array_equal(t.view(np.uint32), rt.view(np.uint32))

@@ -1,0 +1,101 @@
+"""The CPU oracle (oracle/dspbr_oracle.cpp) against golden vectors produced by
+the reference's own shaders (tests/golden/make_golden.py).  CPU only."""
+import numpy as np
+import pytest
+
+from oracle import oracle_lib
+from tests import helpers
+
+
+@pytest.fixture(scope="module")
+def g():
+    return helpers.load_golden()
+
+
+@pytest.fixture(scope="module")
+def orc(g):
+    o = oracle_lib.Oracle()
+    o.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    o.set_ibl(g["env"])
+    return o
+
+
+def test_closest_hit_bitexact(g, orc):
+    tri, t, uv, cnt = orc.trace(g["rays"])
+    np.testing.assert_array_equal(tri, g["hit_tri"])
+    np.testing.assert_array_equal(t.view(np.uint32), g["hit_t"].view(np.uint32))
+    np.testing.assert_array_equal(uv.view(np.uint32), g["hit_uv"].view(np.uint32))
+    assert cnt["rays"] == g["rays"].shape[0] and cnt["aborted"] == 0
+
+
+def test_occlusion_matches(g, orc):
+    occ = orc.trace(g["rays"], mode=2)[0] >= 0
+    np.testing.assert_array_equal(occ.astype(np.int32), g["occluded"])
+
+
+def test_brute_force_agrees_except_ties(g, orc):
+    """app/index.ts:561-596 style all-triangle search: same triangle unless two
+    triangles are hit at t within 1e-6 (documented t-ties)."""
+    bvh_tri = g["hit_tri"]
+    bf_tri, bf_t, _, _ = orc.trace(g["rays"], mode=1)
+    diff = bf_tri != bvh_tri
+    assert diff.mean() < 0.01
+    np.testing.assert_allclose(bf_t[diff], g["hit_t"][diff], rtol=1e-6)
+    np.testing.assert_array_equal(bf_t[~diff].view(np.uint32), g["hit_t"][~diff].view(np.uint32))
+
+
+def test_camera_rays_bitexact(g, orc):
+    fov, near, W, H = g["cam_fov_near_wh"]
+    p = oracle_lib.make_params(g["cam_matrix"], fov, near, int(W), int(H))
+    out = orc.camera_rays(p, g["cam_xy"], g["cam_r2"])
+    np.testing.assert_array_equal(out.view(np.uint32), g["cam_rays"].view(np.uint32))
+
+
+def test_rng_bitexact(g, orc):
+    for (x, y, s), ref in zip(g["rng_args"], g["rng_out"]):
+        np.testing.assert_array_equal(orc.rng(32, int(x), int(y), int(s)), ref)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_bsdf_matches_reference(g, orc, precision):
+    ev, sm, fl = orc.bsdf(g["bsdf_hit"], g["bsdf_wo"], g["bsdf_rnd"], precision)
+    np.testing.assert_array_equal(fl, g["bsdf_flags"])
+    # same arithmetic as the reference in both precisions: agreement to the last bits
+    assert helpers.close_mask(ev, g["bsdf_eval" + precision[1:]], 1e-6, 1e-12).all()
+    assert helpers.close_mask(sm, g["bsdf_sample" + precision[1:]], 1e-6, 1e-9).all()
+
+
+def test_ibl_tables_bitexact(g, orc):
+    t = orc.ibl_tables()
+    for k in ("pdf", "cdf", "yPdf", "yCdf"):
+        np.testing.assert_array_equal(t[k].view(np.uint32), g["ibl_" + k].view(np.uint32), err_msg=k)
+    assert t["totalSum"] == g["ibl_totalSum"][0]
+
+
+def test_ibl_queries(g, orc):
+    s, p, c = orc.ibl(g["ibl_r2"], g["ibl_dirs"], 0.0, mode=1)
+    np.testing.assert_array_equal(s, g["ibl_sample"])
+    np.testing.assert_array_equal(p, g["ibl_pdf_at"])
+    np.testing.assert_array_equal(c, g["ibl_rgb_at"])
+
+
+def test_alias_table_realises_reference_pmf(orc):
+    t = orc.ibl_tables()
+    n = t["aliasProb"].size
+    mass = t["aliasProb"].astype(np.float64) / n
+    np.add.at(mass, t["alias"], (1.0 - t["aliasProb"].astype(np.float64)) / n)
+    h = t["yPdf"].size
+    target = (t["yPdf"][:, None].astype(np.float64) * t["pdf"].reshape(h, -1)).reshape(-1)
+    target /= target.sum()
+    assert np.abs(mass - target).max() < 1e-6
+
+
+def test_small_image_matches_reference(g):
+    o = oracle_lib.Oracle()
+    o.set_scene(g["vertices"], g["indices"], g["image_scene_materials"], g["bvh_nodes"], g["bvh_indices"])
+    o.set_ibl(g["image_env"])
+    W, H, F = (int(x) for x in g["image_whf"])
+    fov, near, _, _ = g["cam_fov_near_wh"]
+    p = oracle_lib.make_params(g["cam_matrix"], fov, near, W, H, max_bounces=8)
+    img = o.render_image(p, F)
+    assert helpers.close_mask(img, g["image"], 1e-5, 1e-6).mean() > 0.999
