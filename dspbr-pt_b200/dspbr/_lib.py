@@ -82,6 +82,8 @@ SIGNATURES = {
     "dspbr_ibl_tables": (C.c_int, [_V, _F, _F, _F, _F, _D]),
     "dspbr_ibl_alias_table": (C.c_int, [_V, _F, _I]),
     "dspbr_ibl_destroy": (C.c_int, [_V]),
+    "dspbr_ibl_tables_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "dspbr_set_scene": (C.c_int, [_V, _V]),
     "dspbr_set_ibl": (C.c_int, [_V, _V]),
     "dspbr_set_camera": (C.c_int, [_V, _F, C.c_float, C.c_float]),

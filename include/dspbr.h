@@ -129,6 +129,21 @@ int dspbr_ibl_tables(const dspbr_ibl* ibl, float* pdf, float* cdf, float* ypdf, 
 /* alias table: prob (w*h float) and alias (w*h int32) */
 int dspbr_ibl_alias_table(const dspbr_ibl* ibl, float* prob, int32_t* alias);
 int dspbr_ibl_destroy(dspbr_ibl* ibl);
+/* Allocation-free table build.  No counterpart in the reference: it exists for
+ * hosts that cannot let a library call cudaMalloc (an engine that owns all
+ * device memory through its own pool, or a frame loop that must not take the
+ * implicit device synchronisation of cudaMalloc / cudaFree).  It writes the
+ * same pdf, cdf, yPdf, yCdf and totalSum as dspbr_ibl_create into buffers the
+ * caller allocated: every pointer is device memory of the current device
+ * (rgba32f w*h*4 floats, pdf and cdf w*h floats, ypdf and ycdf h floats, one
+ * double), and the work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * default stream) without synchronising.  Scratch is a fixed 64 KiB device
+ * array inside the library, so height is limited to 16384 rows; larger maps
+ * are refused with DSPBR_ERR_INVALID.  The first call on a device looks up that
+ * array's address, so make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race on it. */
+int dspbr_ibl_tables_noalloc(const float* rgba32f, int width, int height, float* pdf, float* cdf, float* ypdf,
+                             float* ycdf, double* total_sum, void* stream);
 
 /* ---- viewport state (pathtracing_viewport.ts:147-291) -------------------- */
 int dspbr_set_scene(dspbr_ctx* ctx, dspbr_scene* scene);          /* setScene */
