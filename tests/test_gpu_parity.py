@@ -85,7 +85,7 @@ def test_closest_hit_bitexact_large_scene(ctx, ntris):
     rays = np.concatenate([rays, crays])
     tri, t, uv = trace_gpu(ctx, ds, rays)
     otri, ot, ouv, _ = o.trace(rays)
-    assert (tri >= 0).mean() > 0.1
+    assert (tri >= 0).sum() > 2000  # sparse scenes: most random rays leave the scene
     np.testing.assert_array_equal(tri, otri)
     np.testing.assert_array_equal(t.view(np.uint32), ot.view(np.uint32))
     np.testing.assert_array_equal(uv.view(np.uint32), ouv.view(np.uint32))
