@@ -219,8 +219,9 @@ def run_gpu_arm(args):
     lib, h = v.ctx.lib, v.ctx.h
     # warm-up frames (untimed)
     v.ctx.check(lib.dspbr_render(h, args.warmup))
-    # ---- device-timed region: K frames, events on the render stream ----
-    v.ctx.check(lib.dspbr_set_profiling(h, 1))
+    # ---- device-timed region: K frames in one render call, events on the
+    #      render stream (no per-launch profiling inside it) ----
+    v.ctx.check(lib.dspbr_set_profiling(h, 0))  # also zeroes the launch counters
     d0 = v.diagnostics
     barrier(dist)
     with ClockSampler(local) as clocks:
@@ -230,22 +231,27 @@ def run_gpu_arm(args):
     dev_ms = d1["last_render_ms"]
     rays = (d1["rays_primary"] + d1["rays_extension"] + d1["rays_shadow"]) - \
            (d0["rays_primary"] + d0["rays_extension"] + d0["rays_shadow"])
-    v.ctx.check(lib.dspbr_set_profiling(h, 0))
     t_max = reduce_max(dist, dev_ms)
     rays_all = reduce_sum(dist, float(rays))
     value = rays_all / (t_max * 1e-3) / 1e6
-    extend_ms, extend_launches = d1["extend_ms"], d1["extend_launches"]
     gpu_launches = int(d1["extend_launches"] + d1["connect_launches"] + d1["shade_launches"] + d1["other_launches"])
+
+    # ---- per-kernel device time of the same K frames (untimed, events around
+    #      every launch), for the roofline of k_extend ----
+    v.ctx.check(lib.dspbr_set_profiling(h, 1))
+    v.ctx.check(lib.dspbr_render(h, args.steps))
+    dp = v.diagnostics
+    v.ctx.check(lib.dspbr_set_profiling(h, 0))
+    extend_ms = dp["extend_ms"]
 
     # ---- traversal work of one more frame (untimed), for the roofline ----
     v.ctx.check(lib.dspbr_set_counting(h, 1))
-    v.ctx.check(lib.dspbr_set_profiling(h, 1))
+    d1c = v.diagnostics
     v.ctx.check(lib.dspbr_render(h, 1))
     d2 = v.diagnostics
     v.ctx.check(lib.dspbr_set_counting(h, 0))
-    v.ctx.check(lib.dspbr_set_profiling(h, 0))
     alg_bytes_frame = 64.0 * d2["nodes_closest"] + 40.0 * d2["tris_closest"]
-    rays_closest_frame = (d2["rays_primary"] + d2["rays_extension"]) - (d1["rays_primary"] + d1["rays_extension"])
+    rays_closest_frame = (d2["rays_primary"] + d2["rays_extension"]) - (d1c["rays_primary"] + d1c["rays_extension"])
     peak, peak_kind = peaks()
     ext_ms_frame = extend_ms / max(1, args.steps)
     achieved = alg_bytes_frame / (ext_ms_frame * 1e-3) / 1e9 if ext_ms_frame > 0 else None
@@ -293,8 +299,9 @@ def run_gpu_arm(args):
                          "nodes_per_ray": d2["nodes_closest"] / max(1, rays_closest_frame),
                          "tris_per_ray": d2["tris_closest"] / max(1, rays_closest_frame),
                          "extend_ms_per_frame": ext_ms_frame,
-                         "connect_ms_per_frame": d1["connect_ms"] / max(1, args.steps),
-                         "shade_ms_per_frame": d1["shade_ms"] / max(1, args.steps)},
+                         "connect_ms_per_frame": dp["connect_ms"] / max(1, args.steps),
+                         "shade_ms_per_frame": dp["shade_ms"] / max(1, args.steps),
+                         "iterations": int(d1["extend_launches"])},
             "cpu_baseline": cpu,
             "clocks": cs,
             "rays_per_step": rays / max(1, args.steps),

@@ -8,7 +8,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dspbr.h"
@@ -75,12 +77,14 @@ struct dspbr_scene {
   DevBuf<float4> nodes, tris, verts, materials;
   DevBuf<uint32_t> indices;
   uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
+  bool boxes_finite = true;
   double bvh_build_ms = 0, upload_ms = 0;
   DevScene view() const {
     DevScene s;
     s.nodes = nodes.p; s.tris = tris.p; s.verts = verts.p; s.indices = indices.p; s.materials = materials.p;
     s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
     s.num_materials = int(num_materials);
+    s.boxes_finite = boxes_finite ? 1 : 0;
     return s;
   }
   uint64_t bytes() const { return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes(); }
@@ -115,13 +119,22 @@ struct dspbr_ctx {
   dspbr_scene* scene = nullptr;
   dspbr_ibl* ibl = nullptr;
   uint32_t wave_paths = 1u << 21;
-  // path state
+  // path pool
   uint32_t capacity = 0;
-  DevBuf<float4> org, dir, weight, rad, hit, sh_dir, sh_c, pl_dir, pl_c, result;
+  DevBuf<float4> org, dir, weight, rad, hit, sh_dir, sh_c, pl_dir, pl_c;
   DevBuf<uint64_t> rng;
-  DevBuf<int> sh_flags;
-  DevBuf<uint32_t> q0, q1, qs, counts;
-  DevBuf<unsigned long long> stats;
+  DevBuf<int> sh_flags, bounce;
+  DevBuf<uint32_t> pixel, frame, q0, q1, qs0, qs1, qh, qm, qfree, counts;
+  DevBuf<unsigned long long> stats, items_next;
+  // live-path counts copied back after each iteration, read kLookahead
+  // iterations later to end the host loop
+  static constexpr int kRing = 8, kLookahead = 4;
+  uint32_t* ring = nullptr;  // pinned
+  cudaEvent_t ring_ev[kRing] = {};
+  // render_async: the iteration loop runs on a worker thread
+  std::thread worker;
+  std::atomic<bool> worker_done{true};
+  int worker_rc = 0;
   DevBuf<double4> accum;
   DevBuf<float4> mean;
   uint64_t sample_count = 0;
@@ -155,6 +168,7 @@ struct dspbr_ctx {
   }
   void resolve_marks() {
     for (auto& m : ev_marks) {
+      if (size_t(m.second) + 1 >= ev_used) break;
       float ms = 0;
       cudaEventElapsedTime(&ms, ev_pool[m.second], ev_pool[m.second + 1]);
       kind_ms[m.first] += ms;
@@ -166,6 +180,16 @@ struct dspbr_ctx {
     for (auto e : ev_pool) cudaEventDestroy(e);
   }
 };
+
+// Joins the worker of a render_async call, so that the caller's next stream
+// operation is ordered after all of that render's launches.  Returns the
+// worker's status.
+static int settle(dspbr_ctx* c) {
+  if (c->worker.joinable()) c->worker.join();
+  int rc = c->worker_rc;
+  c->worker_rc = 0;
+  return rc;
+}
 
 extern "C" {
 
@@ -211,10 +235,19 @@ int dspbr_create(int device, dspbr_ctx** out) {
   Status s = c->st();
   if (s.cuda(cudaSetDevice(device), "cudaSetDevice") || s.cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
       s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event") ||
-      s.cuda(c->counts.alloc(4), "counters") || s.cuda(c->stats.alloc(8), "stats") ||
-      s.cuda(cudaMemset(c->stats.p, 0, c->stats.bytes()), "stats")) {
-    delete c;
+      s.cuda(c->counts.alloc(kCntNum), "counters") || s.cuda(c->stats.alloc(8), "stats") ||
+      s.cuda(c->items_next.alloc(1), "counters") ||
+      s.cuda(cudaMemset(c->stats.p, 0, c->stats.bytes()), "stats") ||
+      s.cuda(cudaHostAlloc(reinterpret_cast<void**>(&c->ring), dspbr_ctx::kRing * sizeof(uint32_t), cudaHostAllocDefault),
+             "pinned status")) {
+    dspbr_destroy(c);
     return DSPBR_ERR_CUDA;
+  }
+  for (auto& e : c->ring_ev) {
+    if (s.cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) {
+      dspbr_destroy(c);
+      return DSPBR_ERR_CUDA;
+    }
   }
   *out = c;
   return DSPBR_OK;
@@ -222,10 +255,14 @@ int dspbr_create(int device, dspbr_ctx** out) {
 
 int dspbr_destroy(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
+  settle(c);
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (auto e : c->ring_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->ring) cudaFreeHost(c->ring);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DSPBR_OK;
@@ -243,6 +280,7 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
                        uint32_t num_bvh_nodes, const int32_t* bvh_indices, uint32_t num_bvh_indices,
                        dspbr_scene** out) {
   if (!c || !out) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   *out = nullptr;
   if (!vertices || num_vertices == 0) return s.fail(DSPBR_ERR_INVALID, "scene: empty vertex buffer");
@@ -298,6 +336,8 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     const float* src = bvh_nodes + i * 16;
     float* dst = conv.data() + i * 16;
     std::memcpy(dst, src, 16 * sizeof(float));
+    for (int k = 0; k < 16; ++k)
+      if (k % 4 != 3 && !std::isfinite(src[k])) sc->boxes_finite = false;
     for (int k = 3; k < 16; k += 4) {
       float f = src[k];
       int32_t v = (std::isfinite(f) && f > -2147483648.f && f < 2147483648.f) ? int32_t(f) : -1;
@@ -338,6 +378,7 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
 
 int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32_t first, uint32_t count) {
   if (!sc || !materials || first + count > sc->num_materials) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(sc->ctx); if (rc_) return rc_; }
   Status s = sc->ctx->st();
   TRY_CUDA(s, cudaSetDevice(sc->ctx->device), "cudaSetDevice");
   TRY_CUDA(s, cudaMemcpyAsync(sc->materials.p + size_t(first) * 17, materials, size_t(count) * 272,
@@ -355,6 +396,7 @@ int dspbr_scene_device_bytes(const dspbr_scene* sc, uint64_t* bytes) {
 
 int dspbr_scene_destroy(dspbr_scene* sc) {
   if (!sc) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(sc->ctx); if (rc_) return rc_; }
   cudaSetDevice(sc->ctx->device);
   cudaStreamSynchronize(sc->ctx->stream);
   if (sc->ctx->scene == sc) sc->ctx->scene = nullptr;
@@ -399,6 +441,7 @@ static void build_alias(const std::vector<float>& pdf, const std::vector<float>&
 
 int dspbr_ibl_create(dspbr_ctx* c, const float* rgba, int w, int h, dspbr_ibl** out) {
   if (!c || !out) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   *out = nullptr;
   if (!rgba || w <= 0 || h <= 0) return s.fail(DSPBR_ERR_INVALID, "ibl: empty image");
@@ -469,6 +512,7 @@ int dspbr_ibl_alias_table(const dspbr_ibl* e, float* prob, int32_t* alias) {
 
 int dspbr_ibl_destroy(dspbr_ibl* e) {
   if (!e) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(e->ctx); if (rc_) return rc_; }
   cudaSetDevice(e->ctx->device);
   cudaStreamSynchronize(e->ctx->stream);
   if (e->ctx->ibl == e) e->ctx->ibl = nullptr;
@@ -507,12 +551,14 @@ int dspbr_get_params(const dspbr_ctx* c, dspbr_params* p) {
 }
 int dspbr_set_wave_paths(dspbr_ctx* c, uint32_t paths) {
   if (!c) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   c->wave_paths = paths ? paths : (1u << 21);
   return DSPBR_OK;
 }
 
 int dspbr_resize(dspbr_ctx* c, int w, int h) {
   if (!c || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28)) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "resize");
@@ -526,6 +572,7 @@ int dspbr_resize(dspbr_ctx* c, int w, int h) {
 
 int dspbr_reset(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   c->sample_count = 0;
   if (c->accum.p) {
@@ -544,10 +591,13 @@ static int ensure_paths(dspbr_ctx* c, uint32_t cap) {
       (rc = s.cuda(c->weight.alloc(cap), "paths")) || (rc = s.cuda(c->rad.alloc(cap), "paths")) ||
       (rc = s.cuda(c->hit.alloc(cap), "paths")) || (rc = s.cuda(c->sh_dir.alloc(cap), "paths")) ||
       (rc = s.cuda(c->sh_c.alloc(cap), "paths")) || (rc = s.cuda(c->pl_dir.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->pl_c.alloc(cap), "paths")) || (rc = s.cuda(c->result.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->rng.alloc(cap), "paths")) || (rc = s.cuda(c->sh_flags.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->pl_c.alloc(cap), "paths")) || (rc = s.cuda(c->rng.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->sh_flags.alloc(cap), "paths")) || (rc = s.cuda(c->bounce.alloc(cap), "paths")) ||
+      (rc = s.cuda(c->pixel.alloc(cap), "paths")) || (rc = s.cuda(c->frame.alloc(cap), "paths")) ||
       (rc = s.cuda(c->q0.alloc(cap), "queues")) || (rc = s.cuda(c->q1.alloc(cap), "queues")) ||
-      (rc = s.cuda(c->qs.alloc(cap), "queues"))) {
+      (rc = s.cuda(c->qs0.alloc(cap), "queues")) || (rc = s.cuda(c->qs1.alloc(cap), "queues")) ||
+      (rc = s.cuda(c->qh.alloc(cap), "queues")) || (rc = s.cuda(c->qm.alloc(cap), "queues")) ||
+      (rc = s.cuda(c->qfree.alloc(cap), "queues"))) {
     c->capacity = 0;
     return rc;
   }
@@ -555,7 +605,7 @@ static int ensure_paths(dspbr_ctx* c, uint32_t cap) {
   return DSPBR_OK;
 }
 
-static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int spp) {
+static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int frames) {
   WaveParams p{};
   double film = std::tan(double(c->fov) * 0.5 * M_PI / 180.0) * double(c->near_plane);
   for (int col = 0; col < 3; ++col)
@@ -568,8 +618,8 @@ static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int spp) {
   p.cam.width = c->width;
   p.cam.height = c->height;
   p.npix = c->width * c->height;
-  p.spp = spp;
   p.frame_base = frame_base;
+  p.total_items = uint64_t(p.npix) * uint64_t(frames);
   const dspbr_params& q = c->params;
   p.max_bounces = q.max_bounces;
   p.rng_pcg = q.rng == DSPBR_RNG_PCG;
@@ -593,74 +643,124 @@ static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int spp) {
   return p;
 }
 
-static int enqueue_frames(dspbr_ctx* c, int frames) {
-  Status s = c->st();
-  if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
-  if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
-  if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
-  if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
-  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  uint32_t npix = uint32_t(c->width) * uint32_t(c->height);
-  int spp_max = int(std::max<uint32_t>(1u, c->wave_paths / npix));
-  int rc = ensure_paths(c, npix * uint32_t(std::min(spp_max, frames)));
-  if (rc) return rc;
-  DevScene sv = c->scene->view();
-  DevIbl ev{};
-  if (c->ibl) ev = c->ibl->view();
+static PathBuf path_buf(dspbr_ctx* c, uint32_t capacity) {
   PathBuf b{};
   b.org = c->org.p; b.dir = c->dir.p; b.weight = c->weight.p; b.rad = c->rad.p; b.rng = c->rng.p; b.hit = c->hit.p;
   b.sh_dir = c->sh_dir.p; b.sh_c = c->sh_c.p; b.pl_dir = c->pl_dir.p; b.pl_c = c->pl_c.p; b.sh_flags = c->sh_flags.p;
-  b.result = c->result.p; b.q[0] = c->q0.p; b.q[1] = c->q1.p; b.qs = c->qs.p; b.counts = c->counts.p;
-  b.stats = c->stats.p; b.capacity = c->capacity;
+  b.pixel = c->pixel.p; b.frame = c->frame.p; b.bounce = c->bounce.p;
+  b.q[0] = c->q0.p; b.q[1] = c->q1.p; b.qs[0] = c->qs0.p; b.qs[1] = c->qs1.p; b.qh = c->qh.p; b.qm = c->qm.p;
+  b.qfree = c->qfree.p; b.counts = c->counts.p; b.items_next = c->items_next.p;
+  b.stats = c->stats.p; b.accum = reinterpret_cast<double*>(c->accum.p);
+  b.capacity = capacity;
+  return b;
+}
+
+// The iteration loop of one render call.  Iteration i launches
+//   extend(i&1) -> connect(i&1) -> shade_miss -> shade(->1-(i&1)) -> regen(->1-(i&1))
+// and copies the number of live paths to a pinned ring slot.  The host stays
+// kLookahead iterations ahead of the GPU and stops when a slot reads 0 (no
+// live path and no work item left); `max_iter` bounds the loop in any case.
+static int run_iterations(dspbr_ctx* c, const WaveParams& p, const PathBuf& b, const DevScene& sv, const DevIbl& ev,
+                          uint64_t max_iter) {
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   LaunchCfg lc;
   lc.trace_threads = 128;
   lc.trace_blocks = 148 * 16;
   lc.shade_threads = 128;
   lc.shade_blocks = 148 * 8;
-  TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
-  int left = frames;
-  while (left > 0) {
-    int spp = std::min(left, spp_max);
-    WaveParams p = make_wave(c, uint32_t(c->sample_count + 1), spp);
-    p.count_traversal = c->counting ? 1 : 0;
-    launch_generate(p, b, c->stream);
-    int cur = 0;
-    for (int d = 0; d <= p.max_bounces; ++d) {
-      c->mark_begin(0);
-      launch_extend(sv, b, cur, c->counting, lc, c->stream);
-      c->mark_end();
-      if (d > 0) {
-        c->mark_begin(1);
-        launch_connect(sv, b, c->counting, lc, c->stream);
-        c->mark_end();
-      }
-      cudaMemsetAsync(c->counts.p + (cur ^ 1), 0, 4, c->stream);
-      cudaMemsetAsync(c->counts.p + 2, 0, 4, c->stream);
-      c->mark_begin(2);
-      launch_shade(sv, ev, p, b, cur, d, lc, c->stream);
-      c->mark_end();
-      cur ^= 1;
-    }
-    launch_accumulate(p, b, c->accum.p, c->stream);
-    c->kind_launches[0] += uint64_t(p.max_bounces + 1);
-    c->kind_launches[1] += uint64_t(p.max_bounces);
-    c->kind_launches[2] += uint64_t(p.max_bounces + 1);
-    c->kind_launches[3] += 2;  // generate + accumulate
+  cudaStream_t st = c->stream;
+  launch_init_pool(b, st);
+  launch_regen(p, b, 0, st);
+  c->kind_launches[3] += 2;
+  const int R = dspbr_ctx::kRing, L = dspbr_ctx::kLookahead;
+  for (uint64_t it = 0; it < max_iter; ++it) {
+    const int cur = int(it & 1);
+    c->mark_begin(0);
+    launch_extend(sv, p, b, cur, c->counting, lc, st);
+    c->mark_end();
+    c->mark_begin(1);
+    launch_connect(sv, b, cur, c->counting, lc, st);
+    c->mark_end();
+    c->mark_begin(2);
+    launch_shade_miss(ev, p, b, lc, st);
+    launch_shade(sv, ev, p, b, cur ^ 1, lc, st);
+    launch_regen(p, b, cur ^ 1, st);
+    c->mark_end();
+    c->kind_launches[0] += 1;
+    c->kind_launches[1] += 1;
+    c->kind_launches[2] += 3;
+    TRY_CUDA(s, cudaMemcpyAsync(c->ring + it % R, b.counts + (cur ^ 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+             "status copy");
+    TRY_CUDA(s, cudaEventRecord(c->ring_ev[it % R], st), "status event");
     TRY_CUDA(s, cudaGetLastError(), "render launch");
-    c->sample_count += uint64_t(spp);
-    c->rays_primary += uint64_t(npix) * uint64_t(spp);
-    left -= spp;
+    if (it >= uint64_t(L)) {
+      uint64_t j = it - L;
+      TRY_CUDA(s, cudaEventSynchronize(c->ring_ev[j % R]), "render");
+      if (c->ring[j % R] == 0) break;
+    }
   }
-  TRY_CUDA(s, cudaEventRecord(c->ev1, c->stream), "event");
+  return DSPBR_OK;
+}
+
+static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
+  Status s = c->st();
+  int rc = settle(c);
+  if (rc) return rc;
+  if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
+  if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
+  if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
+  if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  WaveParams p = make_wave(c, uint32_t(c->sample_count + 1), frames);
+  uint32_t pool = uint32_t(std::min<uint64_t>(c->wave_paths, p.total_items));
+  rc = ensure_paths(c, pool);
+  if (rc) return rc;
+  PathBuf b = path_buf(c, pool);
+  DevScene sv = c->scene->view();
+  DevIbl ev{};
+  if (c->ibl) ev = c->ibl->view();
+  // every slot runs its paths back to back: while work items remain all slots
+  // are busy, and a path lives at most max_bounces + 1 iterations
+  uint64_t per_path = uint64_t(p.max_bounces) + 1;
+  uint64_t max_iter = (p.total_items * per_path + pool - 1) / pool + per_path + 2;
+  c->sample_count += uint64_t(frames);
+  c->rays_primary += p.total_items;
+  TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
   c->pending = true;
+  if (!async) {
+    rc = run_iterations(c, p, b, sv, ev, max_iter);
+    if (rc) {
+      c->pending = false;
+      c->ev_marks.clear();
+      c->ev_used = 0;
+      return rc;
+    }
+    TRY_CUDA(s, cudaEventRecord(c->ev1, c->stream), "event");
+    return DSPBR_OK;
+  }
+  c->worker_done.store(false);
+  c->worker = std::thread([c, p, b, sv, ev, max_iter]() {
+    int r = run_iterations(c, p, b, sv, ev, max_iter);
+    if (!r) r = c->st().cuda(cudaEventRecord(c->ev1, c->stream), "event");
+    c->worker_rc = r;
+    c->worker_done.store(true);
+  });
   return DSPBR_OK;
 }
 
 int dspbr_wait(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
   Status s = c->st();
+  int rc = settle(c);
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "render");
+  if (rc) {
+    c->pending = false;
+    c->ev_marks.clear();
+    c->ev_used = 0;
+    return rc;
+  }
   if (c->pending) {
     float ms = 0;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -674,6 +774,8 @@ int dspbr_wait(dspbr_ctx* c) {
 int dspbr_set_counting(dspbr_ctx* c, int enable) {
   if (!c) return DSPBR_ERR_INVALID;
   Status s = c->st();
+  int rc = settle(c);
+  if (rc) return rc;
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   TRY_CUDA(s, cudaMemsetAsync(c->stats.p + 3, 0, 4 * sizeof(unsigned long long), c->stream), "counters");
   c->counting = enable != 0;
@@ -691,15 +793,24 @@ int dspbr_set_profiling(dspbr_ctx* c, int enable) {
 }
 
 int dspbr_render(dspbr_ctx* c, int frames) {
-  int rc = enqueue_frames(c, frames);
-  if (rc) return rc;
+  if (!c) return DSPBR_ERR_INVALID;
+  int rc = enqueue_frames(c, frames, false);
+  if (rc) {
+    dspbr_wait(c);
+    return rc;
+  }
   return dspbr_wait(c);
 }
 
-int dspbr_render_async(dspbr_ctx* c, int frames) { return enqueue_frames(c, frames); }
+int dspbr_render_async(dspbr_ctx* c, int frames) {
+  if (!c) return DSPBR_ERR_INVALID;
+  return enqueue_frames(c, frames, true);
+}
 
 int dspbr_poll(dspbr_ctx* c, int* done) {
   if (!c || !done) return DSPBR_ERR_INVALID;
+  if (!c->worker_done.load()) { *done = 0; return DSPBR_OK; }
+  if (c->worker.joinable()) c->worker.join();
   cudaSetDevice(c->device);
   cudaError_t e = cudaStreamQuery(c->stream);
   if (e == cudaErrorNotReady) { cudaGetLastError(); *done = 0; return DSPBR_OK; }
@@ -710,6 +821,7 @@ int dspbr_poll(dspbr_ctx* c, int* done) {
 
 int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c || !rgba) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   size_t npix = size_t(c->width) * c->height;
   if (num_floats < npix * 4) return s.fail(DSPBR_ERR_INVALID, "read_accum: buffer holds %zu floats, need %zu", num_floats, npix * 4);
@@ -724,6 +836,7 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
 
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   if (!c || !d) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   std::memset(d, 0, sizeof *d);
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -744,8 +857,8 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->bvh_build_ms = c->scene->bvh_build_ms;
     d->upload_ms = c->scene->upload_ms;
   }
-  d->device_bytes = c->org.bytes() * 10 + c->rng.bytes() + c->sh_flags.bytes() + c->q0.bytes() * 3 + c->accum.bytes() +
-                    c->mean.bytes();
+  d->device_bytes = c->org.bytes() * 9 + c->rng.bytes() + c->sh_flags.bytes() + c->bounce.bytes() + c->pixel.bytes() +
+                    c->frame.bytes() + c->q0.bytes() * 7 + c->accum.bytes() + c->mean.bytes();
   d->last_render_ms = c->last_render_ms;
   d->nodes_closest = st[3];
   d->tris_closest = st[4];
@@ -780,6 +893,7 @@ extern "C" {
 int dspbr_trace_closest(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, uint32_t n, int32_t* tri, float* t,
                         float* uv) {
   if (!c || !sc || !rays || !tri || !t || !uv) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   DevBuf<float> r;
@@ -799,13 +913,15 @@ int dspbr_trace_closest(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, 
 
 int dspbr_trace_occluded(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, uint32_t n, int32_t* occ) {
   if (!c || !sc || !rays || !occ) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   DevBuf<float> r;
   DevBuf<int32_t> o;
   int rc;
   if ((rc = up(s, r, rays, size_t(n) * 8, c->stream)) || (rc = s.cuda(o.alloc(std::max(n, 1u)), "alloc"))) return rc;
-  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 1, nullptr, nullptr, nullptr, o.p, c->stream);
+  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 1, nullptr, nullptr, nullptr, o.p,
+                    c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "occluded")) || (rc = down(s, occ, o, n, c->stream))) return rc;
   return s.cuda(cudaStreamSynchronize(c->stream), "occluded");
 }
@@ -813,6 +929,7 @@ int dspbr_trace_occluded(dspbr_ctx* c, const dspbr_scene* sc, const float* rays,
 int dspbr_bsdf_query(dspbr_ctx* c, const dspbr_scene* sc, uint32_t n, const float* hit, const float* wo,
                      const float* rnd, float* eval4, float* sample10, int32_t* flags) {
   if (!c || !sc || !hit || !wo || !rnd || !eval4 || !sample10 || !flags) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   DevBuf<float> dh, dw, dr, de, ds;
@@ -834,6 +951,7 @@ int dspbr_bsdf_query(dspbr_ctx* c, const dspbr_scene* sc, uint32_t n, const floa
 int dspbr_ibl_query(dspbr_ctx* c, const dspbr_ibl* e, uint32_t n, const float* r2, const float* dirs, float* sdp4,
                     float* pdf, float* rgb) {
   if (!c || !e || !r2 || !dirs || !sdp4 || !pdf || !rgb) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   DevBuf<float> dr, dd, ds, dp, dc;
@@ -854,6 +972,7 @@ int dspbr_ibl_query(dspbr_ctx* c, const dspbr_ibl* e, uint32_t n, const float* r
 
 int dspbr_camera_rays(dspbr_ctx* c, uint32_t n, const int32_t* xy, const float* r2, float* rays6) {
   if (!c || !xy || !r2 || !rays6) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
   if (!c->has_camera || c->width <= 0) return s.fail(DSPBR_ERR_STATE, "camera_rays: camera and size required");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");

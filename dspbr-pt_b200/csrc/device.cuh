@@ -31,6 +31,7 @@ struct DevScene {
   const uint32_t* __restrict__ indices;  // 3 per triangle
   const float4* __restrict__ materials;  // 17 float4 per material (68 floats)
   int num_nodes, num_slots, num_tris, num_materials;
+  int boxes_finite;  // every node bound is finite (checked at upload)
 };
 
 struct DevIbl {
@@ -106,13 +107,26 @@ struct Hit {
   float t, u, v;
 };
 
+// bvh_intersect_bounds (bvh.glsl:31-41).  kExactNaN keeps GLSL's min/max
+// (y<x ? y : x), which differs from fminf/fmaxf only when an operand is NaN.
+// No slab value can be NaN when the ray origin and 1/dir are finite and the
+// box bounds are finite; traverse() then takes the FMNMX form, whose decisions
+// are identical (a -0/+0 difference does not change any comparison).
+template <bool kExactNaN>
 DEV float slab(float4 bmin, float4 bmax, v3 org, v3 inv, float tfar) {
   float t0x = __fmul_rn(__fsub_rn(bmin.x, org.x), inv.x), t1x = __fmul_rn(__fsub_rn(bmax.x, org.x), inv.x);
   float t0y = __fmul_rn(__fsub_rn(bmin.y, org.y), inv.y), t1y = __fmul_rn(__fsub_rn(bmax.y, org.y), inv.y);
   float t0z = __fmul_rn(__fsub_rn(bmin.z, org.z), inv.z), t1z = __fmul_rn(__fsub_rn(bmax.z, org.z), inv.z);
-  float tmin = gmax(gmax(gmin(t0x, t1x), gmin(t0y, t1y)), gmin(t0z, t1z));
-  float tmax = gmin(gmin(gmax(t0x, t1x), gmax(t0y, t1y)), gmax(t0z, t1z));
-  if (isnan(tmin) || isnan(tmax) || tmin > tmax || tmax < 0.f || tmin >= tfar) return kBvhFar;
+  float tmin, tmax;
+  if (kExactNaN) {
+    tmin = gmax(gmax(gmin(t0x, t1x), gmin(t0y, t1y)), gmin(t0z, t1z));
+    tmax = gmin(gmin(gmax(t0x, t1x), gmax(t0y, t1y)), gmax(t0z, t1z));
+    if (isnan(tmin) || isnan(tmax)) return kBvhFar;
+  } else {
+    tmin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
+    tmax = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+  }
+  if (tmin > tmax || tmax < 0.f || tmin >= tfar) return kBvhFar;
   return tmin;
 }
 
@@ -142,10 +156,9 @@ DEV v3 inv_dir(v3 d) { return mk(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdi
 // self-reference checks.  kAny: stop at the first accepted triangle (same
 // boolean as the reference's closest-hit isOccluded).  Returns false and sets
 // `aborted` when the step cap ends the loop with work left.
-template <bool kAny>
-DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted, uint32_t* nodes_visited = nullptr,
-                  uint32_t* tris_tested = nullptr) {
-  v3 inv = inv_dir(dir);
+template <bool kAny, bool kExactNaN>
+DEV bool traverse_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfar, Hit& hit, bool& aborted,
+                       uint32_t* nodes_visited, uint32_t* tris_tested) {
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
@@ -177,8 +190,8 @@ DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool&
       }
     } else {
       int left = __float_as_int(n0.w), right = __float_as_int(n1.w);
-      float d0 = slab(n0, n1, org, inv, hit.t);
-      float d1 = slab(n2, n3, org, inv, hit.t);
+      float d0 = slab<kExactNaN>(n0, n1, org, inv, hit.t);
+      float d1 = slab<kExactNaN>(n2, n3, org, inv, hit.t);
       // bvh_push_child (bvh.glsl:141-145): bounded stack, valid node, not self
       auto push = [&](int c) {
         if (top < kStackSize && c >= 0 && c < s.num_nodes && c != ni) stack[top++] = c;
@@ -195,6 +208,17 @@ DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool&
   }
   aborted = (top > 0 && step >= kMaxSteps);
   return hit.tri >= 0;
+}
+
+DEV bool finite3(v3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+template <bool kAny>
+DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted, uint32_t* nodes_visited = nullptr,
+                  uint32_t* tris_tested = nullptr) {
+  v3 inv = inv_dir(dir);
+  if (s.boxes_finite && finite3(org) && finite3(inv))
+    return traverse_impl<kAny, false>(s, org, inv, dir, tfar, hit, aborted, nodes_visited, tris_tested);
+  return traverse_impl<kAny, true>(s, org, inv, dir, tfar, hit, aborted, nodes_visited, tris_tested);
 }
 
 // ---- camera (renderer.frag:129-142, renderer.ts:399-404) -------------------------
@@ -331,7 +355,7 @@ DEV float4 vtx(const DevScene& s, uint32_t vi, int slot) { return __ldg(s.verts 
 // get_onb(n) (utils.glsl:97-102): Spencer & Jones basis, first column
 DEV v3 onb_tangent(v3 n) { return normalize(cross(n, mk(-n.z, n.x, -n.y))); }
 
-DEV Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
+NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
   Surface S;
   uint32_t i0 = __ldg(s.indices + 3 * size_t(tri)), i1 = __ldg(s.indices + 3 * size_t(tri) + 1),
            i2 = __ldg(s.indices + 3 * size_t(tri) + 2);

@@ -1,16 +1,22 @@
-// Wavefront path tracer: generate / extend / connect / shade / accumulate.
+// Wavefront path tracer with path regeneration.
 //
-// One wave traces `spp` samples of every pixel.  The reference evaluates a
-// whole path per fragment (renderer.frag:146-157 -> integrator/misptdl.glsl:
-// 34-93); here each bounce is split into
-//   extend   closest hit for every live path (bvh.glsl:149-216),
-//   connect  any-hit test of the NEE shadow rays emitted by the previous
-//            shade; visible contributions are added to the path radiance,
-//   shade    Russian roulette, absorption, emission, BSDF sampling, NEE
-//            sample generation (misptdl.glsl:54-90, renderer.frag:94-123),
-// and live paths are compacted into the next queue with one atomic per warp
-// (__ballot_sync / __popc).  The per-path arithmetic and RNG consumption order
-// follow the reference exactly; see DESIGN.md for the event_type note.
+// The reference evaluates a whole path per fragment (renderer.frag:146-157 ->
+// integrator/misptdl.glsl:34-93).  Here a render call streams its pixel
+// samples through a fixed pool of path slots; every iteration of the host loop
+// runs
+//   extend      closest hit for every live path (bvh.glsl:149-216); hits and
+//               misses go to separate queues,
+//   connect     any-hit test of the NEE shadow rays emitted by the previous
+//               shade; visible contributions are added to the path radiance,
+//   shade_miss  background / MIS-weighted environment (misptdl.glsl:41-46, 84-88),
+//   shade       RR, absorption, emission, BSDF sampling, NEE sample generation
+//               (misptdl.glsl:54-90, renderer.frag:94-123),
+//   regen       new samples (rng_init + calcuateViewRay) into the slots freed
+//               by terminated paths,
+// so every launch works on a full pool instead of a shrinking per-bounce
+// queue.  Queues are compacted with one atomic per warp (__ballot_sync /
+// __popc); a finished path adds its sample to the pixel's FP64 sums.  The
+// per-path arithmetic and RNG consumption order follow the reference exactly.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -35,78 +41,122 @@ DEV void count_warp(unsigned long long* ctr, bool pred) {
   if ((threadIdx.x & 31) == 0 && m) atomicAdd(ctr, (unsigned long long)__popc(m));
 }
 
-DEV Rng load_rng(const WaveParams& p, const PathBuf& b, uint32_t path) {
-  Rng r;
-  r.state = b.rng[path];
-  if (p.rng_pcg) {
-    uint32_t pixel = path % uint32_t(p.npix), s = path / uint32_t(p.npix);
-    r.inc = pcg_inc(uint64_t(p.frame_base + s) * uint64_t(p.npix) + pixel);
-  } else {
-    r.inc = 0;
-  }
-  return r;
-}
-
-DEV float4 f4(v3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
-
-}  // namespace
-
-// ---- generate: rng_init + calcuateViewRay (renderer.frag:146-150) ------------------
-__global__ void k_generate(WaveParams p, PathBuf b) {
-  uint32_t P = uint32_t(p.npix) * uint32_t(p.spp);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    b.counts[0] = P;
-    b.counts[1] = 0;
-    b.counts[2] = 0;
-  }
-  for (uint32_t path = blockIdx.x * blockDim.x + threadIdx.x; path < P; path += gridDim.x * blockDim.x) {
-    uint32_t pixel = path % uint32_t(p.npix), s = path / uint32_t(p.npix);
-    int px = int(pixel % uint32_t(p.cam.width)), py = int(pixel / uint32_t(p.cam.width));
-    uint32_t frame = p.frame_base + s;
-    Rng r;
-    if (p.rng_pcg) {
-      uint64_t stream = uint64_t(frame) * uint64_t(p.npix) + pixel;
-      r.inc = pcg_inc(stream);
-      r.state = pcg_init(p.seed, stream);
-    } else {
-      Mwc m = mwc_init(int(frame) * p.max_bounces, px, py);
-      r.state = uint64_t(m.x) | (uint64_t(m.y) << 32);
-      r.inc = 0;
-    }
-    float r0 = r.next();
-    float r1 = r.next();
-    v3 org, dir;
-    camera_ray(p.cam, px, py, r0, r1, org, dir);
-    b.org[path] = f4(org, 0.f);
-    b.dir[path] = f4(dir, 0.f);
-    b.weight[path] = make_float4(1.f, 1.f, 1.f, 0.f);
-    b.rad[path] = make_float4(0.f, 0.f, 0.f, 0.f);
-    b.rng[path] = r.state;
-    b.q[0][path] = path;
-  }
-}
-
-// ---- extend: closest hit -----------------------------------------------------------------
 DEV void add_warp(unsigned long long* ctr, uint32_t v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, (unsigned long long)v);
 }
 
+DEV float4 f4(v3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+DEV Rng load_rng(const WaveParams& p, const PathBuf& b, uint32_t slot) {
+  Rng r;
+  r.state = b.rng[slot];
+  r.inc = p.rng_pcg ? pcg_inc(uint64_t(b.frame[slot]) * uint64_t(p.npix) + b.pixel[slot]) : 0;
+  return r;
+}
+
+// A terminated path adds its sample to the pixel sums and frees its slot.
+DEV void finish_path(const PathBuf& b, uint32_t slot, float4 c) {
+  double* a = b.accum + 4 * size_t(b.pixel[slot]);
+  atomicAdd(a + 0, double(c.x));
+  atomicAdd(a + 1, double(c.y));
+  atomicAdd(a + 2, double(c.z));
+  atomicAdd(a + 3, double(c.w));
+}
+
+}  // namespace
+
+// ---- pool set-up -----------------------------------------------------------------------------
+__global__ void k_init_pool(PathBuf b) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.capacity; i += gridDim.x * blockDim.x)
+    b.qfree[i] = i;
+  if (blockIdx.x == 0 && threadIdx.x < kCntNum) {
+    b.counts[threadIdx.x] = threadIdx.x == kCntFree ? b.capacity : 0u;
+    if (threadIdx.x == 0) *b.items_next = 0ull;
+  }
+}
+
+// ---- regen: new samples in free slots (renderer.frag:146-150) ----------------------------
+__global__ void k_regen(WaveParams p, PathBuf b, int next) {
+  const uint32_t nfree = b.counts[kCntFree];
+  const unsigned long long first = *b.items_next;
+  uint32_t* q = b.q[next];
+  uint32_t* cnt = b.counts + next;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // hit / miss queues of the next extend; shade_miss and shade read them before
+    b.counts[kCntMiss] = 0;
+    b.counts[kCntHit] = 0;
+  }
+  for (uint32_t base = blockIdx.x * blockDim.x; base < nfree; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    unsigned long long item = first + i;
+    bool valid = i < nfree && item < p.total_items;
+    uint32_t slot = 0;
+    if (valid) {
+      slot = b.qfree[i];
+      uint32_t pixel = uint32_t(item % uint64_t(p.npix));
+      uint32_t frame = p.frame_base + uint32_t(item / uint64_t(p.npix));
+      int px = int(pixel % uint32_t(p.cam.width)), py = int(pixel / uint32_t(p.cam.width));
+      Rng r;
+      if (p.rng_pcg) {
+        uint64_t stream = uint64_t(frame) * uint64_t(p.npix) + pixel;
+        r.inc = pcg_inc(stream);
+        r.state = pcg_init(p.seed, stream);
+      } else {
+        Mwc m = mwc_init(int(frame) * p.max_bounces, px, py);
+        r.state = uint64_t(m.x) | (uint64_t(m.y) << 32);
+        r.inc = 0;
+      }
+      float r0 = r.next();
+      float r1 = r.next();
+      v3 org, dir;
+      camera_ray(p.cam, px, py, r0, r1, org, dir);
+      b.org[slot] = f4(org, 0.f);
+      b.dir[slot] = f4(dir, 0.f);
+      b.weight[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+      b.rad[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+      b.rng[slot] = r.state;
+      b.pixel[slot] = pixel;
+      b.frame[slot] = frame;
+      b.bounce[slot] = 0;
+    }
+    enqueue(q, cnt, valid, slot);
+  }
+}
+
+// ---- extend: closest hit ------------------------------------------------------------------------
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_extend(DevScene s, PathBuf b, int cur) {
+__global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBuf b, int cur) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // book-keeping of the regen that ran before: consume the free list
+    unsigned long long first = *b.items_next;
+    unsigned long long left = p.total_items > first ? p.total_items - first : 0ull;
+    unsigned long long used = min((unsigned long long)b.counts[kCntFree], left);
+    *b.items_next = first + used;
+    b.counts[kCntFree] = 0;
+    // queues that this iteration's shade fills; their readers ran last iteration
+    b.counts[cur ^ 1] = 0;
+    b.counts[kCntShadow0 + (cur ^ 1)] = 0;
+  }
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
-    bool aborted = false;
-    uint32_t nodes = 0, tris = 0;
+    bool aborted = false, is_hit = false, is_miss = false;
+    uint32_t nodes = 0, tris = 0, slot = 0;
     if (i < count) {
-      uint32_t path = q[i];
-      float4 o = b.org[path], d = b.dir[path];
+      slot = q[i];
+      float4 o = b.org[slot], d = b.dir[slot];
       Hit h;
       traverse<false>(s, mk(o), mk(d), kTfarMax, h, aborted, kCount ? &nodes : nullptr, kCount ? &tris : nullptr);
-      b.hit[path] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+      b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+      is_hit = h.tri >= 0;
+      is_miss = !is_hit;
     }
+    // hits and misses are shaded by different kernels, so shading warps are
+    // either all surface hits or all environment lookups
+    enqueue(b.qh, b.counts + kCntHit, is_hit, slot);
+    enqueue(b.qm, b.counts + kCntMiss, is_miss, slot);
     count_warp(b.stats + 0, i < count);
     count_warp(b.stats + 2, aborted);
     if (kCount) {
@@ -116,43 +166,44 @@ __global__ void __launch_bounds__(128) k_extend(DevScene s, PathBuf b, int cur) 
   }
 }
 
-// ---- connect: shadow rays (bvh.glsl:218-229) ---------------------------------------------
+// ---- connect: NEE shadow rays (bvh.glsl:218-229) ---------------------------------------------
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_connect(DevScene s, PathBuf b) {
-  const uint32_t count = b.counts[2];
+__global__ void __launch_bounds__(128) k_connect(DevScene s, PathBuf b, int cur) {
+  const uint32_t count = b.counts[kCntShadow0 + cur];
+  const uint32_t* qs = b.qs[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool aborted = false;
     int nrays = 0;
     uint32_t nodes = 0, tris = 0;
     if (i < count) {
-      uint32_t path = b.qs[i];
-      int flags = b.sh_flags[path];
-      v3 org = mk(b.org[path]);
+      uint32_t slot = qs[i];
+      int flags = b.sh_flags[slot];
+      v3 org = mk(b.org[slot]);
       v3 add = mk(0.f);
       if (flags & 1) {
-        float4 d = b.sh_dir[path];
+        float4 d = b.sh_dir[slot];
         Hit h;
         bool ab = false;
         // isOccluded normalises the light direction (bvh.glsl:225-229)
         if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
                             kCount ? &tris : nullptr))
-          add = mk(b.sh_c[path]);
+          add = mk(b.sh_c[slot]);
         aborted |= ab;
         ++nrays;
       }
       if (flags & 2) {
-        float4 d = b.pl_dir[path];
+        float4 d = b.pl_dir[slot];
         Hit h;
         bool ab = false;
         if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
                             kCount ? &tris : nullptr))
-          add = add + mk(b.pl_c[path]);
+          add = add + mk(b.pl_c[slot]);
         aborted |= ab;
         ++nrays;
       }
-      float4 L = b.rad[path];
-      b.rad[path] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+      float4 L = b.rad[slot];
+      b.rad[slot] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
     }
     unsigned m1 = __ballot_sync(0xffffffffu, nrays >= 1), m2 = __ballot_sync(0xffffffffu, nrays >= 2);
     if ((threadIdx.x & 31) == 0 && (m1 | m2)) atomicAdd(b.stats + 1, (unsigned long long)(__popc(m1) + __popc(m2)));
@@ -174,49 +225,67 @@ DEV float4 clamp_result(const WaveParams& p, v3 L) {
   return f4(L, 1.f);
 }
 
-// Returns true if the path continues with an extension ray; sets `shadow`
-// when NEE shadow rays were emitted.
-DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t path,
-                    int depth, bool& shadow) {
-  shadow = false;
-  float4 hit = b.hit[path];
-  int tri = __float_as_int(hit.w);
-  float4 o4 = b.org[path], d4 = b.dir[path], w4 = b.weight[path], l4 = b.rad[path];
+// A path whose ray left the scene: background for camera rays
+// (misptdl.glsl:41-46), MIS-weighted environment otherwise (misptdl.glsl:84-88).
+DEV void shade_miss_path(const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t slot) {
+  float4 d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
   v3 dir = mk(d4);
   v3 w = mk(w4);
   float last_pdf = w4.w;
   v3 L = mk(l4);
-  int bounce = depth;
+  if (b.bounce[slot] == 0) {
+    if (p.bg_from_ibl > 0) {
+      v3 env = p.has_ibl ? ibl_eval(e, p.ibl_rot, dir) : mk(0.f);
+      finish_path(b, slot, f4(env * w, 1.f));
+    } else {
+      finish_path(b, slot, make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
+                                       p.bg_color.w));
+    }
+    return;
+  }
+  if (p.has_ibl) {
+    float ipdf = ibl_pdf(e, p.ibl_rot, dir);
+    float mis = mis_balance(last_pdf, ipdf);
+    L = L + ibl_eval(e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
+  }
+  finish_path(b, slot, clamp_result(p, L));
+}
 
-  if (tri < 0) {
-    if (depth == 0) {  // primary miss (misptdl.glsl:41-46)
-      if (p.bg_from_ibl > 0) {
-        v3 env = p.has_ibl ? ibl_eval(e, p.ibl_rot, dir) : mk(0.f);
-        b.result[path] = f4(env * w, 1.f);
-      } else {
-        b.result[path] = make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
-                                     p.bg_color.w);
-      }
-      return false;
+__global__ void __launch_bounds__(256) k_shade_miss(DevIbl e, WaveParams p, PathBuf b) {
+  const uint32_t count = b.counts[kCntMiss];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    uint32_t slot = 0;
+    if (i < count) {
+      slot = b.qm[i];
+      shade_miss_path(e, p, b, slot);
     }
-    // environment hit with MIS against the BSDF pdf (misptdl.glsl:84-88)
-    if (p.has_ibl) {
-      float ipdf = ibl_pdf(e, p.ibl_rot, dir);
-      float mis = mis_balance(last_pdf, ipdf);
-      L = L + ibl_eval(e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
-    }
-    b.result[path] = clamp_result(p, L);
-    return false;
+    enqueue(b.qfree, b.counts + kCntFree, i < count, slot);
   }
+}
+
+// Surface hit.  Returns true if the path continues with an extension ray and
+// sets `shadow` when NEE shadow rays were emitted; otherwise the path's sample
+// has been accumulated.
+DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t slot,
+                    bool& shadow) {
+  shadow = false;
+  float4 hit = b.hit[slot];
+  int tri = __float_as_int(hit.w);
+  float4 o4 = b.org[slot], d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
+  v3 dir = mk(d4);
+  v3 w = mk(w4);
+  v3 L = mk(l4);
+  int bounce = b.bounce[slot];
   if (!(bounce < p.max_bounces)) {  // loop condition (misptdl.glsl:54)
-    b.result[path] = clamp_result(p, L);
+    finish_path(b, slot, clamp_result(p, L));
     return false;
   }
-  Rng rng = load_rng(p, b, path);
+  Rng rng = load_rng(p, b, slot);
   // Russian roulette (renderer.frag:119-123): weight boost every bounce
   w = w * p.rr_factor;
   if (bounce > p.rr_start && rng.next() <= p.rr_prob) {
-    b.result[path] = clamp_result(p, L);
+    finish_path(b, slot, clamp_result(p, L));
     return false;
   }
   v3 org = mk(o4);
@@ -243,7 +312,7 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
     pdf = bs.pdf;
     bw = bs.weight;
     if (pdf < kEpsPdf) {  // absorbed: returns L without the clamp
-      b.result[path] = f4(L, 1.f);
+      finish_path(b, slot, f4(L, 1.f));
       return false;
     }
   }
@@ -262,8 +331,8 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
       float bpdf = bsdf_pdf(S.c, S.n, wi, ld);
       v3 c = ibl_eval(e, p.ibl_rot, ld) * f * cosnl / ipdf;
       if (bpdf > kEpsPdf) c = c * mis_balance(ipdf, bpdf);
-      b.sh_dir[path] = f4(ld, kTfarMax);
-      b.sh_c[path] = f4(c * w, 0.f);
+      b.sh_dir[slot] = f4(ld, kTfarMax);
+      b.sh_c[slot] = f4(c * w, 0.f);
       flags |= 1;
     }
   }
@@ -276,50 +345,39 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
     if (cosnl > kEpsCos) {
       v3 f = bsdf_eval(S.c, S.n, wi, ldn) / fmaxf(fabsf(dot(S.n, ldn)), kEps);
       v3 c = f * (mk(p.pl_emis.x, p.pl_emis.y, p.pl_emis.z) / dist2) * cosnl;
-      b.pl_dir[path] = f4(ldn, sqrtf(dist2));
-      b.pl_c[path] = f4(c * w, 0.f);
+      b.pl_dir[slot] = f4(ldn, sqrtf(dist2));
+      b.pl_c[slot] = f4(c * w, 0.f);
       flags |= 2;
     }
   }
-  b.sh_flags[path] = flags;
+  b.sh_flags[slot] = flags;
   shadow = flags != 0;
 
   w = w * bw;
-  b.org[path] = f4(pos, 0.f);
-  b.dir[path] = f4(wo, 0.f);
-  b.weight[path] = f4(w, pdf);
-  b.rad[path] = f4(L, 0.f);
-  b.rng[path] = rng.state;
+  b.org[slot] = f4(pos, 0.f);
+  b.dir[slot] = f4(wo, 0.f);
+  b.weight[slot] = f4(w, pdf);
+  b.rad[slot] = f4(L, 0.f);
+  b.rng[slot] = rng.state;
+  b.bounce[slot] = bounce + 1;
   return true;
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams p, PathBuf b, int cur, int depth) {
-  const uint32_t count = b.counts[cur];
-  const uint32_t* q = b.q[cur];
-  uint32_t* qn = b.q[cur ^ 1];
-  uint32_t* cn = b.counts + (cur ^ 1);
+__global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams p, PathBuf b, int next) {
+  const uint32_t count = b.counts[kCntHit];
+  uint32_t* qn = b.q[next];
+  uint32_t* cn = b.counts + next;
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool cont = false, shadow = false;
-    uint32_t path = 0;
+    uint32_t slot = 0;
     if (i < count) {
-      path = q[i];
-      cont = shade_path(s, e, p, b, path, depth, shadow);
+      slot = b.qh[i];
+      cont = shade_path(s, e, p, b, slot, shadow);
     }
-    enqueue(qn, cn, cont, path);
-    enqueue(b.qs, b.counts + 2, shadow, path);
-  }
-}
-
-// ---- accumulate: running sum in FP64 per pixel -----------------------------------------
-__global__ void k_accumulate(WaveParams p, PathBuf b, double4* accum) {
-  for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < uint32_t(p.npix); px += gridDim.x * blockDim.x) {
-    double4 a = accum[px];
-    for (int s = 0; s < p.spp; ++s) {
-      float4 r = b.result[size_t(s) * p.npix + px];
-      a.x += double(r.x); a.y += double(r.y); a.z += double(r.z); a.w += double(r.w);
-    }
-    accum[px] = a;
+    enqueue(qn, cn, cont, slot);
+    enqueue(b.qs[next], b.counts + kCntShadow0 + next, shadow, slot);
+    enqueue(b.qfree, b.counts + kCntFree, i < count && !cont, slot);
   }
 }
 
@@ -351,8 +409,8 @@ __global__ void k_gather_tris(const float4* verts, const uint32_t* indices, cons
 }
 
 // ---- kernel-level queries ----------------------------------------------------------------
-__global__ void k_trace_rays(DevScene s, const float4* rays, uint32_t n, int any, int32_t* tri, float* t, float2* uv,
-                             int32_t* occ) {
+__global__ void __launch_bounds__(128) k_trace_rays(DevScene s, const float4* rays, uint32_t n, int any, int32_t* tri,
+                                                    float* t, float2* uv, int32_t* occ) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 a = rays[2 * i], c = rays[2 * i + 1];
     v3 org = mk(a.x, a.y, a.z), dir = mk(a.w, c.x, c.y);
@@ -360,8 +418,7 @@ __global__ void k_trace_rays(DevScene s, const float4* rays, uint32_t n, int any
     bool ab = false;
     if (any) {
       // isOccluded (bvh.glsl:225-229) normalises the direction first
-      bool o = traverse<true>(s, org, normalize_rn(dir), c.z, h, ab);
-      occ[i] = o ? 1 : 0;
+      occ[i] = traverse<true>(s, org, normalize_rn(dir), c.z, h, ab) ? 1 : 0;
     } else {
       traverse<false>(s, org, dir, c.z, h, ab);
       tri[i] = h.tri;
@@ -451,24 +508,27 @@ static int grid_for(uint64_t n, int threads, int cap) {
   return int(b < uint64_t(cap) ? b : uint64_t(cap));
 }
 
-void launch_generate(const WaveParams& p, const PathBuf& b, cudaStream_t st) {
-  uint64_t P = uint64_t(p.npix) * p.spp;
-  k_generate<<<grid_for(P, 256, 148 * 16), 256, 0, st>>>(p, b);
+void launch_init_pool(const PathBuf& b, cudaStream_t st) {
+  k_init_pool<<<grid_for(b.capacity, 256, 148 * 8), 256, 0, st>>>(b);
 }
-void launch_extend(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
-  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
-  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+void launch_regen(const WaveParams& p, const PathBuf& b, int next, cudaStream_t st) {
+  k_regen<<<grid_for(b.capacity, 256, 148 * 16), 256, 0, st>>>(p, b, next);
 }
-void launch_connect(const DevScene& s, const PathBuf& b, bool count, const LaunchCfg& lc, cudaStream_t st) {
-  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b);
-  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b);
+void launch_extend(const DevScene& s, const WaveParams& p, const PathBuf& b, int cur, bool count, const LaunchCfg& lc,
+                   cudaStream_t st) {
+  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, p, b, cur);
+  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, p, b, cur);
 }
-void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int cur, int depth,
+void launch_connect(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
+  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+}
+void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int next,
                   const LaunchCfg& lc, cudaStream_t st) {
-  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(s, e, p, b, cur, depth);
+  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(s, e, p, b, next);
 }
-void launch_accumulate(const WaveParams& p, const PathBuf& b, double4* accum, cudaStream_t st) {
-  k_accumulate<<<grid_for(p.npix, 256, 148 * 8), 256, 0, st>>>(p, b, accum);
+void launch_shade_miss(const DevIbl& e, const WaveParams& p, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
+  k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(e, p, b);
 }
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st) {
   k_mean<<<grid_for(npix, 256, 148 * 8), 256, 0, st>>>(accum, inv_count, out, npix);

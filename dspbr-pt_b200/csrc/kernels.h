@@ -7,26 +7,45 @@
 
 namespace dspbr {
 
-// Per-wave constants of the reference's uniform block (renderer.frag:10-31).
+// Per-render constants of the reference's uniform block (renderer.frag:10-31)
+// plus the work description of one render call.
 struct WaveParams {
   Camera cam;
-  int npix;             // width * height
-  int spp;              // samples per pixel in this wave (path = s * npix + pixel)
-  uint32_t frame_base;  // 1-based progressive frame number of sample 0
+  int npix;              // width * height
+  uint32_t frame_base;   // 1-based progressive frame number of work item 0
+  uint64_t total_items;  // frames * npix; item k = frame frame_base + k / npix, pixel k % npix
   int max_bounces;
-  int rng_pcg;          // 0: MWC of rng.glsl, 1: PCG32
+  int rng_pcg;           // 0: MWC of rng.glsl, 1: PCG32
   uint64_t seed;
   int use_ibl, bg_from_ibl, env_mode, lean, has_ibl;
-  float ibl_rot;        // radians
+  float ibl_rot;         // radians
   float4 bg_color;
   float ray_eps, clamp_threshold;
   float rr_prob, rr_factor;
   int rr_start;
   float4 pl_pos, pl_emis;
-  int count_traversal;  // accumulate node visits / triangle tests into stats[3..6]
+  int count_traversal;   // accumulate node visits / triangle tests into stats[3..6]
 };
 
-// Structure-of-arrays path state, capacity = paths of one wave.
+// Queue counters (uint32 slots of PathBuf::counts).  Iteration i works on
+// parity cur = i & 1: extend reads q[cur], connect reads qs[cur], shade and
+// regen fill q[cur ^ 1] and qs[cur ^ 1].  Counters are reset inside the
+// kernels (extend resets the ones shade fills, regen the ones extend fills),
+// so an iteration is a fixed sequence of five launches.
+enum : int {
+  kCntExt0 = 0,     // extension queues (ping-pong)
+  kCntExt1 = 1,
+  kCntShadow0 = 2,  // NEE shadow queues (ping-pong)
+  kCntShadow1 = 3,
+  kCntMiss = 4,     // paths whose extension ray left the scene
+  kCntHit = 5,      // paths whose extension ray hit a triangle
+  kCntFree = 6,     // free path slots
+  kCntNum = 16
+};
+
+// Structure-of-arrays state of a pool of path slots.  A render call streams
+// its work items (pixel samples) through the pool: a path that terminates
+// accumulates its sample and frees its slot, and the next item takes it.
 struct PathBuf {
   float4* org;      // ray origin (shadow rays of the same vertex share it)
   float4* dir;
@@ -39,13 +58,20 @@ struct PathBuf {
   float4* pl_dir;   // point-light shadow ray dir.xyz, tfar
   float4* pl_c;
   int* sh_flags;    // bit0: IBL shadow ray, bit1: point-light shadow ray
-  float4* result;   // final RGBA of each path
-  uint32_t* q[2];   // extension ray queues (path ids)
-  uint32_t* qs;     // shadow queue (path ids)
-  uint32_t* counts; // [0],[1]: extension queue sizes, [2]: shadow queue size
+  uint32_t* pixel;  // pixel index of the slot's sample
+  uint32_t* frame;  // progressive frame number of the slot's sample
+  int* bounce;      // bounces so far (misptdl.glsl `bounce`)
+  uint32_t* q[2];   // extension queues (slot ids)
+  uint32_t* qs[2];  // shadow queues
+  uint32_t* qh;     // hit queue
+  uint32_t* qm;     // miss queue
+  uint32_t* qfree;  // free slots
+  uint32_t* counts; // kCnt*
+  unsigned long long* items_next;  // next work item to start
   // [0] closest-hit rays, [1] shadow rays, [2] aborted traversals,
   // [3]/[4] nodes visited / triangles tested by closest-hit rays, [5]/[6] by shadow rays
   unsigned long long* stats;
+  double* accum;    // RGBA sums per pixel (FP64)
   uint32_t capacity;
 };
 
@@ -54,12 +80,14 @@ struct LaunchCfg {
   int shade_blocks = 0, shade_threads = 128;
 };
 
-void launch_generate(const WaveParams& p, const PathBuf& b, cudaStream_t st);
-void launch_extend(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
-void launch_connect(const DevScene& s, const PathBuf& b, bool count, const LaunchCfg& lc, cudaStream_t st);
-void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int cur, int depth,
+void launch_init_pool(const PathBuf& b, cudaStream_t st);
+void launch_regen(const WaveParams& p, const PathBuf& b, int next, cudaStream_t st);
+void launch_extend(const DevScene& s, const WaveParams& p, const PathBuf& b, int cur, bool count, const LaunchCfg& lc,
+                   cudaStream_t st);
+void launch_connect(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
+void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int next,
                   const LaunchCfg& lc, cudaStream_t st);
-void launch_accumulate(const WaveParams& p, const PathBuf& b, double4* accum, cudaStream_t st);
+void launch_shade_miss(const DevIbl& e, const WaveParams& p, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
 
 // kernel-level queries (device buffers)

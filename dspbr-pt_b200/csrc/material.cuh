@@ -210,7 +210,7 @@ DEV float ior_to_f0(float t, float i) {
 }
 DEV v3 substrate_f0(float ior) { return mk(ior_to_f0(fmaxf(ior, 1.f), 1.f)); }
 
-DEV v3 film_reflectance(float outside, float film_ior, v3 base_f0, float thick_nm, float cos1) {
+NOINL v3 film_reflectance(float outside, float film_ior, v3 base_f0, float thick_nm, float cos1) {
   float fi = clampf(film_ior, 1.f, 2.5f);
   float c1 = sat(cos1);
   float c2sq = 1.f - outside / fi * (outside / fi) * (1.f - c1 * c1);
@@ -372,7 +372,7 @@ DEV v3 eval_thin_transmission(const Closure& c, const Frame& f, v3 n, v3 v, v3 l
 }
 
 // evaluateThickTransmissionScattering_0 (kernel:1151-1241), ior_i = 1
-DEV v3 eval_thick_transmission(const Closure& c, const Frame& f, v3 coeff, v3 n, v3 v, v3 l, float ior_o) {
+NOINL v3 eval_thick_transmission(const Closure& c, const Frame& f, v3 coeff, v3 n, v3 v, v3 l, float ior_o) {
   v3 lv = to_local(f, v), ll = to_local(f, l);
   float nov = fabsf(lv.z), nol = fabsf(ll.z);
   if (nov <= kEps5 || nol <= kEps5 || dot(n, v) * dot(n, l) >= 0.f) return mk(0.f);
@@ -411,7 +411,7 @@ DEV v3 eval_thick_dispersed(const Closure& c, const Frame& f, v3 coeff, v3 n, v3
 }
 
 // evalDielectricTransmission_0 (kernel:1427-1497)
-DEV v3 eval_dielectric_transmission(const Closure& c, const Frame& f, v3 n, v3 v, v3 l) {
+NOINL v3 eval_dielectric_transmission(const Closure& c, const Frame& f, v3 n, v3 v, v3 l) {
   if (dot(n, v) * dot(n, l) > 0.f) return eval_dielectric_specular(c, f, n, v, l);
   if (c.thin > 0.5f) return eval_thin_transmission(c, f, n, v, l);
   TransCoeffs k = transmission_coeffs(c, n, v);
@@ -550,13 +550,13 @@ DEV v3 eval_diffuse_transmission(const Closure& c, v3 n, v3 l) {
   return c.diffuse_transmission_color * kInvPi * fmaxf(fabsf(dot(n, l)), 0.f);
 }
 
-DEV v3 eval_reflected_base(const Closure& c, const Frame& f, v3 n, v3 v, v3 l) {
+NOINL v3 eval_reflected_base(const Closure& c, const Frame& f, v3 n, v3 v, v3 l) {
   return eval_diffuse(c, n, v, l) + eval_base_specular(c, f, n, v, l) + eval_sheen(c, n, v, l);
 }
 
 // evalMaterialBsdfMixture_0 (kernel:2045-2089): returns BSDF * |cos|.  The
 // adapter passes the same shading normal as base and clearcoat normal.
-DEV v3 bsdf_eval(const Closure& c, v3 n, v3 v, v3 l) {
+NOINL v3 bsdf_eval(const Closure& c, v3 n, v3 v, v3 l) {
   Frame f = aniso_frame(n, c.aniso_tangent);
   if (!(dot(n, v) * dot(n, l) > 0.f))
     return eval_diffuse_transmission(c, n, l) + eval_dielectric_transmission(c, f, n, v, l);
@@ -617,7 +617,7 @@ DEV float dielectric_view_fresnel_max(const Closure& c, v3 n, v3 v) {
   return max3(schlick(c.dielectric_f0, mk(c.dielectric_f90), fmaxf(dot(n, v), 0.f)));
 }
 
-DEV float bsdf_pdf_f(const Closure& c, const Frame& f, v3 n, v3 v, v3 d) {
+NOINL float bsdf_pdf_f(const Closure& c, const Frame& f, v3 n, v3 v, v3 d) {
   float nd = dot(n, d);
   float nol = fmaxf(nd, 0.f);
   float ccnol = fmaxf(dot(n, d), 0.f);
@@ -727,7 +727,7 @@ DEV v3 safe_refract(v3 i, v3 n, float eta) {
 }
 
 // sampleDielectricTransmission_0 (kernel:2881-3145), currentMediumIor = 1
-DEV BsdfSample sample_dielectric_transmission(const Closure& c, const Frame& f, v3 n, v3 v, float u0, float u1,
+NOINL BsdfSample sample_dielectric_transmission(const Closure& c, const Frame& f, v3 n, v3 v, float u0, float u1,
                                               float event_u) {
   BsdfSample s;
   if (c.thin < 0.5f && fabsf(1.f - c.ior) <= kEps4) {
@@ -797,7 +797,7 @@ DEV BsdfSample sample_dielectric_transmission(const Closure& c, const Frame& f, 
 
 // Finishes a sample whose direction came from a reflection-side lobe
 // (kernel:3480-3567 / 3284-3364): value and pdf of the whole mixture.
-DEV BsdfSample finish_reflection_sample(const Closure& c, const Frame& f, v3 n, v3 v, v3 d, float spec, float u0,
+NOINL BsdfSample finish_reflection_sample(const Closure& c, const Frame& f, v3 n, v3 v, v3 d, float spec, float u0,
                                         float u1, bool thin_path, float crossed, float next_ior) {
   BsdfSample s;
   s.crossed = crossed;
@@ -838,7 +838,7 @@ DEV BsdfSample finish_reflection_sample(const Closure& c, const Frame& f, v3 n, 
 
 // sampleMaterialBsdfMixture_0 (kernel:3200-3567).  rnd = (component, lobe.x,
 // lobe.y, boundary) as PbrRandoms (kernel:3570-3575).
-DEV BsdfSample bsdf_sample(const Closure& c, v3 n, v3 v, float choice, float u0, float u1, float event_u) {
+NOINL BsdfSample bsdf_sample(const Closure& c, v3 n, v3 v, float choice, float u0, float u1, float event_u) {
   Frame f = aniso_frame(n, c.aniso_tangent);
   if (is_thin_transmissive(c)) {
     float tb = thin_base_probability(c, n, v);

@@ -12,6 +12,9 @@
 #include <stdint.h>
 
 #define DEV __device__ __forceinline__
+// Large, multiply-called device functions stay out of line: one copy of the
+// code keeps the instruction cache of divergent shading warps from thrashing.
+#define NOINL static __device__ __noinline__
 #define HD __host__ __device__ __forceinline__
 
 namespace dspbr {
