@@ -76,7 +76,11 @@ struct dspbr_scene {
   dspbr_ctx* ctx = nullptr;
   DevBuf<float4> nodes, tris, verts, materials;
   DevBuf<uint32_t> indices;
+  DevBuf<uint8_t> tri_class;
   uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
+  std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
+  std::vector<float> host_materials;
+  uint32_t num_classes = 0;
   bool boxes_finite = true;
   double bvh_build_ms = 0, upload_ms = 0;
   DevScene view() const {
@@ -84,10 +88,13 @@ struct dspbr_scene {
     s.nodes = nodes.p; s.tris = tris.p; s.verts = verts.p; s.indices = indices.p; s.materials = materials.p;
     s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
     s.num_materials = int(num_materials);
+    s.tri_class = tri_class.p;
     s.boxes_finite = boxes_finite ? 1 : 0;
     return s;
   }
-  uint64_t bytes() const { return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes(); }
+  uint64_t bytes() const {
+    return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes();
+  }
 };
 
 struct dspbr_ibl {
@@ -189,6 +196,46 @@ static int settle(dspbr_ctx* c) {
   int rc = c->worker_rc;
   c->worker_rc = 0;
   return rc;
+}
+
+// Shading classes.  Surface hits are queued per class so that a warp of the
+// shading kernel runs one material code path (the DSPBR closure branches on
+// these features).  The class only orders the work; results do not depend on it.
+static uint32_t material_signature(const float* m) {
+  // record offsets: material.ts MaterialData layout (68 floats)
+  uint32_t sig = 0;
+  if (m[7] > 0.f) sig |= 1u;                                   // transmission
+  if (m[7] > 0.f && m[35] > 0.5f) sig |= 2u;                   // thin-walled transmission
+  if (m[40] > 0.f) sig |= 4u;                                  // iridescence
+  if (m[16] > 0.f || m[17] > 0.f || m[18] > 0.f) sig |= 8u;    // sheen
+  if (m[24] > 0.f) sig |= 16u;                                 // clearcoat
+  if (m[3] >= 1.f) sig |= 32u;                                 // pure metal
+  if (m[64] > 0.f) sig |= 64u;                                 // dispersion
+  if (m[26] > 0.f) sig |= 128u;                                // diffuse transmission
+  if (m[5] != 0.f) sig |= 256u;                                // anisotropy
+  if (m[8] < 1.f || m[27] > 0.f) sig |= 512u;                  // cutout
+  return sig;
+}
+
+static int classify_triangles(Status& s, dspbr_scene* sc, cudaStream_t st) {
+  std::vector<uint32_t> sigs;
+  std::vector<uint8_t> mat_class(sc->num_materials);
+  for (uint32_t m = 0; m < sc->num_materials; ++m) {
+    uint32_t sig = material_signature(sc->host_materials.data() + size_t(m) * 68);
+    size_t k = std::find(sigs.begin(), sigs.end(), sig) - sigs.begin();
+    if (k == sigs.size()) sigs.push_back(sig);
+    mat_class[m] = uint8_t(k % kNumClasses);
+  }
+  sc->num_classes = uint32_t(std::min<size_t>(sigs.size(), kNumClasses));
+  std::vector<uint8_t> cls(std::max<size_t>(sc->tri_material.size(), 1), 0);
+  for (size_t t = 0; t < sc->tri_material.size(); ++t) cls[t] = mat_class[sc->tri_material[t]];
+  if (!sc->tri_class.p) {
+    int rc = s.cuda(sc->tri_class.alloc(cls.size()), "alloc triangle classes");
+    if (rc) return rc;
+  }
+  int rc = s.cuda(cudaMemcpyAsync(sc->tri_class.p, cls.data(), cls.size(), cudaMemcpyHostToDevice, st), "upload classes");
+  if (rc) return rc;
+  return s.cuda(cudaStreamSynchronize(st), "upload classes");
 }
 
 extern "C" {
@@ -365,6 +412,14 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     delete sc;
     return rc;
   }
+  sc->host_materials.assign(materials, materials + size_t(num_materials) * 68);
+  sc->tri_material.resize(sc->num_tris);
+  for (uint32_t t = 0; t < sc->num_tris; ++t)
+    sc->tri_material[t] = uint32_t(vertices[size_t(indices[3 * size_t(t)]) * 20 + 3]);
+  if ((rc = classify_triangles(s, sc, c->stream))) {
+    delete sc;
+    return rc;
+  }
   if (num_bvh_indices)
     launch_gather_tris(sc->verts.p, sc->indices.p, remap.p, num_bvh_indices, sc->num_tris, sc->tris.p, c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) || (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload"))) {
@@ -384,6 +439,8 @@ int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32
   TRY_CUDA(s, cudaMemcpyAsync(sc->materials.p + size_t(first) * 17, materials, size_t(count) * 272,
                               cudaMemcpyHostToDevice, sc->ctx->stream), "update materials");
   TRY_CUDA(s, cudaStreamSynchronize(sc->ctx->stream), "update materials");
+  std::copy(materials, materials + size_t(count) * 68, sc->host_materials.begin() + size_t(first) * 68);
+  { int rc_ = classify_triangles(s, sc, sc->ctx->stream); if (rc_) return rc_; }
   dspbr_reset(sc->ctx);
   return DSPBR_OK;
 }
@@ -596,7 +653,7 @@ static int ensure_paths(dspbr_ctx* c, uint32_t cap) {
       (rc = s.cuda(c->pixel.alloc(cap), "paths")) || (rc = s.cuda(c->frame.alloc(cap), "paths")) ||
       (rc = s.cuda(c->q0.alloc(cap), "queues")) || (rc = s.cuda(c->q1.alloc(cap), "queues")) ||
       (rc = s.cuda(c->qs0.alloc(cap), "queues")) || (rc = s.cuda(c->qs1.alloc(cap), "queues")) ||
-      (rc = s.cuda(c->qh.alloc(cap), "queues")) || (rc = s.cuda(c->qm.alloc(cap), "queues")) ||
+      (rc = s.cuda(c->qh.alloc(size_t(cap) * kNumClasses), "queues")) || (rc = s.cuda(c->qm.alloc(cap), "queues")) ||
       (rc = s.cuda(c->qfree.alloc(cap), "queues"))) {
     c->capacity = 0;
     return rc;
@@ -858,7 +915,7 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->upload_ms = c->scene->upload_ms;
   }
   d->device_bytes = c->org.bytes() * 9 + c->rng.bytes() + c->sh_flags.bytes() + c->bounce.bytes() + c->pixel.bytes() +
-                    c->frame.bytes() + c->q0.bytes() * 7 + c->accum.bytes() + c->mean.bytes();
+                    c->frame.bytes() + c->q0.bytes() * 6 + c->qh.bytes() + c->accum.bytes() + c->mean.bytes();
   d->last_render_ms = c->last_render_ms;
   d->nodes_closest = st[3];
   d->tris_closest = st[4];

@@ -30,6 +30,7 @@ struct DevScene {
   const float4* __restrict__ verts;      // 5 float4 per vertex (20-float record)
   const uint32_t* __restrict__ indices;  // 3 per triangle
   const float4* __restrict__ materials;  // 17 float4 per material (68 floats)
+  const uint8_t* __restrict__ tri_class;  // shading class per mesh triangle
   int num_nodes, num_slots, num_tris, num_materials;
   int boxes_finite;  // every node bound is finite (checked at upload)
 };

@@ -36,6 +36,20 @@ DEV void enqueue(uint32_t* q, uint32_t* counter, bool pred, uint32_t value) {
   if (pred) q[base + __popc(m & ((1u << lane) - 1u))] = value;
 }
 
+// Append to one of several queues (queue `key` starts at q + key * stride):
+// lanes with the same key share one atomic.
+DEV void enqueue_keyed(uint32_t* q, uint32_t* counters, uint32_t stride, bool pred, int key, uint32_t value) {
+  if (!__ballot_sync(0xffffffffu, pred)) return;
+  int k = pred ? key : -1;
+  unsigned peers = __match_any_sync(0xffffffffu, k);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if (pred && lane == leader) base = atomicAdd(counters + key, uint32_t(__popc(peers)));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (pred) q[size_t(key) * stride + base + __popc(peers & ((1u << lane) - 1u))] = value;
+}
+
 DEV void count_warp(unsigned long long* ctr, bool pred) {
   unsigned m = __ballot_sync(0xffffffffu, pred);
   if ((threadIdx.x & 31) == 0 && m) atomicAdd(ctr, (unsigned long long)__popc(m));
@@ -82,10 +96,10 @@ __global__ void k_regen(WaveParams p, PathBuf b, int next) {
   const unsigned long long first = *b.items_next;
   uint32_t* q = b.q[next];
   uint32_t* cnt = b.counts + next;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x < kNumClasses) {
     // hit / miss queues of the next extend; shade_miss and shade read them before
-    b.counts[kCntMiss] = 0;
-    b.counts[kCntHit] = 0;
+    b.counts[kCntHit0 + threadIdx.x] = 0;
+    if (threadIdx.x == 0) b.counts[kCntMiss] = 0;
   }
   for (uint32_t base = blockIdx.x * blockDim.x; base < nfree; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
@@ -144,6 +158,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBu
     uint32_t i = base + threadIdx.x;
     bool aborted = false, is_hit = false, is_miss = false;
     uint32_t nodes = 0, tris = 0, slot = 0;
+    int cls = 0;
     if (i < count) {
       slot = q[i];
       float4 o = b.org[slot], d = b.dir[slot];
@@ -152,10 +167,11 @@ __global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBu
       b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
+      if (is_hit) cls = __ldg(s.tri_class + h.tri);
     }
-    // hits and misses are shaded by different kernels, so shading warps are
-    // either all surface hits or all environment lookups
-    enqueue(b.qh, b.counts + kCntHit, is_hit, slot);
+    // misses go to the environment kernel, hits to the queue of their
+    // material's shading class
+    enqueue_keyed(b.qh, b.counts + kCntHit0, b.capacity, is_hit, cls, slot);
     enqueue(b.qm, b.counts + kCntMiss, is_miss, slot);
     count_warp(b.stats + 0, i < count);
     count_warp(b.stats + 2, aborted);
@@ -364,7 +380,18 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
 }
 
 __global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams p, PathBuf b, int next) {
-  const uint32_t count = b.counts[kCntHit];
+  // the class queues, read as one sequence in class order
+  __shared__ uint32_t start[kNumClasses + 1];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int k = 0; k < kNumClasses; ++k) {
+      start[k] = acc;
+      acc += b.counts[kCntHit0 + k];
+    }
+    start[kNumClasses] = acc;
+  }
+  __syncthreads();
+  const uint32_t count = start[kNumClasses];
   uint32_t* qn = b.q[next];
   uint32_t* cn = b.counts + next;
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -372,7 +399,10 @@ __global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams 
     bool cont = false, shadow = false;
     uint32_t slot = 0;
     if (i < count) {
-      slot = b.qh[i];
+      int k = 0;
+#pragma unroll
+      for (int j = 1; j < kNumClasses; ++j) k += i >= start[j] ? 1 : 0;
+      slot = b.qh[size_t(k) * b.capacity + (i - start[k])];
       cont = shade_path(s, e, p, b, slot, shadow);
     }
     enqueue(qn, cn, cont, slot);

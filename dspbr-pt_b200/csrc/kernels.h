@@ -38,10 +38,12 @@ enum : int {
   kCntShadow0 = 2,  // NEE shadow queues (ping-pong)
   kCntShadow1 = 3,
   kCntMiss = 4,     // paths whose extension ray left the scene
-  kCntHit = 5,      // paths whose extension ray hit a triangle
   kCntFree = 6,     // free path slots
-  kCntNum = 16
+  kCntHit0 = 8,     // paths whose extension ray hit a triangle, one queue per shading class
+  kCntNum = 32
 };
+constexpr int kNumClasses = 16;
+static_assert(kCntHit0 + kNumClasses <= kCntNum, "counter block too small");
 
 // Structure-of-arrays state of a pool of path slots.  A render call streams
 // its work items (pixel samples) through the pool: a path that terminates
@@ -63,7 +65,7 @@ struct PathBuf {
   int* bounce;      // bounces so far (misptdl.glsl `bounce`)
   uint32_t* q[2];   // extension queues (slot ids)
   uint32_t* qs[2];  // shadow queues
-  uint32_t* qh;     // hit queue
+  uint32_t* qh;     // hit queues: class k at qh + k * capacity
   uint32_t* qm;     // miss queue
   uint32_t* qfree;  // free slots
   uint32_t* counts; // kCnt*
