@@ -260,14 +260,21 @@ def run_gpu_arm(args):
     #      one frame, read back of the accumulation buffer (D2H) ----
     cam = PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near)
     v.resetAccumulation()
-    e2e_steps = max(1, min(args.steps, 5))
+    img = v.allocReadbackBuffer()  # the caller's frame buffer, page-locked, reused every step
+    e2e_steps = max(1, min(args.steps, 10))
     d3 = v.diagnostics
+    parts = np.zeros(3)
     barrier(dist)
     t0 = time.perf_counter()
     for k in range(e2e_steps):
+        ta = time.perf_counter()
         v.setCamera(cam)
+        tb = time.perf_counter()
         v.start(1)
-        img = v.readAccumulation()
+        tc = time.perf_counter()
+        v.readAccumulation(out=img)
+        td = time.perf_counter()
+        parts += (tb - ta, tc - tb, td - tc)
     t1 = time.perf_counter()
     d4 = v.diagnostics
     rays_e2e = (d4["rays_primary"] + d4["rays_extension"] + d4["rays_shadow"]) - \
@@ -275,6 +282,8 @@ def run_gpu_arm(args):
     e2e_t = reduce_max(dist, t1 - t0)
     e2e_rays = reduce_sum(dist, float(rays_e2e))
     e2e_value = e2e_rays / e2e_t / 1e6
+    e2e_parts = {"set_camera_ms": 1e3 * parts[0] / e2e_steps, "render_1_frame_ms": 1e3 * parts[1] / e2e_steps,
+                 "read_accumulation_ms": 1e3 * parts[2] / e2e_steps}
     cs = clocks.summary()
 
     if rank == 0:
@@ -289,7 +298,8 @@ def run_gpu_arm(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene + env map, no assets)",
             "config": config_of(sc),
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 64 + 8 + 4 * 52,
-                    "d2h_bytes_per_step": int(img.nbytes), "steps": e2e_steps},
+                    "d2h_bytes_per_step": int(img.nbytes), "steps": e2e_steps,
+                    "per_step": e2e_parts},
             "gpu_launches": gpu_launches,
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -144,6 +144,8 @@ struct dspbr_ctx {
   int worker_rc = 0;
   DevBuf<double4> accum;
   DevBuf<float4> mean;
+  float* stage = nullptr;  // page-locked staging for readback into pageable memory
+  size_t stage_bytes = 0;
   uint64_t sample_count = 0;
   uint64_t rays_primary = 0;
   double last_render_ms = 0;
@@ -310,6 +312,7 @@ int dspbr_destroy(dspbr_ctx* c) {
   for (auto e : c->ring_ev)
     if (e) cudaEventDestroy(e);
   if (c->ring) cudaFreeHost(c->ring);
+  if (c->stage) cudaFreeHost(c->stage);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DSPBR_OK;
@@ -876,6 +879,26 @@ int dspbr_poll(dspbr_ctx* c, int* done) {
   return dspbr_wait(c);
 }
 
+// Host copy with several threads: a single thread copies well below the
+// host memory bandwidth.
+static void parallel_copy(void* dst, const void* src, size_t bytes) {
+  const size_t kChunk = size_t(4) << 20;
+  unsigned nt = std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 8u);
+  if (bytes < 2 * kChunk || nt < 2) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  size_t per = (bytes + nt - 1) / nt;
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; ++i) {
+    size_t o = size_t(i) * per;
+    if (o >= bytes) break;
+    th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(per, bytes - o)); });
+  }
+  std::memcpy(dst, src, std::min(per, bytes));
+  for (auto& t : th) t.join();
+}
+
 int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c || !rgba) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
@@ -886,9 +909,44 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
   launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
-  TRY_CUDA(s, cudaMemcpyAsync(rgba, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
+  const size_t bytes = npix * 16;
+  cudaPointerAttributes attr{};
+  bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (pinned) {
+    TRY_CUDA(s, cudaMemcpyAsync(rgba, c->mean.p, bytes, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
+    TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read accumulation");
+    return DSPBR_OK;
+  }
+  if (c->stage_bytes < bytes) {
+    if (c->stage) cudaFreeHost(c->stage);
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+    TRY_CUDA(s, cudaHostAlloc(reinterpret_cast<void**>(&c->stage), bytes, cudaHostAllocDefault), "alloc staging");
+    c->stage_bytes = bytes;
+  }
+  TRY_CUDA(s, cudaMemcpyAsync(c->stage, c->mean.p, bytes, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read accumulation");
+  parallel_copy(rgba, c->stage, bytes);
   return DSPBR_OK;
+}
+
+int dspbr_host_alloc(dspbr_ctx* c, size_t bytes, void** out) {
+  if (!c || !out || bytes == 0) return DSPBR_ERR_INVALID;
+  *out = nullptr;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaHostAlloc(out, bytes, cudaHostAllocDefault), "host alloc");
+  return DSPBR_OK;
+}
+
+int dspbr_host_free(dspbr_ctx* c, void* ptr) {
+  if (!ptr) return DSPBR_ERR_INVALID;
+  cudaError_t e = cudaFreeHost(ptr);
+  if (e == cudaSuccess) return DSPBR_OK;
+  if (c) return c->st().cuda(e, "host free");
+  cudaGetLastError();
+  return DSPBR_ERR_CUDA;
 }
 
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {

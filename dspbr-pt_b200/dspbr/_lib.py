@@ -96,6 +96,8 @@ SIGNATURES = {
     "dspbr_poll": (C.c_int, [_V, _I]),
     "dspbr_wait": (C.c_int, [_V]),
     "dspbr_read_accum": (C.c_int, [_V, _F, C.c_size_t]),
+    "dspbr_host_alloc": (C.c_int, [_V, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "dspbr_host_free": (C.c_int, [_V, _V]),
     "dspbr_get_diagnostics": (C.c_int, [_V, C.POINTER(Diag)]),
     "dspbr_set_wave_paths": (C.c_int, [_V, C.c_uint32]),
     "dspbr_set_counting": (C.c_int, [_V, C.c_int]),

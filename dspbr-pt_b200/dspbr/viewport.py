@@ -79,6 +79,17 @@ class Context:
     def check(self, rc):
         check(rc, self.h)
 
+    def host_array(self, shape, dtype=np.float32) -> np.ndarray:
+        """numpy array over page-locked host memory (dspbr_host_alloc)."""
+        import weakref
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = C.c_void_p()
+        self.check(self.lib.dspbr_host_alloc(self.h, n, C.byref(p)))
+        raw = (C.c_byte * n).from_address(p.value)
+        # freed with the buffer, also after the context is closed
+        weakref.finalize(raw, self.lib.dspbr_host_free, None, C.c_void_p(p.value))
+        return np.frombuffer(raw, dtype=dtype).reshape(shape)
+
 
 class DeviceScene:
     """Scene resident on the device (dspbr_scene)."""
@@ -326,11 +337,25 @@ class PathtracingViewport:
         self.ctx.check(self.ctx.lib.dspbr_reset(self.ctx.h))
         self._emit_diag()
 
-    def readAccumulation(self) -> np.ndarray:
-        """Running mean, (height, width, 4) float32, row 0 = bottom row."""
-        out = np.zeros((self.height, self.width, 4), np.float32)
+    def readAccumulation(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Running mean, (height, width, 4) float32, row 0 = bottom row.
+
+        With `out` (a C-contiguous float32 array of that shape, e.g. from
+        allocReadbackBuffer()) the image is written there and `out` returned;
+        otherwise a new array is returned."""
+        shape = (self.height, self.width, 4)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError(f"readAccumulation: out must be a C-contiguous float32 array of shape {shape}")
         self.ctx.check(self.ctx.lib.dspbr_read_accum(self.ctx.h, fptr(out), out.size))
         return out
+
+    def allocReadbackBuffer(self) -> np.ndarray:
+        """A (height, width, 4) float32 array in page-locked host memory: the
+        readback into it is a single device-to-host DMA.  Freed when the array
+        is garbage collected."""
+        return self.ctx.host_array((self.height, self.width, 4))
 
     @property
     def diagnostics(self) -> dict:

@@ -165,6 +165,12 @@ int dspbr_wait(dspbr_ctx* ctx);
 /* readAccumulation (absent in the reference, which only displays): running
  * mean RGBA32F, width*height*4 floats, row 0 = bottom row (gl_FragCoord.y 0.5). */
 int dspbr_read_accum(dspbr_ctx* ctx, float* rgba, size_t num_floats);
+/* Page-locked host memory for readback buffers.  dspbr_read_accum into such
+ * a buffer is one device-to-host DMA; into ordinary memory it goes through an
+ * internal page-locked staging buffer.  dspbr_host_free accepts ctx == NULL
+ * (for buffers that outlive their context). */
+int dspbr_host_alloc(dspbr_ctx* ctx, size_t bytes, void** out);
+int dspbr_host_free(dspbr_ctx* ctx, void* ptr);
 int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
 /* paths per wave (0 = default 2^21); the wave covers min(frames, paths/pixels)
  * samples of every pixel.  Set by the autotuner. */

@@ -338,6 +338,12 @@ def test_progressive_accumulation_and_reset():
     v = _viewport(sc, 48, 32, {"maxBounces": 4})
     v.start(3)
     a = v.readAccumulation()
+    # readback into page-locked memory (one DMA) gives the same bytes
+    pinned = v.allocReadbackBuffer()
+    assert v.readAccumulation(out=pinned) is pinned
+    np.testing.assert_array_equal(pinned, a)
+    with pytest.raises(ValueError):
+        v.readAccumulation(out=np.zeros((32, 48, 3), np.float32))
     v.start(5)  # continues to 5 samples
     assert v.diagnostics["sample_count"] == 5
     b = v.readAccumulation()
