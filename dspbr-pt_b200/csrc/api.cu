@@ -9,186 +9,59 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "dspbr.h"
+#include "engine.h"
+#include "host.h"
 #include "kernels.h"
+#include "objects.h"
 
 using namespace dspbr;
 
-namespace {
-
-template <class T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  ~DevBuf() { reset(); }
-  void reset() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  cudaError_t alloc(size_t count) {
-    reset();
-    if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
-    if (e == cudaSuccess) n = count;
-    else p = nullptr;
-    return e;
-  }
-  size_t bytes() const { return n * sizeof(T); }
-};
-
-struct Status {
-  std::string* err;
-  int fail(int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    std::vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    if (err) *err = buf;
-    return code;
-  }
-  int cuda(cudaError_t e, const char* what) {
-    if (e == cudaSuccess) return DSPBR_OK;
-    cudaGetLastError();
-    return fail(e == cudaErrorMemoryAllocation ? DSPBR_ERR_OOM : DSPBR_ERR_CUDA, "%s: %s", what,
-                cudaGetErrorString(e));
-  }
-};
-
-#define TRY_CUDA(st, expr, what)                 \
-  do {                                           \
-    int rc_ = (st).cuda((expr), (what));         \
-    if (rc_ != DSPBR_OK) return rc_;             \
-  } while (0)
-
-double now_ms() {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+namespace dspbr {
+WaveParams make_job_params(const dspbr_params& q, const float matrix[16], float fov, float near_plane, int width,
+                           int height, bool has_ibl, uint32_t frame_base) {
+  WaveParams p{};
+  double film = std::tan(double(fov) * 0.5 * M_PI / 180.0) * double(near_plane);
+  for (int col = 0; col < 3; ++col)
+    for (int r = 0; r < 3; ++r) p.cam.m[col * 3 + r] = matrix[col * 4 + r];
+  p.cam.pos[0] = matrix[12]; p.cam.pos[1] = matrix[13]; p.cam.pos[2] = matrix[14];
+  p.cam.film_height = float(film);
+  p.cam.focal = near_plane;
+  p.cam.inv_res[0] = float(1.0 / width);
+  p.cam.inv_res[1] = float(1.0 / height);
+  p.cam.width = width;
+  p.cam.height = height;
+  p.npix = width * height;
+  p.frame_base = frame_base;
+  p.max_bounces = q.max_bounces;
+  p.rng_pcg = q.rng == DSPBR_RNG_PCG;
+  p.seed = q.seed;
+  p.use_ibl = q.use_ibl ? 1 : 0;
+  p.bg_from_ibl = q.background_from_ibl ? 1 : 0;
+  p.env_mode = q.env_sampling == DSPBR_ENV_CDF ? 1 : 0;
+  p.lean = q.profile == DSPBR_PROFILE_LEAN;
+  p.has_ibl = has_ibl;
+  p.ibl_rot = float(double(q.ibl_rotation_deg) / 180.0 * M_PI);
+  p.bg_color = make_float4(q.background_color[0], q.background_color[1], q.background_color[2], q.background_color[3]);
+  p.ray_eps = q.ray_eps;
+  p.clamp_threshold = q.clamp_threshold;
+  p.rr_prob = q.rr_termination_prob;
+  p.rr_factor = 1.0f / (1.0f - q.rr_termination_prob);
+  p.rr_start = q.rr_start_depth;
+  p.pl_pos = make_float4(q.point_light_position[0], q.point_light_position[1], q.point_light_position[2],
+                         q.point_light_position[3]);
+  p.pl_emis = make_float4(q.point_light_emission[0], q.point_light_emission[1], q.point_light_emission[2],
+                          q.point_light_emission[3]);
+  return p;
 }
 
-}  // namespace
+}  // namespace dspbr
 
-struct dspbr_scene {
-  dspbr_ctx* ctx = nullptr;
-  DevBuf<float4> nodes, tris, verts, materials;
-  DevBuf<uint32_t> indices;
-  DevBuf<uint8_t> tri_class;
-  uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
-  std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
-  std::vector<float> host_materials;
-  uint32_t num_classes = 0;
-  bool boxes_finite = true;
-  double bvh_build_ms = 0, upload_ms = 0;
-  DevScene view() const {
-    DevScene s;
-    s.nodes = nodes.p; s.tris = tris.p; s.verts = verts.p; s.indices = indices.p; s.materials = materials.p;
-    s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
-    s.num_materials = int(num_materials);
-    s.tri_class = tri_class.p;
-    s.boxes_finite = boxes_finite ? 1 : 0;
-    return s;
-  }
-  uint64_t bytes() const {
-    return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes();
-  }
-};
-
-struct dspbr_ibl {
-  dspbr_ctx* ctx = nullptr;
-  DevBuf<float4> rgba;
-  DevBuf<float> pdf, cdf, ypdf, ycdf, alias_prob, lum, rowsum;
-  DevBuf<int> alias_idx;
-  DevBuf<double> total;
-  double total_sum = 0;
-  int w = 0, h = 0;
-  DevIbl view() const {
-    DevIbl e;
-    e.rgba = rgba.p; e.pdf = pdf.p; e.cdf = cdf.p; e.ypdf = ypdf.p; e.ycdf = ycdf.p;
-    e.alias_prob = alias_prob.p; e.alias_idx = alias_idx.p; e.w = w; e.h = h;
-    return e;
-  }
-};
-
-struct dspbr_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::string err;
-  dspbr_params params{};
-  float matrix[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
-  float fov = 45.f, near_plane = 0.01f;
-  bool has_camera = false;
-  int width = 0, height = 0;
-  dspbr_scene* scene = nullptr;
-  dspbr_ibl* ibl = nullptr;
-  uint32_t wave_paths = 1u << 21;
-  // path pool
-  uint32_t capacity = 0;
-  DevBuf<float4> org, dir, weight, rad, hit, sh_dir, sh_c, pl_dir, pl_c;
-  DevBuf<uint64_t> rng;
-  DevBuf<int> sh_flags, bounce;
-  DevBuf<uint32_t> pixel, frame, q0, q1, qs0, qs1, qh, qm, qfree, counts;
-  DevBuf<unsigned long long> stats, items_next;
-  // live-path counts copied back after each iteration, read kLookahead
-  // iterations later to end the host loop
-  static constexpr int kRing = 8, kLookahead = 4;
-  uint32_t* ring = nullptr;  // pinned
-  cudaEvent_t ring_ev[kRing] = {};
-  // render_async: the iteration loop runs on a worker thread
-  std::thread worker;
-  std::atomic<bool> worker_done{true};
-  int worker_rc = 0;
-  DevBuf<double4> accum;
-  DevBuf<float4> mean;
-  float* stage = nullptr;  // page-locked staging for readback into pageable memory
-  size_t stage_bytes = 0;
-  uint64_t sample_count = 0;
-  uint64_t rays_primary = 0;
-  double last_render_ms = 0;
-  bool pending = false;
-  bool counting = false;
-  bool profiling = false;
-  // profiling: event pairs per launch, resolved at dspbr_wait
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, int>> ev_marks;  // (kind, first event index)
-  size_t ev_used = 0;
-  double kind_ms[3] = {0, 0, 0};
-  uint64_t kind_launches[4] = {0, 0, 0, 0};
-  Status st() { return Status{&err}; }
-  cudaEvent_t next_event() {
-    if (ev_used == ev_pool.size()) {
-      cudaEvent_t e;
-      cudaEventCreate(&e);
-      ev_pool.push_back(e);
-    }
-    return ev_pool[ev_used++];
-  }
-  void mark_begin(int kind) {
-    if (!profiling) return;
-    ev_marks.push_back({kind, int(ev_used)});
-    cudaEventRecord(next_event(), stream);
-  }
-  void mark_end() {
-    if (profiling) cudaEventRecord(next_event(), stream);
-  }
-  void resolve_marks() {
-    for (auto& m : ev_marks) {
-      if (size_t(m.second) + 1 >= ev_used) break;
-      float ms = 0;
-      cudaEventElapsedTime(&ms, ev_pool[m.second], ev_pool[m.second + 1]);
-      kind_ms[m.first] += ms;
-    }
-    ev_marks.clear();
-    ev_used = 0;
-  }
-  ~dspbr_ctx() {
-    for (auto e : ev_pool) cudaEventDestroy(e);
-  }
-};
 
 // Joins the worker of a render_async call, so that the caller's next stream
 // operation is ordered after all of that render's launches.  Returns the
@@ -283,20 +156,14 @@ int dspbr_create(int device, dspbr_ctx** out) {
   dspbr_params_default(&c->params);
   Status s = c->st();
   if (s.cuda(cudaSetDevice(device), "cudaSetDevice") || s.cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
-      s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event") ||
-      s.cuda(c->counts.alloc(kCntNum), "counters") || s.cuda(c->stats.alloc(8), "stats") ||
-      s.cuda(c->items_next.alloc(1), "counters") ||
-      s.cuda(cudaMemset(c->stats.p, 0, c->stats.bytes()), "stats") ||
-      s.cuda(cudaHostAlloc(reinterpret_cast<void**>(&c->ring), dspbr_ctx::kRing * sizeof(uint32_t), cudaHostAllocDefault),
-             "pinned status")) {
+      s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event")) {
     dspbr_destroy(c);
     return DSPBR_ERR_CUDA;
   }
-  for (auto& e : c->ring_ev) {
-    if (s.cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) {
-      dspbr_destroy(c);
-      return DSPBR_ERR_CUDA;
-    }
+  c->eng.reset(new Engine(device, c->stream, &c->err));
+  if (int rc = c->eng->init()) {
+    dspbr_destroy(c);
+    return rc;
   }
   *out = c;
   return DSPBR_OK;
@@ -309,9 +176,7 @@ int dspbr_destroy(dspbr_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
-  for (auto e : c->ring_ev)
-    if (e) cudaEventDestroy(e);
-  if (c->ring) cudaFreeHost(c->ring);
+  c->eng.reset();
   if (c->stage) cudaFreeHost(c->stage);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -642,125 +507,9 @@ int dspbr_reset(dspbr_ctx* c) {
   return DSPBR_OK;
 }
 
-static int ensure_paths(dspbr_ctx* c, uint32_t cap) {
-  Status s = c->st();
-  if (c->capacity >= cap) return DSPBR_OK;
-  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "sync");
-  int rc;
-  if ((rc = s.cuda(c->org.alloc(cap), "paths")) || (rc = s.cuda(c->dir.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->weight.alloc(cap), "paths")) || (rc = s.cuda(c->rad.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->hit.alloc(cap), "paths")) || (rc = s.cuda(c->sh_dir.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->sh_c.alloc(cap), "paths")) || (rc = s.cuda(c->pl_dir.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->pl_c.alloc(cap), "paths")) || (rc = s.cuda(c->rng.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->sh_flags.alloc(cap), "paths")) || (rc = s.cuda(c->bounce.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->pixel.alloc(cap), "paths")) || (rc = s.cuda(c->frame.alloc(cap), "paths")) ||
-      (rc = s.cuda(c->q0.alloc(cap), "queues")) || (rc = s.cuda(c->q1.alloc(cap), "queues")) ||
-      (rc = s.cuda(c->qs0.alloc(cap), "queues")) || (rc = s.cuda(c->qs1.alloc(cap), "queues")) ||
-      (rc = s.cuda(c->qh.alloc(size_t(cap) * kNumClasses), "queues")) || (rc = s.cuda(c->qm.alloc(cap), "queues")) ||
-      (rc = s.cuda(c->qfree.alloc(cap), "queues"))) {
-    c->capacity = 0;
-    return rc;
-  }
-  c->capacity = cap;
-  return DSPBR_OK;
-}
-
-static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base, int frames) {
-  WaveParams p{};
-  double film = std::tan(double(c->fov) * 0.5 * M_PI / 180.0) * double(c->near_plane);
-  for (int col = 0; col < 3; ++col)
-    for (int r = 0; r < 3; ++r) p.cam.m[col * 3 + r] = c->matrix[col * 4 + r];
-  p.cam.pos[0] = c->matrix[12]; p.cam.pos[1] = c->matrix[13]; p.cam.pos[2] = c->matrix[14];
-  p.cam.film_height = float(film);
-  p.cam.focal = c->near_plane;
-  p.cam.inv_res[0] = float(1.0 / c->width);
-  p.cam.inv_res[1] = float(1.0 / c->height);
-  p.cam.width = c->width;
-  p.cam.height = c->height;
-  p.npix = c->width * c->height;
-  p.frame_base = frame_base;
-  p.total_items = uint64_t(p.npix) * uint64_t(frames);
-  const dspbr_params& q = c->params;
-  p.max_bounces = q.max_bounces;
-  p.rng_pcg = q.rng == DSPBR_RNG_PCG;
-  p.seed = q.seed;
-  p.use_ibl = q.use_ibl ? 1 : 0;
-  p.bg_from_ibl = q.background_from_ibl ? 1 : 0;
-  p.env_mode = q.env_sampling == DSPBR_ENV_CDF ? 1 : 0;
-  p.lean = q.profile == DSPBR_PROFILE_LEAN;
-  p.has_ibl = c->ibl != nullptr;
-  p.ibl_rot = float(double(q.ibl_rotation_deg) / 180.0 * M_PI);
-  p.bg_color = make_float4(q.background_color[0], q.background_color[1], q.background_color[2], q.background_color[3]);
-  p.ray_eps = q.ray_eps;
-  p.clamp_threshold = q.clamp_threshold;
-  p.rr_prob = q.rr_termination_prob;
-  p.rr_factor = 1.0f / (1.0f - q.rr_termination_prob);
-  p.rr_start = q.rr_start_depth;
-  p.pl_pos = make_float4(q.point_light_position[0], q.point_light_position[1], q.point_light_position[2],
-                         q.point_light_position[3]);
-  p.pl_emis = make_float4(q.point_light_emission[0], q.point_light_emission[1], q.point_light_emission[2],
-                          q.point_light_emission[3]);
-  return p;
-}
-
-static PathBuf path_buf(dspbr_ctx* c, uint32_t capacity) {
-  PathBuf b{};
-  b.org = c->org.p; b.dir = c->dir.p; b.weight = c->weight.p; b.rad = c->rad.p; b.rng = c->rng.p; b.hit = c->hit.p;
-  b.sh_dir = c->sh_dir.p; b.sh_c = c->sh_c.p; b.pl_dir = c->pl_dir.p; b.pl_c = c->pl_c.p; b.sh_flags = c->sh_flags.p;
-  b.pixel = c->pixel.p; b.frame = c->frame.p; b.bounce = c->bounce.p;
-  b.q[0] = c->q0.p; b.q[1] = c->q1.p; b.qs[0] = c->qs0.p; b.qs[1] = c->qs1.p; b.qh = c->qh.p; b.qm = c->qm.p;
-  b.qfree = c->qfree.p; b.counts = c->counts.p; b.items_next = c->items_next.p;
-  b.stats = c->stats.p; b.accum = reinterpret_cast<double*>(c->accum.p);
-  b.capacity = capacity;
-  return b;
-}
-
-// The iteration loop of one render call.  Iteration i launches
-//   extend(i&1) -> connect(i&1) -> shade_miss -> shade(->1-(i&1)) -> regen(->1-(i&1))
-// and copies the number of live paths to a pinned ring slot.  The host stays
-// kLookahead iterations ahead of the GPU and stops when a slot reads 0 (no
-// live path and no work item left); `max_iter` bounds the loop in any case.
-static int run_iterations(dspbr_ctx* c, const WaveParams& p, const PathBuf& b, const DevScene& sv, const DevIbl& ev,
-                          uint64_t max_iter) {
-  Status s = c->st();
-  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  LaunchCfg lc;
-  lc.trace_threads = 128;
-  lc.trace_blocks = 148 * 16;
-  lc.shade_threads = 128;
-  lc.shade_blocks = 148 * 8;
-  cudaStream_t st = c->stream;
-  launch_init_pool(b, st);
-  launch_regen(p, b, 0, st);
-  c->kind_launches[3] += 2;
-  const int R = dspbr_ctx::kRing, L = dspbr_ctx::kLookahead;
-  for (uint64_t it = 0; it < max_iter; ++it) {
-    const int cur = int(it & 1);
-    c->mark_begin(0);
-    launch_extend(sv, p, b, cur, c->counting, lc, st);
-    c->mark_end();
-    c->mark_begin(1);
-    launch_connect(sv, b, cur, c->counting, lc, st);
-    c->mark_end();
-    c->mark_begin(2);
-    launch_shade_miss(ev, p, b, lc, st);
-    launch_shade(sv, ev, p, b, cur ^ 1, lc, st);
-    launch_regen(p, b, cur ^ 1, st);
-    c->mark_end();
-    c->kind_launches[0] += 1;
-    c->kind_launches[1] += 1;
-    c->kind_launches[2] += 3;
-    TRY_CUDA(s, cudaMemcpyAsync(c->ring + it % R, b.counts + (cur ^ 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
-             "status copy");
-    TRY_CUDA(s, cudaEventRecord(c->ring_ev[it % R], st), "status event");
-    TRY_CUDA(s, cudaGetLastError(), "render launch");
-    if (it >= uint64_t(L)) {
-      uint64_t j = it - L;
-      TRY_CUDA(s, cudaEventSynchronize(c->ring_ev[j % R]), "render");
-      if (c->ring[j % R] == 0) break;
-    }
-  }
-  return DSPBR_OK;
+static WaveParams make_wave(const dspbr_ctx* c, uint32_t frame_base) {
+  return make_job_params(c->params, c->matrix, c->fov, c->near_plane, c->width, c->height, c->ibl != nullptr,
+                         frame_base);
 }
 
 static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
@@ -772,36 +521,44 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
   if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
   if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  WaveParams p = make_wave(c, uint32_t(c->sample_count + 1), frames);
-  uint32_t pool = uint32_t(std::min<uint64_t>(c->wave_paths, p.total_items));
-  rc = ensure_paths(c, pool);
-  if (rc) return rc;
-  PathBuf b = path_buf(c, pool);
-  DevScene sv = c->scene->view();
-  DevIbl ev{};
-  if (c->ibl) ev = c->ibl->view();
-  // every slot runs its paths back to back: while work items remain all slots
-  // are busy, and a path lives at most max_bounces + 1 iterations
-  uint64_t per_path = uint64_t(p.max_bounces) + 1;
-  uint64_t max_iter = (p.total_items * per_path + pool - 1) / pool + per_path + 2;
+  Engine& E = *c->eng;
+  Job job{};
+  job.p = make_wave(c, uint32_t(c->sample_count + 1));
+  job.s = c->scene->view();
+  if (c->ibl) job.e = c->ibl->view();
+  job.accum = reinterpret_cast<double*>(c->accum.p);
+  const unsigned long long items = uint64_t(job.p.npix) * uint64_t(frames);
+  // pool: up to wave_paths slots, no more than the work needs; it is kept
+  // between renders unless the limit drops below it
+  uint32_t want = uint32_t(std::min<uint64_t>(c->wave_paths, items));
+  if (E.capacity() < want || E.capacity() > c->wave_paths) {
+    if ((rc = E.ensure_pool(want))) return rc;
+  }
+  const uint64_t pool = E.capacity();
+  // every slot runs paths back to back: while work items remain all slots are
+  // busy, and a path lives at most max_bounces + 1 iterations
+  const uint64_t per_path = uint64_t(job.p.max_bounces) + 1;
+  const unsigned long long max_iter = (items * per_path + pool - 1) / pool + per_path + 4;
+  if ((rc = E.set_job(0, job, items)) || (rc = E.set_active({0}))) return rc;
   c->sample_count += uint64_t(frames);
-  c->rays_primary += p.total_items;
+  c->rays_primary += items;
   TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
   c->pending = true;
+  const bool counting = c->counting;
   if (!async) {
-    rc = run_iterations(c, p, b, sv, ev, max_iter);
+    rc = E.run_until_done(0, max_iter, counting);
     if (rc) {
       c->pending = false;
-      c->ev_marks.clear();
-      c->ev_used = 0;
+      E.clear_marks();
       return rc;
     }
     TRY_CUDA(s, cudaEventRecord(c->ev1, c->stream), "event");
     return DSPBR_OK;
   }
   c->worker_done.store(false);
-  c->worker = std::thread([c, p, b, sv, ev, max_iter]() {
-    int r = run_iterations(c, p, b, sv, ev, max_iter);
+  c->worker = std::thread([c, max_iter, counting]() {
+    int r = c->st().cuda(cudaSetDevice(c->device), "cudaSetDevice");
+    if (!r) r = c->eng->run_until_done(0, max_iter, counting);
     if (!r) r = c->st().cuda(cudaEventRecord(c->ev1, c->stream), "event");
     c->worker_rc = r;
     c->worker_done.store(true);
@@ -817,8 +574,7 @@ int dspbr_wait(dspbr_ctx* c) {
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "render");
   if (rc) {
     c->pending = false;
-    c->ev_marks.clear();
-    c->ev_used = 0;
+    c->eng->clear_marks();
     return rc;
   }
   if (c->pending) {
@@ -827,7 +583,7 @@ int dspbr_wait(dspbr_ctx* c) {
     c->last_render_ms = ms;
     c->pending = false;
   }
-  c->resolve_marks();
+  c->eng->resolve_marks();
   return DSPBR_OK;
 }
 
@@ -837,7 +593,7 @@ int dspbr_set_counting(dspbr_ctx* c, int enable) {
   int rc = settle(c);
   if (rc) return rc;
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  TRY_CUDA(s, cudaMemsetAsync(c->stats.p + 3, 0, 4 * sizeof(unsigned long long), c->stream), "counters");
+  TRY_CUDA(s, cudaMemsetAsync(c->eng->stats() + 3, 0, 4 * sizeof(unsigned long long), c->stream), "counters");
   c->counting = enable != 0;
   return DSPBR_OK;
 }
@@ -846,9 +602,9 @@ int dspbr_set_profiling(dspbr_ctx* c, int enable) {
   if (!c) return DSPBR_ERR_INVALID;
   int rc = dspbr_wait(c);
   if (rc) return rc;
-  c->profiling = enable != 0;
-  for (double& v : c->kind_ms) v = 0;
-  for (uint64_t& v : c->kind_launches) v = 0;
+  c->eng->profiling = enable != 0;
+  for (double& v : c->eng->kind_ms) v = 0;
+  for (auto& v : c->eng->kind_launches) v = 0;
   return DSPBR_OK;
 }
 
@@ -956,7 +712,7 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   std::memset(d, 0, sizeof *d);
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  TRY_CUDA(s, cudaMemcpyAsync(st, c->stats.p, sizeof st, cudaMemcpyDeviceToHost, c->stream), "read stats");
+  TRY_CUDA(s, cudaMemcpyAsync(st, c->eng->stats(), sizeof st, cudaMemcpyDeviceToHost, c->stream), "read stats");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read stats");
   d->sample_count = c->sample_count;
   d->width = c->width;
@@ -972,20 +728,19 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->bvh_build_ms = c->scene->bvh_build_ms;
     d->upload_ms = c->scene->upload_ms;
   }
-  d->device_bytes = c->org.bytes() * 9 + c->rng.bytes() + c->sh_flags.bytes() + c->bounce.bytes() + c->pixel.bytes() +
-                    c->frame.bytes() + c->q0.bytes() * 6 + c->qh.bytes() + c->accum.bytes() + c->mean.bytes();
+  d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->mean.bytes();
   d->last_render_ms = c->last_render_ms;
   d->nodes_closest = st[3];
   d->tris_closest = st[4];
   d->nodes_shadow = st[5];
   d->tris_shadow = st[6];
-  d->extend_ms = c->kind_ms[0];
-  d->connect_ms = c->kind_ms[1];
-  d->shade_ms = c->kind_ms[2];
-  d->extend_launches = c->kind_launches[0];
-  d->connect_launches = c->kind_launches[1];
-  d->shade_launches = c->kind_launches[2];
-  d->other_launches = c->kind_launches[3];
+  d->extend_ms = c->eng->kind_ms[0];
+  d->connect_ms = c->eng->kind_ms[1];
+  d->shade_ms = c->eng->kind_ms[2];
+  d->extend_launches = c->eng->kind_launches[0];
+  d->connect_launches = c->eng->kind_launches[1];
+  d->shade_launches = c->eng->kind_launches[2];
+  d->other_launches = c->eng->kind_launches[3];
   return DSPBR_OK;
 }
 
@@ -1097,7 +852,7 @@ int dspbr_camera_rays(dspbr_ctx* c, uint32_t n, const int32_t* xy, const float* 
   if ((rc = up(s, dxy, xy, size_t(n) * 2, c->stream)) || (rc = up(s, dr, r2, size_t(n) * 2, c->stream)) ||
       (rc = s.cuda(dout.alloc(std::max(n, 1u) * size_t(6)), "alloc")))
     return rc;
-  WaveParams p = make_wave(c, 1, 1);
+  WaveParams p = make_wave(c, 1);
   launch_camera_rays(p.cam, n, dxy.p, dr.p, dout.p, c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "camera rays")) || (rc = down(s, rays6, dout, size_t(n) * 6, c->stream)))
     return rc;

@@ -1,0 +1,107 @@
+// Render engine: one path pool, a device job table and the iteration loop
+// over them.  A context's progressive render is one job run to completion; the
+// server keeps many jobs active in one engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "host.h"
+#include "kernels.h"
+
+namespace dspbr {
+
+// The active list travels to the device as a kernel argument: table updates
+// need no staging memory and stay ordered on the engine's stream.
+struct ActiveList {
+  int n;
+  int slot[kMaxJobs];
+};
+
+class Engine {
+ public:
+  Engine(int device, cudaStream_t stream, std::string* err) : device_(device), stream_(stream), err_(err) {}
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Job table, counters and the mapped status record (first use).
+  int init();
+  // Grows the path pool to `capacity` slots.  Only while no job is active.
+  int ensure_pool(uint32_t capacity);
+  // Drops every path: all slots free, queues empty.  Only while no job is active.
+  int reset_pool();
+  uint32_t capacity() const { return capacity_; }
+  size_t pool_bytes() const;
+  void set_launch(const LaunchCfg& lc);
+  const LaunchCfg& launch() const { return lc_; }
+
+  // Table updates, enqueued on the stream (ordered before later iterations).
+  int set_job(int slot, const Job& job, unsigned long long items_total);
+  int cancel_job(int slot);
+  int set_active(const std::vector<int>& order);
+
+  // Enqueues at least `n` iterations (two per graph launch when the graph is
+  // usable) and returns how many were enqueued in `done`.
+  int iterate(int n, bool counting, int* done);
+  // Runs iterations until job `slot` has started all items and has no live
+  // path, keeping `lookahead` steps queued; `max_iter` bounds the loop.
+  int run_until_done(int slot, unsigned long long max_iter, bool counting);
+  bool job_done(int slot) const;
+  const volatile HostStatus* status() const { return h_status_; }
+
+  // Per-kind device time (extend / connect / shade+regen+commit) with events
+  // around every launch, and launch counts.
+  bool profiling = false;
+  double kind_ms[3] = {0, 0, 0};
+  unsigned long long kind_launches[4] = {0, 0, 0, 0};  // extend, connect, shade-side, other
+  void resolve_marks();
+  void clear_marks();
+
+  unsigned long long* stats() const { return stats_.p; }
+  Sched sched() const;
+  PathBuf paths() const;
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  int one_iteration(bool counting);
+  int capture_graph();
+  void drop_graph();
+  cudaEvent_t next_event();
+  void mark_begin(int kind);
+  void mark_end();
+
+  int device_;
+  cudaStream_t stream_;
+  std::string* err_;
+  bool ready_ = false;
+  uint32_t capacity_ = 0;
+  int cur_ = 0;  // parity of the next iteration
+  LaunchCfg lc_;
+  // pool
+  DevBuf<float4> org_, dir_, weight_, rad_, hit_, sh_dir_, sh_c_, pl_dir_, pl_c_;
+  DevBuf<uint64_t> rng_;
+  DevBuf<int> sh_flags_, bounce_;
+  DevBuf<uint32_t> pixel_, frame_, job_, q0_, q1_, qs0_, qs1_, qh_, qm_, qfree_;
+  // job table and counters
+  DevBuf<Job> jobs_;
+  DevBuf<JobState> js_;
+  DevBuf<int> active_;  // kMaxJobs + 1: list, then its length
+  DevBuf<uint32_t> counts_;
+  DevBuf<unsigned long long> cursors_;  // free head, free tail, iteration
+  DevBuf<unsigned long long> stats_;
+  HostStatus* h_status_ = nullptr;
+  HostStatus* d_status_ = nullptr;
+  // two iterations (parity 0 then 1) captured once
+  cudaGraphExec_t graph_ = nullptr;
+  // loop events and profiling events
+  static constexpr int kRing = 8, kLookahead = 4;
+  cudaEvent_t ring_[kRing] = {};
+  std::vector<cudaEvent_t> ev_pool_;
+  std::vector<std::pair<int, int>> ev_marks_;
+  size_t ev_used_ = 0;
+};
+
+}  // namespace dspbr

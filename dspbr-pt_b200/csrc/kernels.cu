@@ -1,21 +1,24 @@
-// Wavefront path tracer with path regeneration.
+// Wavefront path tracer with path regeneration over a table of jobs.
 //
 // The reference evaluates a whole path per fragment (renderer.frag:146-157 ->
-// integrator/misptdl.glsl:34-93).  Here a render call streams its pixel
-// samples through a fixed pool of path slots; every iteration of the host loop
-// runs
-//   extend      closest hit for every live path (bvh.glsl:149-216); hits and
-//               misses go to separate queues,
+// integrator/misptdl.glsl:34-93).  Here the pixel samples of one or many
+// render jobs stream through a fixed pool of path slots; every iteration runs
+//   extend      closest hit for every live path (bvh.glsl:149-216); misses go
+//               to one queue, hits to the queue of their material class,
 //   connect     any-hit test of the NEE shadow rays emitted by the previous
 //               shade; visible contributions are added to the path radiance,
 //   shade_miss  background / MIS-weighted environment (misptdl.glsl:41-46, 84-88),
 //   shade       RR, absorption, emission, BSDF sampling, NEE sample generation
 //               (misptdl.glsl:54-90, renderer.frag:94-123),
-//   regen       new samples (rng_init + calcuateViewRay) into the slots freed
-//               by terminated paths,
+//   regen       new samples (rng_init + calcuateViewRay) of the active jobs,
+//               in priority order, into the slots freed by terminated paths,
+//   commit      job progress, free-list head, queue counter resets and the
+//               status record for the host,
 // so every launch works on a full pool instead of a shrinking per-bounce
-// queue.  Queues are compacted with one atomic per warp (__ballot_sync /
-// __popc); a finished path adds its sample to the pixel's FP64 sums.  The
+// queue, and an iteration is a fixed launch sequence whose arguments never
+// change (it can be captured in a CUDA graph).  Queues are compacted with one
+// atomic per warp (__ballot_sync / __popc, __match_any_sync for keyed
+// queues); a finished path adds its sample to its job's FP64 pixel sums.  The
 // per-path arithmetic and RNG consumption order follow the reference exactly.
 #include <cuda_runtime.h>
 
@@ -69,13 +72,58 @@ DEV Rng load_rng(const WaveParams& p, const PathBuf& b, uint32_t slot) {
   return r;
 }
 
-// A terminated path adds its sample to the pixel sums and frees its slot.
-DEV void finish_path(const PathBuf& b, uint32_t slot, float4 c) {
-  double* a = b.accum + 4 * size_t(b.pixel[slot]);
+// A terminated path adds its sample to its job's pixel sums; the caller
+// frees the slot (free_slots).
+DEV void finish_path(const Job& J, const PathBuf& b, uint32_t slot, float4 c) {
+  double* a = J.accum + 4 * size_t(b.pixel[slot]);
   atomicAdd(a + 0, double(c.x));
   atomicAdd(a + 1, double(c.y));
   atomicAdd(a + 2, double(c.z));
   atomicAdd(a + 3, double(c.w));
+}
+
+// Frees the slots of terminated paths: free-list append (ring buffer, 64-bit
+// cursors) and the live-path count of each job, one atomic per job per warp.
+DEV void free_slots(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot, uint32_t job) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(b.free_tail, (unsigned long long)__popc(m));
+  uint32_t pos = 0;
+  if (lane == leader) pos = uint32_t(base % b.capacity);
+  pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(m & ((1u << lane) - 1u));
+  while (pos >= b.capacity) pos -= b.capacity;
+  if (pred) b.qfree[pos] = slot;
+  unsigned peers = __match_any_sync(0xffffffffu, pred ? int(job) : -1);
+  if (pred && lane == __ffs(peers) - 1) atomicSub(&sc.js[job].live, uint32_t(__popc(peers)));
+}
+
+// Exclusive prefix sum over the block (blockDim.x == kMaxJobs threads).
+DEV unsigned long long block_scan(unsigned long long v, unsigned long long* sh, unsigned long long& total) {
+  const int t = threadIdx.x;
+  sh[t] = v;
+  __syncthreads();
+  for (int off = 1; off < kMaxJobs; off <<= 1) {
+    unsigned long long add = t >= off ? sh[t - off] : 0ull;
+    __syncthreads();
+    sh[t] += add;
+    __syncthreads();
+  }
+  unsigned long long inc = sh[t];
+  total = sh[kMaxJobs - 1];
+  __syncthreads();
+  return inc - v;
+}
+
+// Work items not yet started of active job number `a` (0 beyond the list).
+DEV unsigned long long remaining(const Sched& sc, int a, int n, int& j) {
+  j = -1;
+  if (a >= n) return 0ull;
+  j = sc.active[a];
+  unsigned long long next = sc.js[j].items_next, total = sc.js[j].items_total;
+  return total > next ? total - next : 0ull;
 }
 
 }  // namespace
@@ -85,31 +133,58 @@ __global__ void k_init_pool(PathBuf b) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.capacity; i += gridDim.x * blockDim.x)
     b.qfree[i] = i;
   if (blockIdx.x == 0 && threadIdx.x < kCntNum) {
-    b.counts[threadIdx.x] = threadIdx.x == kCntFree ? b.capacity : 0u;
-    if (threadIdx.x == 0) *b.items_next = 0ull;
+    b.counts[threadIdx.x] = 0u;
+    if (threadIdx.x == 0) {
+      *b.free_head = 0ull;
+      *b.free_tail = b.capacity;
+    }
   }
 }
 
 // ---- regen: new samples in free slots (renderer.frag:146-150) ----------------------------
-__global__ void k_regen(WaveParams p, PathBuf b, int next) {
-  const uint32_t nfree = b.counts[kCntFree];
-  const unsigned long long first = *b.items_next;
+// Free slot i (in free-list order) takes the i-th unstarted work item of the
+// active jobs in priority order.
+__global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int next) {
+  __shared__ unsigned long long scan[kMaxJobs];
+  __shared__ unsigned long long pre[kMaxJobs];
+  __shared__ int act[kMaxJobs];
+  const int n = min(*sc.nactive, kMaxJobs);
+  int j;
+  unsigned long long rem = remaining(sc, threadIdx.x, n, j), total;
+  pre[threadIdx.x] = block_scan(rem, scan, total);
+  act[threadIdx.x] = j;
+  __syncthreads();
+  const unsigned long long head = *b.free_head;
+  const unsigned long long nfree = *b.free_tail - head;
+  const uint32_t avail = uint32_t(min(nfree, total));
+  const uint32_t head_pos = uint32_t(head % b.capacity);
   uint32_t* q = b.q[next];
   uint32_t* cnt = b.counts + next;
-  if (blockIdx.x == 0 && threadIdx.x < kNumClasses) {
-    // hit / miss queues of the next extend; shade_miss and shade read them before
-    b.counts[kCntHit0 + threadIdx.x] = 0;
-    if (threadIdx.x == 0) b.counts[kCntMiss] = 0;
-  }
-  for (uint32_t base = blockIdx.x * blockDim.x; base < nfree; base += gridDim.x * blockDim.x) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < avail; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
-    unsigned long long item = first + i;
-    bool valid = i < nfree && item < p.total_items;
+    bool valid = i < avail;
     uint32_t slot = 0;
     if (valid) {
-      slot = b.qfree[i];
-      uint32_t pixel = uint32_t(item % uint64_t(p.npix));
-      uint32_t frame = p.frame_base + uint32_t(item / uint64_t(p.npix));
+      int lo = 0, hi = n - 1;  // last active job whose range starts at or before i
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= i) lo = mid;
+        else hi = mid - 1;
+      }
+      const int jj = act[lo];
+      const WaveParams& p = sc.jobs[jj].p;
+      unsigned long long item = sc.js[jj].items_next + (i - pre[lo]);
+      uint32_t pos = head_pos + i;  // i < capacity
+      if (pos >= b.capacity) pos -= b.capacity;
+      slot = b.qfree[pos];
+      uint32_t pixel, frame;
+      if (item <= 0xffffffffull) {
+        pixel = uint32_t(item) % uint32_t(p.npix);
+        frame = p.frame_base + uint32_t(item) / uint32_t(p.npix);
+      } else {
+        pixel = uint32_t(item % uint64_t(p.npix));
+        frame = p.frame_base + uint32_t(item / uint64_t(p.npix));
+      }
       int px = int(pixel % uint32_t(p.cam.width)), py = int(pixel / uint32_t(p.cam.width));
       Rng r;
       if (p.rng_pcg) {
@@ -133,25 +208,61 @@ __global__ void k_regen(WaveParams p, PathBuf b, int next) {
       b.pixel[slot] = pixel;
       b.frame[slot] = frame;
       b.bounce[slot] = 0;
+      b.job[slot] = uint32_t(jj);
     }
     enqueue(q, cnt, valid, slot);
   }
 }
 
+// ---- commit: book-keeping of one iteration (one block of kMaxJobs threads) -----------------
+__global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cur) {
+  __shared__ unsigned long long scan[kMaxJobs];
+  const int n = min(*sc.nactive, kMaxJobs);
+  int j;
+  unsigned long long rem = remaining(sc, threadIdx.x, n, j), total;
+  unsigned long long pre = block_scan(rem, scan, total);
+  const unsigned long long head = *b.free_head;
+  const unsigned long long avail = min(*b.free_tail - head, total);
+  // the regen that just ran gave job a the items [pre, pre + rem) clipped to avail
+  if (j >= 0 && avail > pre) {
+    unsigned long long took = min(avail - pre, rem);
+    sc.js[j].items_next += took;
+    sc.js[j].live += uint32_t(took);
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t == 0) {
+    *b.free_head = head + avail;
+    b.counts[cur] = 0;                 // q[cur]: consumed by this iteration's extend
+    b.counts[kCntShadow0 + cur] = 0;   // qs[cur]: consumed by this iteration's connect
+    b.counts[kCntMiss] = 0;
+  }
+  if (t < kNumClasses) b.counts[kCntHit0 + t] = 0;
+  // status for the host (mapped memory)
+  if (j >= 0) {
+    volatile JobStatus* s = &sc.status->job[j];
+    const unsigned long long nx = sc.js[j].items_next, tot = sc.js[j].items_total;
+    const unsigned int live = sc.js[j].live;
+    s->items_next = nx;
+    s->items_total = tot;
+    s->live = live;
+    if (nx >= tot && live == 0u) s->done = 1u;
+  }
+  __syncthreads();
+  if (t == 0) {
+    unsigned long long it = *sc.iteration + 1;
+    *sc.iteration = it;
+    volatile HostStatus* hs = sc.status;
+    hs->live_paths = b.counts[cur ^ 1];
+    hs->nactive = uint32_t(n);
+    __threadfence_system();
+    hs->iteration = it;
+  }
+}
+
 // ---- extend: closest hit ------------------------------------------------------------------------
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBuf b, int cur) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // book-keeping of the regen that ran before: consume the free list
-    unsigned long long first = *b.items_next;
-    unsigned long long left = p.total_items > first ? p.total_items - first : 0ull;
-    unsigned long long used = min((unsigned long long)b.counts[kCntFree], left);
-    *b.items_next = first + used;
-    b.counts[kCntFree] = 0;
-    // queues that this iteration's shade fills; their readers ran last iteration
-    b.counts[cur ^ 1] = 0;
-    b.counts[kCntShadow0 + (cur ^ 1)] = 0;
-  }
+__global__ void __launch_bounds__(256) k_extend(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -161,6 +272,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBu
     int cls = 0;
     if (i < count) {
       slot = q[i];
+      const DevScene s = sc.jobs[b.job[slot]].s;
       float4 o = b.org[slot], d = b.dir[slot];
       Hit h;
       traverse<false>(s, mk(o), mk(d), kTfarMax, h, aborted, kCount ? &nodes : nullptr, kCount ? &tris : nullptr);
@@ -184,7 +296,7 @@ __global__ void __launch_bounds__(128) k_extend(DevScene s, WaveParams p, PathBu
 
 // ---- connect: NEE shadow rays (bvh.glsl:218-229) ---------------------------------------------
 template <bool kCount>
-__global__ void __launch_bounds__(128) k_connect(DevScene s, PathBuf b, int cur) {
+__global__ void __launch_bounds__(256) k_connect(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[kCntShadow0 + cur];
   const uint32_t* qs = b.qs[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -194,6 +306,7 @@ __global__ void __launch_bounds__(128) k_connect(DevScene s, PathBuf b, int cur)
     uint32_t nodes = 0, tris = 0;
     if (i < count) {
       uint32_t slot = qs[i];
+      const DevScene s = sc.jobs[b.job[slot]].s;
       int flags = b.sh_flags[slot];
       v3 org = mk(b.org[slot]);
       v3 add = mk(0.f);
@@ -243,7 +356,10 @@ DEV float4 clamp_result(const WaveParams& p, v3 L) {
 
 // A path whose ray left the scene: background for camera rays
 // (misptdl.glsl:41-46), MIS-weighted environment otherwise (misptdl.glsl:84-88).
-DEV void shade_miss_path(const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t slot) {
+DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
+  const uint32_t j = b.job[slot];
+  const Job& J = sc.jobs[j];
+  const WaveParams& p = J.p;
   float4 d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
   v3 dir = mk(d4);
   v3 w = mk(w4);
@@ -251,41 +367,46 @@ DEV void shade_miss_path(const DevIbl& e, const WaveParams& p, const PathBuf& b,
   v3 L = mk(l4);
   if (b.bounce[slot] == 0) {
     if (p.bg_from_ibl > 0) {
-      v3 env = p.has_ibl ? ibl_eval(e, p.ibl_rot, dir) : mk(0.f);
-      finish_path(b, slot, f4(env * w, 1.f));
+      v3 env = p.has_ibl ? ibl_eval(J.e, p.ibl_rot, dir) : mk(0.f);
+      finish_path(J, b, slot, f4(env * w, 1.f));
     } else {
-      finish_path(b, slot, make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
-                                       p.bg_color.w));
+      finish_path(J, b, slot,
+                  make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
+                              p.bg_color.w));
     }
     return;
   }
   if (p.has_ibl) {
-    float ipdf = ibl_pdf(e, p.ibl_rot, dir);
+    float ipdf = ibl_pdf(J.e, p.ibl_rot, dir);
     float mis = mis_balance(last_pdf, ipdf);
-    L = L + ibl_eval(e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
+    L = L + ibl_eval(J.e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
   }
-  finish_path(b, slot, clamp_result(p, L));
+  finish_path(J, b, slot, clamp_result(p, L));
 }
 
-__global__ void __launch_bounds__(256) k_shade_miss(DevIbl e, WaveParams p, PathBuf b) {
+__global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
   const uint32_t count = b.counts[kCntMiss];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     uint32_t slot = 0;
+    uint32_t job = 0;
     if (i < count) {
       slot = b.qm[i];
-      shade_miss_path(e, p, b, slot);
+      job = b.job[slot];
+      shade_miss_path(sc, b, slot);
     }
-    enqueue(b.qfree, b.counts + kCntFree, i < count, slot);
+    free_slots(sc, b, i < count, slot, job);
   }
 }
 
 // Surface hit.  Returns true if the path continues with an extension ray and
 // sets `shadow` when NEE shadow rays were emitted; otherwise the path's sample
 // has been accumulated.
-DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, uint32_t slot,
-                    bool& shadow) {
+DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shadow) {
   shadow = false;
+  const uint32_t j = b.job[slot];
+  const Job& J = sc.jobs[j];
+  const WaveParams& p = J.p;
   float4 hit = b.hit[slot];
   int tri = __float_as_int(hit.w);
   float4 o4 = b.org[slot], d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
@@ -294,20 +415,20 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
   v3 L = mk(l4);
   int bounce = b.bounce[slot];
   if (!(bounce < p.max_bounces)) {  // loop condition (misptdl.glsl:54)
-    finish_path(b, slot, clamp_result(p, L));
+    finish_path(J, b, slot, clamp_result(p, L));
     return false;
   }
   Rng rng = load_rng(p, b, slot);
   // Russian roulette (renderer.frag:119-123): weight boost every bounce
   w = w * p.rr_factor;
   if (bounce > p.rr_start && rng.next() <= p.rr_prob) {
-    finish_path(b, slot, clamp_result(p, L));
+    finish_path(J, b, slot, clamp_result(p, L));
     return false;
   }
   v3 org = mk(o4);
   v3 wi = -dir;
   v3 pos = org + dir * hit.x;
-  Surface S = make_surface(s, tri, hit.y, hit.z, pos, wi, p.lean != 0);
+  Surface S = make_surface(J.s, tri, hit.y, hit.z, pos, wi, p.lean != 0);
   if (S.backside && !S.thin_walled) {  // Beer-Lambert absorption (misptdl.glsl:60-63)
     v3 sigma = -vlog(S.att_color) / S.att_dist;
     w = w * vexp(-sigma * hit.x);
@@ -328,7 +449,7 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
     pdf = bs.pdf;
     bw = bs.weight;
     if (pdf < kEpsPdf) {  // absorbed: returns L without the clamp
-      finish_path(b, slot, f4(L, 1.f));
+      finish_path(J, b, slot, f4(L, 1.f));
       return false;
     }
   }
@@ -340,12 +461,12 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
   int flags = 0;
   if (p.use_ibl > 0 && p.has_ibl) {
     float ipdf;
-    v3 ld = ibl_sample(e, p.ibl_rot, p.env_mode, r0, r1, ipdf);
+    v3 ld = ibl_sample(J.e, p.ibl_rot, p.env_mode, r0, r1, ipdf);
     float cosnl = sat(dot(ld, n_nee));
     if (cosnl > kEpsCos && ipdf > kEpsPdf) {
       v3 f = bsdf_eval(S.c, S.n, wi, ld) / fmaxf(fabsf(dot(S.n, ld)), kEps);
       float bpdf = bsdf_pdf(S.c, S.n, wi, ld);
-      v3 c = ibl_eval(e, p.ibl_rot, ld) * f * cosnl / ipdf;
+      v3 c = ibl_eval(J.e, p.ibl_rot, ld) * f * cosnl / ipdf;
       if (bpdf > kEpsPdf) c = c * mis_balance(ipdf, bpdf);
       b.sh_dir[slot] = f4(ld, kTfarMax);
       b.sh_c[slot] = f4(c * w, 0.f);
@@ -379,7 +500,7 @@ DEV bool shade_path(const DevScene& s, const DevIbl& e, const WaveParams& p, con
   return true;
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams p, PathBuf b, int next) {
+__global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
   // the class queues, read as one sequence in class order
   __shared__ uint32_t start[kNumClasses + 1];
   if (threadIdx.x == 0) {
@@ -397,17 +518,18 @@ __global__ void __launch_bounds__(128) k_shade(DevScene s, DevIbl e, WaveParams 
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     bool cont = false, shadow = false;
-    uint32_t slot = 0;
+    uint32_t slot = 0, job = 0;
     if (i < count) {
       int k = 0;
 #pragma unroll
-      for (int j = 1; j < kNumClasses; ++j) k += i >= start[j] ? 1 : 0;
+      for (int jk = 1; jk < kNumClasses; ++jk) k += i >= start[jk] ? 1 : 0;
       slot = b.qh[size_t(k) * b.capacity + (i - start[k])];
-      cont = shade_path(s, e, p, b, slot, shadow);
+      job = b.job[slot];
+      cont = shade_path(sc, b, slot, shadow);
     }
     enqueue(qn, cn, cont, slot);
     enqueue(b.qs[next], b.counts + kCntShadow0 + next, shadow, slot);
-    enqueue(b.qfree, b.counts + kCntFree, i < count && !cont, slot);
+    free_slots(sc, b, i < count && !cont, slot, job);
   }
 }
 
@@ -541,24 +663,25 @@ static int grid_for(uint64_t n, int threads, int cap) {
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
   k_init_pool<<<grid_for(b.capacity, 256, 148 * 8), 256, 0, st>>>(b);
 }
-void launch_regen(const WaveParams& p, const PathBuf& b, int next, cudaStream_t st) {
-  k_regen<<<grid_for(b.capacity, 256, 148 * 16), 256, 0, st>>>(p, b, next);
+void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st) {
+  k_regen<<<grid_for(b.capacity, kMaxJobs, 148 * 8), kMaxJobs, 0, st>>>(sc, b, next);
 }
-void launch_extend(const DevScene& s, const WaveParams& p, const PathBuf& b, int cur, bool count, const LaunchCfg& lc,
-                   cudaStream_t st) {
-  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, p, b, cur);
-  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, p, b, cur);
+void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st) {
+  k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur);
 }
-void launch_connect(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
-  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
-  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(s, b, cur);
+void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
+  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
+  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
 }
-void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int next,
-                  const LaunchCfg& lc, cudaStream_t st) {
-  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(s, e, p, b, next);
+void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
+  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
+  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
 }
-void launch_shade_miss(const DevIbl& e, const WaveParams& p, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
-  k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(e, p, b);
+void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st) {
+  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
+}
+void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
+  k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(sc, b);
 }
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st) {
   k_mean<<<grid_for(npix, 256, 148 * 8), 256, 0, st>>>(accum, inv_count, out, npix);

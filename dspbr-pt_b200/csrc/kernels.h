@@ -7,13 +7,12 @@
 
 namespace dspbr {
 
-// Per-render constants of the reference's uniform block (renderer.frag:10-31)
-// plus the work description of one render call.
+// Per-job constants of the reference's uniform block (renderer.frag:10-31)
+// plus the job's image layout.
 struct WaveParams {
   Camera cam;
   int npix;              // width * height
   uint32_t frame_base;   // 1-based progressive frame number of work item 0
-  uint64_t total_items;  // frames * npix; item k = frame frame_base + k / npix, pixel k % npix
   int max_bounces;
   int rng_pcg;           // 0: MWC of rng.glsl, 1: PCG32
   uint64_t seed;
@@ -24,30 +23,62 @@ struct WaveParams {
   float rr_prob, rr_factor;
   int rr_start;
   float4 pl_pos, pl_emis;
-  int count_traversal;   // accumulate node visits / triangle tests into stats[3..6]
+};
+
+// One render job: a viewport of one scene, rendered for a number of
+// progressive frames.  Work item k of a job is pixel k % npix of frame
+// frame_base + k / npix.  Jobs live in a device table; paths refer to their
+// job by slot index, so jobs of different scenes, sizes and settings share
+// one path pool and one set of launches.
+struct Job {
+  WaveParams p;
+  DevScene s;
+  DevIbl e;
+  double* accum;         // RGBA sums per pixel (FP64)
+};
+
+// Device-updated progress of a job.
+struct JobState {
+  unsigned long long items_next;   // next work item to start
+  unsigned long long items_total;  // frames * npix (lowered to items_next to cancel)
+  unsigned int live;               // paths of this job in the pool
+  unsigned int pad;
+};
+
+constexpr int kMaxJobs = 256;  // job table slots = most jobs active at once
+
+// Progress record the commit kernel writes to mapped host memory after every
+// iteration; the host reads it after an event that follows the iteration.
+struct JobStatus {
+  unsigned long long items_next, items_total;
+  unsigned int live;
+  unsigned int done;  // set once every item has started and no path is live (single 32-bit store)
+};
+struct HostStatus {
+  unsigned long long iteration;     // iterations committed so far
+  unsigned int live_paths;          // paths queued for the next extend
+  unsigned int nactive;
+  JobStatus job[kMaxJobs];          // by job slot
 };
 
 // Queue counters (uint32 slots of PathBuf::counts).  Iteration i works on
 // parity cur = i & 1: extend reads q[cur], connect reads qs[cur], shade and
-// regen fill q[cur ^ 1] and qs[cur ^ 1].  Counters are reset inside the
-// kernels (extend resets the ones shade fills, regen the ones extend fills),
-// so an iteration is a fixed sequence of five launches.
+// regen fill q[cur ^ 1] and qs[cur ^ 1]; commit resets what was consumed.
 enum : int {
   kCntExt0 = 0,     // extension queues (ping-pong)
   kCntExt1 = 1,
   kCntShadow0 = 2,  // NEE shadow queues (ping-pong)
   kCntShadow1 = 3,
   kCntMiss = 4,     // paths whose extension ray left the scene
-  kCntFree = 6,     // free path slots
   kCntHit0 = 8,     // paths whose extension ray hit a triangle, one queue per shading class
   kCntNum = 32
 };
 constexpr int kNumClasses = 16;
 static_assert(kCntHit0 + kNumClasses <= kCntNum, "counter block too small");
 
-// Structure-of-arrays state of a pool of path slots.  A render call streams
-// its work items (pixel samples) through the pool: a path that terminates
-// accumulates its sample and frees its slot, and the next item takes it.
+// Structure-of-arrays state of a pool of path slots.  Jobs stream their work
+// items through the pool: a path that terminates accumulates its sample into
+// its job's image and frees its slot, and the next work item takes it.
 struct PathBuf {
   float4* org;      // ray origin (shadow rays of the same vertex share it)
   float4* dir;
@@ -63,33 +94,43 @@ struct PathBuf {
   uint32_t* pixel;  // pixel index of the slot's sample
   uint32_t* frame;  // progressive frame number of the slot's sample
   int* bounce;      // bounces so far (misptdl.glsl `bounce`)
+  uint32_t* job;    // job slot of the path
   uint32_t* q[2];   // extension queues (slot ids)
   uint32_t* qs[2];  // shadow queues
   uint32_t* qh;     // hit queues: class k at qh + k * capacity
   uint32_t* qm;     // miss queue
-  uint32_t* qfree;  // free slots
+  uint32_t* qfree;  // free slots: ring buffer [free_head, free_tail) mod capacity
+  unsigned long long* free_head;
+  unsigned long long* free_tail;
   uint32_t* counts; // kCnt*
-  unsigned long long* items_next;  // next work item to start
   // [0] closest-hit rays, [1] shadow rays, [2] aborted traversals,
   // [3]/[4] nodes visited / triangles tested by closest-hit rays, [5]/[6] by shadow rays
   unsigned long long* stats;
-  double* accum;    // RGBA sums per pixel (FP64)
   uint32_t capacity;
 };
 
+// The job table as the kernels see it.
+struct Sched {
+  const Job* jobs;        // kMaxJobs slots
+  JobState* js;           // kMaxJobs slots
+  const int* active;      // job slots in priority order
+  const int* nactive;
+  HostStatus* status;     // mapped host memory (device pointer)
+  unsigned long long* iteration;
+};
+
 struct LaunchCfg {
-  int trace_blocks = 0, trace_threads = 128;
-  int shade_blocks = 0, shade_threads = 128;
+  int trace_blocks = 148 * 16, trace_threads = 128;
+  int shade_blocks = 148 * 8, shade_threads = 128;
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
-void launch_regen(const WaveParams& p, const PathBuf& b, int next, cudaStream_t st);
-void launch_extend(const DevScene& s, const WaveParams& p, const PathBuf& b, int cur, bool count, const LaunchCfg& lc,
-                   cudaStream_t st);
-void launch_connect(const DevScene& s, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
-void launch_shade(const DevScene& s, const DevIbl& e, const WaveParams& p, const PathBuf& b, int next,
-                  const LaunchCfg& lc, cudaStream_t st);
-void launch_shade_miss(const DevIbl& e, const WaveParams& p, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
+void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
+void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
+void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
+void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st);
+void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
+void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
 
 // kernel-level queries (device buffers)

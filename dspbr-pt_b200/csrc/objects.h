@@ -1,0 +1,94 @@
+// Internal definitions of the C ABI's opaque handles, shared by the context
+// API (api.cu) and the server (server.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "dspbr.h"
+#include "engine.h"
+#include "host.h"
+#include "kernels.h"
+
+struct dspbr_scene {
+  dspbr_ctx* ctx = nullptr;
+  dspbr::DevBuf<float4> nodes, tris, verts, materials;
+  dspbr::DevBuf<uint32_t> indices;
+  dspbr::DevBuf<uint8_t> tri_class;
+  uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
+  std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
+  std::vector<float> host_materials;
+  uint32_t num_classes = 0;
+  bool boxes_finite = true;
+  double bvh_build_ms = 0, upload_ms = 0;
+  dspbr::DevScene view() const {
+    dspbr::DevScene s;
+    s.nodes = nodes.p; s.tris = tris.p; s.verts = verts.p; s.indices = indices.p; s.materials = materials.p;
+    s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
+    s.num_materials = int(num_materials);
+    s.tri_class = tri_class.p;
+    s.boxes_finite = boxes_finite ? 1 : 0;
+    return s;
+  }
+  uint64_t bytes() const {
+    return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes();
+  }
+};
+
+struct dspbr_ibl {
+  dspbr_ctx* ctx = nullptr;
+  dspbr::DevBuf<float4> rgba;
+  dspbr::DevBuf<float> pdf, cdf, ypdf, ycdf, alias_prob, lum, rowsum;
+  dspbr::DevBuf<int> alias_idx;
+  dspbr::DevBuf<double> total;
+  double total_sum = 0;
+  int w = 0, h = 0;
+  dspbr::DevIbl view() const {
+    dspbr::DevIbl e;
+    e.rgba = rgba.p; e.pdf = pdf.p; e.cdf = cdf.p; e.ypdf = ypdf.p; e.ycdf = ycdf.p;
+    e.alias_prob = alias_prob.p; e.alias_idx = alias_idx.p; e.w = w; e.h = h;
+    return e;
+  }
+};
+
+struct dspbr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  dspbr_params params{};
+  float matrix[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  float fov = 45.f, near_plane = 0.01f;
+  bool has_camera = false;
+  int width = 0, height = 0;
+  dspbr_scene* scene = nullptr;
+  dspbr_ibl* ibl = nullptr;
+  uint32_t wave_paths = 1u << 21;
+  std::unique_ptr<dspbr::Engine> eng;  // path pool + job table; this context's render is job slot 0
+  // render_async: the iteration loop runs on a worker thread
+  std::thread worker;
+  std::atomic<bool> worker_done{true};
+  int worker_rc = 0;
+  dspbr::DevBuf<double4> accum;
+  dspbr::DevBuf<float4> mean;
+  float* stage = nullptr;  // page-locked staging for readback into pageable memory
+  size_t stage_bytes = 0;
+  uint64_t sample_count = 0;
+  uint64_t rays_primary = 0;
+  double last_render_ms = 0;
+  bool pending = false;
+  bool counting = false;
+  dspbr::Status st() { return dspbr::Status{&err}; }
+};
+
+
+namespace dspbr {
+// Uniform block values of one job from the renderer settings and camera
+// (renderer.ts:399-431 updatePathracingUniforms).
+WaveParams make_job_params(const dspbr_params& q, const float matrix[16], float fov, float near_plane, int width,
+                           int height, bool has_ibl, uint32_t frame_base);
+}  // namespace dspbr

@@ -55,6 +55,39 @@ class Diag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("path_pool", C.c_uint32), ("max_active", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
+                ("reserved", C.c_int32 * 8)]
+
+
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("ibl", C.c_void_p), ("camera", C.c_float * 16), ("fov_deg", C.c_float),
+                ("near_plane", C.c_float), ("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("params", Params), ("out_rgba", C.POINTER(C.c_float)), ("tag", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("tag", C.c_uint64), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
+                ("done_ms", C.c_double), ("device_bytes", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("cancelled", C.c_uint64), ("failed", C.c_uint64), ("queued", C.c_uint64), ("running", C.c_uint64),
+                ("iterations", C.c_uint64), ("rays_closest", C.c_uint64), ("rays_shadow", C.c_uint64),
+                ("bytes_in_use", C.c_uint64), ("bytes_peak", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("path_pool", C.c_uint32), ("trace_threads", C.c_int32),
+                ("trace_blocks", C.c_int32), ("shade_threads", C.c_int32), ("shade_blocks", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = 0, 1, 2, 3, 4
+
 _F = C.POINTER(C.c_float)
 _I = C.POINTER(C.c_int32)
 _U = C.POINTER(C.c_uint32)
@@ -107,6 +140,15 @@ SIGNATURES = {
     "dspbr_bsdf_query": (C.c_int, [_V, _V, C.c_uint32, _F, _F, _F, _F, _F, _I]),
     "dspbr_ibl_query": (C.c_int, [_V, _V, C.c_uint32, _F, _F, _F, _F, _F]),
     "dspbr_camera_rays": (C.c_int, [_V, C.c_uint32, _I, _F, _F]),
+    "dspbr_server_create": (C.c_int, [_V, C.POINTER(ServerConfig), _PV]),
+    "dspbr_server_submit": (C.c_int, [_V, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "dspbr_server_poll": (C.c_int, [_V, C.c_uint64, C.POINTER(RequestInfo)]),
+    "dspbr_server_wait": (C.c_int, [_V, C.c_uint64, C.c_int, C.POINTER(RequestInfo)]),
+    "dspbr_server_cancel": (C.c_int, [_V, C.c_uint64]),
+    "dspbr_server_release": (C.c_int, [_V, C.c_uint64]),
+    "dspbr_server_get_stats": (C.c_int, [_V, C.POINTER(ServerStats)]),
+    "dspbr_server_autotune": (C.c_int, [_V, C.POINTER(Request), C.c_int, C.c_double]),
+    "dspbr_server_destroy": (C.c_int, [_V]),
 }
 
 _lib = None

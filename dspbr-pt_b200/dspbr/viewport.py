@@ -182,6 +182,46 @@ def look_at_matrix(position, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
     return e
 
 
+DISPLAY_SETTINGS = ("exposure", "toneMapping", "pixelRatio", "interactionPixelRatio", "enableGamma", "enableFxaa",
+                    "tileResolution", "debugMode")
+
+
+def apply_settings(p, settings: dict, display: dict | None = None) -> None:
+    """PathtracingViewportSettings (pathtracing_viewport.ts:147-170) onto a
+    dspbr_params; display-only keys go to `display` (or are ignored)."""
+    for k, v in settings.items():
+        if k == "maxBounces":
+            p.max_bounces = int(v)
+        elif k == "useIBL":
+            p.use_ibl = int(bool(v))
+        elif k == "showBackground":
+            p.background_from_ibl = int(bool(v))
+        elif k == "iblRotationDegrees":
+            p.ibl_rotation_deg = float(v)
+        elif k == "backgroundColor":
+            for j in range(4):
+                p.background_color[j] = float(v[j])
+        elif k == "rayEps":
+            p.ray_eps = float(v)
+        elif k == "clampThreshold":
+            p.clamp_threshold = float(v)
+        elif k in DISPLAY_SETTINGS:
+            if display is not None:
+                display[k] = v
+        elif k == "rng":
+            p.rng = _lib.RNG_PCG if v == "pcg" else _lib.RNG_MWC
+        elif k == "seed":
+            p.seed = int(v)
+        elif k == "envSampling":
+            p.env_sampling = _lib.ENV_CDF if v == "cdf" else _lib.ENV_ALIAS
+        elif k == "russianRouletteStartDepth":
+            p.rr_start_depth = int(v)
+        elif k == "materialProfile":
+            p.profile = _lib.PROFILE_LEAN if v == "webgl-lean" else _lib.PROFILE_FULL
+        else:
+            raise KeyError(f"unknown setting {k!r}")
+
+
 class PathtracingViewport:
     """Drop-in for PathtracingViewport (pathtracing_viewport.ts:100-342) on a B200."""
 
@@ -221,35 +261,7 @@ class PathtracingViewport:
 
     # ---- settings (pathtracing_viewport.ts:147-170) ----
     def setSettings(self, settings: dict) -> None:
-        p = self.params
-        for k, v in settings.items():
-            if k == "maxBounces":
-                p.max_bounces = int(v)
-            elif k == "useIBL":
-                p.use_ibl = int(bool(v))
-            elif k == "showBackground":
-                p.background_from_ibl = int(bool(v))
-            elif k == "iblRotationDegrees":
-                p.ibl_rotation_deg = float(v)
-            elif k == "backgroundColor":
-                for j in range(4):
-                    p.background_color[j] = float(v[j])
-            elif k == "rayEps":
-                p.ray_eps = float(v)
-            elif k == "clampThreshold":
-                p.clamp_threshold = float(v)
-            elif k in self._display:
-                self._display[k] = v
-            elif k == "rng":
-                p.rng = _lib.RNG_PCG if v == "pcg" else _lib.RNG_MWC
-            elif k == "seed":
-                p.seed = int(v)
-            elif k == "envSampling":
-                p.env_sampling = _lib.ENV_CDF if v == "cdf" else _lib.ENV_ALIAS
-            elif k == "russianRouletteStartDepth":
-                p.rr_start_depth = int(v)
-            else:
-                raise KeyError(f"unknown setting {k!r}")
+        apply_settings(self.params, settings, self._display)
         self._apply_params()
         self._emit_diag()
 

@@ -202,6 +202,78 @@ int dspbr_ibl_query(dspbr_ctx* ctx, const dspbr_ibl* ibl, uint32_t n, const floa
 /* camera rays (renderer.frag:129-142) for pixels xy with jitter r2: n x 6 (org, dir) */
 int dspbr_camera_rays(dspbr_ctx* ctx, uint32_t n, const int32_t* xy, const float* r2, float* rays6);
 
+/* ---- serving: continuous batching of render requests --------------------
+ * The reference renders one viewport per WebGL context, one frame per
+ * animation frame (renderer.ts:512-565).  A server renders many requests --
+ * each a viewport of a resident scene at its own resolution, spp and
+ * settings -- in one path pool: requests are admitted while the GPU works on
+ * others (as pool slots and the HBM budget allow), their paths share every
+ * launch, and each result is the image the same request renders alone.  A
+ * driver thread owns the server's CUDA stream; the calls below are
+ * thread-safe. */
+typedef struct dspbr_server_config {
+  uint32_t path_pool;         /* path slots (0: 2^21) */
+  int max_active;             /* requests in flight at once, 1..256 (0: 256) */
+  uint64_t hbm_budget_bytes;  /* path pool + scenes in use + request buffers (0: 120 GB) */
+  int reserved[8];
+} dspbr_server_config;
+
+typedef struct dspbr_request {
+  const dspbr_scene* scene;   /* created on the server's context */
+  const dspbr_ibl* ibl;       /* NULL: no environment */
+  float camera[16];           /* camera-to-world, column-major (setCamera) */
+  float fov_deg, near_plane;
+  int width, height;
+  int spp;                    /* progressive frames, 1 sample per pixel each */
+  dspbr_params params;
+  float* out_rgba;            /* caller's buffer of width*height*4 floats; holds the mean once the request is done */
+  uint64_t tag;               /* returned in dspbr_request_info */
+} dspbr_request;
+
+enum {
+  DSPBR_REQ_QUEUED = 0,
+  DSPBR_REQ_RUNNING = 1,
+  DSPBR_REQ_DONE = 2,
+  DSPBR_REQ_CANCELLED = 3,
+  DSPBR_REQ_FAILED = 4
+};
+
+typedef struct dspbr_request_info {
+  int state;                  /* DSPBR_REQ_* */
+  uint64_t tag;
+  double submit_ms, admit_ms, done_ms;  /* steady clock, milliseconds */
+  uint64_t device_bytes;      /* request buffers charged to the budget */
+} dspbr_request_info;
+
+typedef struct dspbr_server_stats {
+  uint64_t submitted, admitted, completed, cancelled, failed, queued, running;
+  uint64_t iterations;        /* wavefront iterations run */
+  uint64_t rays_closest, rays_shadow;
+  uint64_t bytes_in_use, bytes_peak;
+  double p50_ms, p99_ms;      /* submit -> done latency of completed requests */
+  uint32_t path_pool;
+  int trace_threads, trace_blocks, shade_threads, shade_blocks;  /* launch sizes in use */
+} dspbr_server_stats;
+
+int dspbr_server_create(dspbr_ctx* ctx, const dspbr_server_config* cfg, dspbr_server** out);
+/* queue a request; DSPBR_ERR_ADMISSION if it can never fit the budget */
+int dspbr_server_submit(dspbr_server* srv, const dspbr_request* req, uint64_t* id);
+int dspbr_server_poll(dspbr_server* srv, uint64_t id, dspbr_request_info* info);
+/* blocks until the request is done, cancelled or failed, or timeout_ms passes
+ * (timeout_ms < 0: no limit); returns DSPBR_ERR_STATE on timeout */
+int dspbr_server_wait(dspbr_server* srv, uint64_t id, int timeout_ms, dspbr_request_info* info);
+/* no further samples start; the request ends as DSPBR_REQ_CANCELLED and its
+ * buffer is not written */
+int dspbr_server_cancel(dspbr_server* srv, uint64_t id);
+/* forgets a finished request (its info is no longer available) */
+int dspbr_server_release(dspbr_server* srv, uint64_t id);
+int dspbr_server_get_stats(dspbr_server* srv, dspbr_server_stats* stats);
+/* Autotuner: renders the sample requests (results discarded) under candidate
+ * path-pool sizes and extend/connect/shade block sizes, keeps the fastest in
+ * rays per second.  Call while the server is idle.  seconds bounds the time. */
+int dspbr_server_autotune(dspbr_server* srv, const dspbr_request* samples, int n, double seconds);
+int dspbr_server_destroy(dspbr_server* srv);
+
 #ifdef __cplusplus
 }
 #endif
