@@ -185,6 +185,171 @@ def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0):
     return tot_rays / tot_t / 1e6, cores, sample, vals, kind
 
 
+# ---- batching / serving ---------------------------------------------------------------------
+def _load_scene_set(ctx, scenes):
+    from dspbr.viewport import Bvh, DeviceIbl, DeviceScene
+    out = []
+    for sc in scenes:
+        sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+        out.append((DeviceScene(ctx, sc.vertices, sc.indices, sc.materials, sc.bvh), DeviceIbl(ctx, sc.env), sc))
+    return out
+
+
+def _submit(srv, dev, r, out=None):
+    from dspbr.viewport import PathtracingCamera
+    ds, di, _ = dev[r["scene"]]
+    cam = PathtracingCamera(r["camera"].matrix_world, r["camera"].fov, r["camera"].near)
+    return srv.submit(ds, di, cam, r["width"], r["height"], r["spp"], {"maxBounces": r["maxBounces"]}, out=out)
+
+
+def _one_at_a_time(ctx, dev, mix):
+    """The same requests through the single-viewport API (dspbr_set_scene /
+    set_camera / resize / render / read_accum), one after the other, scenes
+    resident.  Returns per-request service times (s) and the images."""
+    import ctypes as C
+    from dspbr import _lib
+    lib, h = ctx.lib, ctx.h
+    times, imgs = [], []
+    for r in mix:
+        t0 = time.perf_counter()
+        ds, di, _ = dev[r["scene"]]
+        p = _lib.default_params()
+        p.max_bounces = r["maxBounces"]
+        m = np.ascontiguousarray(r["camera"].matrix_world, np.float32).reshape(16)
+        ctx.check(lib.dspbr_set_scene(h, ds.h))
+        ctx.check(lib.dspbr_set_ibl(h, di.h))
+        ctx.check(lib.dspbr_set_params(h, C.byref(p)))
+        ctx.check(lib.dspbr_set_camera(h, _lib.fptr(m), float(r["camera"].fov), float(r["camera"].near)))
+        ctx.check(lib.dspbr_resize(h, r["width"], r["height"]))
+        ctx.check(lib.dspbr_render(h, r["spp"]))
+        out = np.empty((r["height"], r["width"], 4), np.float32)
+        ctx.check(lib.dspbr_read_accum(h, _lib.fptr(out), out.size))
+        times.append(time.perf_counter() - t0)
+        imgs.append(out)
+    return times, imgs
+
+
+def _rays(srv):
+    st = srv.stats()
+    return st["rays_closest"] + st["rays_shadow"]
+
+
+def _pct(v, q):
+    v = sorted(v)
+    return float(v[min(len(v) - 1, int(round(q * (len(v) - 1))))]) if v else None
+
+
+def serving_section(local, quick=False):
+    """Batching (64 viewports over 8 scenes of 10k-2M triangles, 128^2-1024^2,
+    1-64 spp) and serving (Poisson arrivals over 16 scenes of 50k-4M
+    triangles, 256^2-1920x1080, 16-256 spp, 12 bounces, 120 GB budget) against
+    the same requests rendered one at a time."""
+    import threading
+    from dspbr import synth
+    from dspbr.server import Server
+    from dspbr.viewport import Context, PathtracingCamera
+    ctx = Context(local)
+    res = {}
+    # ---- batching ----
+    t0 = time.perf_counter()
+    nb = 8 if not quick else 3
+    bdev = _load_scene_set(ctx, synth.scene_set(11, nb, 10_000, 2_000_000 if not quick else 100_000, (1024, 512)))
+    mix = synth.request_mix(12, 64 if not quick else 8, nb, 128 * 128, 1024 * 1024, 1, 64, 30.0, 90.0, 12)
+    gen_s = time.perf_counter() - t0
+    srv = Server(ctx, hbm_budget_bytes=120 << 30)
+    samples = []
+    for k in range(min(4, len(mix))):
+        c = mix[k]["camera"]
+        samples.append(srv.request(bdev[mix[k]["scene"]][0], bdev[mix[k]["scene"]][1],
+                                   PathtracingCamera(c.matrix_world, c.fov, c.near), 512, 512, 64,
+                                   {"maxBounces": 12})[0])
+    tuned = srv.autotune(samples, seconds=8.0 if not quick else 2.0)
+    # warm-up request (graph capture, memory pool)
+    srv.wait(_submit(srv, bdev, dict(mix[0], spp=1)))
+    r0 = _rays(srv)
+    t0 = time.perf_counter()
+    ids = [_submit(srv, bdev, r) for r in mix]
+    done = [srv.wait(i) for i in ids]
+    t_batch = time.perf_counter() - t0
+    rays_b = _rays(srv) - r0
+    lat = [d["done_ms"] - d["submit_ms"] for _, d in done]
+    t_single, imgs1 = _one_at_a_time(ctx, bdev, mix)
+    diff = max(float(np.max(np.abs(done[k][0] - imgs1[k]))) for k in range(len(mix)))
+    spp_total = sum(r["spp"] for r in mix)
+    res["batching"] = {
+        "requests": len(mix), "scenes": nb, "scene_triangles": [int(d[2].num_triangles) for d in bdev],
+        "batched_s": t_batch, "one_at_a_time_s": float(sum(t_single)),
+        "requests_per_s": len(mix) / t_batch, "one_at_a_time_requests_per_s": len(mix) / sum(t_single),
+        "speedup": float(sum(t_single)) / t_batch,
+        "sample_frames_per_s": spp_total / t_batch, "mrays_per_s": rays_b / t_batch / 1e6,
+        "p50_ms": _pct(lat, 0.5), "p99_ms": _pct(lat, 0.99),
+        "max_abs_diff_vs_one_at_a_time": diff, "scene_gen_s": gen_s,
+        "autotuned": {k: tuned[k] for k in ("path_pool", "trace_threads", "trace_blocks", "shade_threads",
+                                            "shade_blocks")}}
+    for i in ids:
+        srv.release(i)
+    for d in bdev:
+        d[0].close()
+        d[1].close()
+    # ---- serving ----
+    t0 = time.perf_counter()
+    ns = 16 if not quick else 3
+    sdev = _load_scene_set(ctx, synth.scene_set(21, ns, 50_000, 4_000_000 if not quick else 100_000, (1024, 512)))
+    n = 32 if not quick else 6
+    smix = synth.request_mix(22, n, ns, 256 * 256, 1920 * 1080, 16, 256, 30.0, 90.0, 12, aspect_hi=16 / 9)
+    gen_s = time.perf_counter() - t0
+    t_single, imgs1 = _one_at_a_time(ctx, sdev, smix)
+    rates = []
+    for rate in ((10.0, 50.0, 200.0, 500.0) if not quick else (50.0,)):
+        arr = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))
+        outs = [np.empty((r["height"], r["width"], 4), np.float32) for r in smix]
+        ids = [None] * n
+        r0 = _rays(srv)
+        start = time.perf_counter()
+
+        def feeder():
+            for k, r in enumerate(smix):
+                dt = start + arr[k] - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = _submit(srv, sdev, r, out=outs[k])
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        th.join()
+        infos = [srv.wait(i)[1] for i in ids]
+        span = (max(d["done_ms"] for d in infos) - min(d["submit_ms"] for d in infos)) / 1e3
+        lat = [d["done_ms"] - d["submit_ms"] for d in infos]
+        # the same arrivals served one at a time (FIFO, measured service times)
+        fin, lat1 = 0.0, []
+        for a, sv in zip(arr, t_single):
+            fin = max(fin, a) + sv
+            lat1.append(1e3 * (fin - a))
+        span1 = fin - arr[0]
+        diff = max(float(np.max(np.abs(outs[k] - imgs1[k]))) for k in range(n))
+        rates.append({"rate_req_s": rate, "requests": n, "frames_per_s": n / span,
+                      "sample_frames_per_s": sum(r["spp"] for r in smix) / span,
+                      "mrays_per_s": (_rays(srv) - r0) / span / 1e6,
+                      "p50_ms": _pct(lat, 0.5), "p99_ms": _pct(lat, 0.99),
+                      "one_at_a_time": {"frames_per_s": n / span1, "p50_ms": _pct(lat1, 0.5),
+                                        "p99_ms": _pct(lat1, 0.99)},
+                      "frames_per_s_ratio": (n / span) / (n / span1),
+                      "max_abs_diff_vs_one_at_a_time": diff})
+        for i in ids:
+            srv.release(i)
+    st = srv.stats()
+    res["serving"] = {"scenes": ns, "scene_triangles": [int(d[2].num_triangles) for d in sdev],
+                      "hbm_budget_gb": 120, "bytes_peak": st["bytes_peak"], "scene_gen_s": gen_s,
+                      "one_at_a_time_service_s": {"p50": _pct(t_single, 0.5), "max": max(t_single)},
+                      "rates": rates}
+    srv.close()
+    for d in sdev:
+        d[0].close()
+        d[1].close()
+    ctx.close()
+    return res
+
+
 def run_reference_arm(args):
     rank, ws, local, dist = dist_setup()
     if rank != 0:
@@ -285,6 +450,10 @@ def run_gpu_arm(args):
     e2e_parts = {"set_camera_ms": 1e3 * parts[0] / e2e_steps, "render_1_frame_ms": 1e3 * parts[1] / e2e_steps,
                  "read_accumulation_ms": 1e3 * parts[2] / e2e_steps}
     cs = clocks.summary()
+    v.dispose()
+    serving = None
+    if ws == 1 and not args.no_serving:
+        serving = serving_section(local, quick=args.quick_serving)
 
     if rank == 0:
         cpu = None
@@ -317,8 +486,9 @@ def run_gpu_arm(args):
             "rays_per_step": rays / max(1, args.steps),
             "traversal_aborted": d1["traversal_aborted"],
         }
+        if serving is not None:
+            line.update(serving)
         print(json.dumps(line))
-    v.dispose()
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -331,6 +501,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the batching / serving sections")
+    ap.add_argument("--quick-serving", action="store_true", help="small batching / serving mixes (smoke runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -100,9 +100,17 @@ DEV void free_slots(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot,
   if (pred && lane == __ffs(peers) - 1) atomicSub(&sc.js[job].live, uint32_t(__popc(peers)));
 }
 
-// Exclusive prefix sum over the block (blockDim.x == kMaxJobs threads).
-DEV unsigned long long block_scan(unsigned long long v, unsigned long long* sh, unsigned long long& total) {
+// Exclusive prefix sum over the block (blockDim.x == kMaxJobs threads); `n`
+// values are non-zero at most (a single active job needs no scan).
+DEV unsigned long long block_scan(unsigned long long v, unsigned long long* sh, unsigned long long& total, int n) {
   const int t = threadIdx.x;
+  if (n <= 1) {
+    if (t == 0) sh[0] = v;
+    __syncthreads();
+    total = sh[0];
+    __syncthreads();
+    return 0ull;
+  }
   sh[t] = v;
   __syncthreads();
   for (int off = 1; off < kMaxJobs; off <<= 1) {
@@ -151,7 +159,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
   const int n = min(*sc.nactive, kMaxJobs);
   int j;
   unsigned long long rem = remaining(sc, threadIdx.x, n, j), total;
-  pre[threadIdx.x] = block_scan(rem, scan, total);
+  pre[threadIdx.x] = block_scan(rem, scan, total, n);
   act[threadIdx.x] = j;
   __syncthreads();
   const unsigned long long head = *b.free_head;
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
   const int n = min(*sc.nactive, kMaxJobs);
   int j;
   unsigned long long rem = remaining(sc, threadIdx.x, n, j), total;
-  unsigned long long pre = block_scan(rem, scan, total);
+  unsigned long long pre = block_scan(rem, scan, total, n);
   const unsigned long long head = *b.free_head;
   const unsigned long long avail = min(*b.free_tail - head, total);
   // the regen that just ran gave job a the items [pre, pre + rem) clipped to avail
@@ -359,7 +367,7 @@ DEV float4 clamp_result(const WaveParams& p, v3 L) {
 DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
   const uint32_t j = b.job[slot];
   const Job& J = sc.jobs[j];
-  const WaveParams& p = J.p;
+  const WaveParams p = J.p;  // local copy: the outlined material calls would force reloads
   float4 d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
   v3 dir = mk(d4);
   v3 w = mk(w4);
@@ -406,7 +414,7 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
   shadow = false;
   const uint32_t j = b.job[slot];
   const Job& J = sc.jobs[j];
-  const WaveParams& p = J.p;
+  const WaveParams p = J.p;  // local copy: the outlined material calls would force reloads
   float4 hit = b.hit[slot];
   int tri = __float_as_int(hit.w);
   float4 o4 = b.org[slot], d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];

@@ -428,3 +428,37 @@ def make_sized(seed: int, target_tris: int, env_size=(1024, 512)) -> Scene:
 
 
 WORKLOADS = {"small": make_small, "large": make_large, "divergence": make_divergence}
+
+
+# ---- request mixes of the batching / serving configurations ----------------
+def scene_set(seed: int, n: int, lo_tris: int, hi_tris: int, env_size=(1024, 512)) -> list[Scene]:
+    """n resident scenes with log-uniform triangle counts in [lo_tris, hi_tris]
+    (endpoints included), generated like the large configuration."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(np.linspace(np.log(lo_tris), np.log(hi_tris), n))
+    rng.shuffle(counts)
+    return [make_sized(seed * 1000 + k, int(c), env_size) for k, c in enumerate(counts)]
+
+
+def request_mix(seed: int, n: int, n_scenes: int, px_lo: int, px_hi: int, spp_lo: int, spp_hi: int,
+                fov_lo: float = 30.0, fov_hi: float = 90.0, max_bounces: int = 12, aspect_hi: float = 1.0) -> list[dict]:
+    """n viewport requests: scene index, random camera around the 100 m
+    instance cube, pixel count log-uniform in [px_lo, px_hi] (aspect ratio
+    uniform in [1, aspect_hi]), spp uniform in [spp_lo, spp_hi], fov uniform."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        npx = float(np.exp(rng.uniform(np.log(px_lo), np.log(px_hi))))
+        a = float(rng.uniform(1.0, aspect_hi))
+        w = max(1, int(round(np.sqrt(npx * a))))
+        h = max(1, int(round(npx / w)))
+        d = rng.normal(size=3)
+        d[1] = abs(d[1]) + 0.2
+        d /= np.linalg.norm(d)
+        pos = d * rng.uniform(110.0, 170.0)
+        target = rng.uniform(-25.0, 25.0, 3)
+        fov = float(rng.uniform(fov_lo, fov_hi))
+        cam = Camera.look_at(pos, target, fov=fov, near=0.1)
+        out.append({"scene": int(rng.integers(0, n_scenes)), "camera": cam, "width": w, "height": h,
+                    "spp": int(rng.integers(spp_lo, spp_hi + 1)), "maxBounces": max_bounces})
+    return out

@@ -1211,7 +1211,9 @@ void trace_path(const Scene& s, const Ibl* I, const Params& P, int px, int py, u
     out[3] = R(1);
   };
   // last_bounce_specular reads the event_type that configure_gltf_material
-  // leaves zero-initialised, so it is false at every bounce.
+  // leaves zero-initialised (material.glsl never assigns it, and WebGL
+  // zero-initialises locals), so it is false at every bounce: NEE runs on
+  // every bounce and the env MIS weight always applies (misptdl.glsl:68-86).
   while (bounce < P.max_bounces) {
     w = w * rr_factor;
     if (bounce > P.rr_start && rng.next() <= R(P.rr_prob)) break;
