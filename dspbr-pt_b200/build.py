@@ -13,7 +13,11 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "dspbr", "libdspbr_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["api.cu", "engine.cu", "server.cu", "kernels.cu", "ibl.cu", "ibl_noalloc.cu", "bvh_build.cpp"]
+SOURCES = ["api.cu", "engine.cu", "server.cu", "display.cu", "kernels.cu", "ibl.cu", "ibl_noalloc.cu", "bvh_build.cpp"]
+
+
+# files whose arithmetic must round every operation like the shader it restates
+NO_FMA = {"display.cu"}
 
 
 def sources():
@@ -40,6 +44,8 @@ def build(force=False, verbose=False):
                "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
+        if os.path.basename(src) in NO_FMA:
+            cmd.insert(1, "-fmad=false")
         subprocess.run(cmd, check=True)
         objs.append(obj)
     cmd = [NVCC, "-shared", *ARCH, "-o", OUT, *objs, "-lpthread"]

@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "display.h"
 #include "dspbr.h"
 #include "engine.h"
 #include "host.h"
@@ -490,6 +491,7 @@ int dspbr_resize(dspbr_ctx* c, int w, int h) {
   size_t npix = size_t(w) * h;
   TRY_CUDA(s, c->accum.alloc(npix), "alloc accumulation");
   TRY_CUDA(s, c->mean.alloc(npix), "alloc readback");
+  c->display.reset();
   c->width = w;
   c->height = h;
   return dspbr_reset(c);
@@ -655,6 +657,31 @@ static void parallel_copy(void* dst, const void* src, size_t bytes) {
   for (auto& t : th) t.join();
 }
 
+// Device-to-host copy of a result: one DMA into page-locked memory, else
+// through the context's page-locked staging buffer and a parallel host copy.
+static int copy_out(dspbr_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
+  Status s = c->st();
+  cudaPointerAttributes attr{};
+  bool pinned = cudaPointerGetAttributes(&attr, dst) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (pinned) {
+    TRY_CUDA(s, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream), what);
+    TRY_CUDA(s, cudaStreamSynchronize(c->stream), what);
+    return DSPBR_OK;
+  }
+  if (c->stage_bytes < bytes) {
+    if (c->stage) cudaFreeHost(c->stage);
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+    TRY_CUDA(s, cudaHostAlloc(reinterpret_cast<void**>(&c->stage), bytes, cudaHostAllocDefault), "alloc staging");
+    c->stage_bytes = bytes;
+  }
+  TRY_CUDA(s, cudaMemcpyAsync(c->stage, src, bytes, cudaMemcpyDeviceToHost, c->stream), what);
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), what);
+  parallel_copy(dst, c->stage, bytes);
+  return DSPBR_OK;
+}
+
 int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c || !rgba) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
@@ -665,26 +692,97 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
   launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
-  const size_t bytes = npix * 16;
-  cudaPointerAttributes attr{};
-  bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
-  cudaGetLastError();
-  if (pinned) {
-    TRY_CUDA(s, cudaMemcpyAsync(rgba, c->mean.p, bytes, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
-    TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read accumulation");
-    return DSPBR_OK;
+  return copy_out(c, rgba, c->mean.p, npix * 16, "read accumulation");
+}
+
+// tonemap (+ FXAA) of the running mean into `out` (float4 or uchar4 per pixel)
+static int display_pass(dspbr_ctx* c, const dspbr_display* d, bool bytes8, void** out) {
+  Status s = c->st();
+  size_t npix = size_t(c->width) * c->height;
+  if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_display: no image");
+  if (!(d->exposure == d->exposure)) return s.fail(DSPBR_ERR_INVALID, "read_display: exposure is NaN");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  if (!c->display.p) TRY_CUDA(s, c->display.alloc(npix), "alloc display buffer");
+  DisplayParams p;
+  p.exposure = d->exposure;
+  p.mode = d->tonemapping;
+  p.gamma = d->gamma != 0;
+  const double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
+  float4* f = c->display.p;
+  uchar4* b = reinterpret_cast<uchar4*>(c->mean.p);  // the mean buffer holds 16 B per pixel
+  if (d->fxaa) {
+    launch_tonemap(c->accum.p, inv, p, c->mean.p, int(npix), c->stream);
+    if (bytes8) launch_fxaa8(c->mean.p, c->width, c->height, reinterpret_cast<uchar4*>(f), c->stream);
+    else launch_fxaa(c->mean.p, c->width, c->height, f, c->stream);
+    *out = f;
+  } else if (bytes8) {
+    launch_tonemap8(c->accum.p, inv, p, b, int(npix), c->stream);
+    *out = b;
+  } else {
+    launch_tonemap(c->accum.p, inv, p, f, int(npix), c->stream);
+    *out = f;
   }
-  if (c->stage_bytes < bytes) {
-    if (c->stage) cudaFreeHost(c->stage);
-    c->stage = nullptr;
-    c->stage_bytes = 0;
-    TRY_CUDA(s, cudaHostAlloc(reinterpret_cast<void**>(&c->stage), bytes, cudaHostAllocDefault), "alloc staging");
-    c->stage_bytes = bytes;
+  return s.cuda(cudaGetLastError(), "display pass");
+}
+
+int dspbr_read_display(dspbr_ctx* c, const dspbr_display* d, float* rgba, size_t num_floats) {
+  if (!c || !d || !rgba) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  size_t npix = size_t(c->width) * c->height;
+  if (num_floats < npix * 4)
+    return c->st().fail(DSPBR_ERR_INVALID, "read_display: buffer holds %zu floats, need %zu", num_floats, npix * 4);
+  void* src = nullptr;
+  int rc = display_pass(c, d, false, &src);
+  if (rc) return rc;
+  return copy_out(c, rgba, src, npix * 16, "read display");
+}
+
+int dspbr_read_display_rgba8(dspbr_ctx* c, const dspbr_display* d, uint8_t* rgba8, size_t num_bytes) {
+  if (!c || !d || !rgba8) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  size_t npix = size_t(c->width) * c->height;
+  if (num_bytes < npix * 4)
+    return c->st().fail(DSPBR_ERR_INVALID, "read_display_rgba8: buffer holds %zu bytes, need %zu", num_bytes, npix * 4);
+  void* src = nullptr;
+  int rc = display_pass(c, d, true, &src);
+  if (rc) return rc;
+  return copy_out(c, rgba8, src, npix * 4, "read display");
+}
+
+int dspbr_display_image(dspbr_ctx* c, const float* rgba, int w, int h, const dspbr_display* d, float* out_rgba,
+                        uint8_t* out_rgba8) {
+  if (!c || !rgba || !d || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28)) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  const size_t npix = size_t(w) * h;
+  // the image as one-sample sums: exactly the floats given (double holds them)
+  std::vector<double> sums(npix * 4);
+  for (size_t i = 0; i < npix * 4; ++i) sums[i] = double(rgba[i]);
+  DevBuf<double4> acc;
+  DevBuf<float4> tm, out;
+  DevBuf<uchar4> out8;
+  TRY_CUDA(s, acc.alloc(npix), "alloc");
+  TRY_CUDA(s, tm.alloc(npix), "alloc");
+  TRY_CUDA(s, out.alloc(npix), "alloc");
+  TRY_CUDA(s, out8.alloc(npix), "alloc");
+  TRY_CUDA(s, cudaMemcpyAsync(acc.p, sums.data(), npix * 32, cudaMemcpyHostToDevice, c->stream), "upload");
+  DisplayParams p;
+  p.exposure = d->exposure;
+  p.mode = d->tonemapping;
+  p.gamma = d->gamma != 0;
+  if (d->fxaa) {
+    launch_tonemap(acc.p, 1.0, p, tm.p, int(npix), c->stream);
+    if (out_rgba) launch_fxaa(tm.p, w, h, out.p, c->stream);
+    if (out_rgba8) launch_fxaa8(tm.p, w, h, out8.p, c->stream);
+  } else {
+    if (out_rgba) launch_tonemap(acc.p, 1.0, p, out.p, int(npix), c->stream);
+    if (out_rgba8) launch_tonemap8(acc.p, 1.0, p, out8.p, int(npix), c->stream);
   }
-  TRY_CUDA(s, cudaMemcpyAsync(c->stage, c->mean.p, bytes, cudaMemcpyDeviceToHost, c->stream), "read accumulation");
-  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read accumulation");
-  parallel_copy(rgba, c->stage, bytes);
-  return DSPBR_OK;
+  TRY_CUDA(s, cudaGetLastError(), "display pass");
+  if (out_rgba) TRY_CUDA(s, cudaMemcpyAsync(out_rgba, out.p, npix * 16, cudaMemcpyDeviceToHost, c->stream), "download");
+  if (out_rgba8) TRY_CUDA(s, cudaMemcpyAsync(out_rgba8, out8.p, npix * 4, cudaMemcpyDeviceToHost, c->stream), "download");
+  return s.cuda(cudaStreamSynchronize(c->stream), "display image");
 }
 
 int dspbr_host_alloc(dspbr_ctx* c, size_t bytes, void** out) {

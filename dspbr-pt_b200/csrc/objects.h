@@ -75,6 +75,7 @@ struct dspbr_ctx {
   int worker_rc = 0;
   dspbr::DevBuf<double4> accum;
   dspbr::DevBuf<float4> mean;
+  dspbr::DevBuf<float4> display;  // display epilogue output (allocated on first use)
   float* stage = nullptr;  // page-locked staging for readback into pageable memory
   size_t stage_bytes = 0;
   uint64_t sample_count = 0;

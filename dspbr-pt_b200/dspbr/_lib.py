@@ -55,6 +55,25 @@ class Diag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Display(C.Structure):
+    _fields_ = [("exposure", C.c_float), ("tonemapping", C.c_int32), ("gamma", C.c_int32), ("fxaa", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
+
+
+TONEMAPPING_MODES = ["None", "Reinhard", "Cineon", "AcesFilm"]  # renderer.ts:192
+
+
+def display_params(exposure=1.0, toneMapping="None", enableGamma=True, enableFxaa=False, **_) -> Display:
+    """Display settings of the viewport -> dspbr_display.  A mode name outside
+    tonemappingModes selects no operator, as the reference's indexOf() = -1 does."""
+    d = Display()
+    d.exposure = float(exposure)
+    d.tonemapping = TONEMAPPING_MODES.index(toneMapping) if toneMapping in TONEMAPPING_MODES else -1
+    d.gamma = int(bool(enableGamma))
+    d.fxaa = int(bool(enableFxaa))
+    return d
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("path_pool", C.c_uint32), ("max_active", C.c_int32), ("hbm_budget_bytes", C.c_uint64),
                 ("reserved", C.c_int32 * 8)]
@@ -130,6 +149,9 @@ SIGNATURES = {
     "dspbr_wait": (C.c_int, [_V]),
     "dspbr_read_accum": (C.c_int, [_V, _F, C.c_size_t]),
     "dspbr_host_alloc": (C.c_int, [_V, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "dspbr_read_display": (C.c_int, [_V, C.POINTER(Display), _F, C.c_size_t]),
+    "dspbr_read_display_rgba8": (C.c_int, [_V, C.POINTER(Display), C.POINTER(C.c_uint8), C.c_size_t]),
+    "dspbr_display_image": (C.c_int, [_V, _F, C.c_int, C.c_int, C.POINTER(Display), _F, C.POINTER(C.c_uint8)]),
     "dspbr_host_free": (C.c_int, [_V, _V]),
     "dspbr_get_diagnostics": (C.c_int, [_V, C.POINTER(Diag)]),
     "dspbr_set_wave_paths": (C.c_int, [_V, C.c_uint32]),

@@ -186,6 +186,9 @@ DISPLAY_SETTINGS = ("exposure", "toneMapping", "pixelRatio", "interactionPixelRa
                     "tileResolution", "debugMode")
 
 
+RESETTING_DISPLAY_SETTINGS = ("exposure", "enableGamma", "debugMode", "pixelRatio")
+
+
 def apply_settings(p, settings: dict, display: dict | None = None) -> None:
     """PathtracingViewportSettings (pathtracing_viewport.ts:147-170) onto a
     dspbr_params; display-only keys go to `display` (or are ignored)."""
@@ -262,7 +265,11 @@ class PathtracingViewport:
     # ---- settings (pathtracing_viewport.ts:147-170) ----
     def setSettings(self, settings: dict) -> None:
         apply_settings(self.params, settings, self._display)
-        self._apply_params()
+        # the renderer setters of exposure, enableGamma, debugMode and every
+        # render setting reset the accumulation; toneMapping, enableFxaa,
+        # interactionPixelRatio and tileResolution do not (renderer.ts:172-306)
+        if any(k not in DISPLAY_SETTINGS or k in RESETTING_DISPLAY_SETTINGS for k in settings):
+            self._apply_params()
         self._emit_diag()
 
     def _apply_params(self):
@@ -361,6 +368,21 @@ class PathtracingViewport:
         elif out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
             raise ValueError(f"readAccumulation: out must be a C-contiguous float32 array of shape {shape}")
         self.ctx.check(self.ctx.lib.dspbr_read_accum(self.ctx.h, fptr(out), out.size))
+        return out
+
+    def readDisplay(self, rgba8: bool = True) -> np.ndarray:
+        """The presented frame: the running mean through the reference's
+        tone-mapping / gamma / FXAA passes with the viewport's display
+        settings (exposure, toneMapping, enableGamma, enableFxaa;
+        renderer.ts:666-700).  rgba8: the 8-bit canvas bytes, else RGBA32F."""
+        d = _lib.display_params(**self._display)
+        if rgba8:
+            out = np.empty((self.height, self.width, 4), np.uint8)
+            self.ctx.check(self.ctx.lib.dspbr_read_display_rgba8(self.ctx.h, C.byref(d),
+                                                                 out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size))
+        else:
+            out = np.empty((self.height, self.width, 4), np.float32)
+            self.ctx.check(self.ctx.lib.dspbr_read_display(self.ctx.h, C.byref(d), fptr(out), out.size))
         return out
 
     def allocReadbackBuffer(self) -> np.ndarray:

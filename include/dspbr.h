@@ -165,6 +165,31 @@ int dspbr_wait(dspbr_ctx* ctx);
 /* readAccumulation (absent in the reference, which only displays): running
  * mean RGBA32F, width*height*4 floats, row 0 = bottom row (gl_FragCoord.y 0.5). */
 int dspbr_read_accum(dspbr_ctx* ctx, float* rgba, size_t num_floats);
+/* Display epilogue (renderer.ts:666-700): the accumulation mean through
+ * tonemap.frag (exposure, operator, gamma) and optionally fxaa.frag -- the
+ * reference's "postprocess" buffer -- as RGBA32F, or converted to the 8-bit
+ * canvas bytes. */
+typedef struct dspbr_display {
+  float exposure;             /* renderer.ts `exposure` (1.0) */
+  int tonemapping;            /* DSPBR_TONEMAP_*: renderer.ts tonemappingModes index */
+  int gamma;                  /* enableGamma: pow(c, 1/2.2) */
+  int fxaa;                   /* enableFxaa */
+  int reserved[4];
+} dspbr_display;
+enum {
+  DSPBR_TONEMAP_OFF = -1,     /* a mode name not in tonemappingModes: no operator, no exposure */
+  DSPBR_TONEMAP_NONE = 0,     /* "None": exposure only */
+  DSPBR_TONEMAP_REINHARD = 1,
+  DSPBR_TONEMAP_CINEON = 2,
+  DSPBR_TONEMAP_ACES = 3,     /* "AcesFilm" */
+  DSPBR_TONEMAP_UNCHARTED2 = 4
+};
+int dspbr_read_display(dspbr_ctx* ctx, const dspbr_display* display, float* rgba, size_t num_floats);
+int dspbr_read_display_rgba8(dspbr_ctx* ctx, const dspbr_display* display, uint8_t* rgba8, size_t num_bytes);
+/* The same epilogue on a caller's RGBA32F image (width*height*4 floats), for
+ * hosts that accumulate elsewhere; either output may be NULL. */
+int dspbr_display_image(dspbr_ctx* ctx, const float* rgba, int width, int height, const dspbr_display* display,
+                        float* out_rgba, uint8_t* out_rgba8);
 /* Page-locked host memory for readback buffers.  dspbr_read_accum into such
  * a buffer is one device-to-host DMA; into ordinary memory it goes through an
  * internal page-locked staging buffer.  dspbr_host_free accepts ctx == NULL

@@ -195,14 +195,48 @@ def translate(ref_root, chunk_dir, fp32):
     return src
 
 
+POST_SHADERS = {"tonemap": "tonemap.frag", "fxaa": "fxaa.frag"}
+
+
+def translate_post(ref_root, fp32):
+    """The display epilogue shaders (tonemap.frag, fxaa.frag), each in its own
+    namespace.  Their uniforms become namespace globals the harness sets;
+    `in v_uv` / `out` colour / gl_FragCoord are the harness's per-fragment
+    built-ins.  The output variable is renamed to out_FragColor."""
+    sd = os.path.join(ref_root, SHADER_DIR)
+    parts = []
+    for ns, fname in POST_SHADERS.items():
+        with open(os.path.join(sd, fname)) as f:
+            src = f.read()
+        src = re.sub(r"#version[^\n]*\n", "", src)
+        src = re.sub(r"precision\s+\w+\s+\w+\s*;", "", src)
+        src = re.sub(r"\b(?:mediump|highp|lowp)\s+", "", src)
+        src, n = re.subn(r"\buniform\s+", "", src)
+        expect(n >= 2, True, f"uniforms of {fname}")
+        src = re.sub(r"\bin\s+vec2\s+v_uv\s*;", "", src)
+        src, n = re.subn(r"\bout\s+vec4\s+(\w+)\s*;", "", src)
+        expect(n, 1, f"output of {fname}")
+        src = re.sub(r"\bout_color\b", "out_FragColor", src)
+        src = zero_init(src)
+        src = rewrite_params(src)
+        src = re.sub(r"\.(xyz|rgb|xy|yx|zw|rg)\b(?!\s*\()", r".\1()", src)
+        src, n = re.subn(r"\bvoid\s+main\s*\(\s*\)", "void glsl_main()", src)
+        expect(n, 1, f"main of {fname}")
+        src = re.sub(r"\bfloat\b", "real", src)
+        src = rewrite_literals(src, fp32)
+        parts.append(f"namespace post_{ns} {{\n// ---- {fname}\n{src}\n}}  // namespace post_{ns}\n")
+    return "\n".join(parts)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of the reference checkout")
     ap.add_argument("--chunks", required=True)
     ap.add_argument("--out", required=True)
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--post", action="store_true", help="translate the display epilogue shaders instead")
     a = ap.parse_args()
-    src = translate(a.ref, a.chunks, fp32=not a.fp64)
+    src = translate_post(a.ref, fp32=not a.fp64) if a.post else translate(a.ref, a.chunks, fp32=not a.fp64)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     with open(a.out, "w") as f:
         f.write("// GENERATED at build time from the reference shaders; not committed.\n")

@@ -201,6 +201,7 @@ static inline vec3 operator*(const mat3& m, const vec3& v) {
 struct sampler2D {
   const float* data = nullptr;
   int w = 0, h = 0, channels = 4;
+  bool nearest_clamp = false;  // NEAREST + CLAMP_TO_EDGE (render buffers, gl_utils.ts:22-30)
 };
 struct isampler2D {
   const int32_t* data = nullptr;
@@ -217,8 +218,15 @@ static inline ivec4 texelFetch(const isampler2D& s, ivec2 p, int) {
   return ivec4{s.data[size_t(p.y) * s.w + p.x], 0, 0, 1};
 }
 static inline int glsl_wrap_repeat(int i, int n) { int m = i % n; return m < 0 ? m + n : m; }
-// LINEAR + REPEAT filtering, level 0 (GLSL ES 3.00 / GL ES 3.0 spec 3.8.10).
+// LINEAR + REPEAT filtering, level 0 (GLSL ES 3.00 / GL ES 3.0 spec 3.8.10),
+// or NEAREST + CLAMP_TO_EDGE: texel floor(uv * size) clamped to the image.
 static inline vec4 texture(const sampler2D& s, vec2 uv) {
+  if (s.nearest_clamp) {
+    int i = int(std::floor(uv.x * real(s.w))), j = int(std::floor(uv.y * real(s.h)));
+    i = i < 0 ? 0 : (i >= s.w ? s.w - 1 : i);
+    j = j < 0 ? 0 : (j >= s.h ? s.h - 1 : j);
+    return texelFetch(s, ivec2(i, j), 0);
+  }
   real u = uv.x * real(s.w) - real(0.5), v = uv.y * real(s.h) - real(0.5);
   real fu = std::floor(u), fv = std::floor(v);
   real a = u - fu, b = v - fv;

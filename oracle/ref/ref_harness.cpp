@@ -50,6 +50,10 @@ sampler2D u_sampler_env_map, u_sampler_env_map_pdf, u_sampler_env_map_cdf, u_sam
 const f32* glsl_material_table = nullptr;
 
 #include REF_SOURCE
+#ifdef REF_POST_SOURCE
+// display epilogue (tonemap.frag, fxaa.frag), renderer.ts:668-690
+#include REF_POST_SOURCE
+#endif
 }  // namespace glsl
 using namespace glsl;
 
@@ -335,5 +339,40 @@ void REF(ibl)(int n, const float* r2, const float* dirs, float* sdirpdf4, float*
     rgb3[3 * i] = float(c.x); rgb3[3 * i + 1] = float(c.y); rgb3[3 * i + 2] = float(c.z);
   }
 }
+
+#ifdef REF_POST_SOURCE
+// Tone-mapping pass over an RGBA32F image (the accumulation mean), as the
+// reference draws it into the "postprocess" buffer: one fragment per pixel,
+// v_uv at the pixel centre, NEAREST sampling (gl_utils.ts:22-30).
+void REF(tonemap)(const float* rgba, int W, int H, float exposure, int gamma, int mode, float* out) {
+  post_tonemap::tex = sampler2D{rgba, W, H, 4, true};
+  post_tonemap::exposure = real(exposure);
+  post_tonemap::gamma = gamma != 0;
+  post_tonemap::tonemappingMode = mode;
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      v_uv = vec2(real(2 * x + 1) / real(W) - real(1), real(2 * y + 1) / real(H) - real(1));
+      gl_FragCoord = vec4(real(x) + real(0.5), real(y) + real(0.5), real(0.5), real(1));
+      post_tonemap::glsl_main();
+      float* o = out + 4 * (size_t(y) * W + x);
+      o[0] = float(out_FragColor.x); o[1] = float(out_FragColor.y); o[2] = float(out_FragColor.z);
+      o[3] = float(out_FragColor.w);
+    }
+}
+
+// FXAA pass (fxaa.frag) over the tone-mapped RGBA32F image.
+void REF(fxaa)(const float* rgba, int W, int H, float* out) {
+  post_fxaa::tex = sampler2D{rgba, W, H, 4, true};
+  post_fxaa::u_inv_res = vec2(real(1) / real(W), real(1) / real(H));
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      gl_FragCoord = vec4(real(x) + real(0.5), real(y) + real(0.5), real(0.5), real(1));
+      post_fxaa::glsl_main();
+      float* o = out + 4 * (size_t(y) * W + x);
+      o[0] = float(out_FragColor.x); o[1] = float(out_FragColor.y); o[2] = float(out_FragColor.z);
+      o[3] = float(out_FragColor.w);
+    }
+}
+#endif
 
 }  // extern "C"

@@ -141,6 +141,25 @@ class GlslReference:
                        pdf.ctypes.data_as(_F), rgb.ctypes.data_as(_F))
         return sdp, pdf, rgb
 
+    def tonemap(self, rgba, exposure: float, gamma: bool, mode: int) -> np.ndarray:
+        """tonemap.frag over an (H, W, 4) RGBA32F image (renderer.ts:668-676)."""
+        img = np.ascontiguousarray(rgba, np.float32)
+        out = np.zeros_like(img)
+        fn = self.fn("tonemap")
+        fn.argtypes = [_F, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, _F]
+        fn(img.ctypes.data_as(_F), img.shape[1], img.shape[0], float(exposure), int(bool(gamma)), int(mode),
+           out.ctypes.data_as(_F))
+        return out
+
+    def fxaa(self, rgba) -> np.ndarray:
+        """fxaa.frag over an (H, W, 4) RGBA32F image (renderer.ts:678-686)."""
+        img = np.ascontiguousarray(rgba, np.float32)
+        out = np.zeros_like(img)
+        fn = self.fn("fxaa")
+        fn.argtypes = [_F, C.c_int, C.c_int, _F]
+        fn(img.ctypes.data_as(_F), img.shape[1], img.shape[0], out.ctypes.data_as(_F))
+        return out
+
 
 def uniform_block(camera_matrix, fov_deg, near, width, height, frame, max_bounces, use_ibl=1, ibl_rotation=0.0,
                   background_from_ibl=1, background_color=(0, 0, 0, 1), ray_eps=1e-4, clamp_threshold=3.0,

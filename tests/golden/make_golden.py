@@ -26,6 +26,21 @@ from tests import helpers  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
+def display_test_image(w, h):
+    """Seeded HDR image: log-uniform radiance noise, a bright disc with a hard
+    edge, diagonal stripes and a zero / negative-free alpha ramp."""
+    rng = np.random.default_rng(15)
+    y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+    img = np.exp(rng.uniform(np.log(1e-4), np.log(20.0), (h, w, 3))).astype(np.float32)
+    disc = (x - w * 0.6) ** 2 + (y - h * 0.4) ** 2 < (0.25 * h) ** 2
+    img[disc] = [8.0, 6.0, 3.0]
+    stripes = ((x + y) // 3) % 2 == 0
+    img[stripes & ~disc] *= 0.05
+    img[:, :2] = 0.0
+    alpha = (x / (w - 1)).astype(np.float32)[..., None]
+    return np.ascontiguousarray(np.concatenate([img, alpha], -1), np.float32)
+
+
 def main():
     sc = synth.make_small(0)
     bvh = Bvh.build(sc.vertices, sc.indices, 20)
@@ -79,6 +94,18 @@ def main():
     g["image_env"] = sc.env
     g["image_whf"] = np.array([W, H, F], np.int32)
     g["image"] = acc
+    # display epilogue (tonemap.frag, fxaa.frag) over an HDR test image with
+    # hard edges and a dark-to-bright ramp, and over the rendered image
+    hdr = display_test_image(48, 40)
+    g["display_hdr"] = hdr
+    modes = [-1, 0, 1, 2, 3, 4]
+    g["display_modes"] = np.array(modes, np.int32)
+    for gamma in (0, 1):
+        g[f"display_tonemap_g{gamma}"] = np.stack([r32.tonemap(hdr, 1.7, gamma, m) for m in modes])
+    tm = r32.tonemap(hdr, 1.0, 1, 3)
+    g["display_fxaa_in"] = tm
+    g["display_fxaa"] = r32.fxaa(tm)
+    g["display_image_aces_fxaa"] = r32.fxaa(r32.tonemap(acc, 1.0, 1, 3))
     np.savez_compressed(os.path.join(OUT, "reference_small.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_small.npz"))
 

@@ -87,3 +87,9 @@ def close_mask(a, b, rtol, atol):
     with np.errstate(invalid="ignore"):
         near = np.abs(a - b) <= atol + rtol * np.abs(b)
     return same | near
+
+
+def camera_of(scene):
+    """PathtracingCamera of a synth.Scene's camera."""
+    from dspbr.viewport import PathtracingCamera
+    return PathtracingCamera(scene.camera.matrix_world, scene.camera.fov, scene.camera.near)

@@ -1,0 +1,99 @@
+"""Host-side logic without a GPU: viewport settings semantics, display-mode
+mapping, seeded request mixes, and the benchmark's multi-rank (replica)
+reductions over gloo with world size 2."""
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+from dspbr import _lib, synth, viewport
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+class _Recorder(viewport.PathtracingViewport):
+    """PathtracingViewport whose device calls are recorded instead of made."""
+
+    def __init__(self):
+        self.params = _lib.default_params()
+        self._display = {"exposure": 1.0, "toneMapping": "None", "enableGamma": True, "enableFxaa": False}
+        self._listeners = {e: set() for e in self.EVENTS}
+        self.applied = 0
+
+    def _apply_params(self):
+        self.applied += 1
+
+
+def test_settings_reset_accumulation_like_the_reference_setters():
+    v = _Recorder()
+    # renderer.ts: tonemapping / enableFxaa setters keep the accumulation
+    v.setSettings({"toneMapping": "AcesFilm"})
+    v.setSettings({"enableFxaa": True, "tileResolution": 2, "interactionPixelRatio": 0.5})
+    assert v.applied == 0
+    # exposure / enableGamma / render settings reset it (renderer.ts:176-303)
+    for s in ({"exposure": 2.0}, {"enableGamma": False}, {"maxBounces": 3}, {"rayEps": 1e-3},
+              {"backgroundColor": [0, 0, 0, 1]}):
+        before = v.applied
+        v.setSettings(s)
+        assert v.applied == before + 1, s
+    assert v.params.max_bounces == 3 and abs(v.params.ray_eps - 1e-3) < 1e-9
+    with pytest.raises(KeyError):
+        v.setSettings({"noSuchSetting": 1})
+
+
+def test_display_mode_mapping():
+    # renderer.ts:192 tonemappingModes; indexOf() of an unknown name is -1
+    assert _lib.display_params(toneMapping="None").tonemapping == 0
+    assert _lib.display_params(toneMapping="AcesFilm").tonemapping == 3
+    assert _lib.display_params(toneMapping="Uncharted2").tonemapping == -1
+    d = _lib.display_params(exposure=2.5, enableGamma=False, enableFxaa=True)
+    assert (d.exposure, d.gamma, d.fxaa) == (2.5, 0, 1)
+
+
+def test_request_mix_is_seeded_and_in_range():
+    a = synth.request_mix(3, 50, 8, 128 * 128, 1024 * 1024, 1, 64)
+    b = synth.request_mix(3, 50, 8, 128 * 128, 1024 * 1024, 1, 64)
+    assert [(r["scene"], r["width"], r["height"], r["spp"]) for r in a] == \
+           [(r["scene"], r["width"], r["height"], r["spp"]) for r in b]
+    for r in a:
+        npx = r["width"] * r["height"]
+        assert 0.9 * 128 * 128 <= npx <= 1.1 * 1024 * 1024
+        assert 1 <= r["spp"] <= 64 and 0 <= r["scene"] < 8 and 30 <= r["camera"].fov <= 90
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, port, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": "2", "LOCAL_RANK": str(rank)})
+    sys.path.insert(0, ROOT)
+    import bench
+    r, ws, local, dist = bench.dist_setup()
+    mx = bench.reduce_max(dist, 1.5 + r)
+    sm = bench.reduce_sum(dist, 1.0 + r)
+    bench.barrier(dist)
+    dist.destroy_process_group()
+    q.put((r, ws, local, mx, sm))
+
+
+def test_bench_replica_reductions_gloo_world_size_2():
+    """bench.py --gpus N: every rank renders its own replica; device time is
+    the max over ranks and rays the sum (no collective on the data path)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(k, port, q)) for k in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert [r[:3] for r in res] == [(0, 2, 0), (1, 2, 1)]
+    assert all(r[3] == 2.5 and r[4] == 3.0 for r in res)

@@ -99,3 +99,40 @@ def test_small_image_matches_reference(g):
     p = oracle_lib.make_params(g["cam_matrix"], fov, near, W, H, max_bounces=8)
     img = o.render_image(p, F)
     assert helpers.close_mask(img, g["image"], 1e-5, 1e-6).mean() > 0.999
+
+
+def _ulps(a, b):
+    ia = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    ib = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    return np.abs(ia - ib)
+
+
+@pytest.mark.parametrize("gamma", [0, 1])
+def test_display_restatement_matches_reference(g, gamma):
+    """tonemap.frag restated in numpy vs the reference shader's own output."""
+    from oracle import display_oracle
+    for k, mode in enumerate(g["display_modes"]):
+        ref = g[f"display_tonemap_g{gamma}"][k]
+        out = display_oracle.tonemap(g["display_hdr"], 1.7, gamma, int(mode))
+        # numpy's float32 pow vs the host libm: a few ulps; everything else exact
+        assert _ulps(out, ref).max() <= (0 if (gamma == 0 and mode != 2) else 4), f"mode {mode}"
+    np.testing.assert_array_equal(display_oracle.tonemap(g["display_hdr"], 1.7, 0, -1), g["display_hdr"])
+
+
+def test_fxaa_restatement_matches_reference(g):
+    from oracle import display_oracle
+    np.testing.assert_array_equal(display_oracle.fxaa(g["display_fxaa_in"]), g["display_fxaa"])
+    out = display_oracle.fxaa(display_oracle.tonemap(g["image"], 1.0, 1, 3))
+    assert _ulps(out, g["display_image_aces_fxaa"]).max() <= 4
+
+
+def test_display_golden_reproduces_from_reference_build(g):
+    from oracle import ref_lib
+    if not ref_lib.available("f32"):
+        pytest.skip("oracle/_ref not built (reference checkout absent)")
+    r = ref_lib.GlslReference("f32")
+    for gamma in (0, 1):
+        for k, mode in enumerate(g["display_modes"]):
+            np.testing.assert_array_equal(r.tonemap(g["display_hdr"], 1.7, gamma, int(mode)),
+                                          g[f"display_tonemap_g{gamma}"][k])
+    np.testing.assert_array_equal(r.fxaa(g["display_fxaa_in"]), g["display_fxaa"])
