@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "bvh_wide.h"
 #include "display.h"
 #include "dspbr.h"
 #include "engine.h"
@@ -72,6 +73,27 @@ static int settle(dspbr_ctx* c) {
   int rc = c->worker_rc;
   c->worker_rc = 0;
   return rc;
+}
+
+// Reference-layout nodes for the device: child index / count / first become
+// the shader's int() of the stored floats (int bits in lanes 3, 7, 11, 15).
+// Returns whether every box bound is finite.
+static bool convert_bvh_nodes(const float* nodes, uint32_t num_nodes, std::vector<float>& conv) {
+  bool finite = true;
+  conv.resize(size_t(num_nodes) * 16);
+  for (size_t i = 0; i < size_t(num_nodes); ++i) {
+    const float* src = nodes + i * 16;
+    float* dst = conv.data() + i * 16;
+    std::memcpy(dst, src, 16 * sizeof(float));
+    for (int k = 0; k < 16; ++k)
+      if (k % 4 != 3 && !std::isfinite(src[k])) finite = false;
+    for (int k = 3; k < 16; k += 4) {
+      float f = src[k];
+      int32_t v = (std::isfinite(f) && f > -2147483648.f && f < 2147483648.f) ? int32_t(f) : -1;
+      std::memcpy(dst + k, &v, 4);
+    }
+  }
+  return finite;
 }
 
 // Shading classes.  Surface hits are queued per class so that a warp of the
@@ -246,20 +268,8 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
   sc->bvh_build_ms = now_ms() - t0;
   if (num_bvh_nodes == 0) { delete sc; return s.fail(DSPBR_ERR_INVALID, "scene: empty BVH"); }
   t0 = now_ms();
-  // child index / count / first: the shader's int() of the stored floats
-  std::vector<float> conv(size_t(num_bvh_nodes) * 16);
-  for (size_t i = 0; i < size_t(num_bvh_nodes); ++i) {
-    const float* src = bvh_nodes + i * 16;
-    float* dst = conv.data() + i * 16;
-    std::memcpy(dst, src, 16 * sizeof(float));
-    for (int k = 0; k < 16; ++k)
-      if (k % 4 != 3 && !std::isfinite(src[k])) sc->boxes_finite = false;
-    for (int k = 3; k < 16; k += 4) {
-      float f = src[k];
-      int32_t v = (std::isfinite(f) && f > -2147483648.f && f < 2147483648.f) ? int32_t(f) : -1;
-      std::memcpy(dst + k, &v, 4);
-    }
-  }
+  std::vector<float> conv;
+  sc->boxes_finite = convert_bvh_nodes(bvh_nodes, num_bvh_nodes, conv);
   sc->num_nodes = num_bvh_nodes;
   sc->num_slots = num_bvh_indices;
   sc->num_tris = num_indices / 3;
@@ -280,6 +290,21 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
       (rc = s.cuda(cudaMemcpyAsync(remap.p, bvh_indices, size_t(num_bvh_indices) * 4, cudaMemcpyHostToDevice, c->stream), "upload remap"))) {
     delete sc;
     return rc;
+  }
+  {
+    // the 4-wide BVH for the path kernels, collapsed from the same binary tree
+    WideBvh wb = collapse_bvh4(conv.data(), num_bvh_nodes, num_bvh_indices);
+    sc->wroot = wb.root;
+    if ((rc = s.cuda(sc->wnodes.alloc(std::max<size_t>(wb.nodes.size(), 1) * 8), "alloc wide nodes")) ||
+        (rc = s.cuda(sc->wleaves.alloc(std::max<size_t>(wb.leaves.size(), 1)), "alloc wide leaves")) ||
+        (rc = s.cuda(cudaMemcpyAsync(sc->wnodes.p, wb.nodes.data(), wb.nodes.size() * sizeof(WideNode4),
+                                     cudaMemcpyHostToDevice, c->stream), "upload wide nodes")) ||
+        (rc = s.cuda(cudaMemcpyAsync(sc->wleaves.p, wb.leaves.data(), wb.leaves.size() * sizeof(WideLeaf),
+                                     cudaMemcpyHostToDevice, c->stream), "upload wide leaves")) ||
+        (rc = s.cuda(cudaStreamSynchronize(c->stream), "upload wide BVH"))) {
+      delete sc;
+      return rc;
+    }
   }
   sc->host_materials.assign(materials, materials + size_t(num_materials) * 68);
   sc->tri_material.resize(sc->num_tris);
@@ -527,6 +552,7 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
   Job job{};
   job.p = make_wave(c, uint32_t(c->sample_count + 1));
   job.s = c->scene->view();
+  job.s.wide = c->params.traversal == DSPBR_TRAVERSAL_WIDE;
   if (c->ibl) job.e = c->ibl->view();
   job.accum = reinterpret_cast<double*>(c->accum.p);
   const unsigned long long items = uint64_t(job.p.npix) * uint64_t(frames);
@@ -749,6 +775,20 @@ int dspbr_read_display_rgba8(dspbr_ctx* c, const dspbr_display* d, uint8_t* rgba
   return copy_out(c, rgba8, src, npix * 4, "read display");
 }
 
+int dspbr_bvh_wide(const float* nodes, uint32_t num_nodes, uint32_t num_indices, uint32_t* num_wide_nodes,
+                   uint32_t* num_wide_leaves, int32_t* root, float* wide_nodes, int32_t* wide_leaves) {
+  if (!nodes || num_nodes == 0) return DSPBR_ERR_INVALID;
+  std::vector<float> conv;
+  convert_bvh_nodes(nodes, num_nodes, conv);
+  WideBvh wb = collapse_bvh4(conv.data(), num_nodes, num_indices);
+  if (num_wide_nodes) *num_wide_nodes = uint32_t(wb.nodes.size());
+  if (num_wide_leaves) *num_wide_leaves = uint32_t(wb.leaves.size());
+  if (root) *root = wb.root;
+  if (wide_nodes && !wb.nodes.empty()) std::memcpy(wide_nodes, wb.nodes.data(), wb.nodes.size() * sizeof(WideNode4));
+  if (wide_leaves && !wb.leaves.empty()) std::memcpy(wide_leaves, wb.leaves.data(), wb.leaves.size() * sizeof(WideLeaf));
+  return DSPBR_OK;
+}
+
 int dspbr_display_image(dspbr_ctx* c, const float* rgba, int w, int h, const dspbr_display* d, float* out_rgba,
                         uint8_t* out_rgba8) {
   if (!c || !rgba || !d || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28)) return DSPBR_ERR_INVALID;
@@ -871,7 +911,9 @@ int dspbr_trace_closest(dspbr_ctx* c, const dspbr_scene* sc, const float* rays, 
   if ((rc = up(s, r, rays, size_t(n) * 8, c->stream)) || (rc = s.cuda(dt.alloc(std::max(n, 1u)), "alloc")) ||
       (rc = s.cuda(dtt.alloc(std::max(n, 1u)), "alloc")) || (rc = s.cuda(duv.alloc(2 * size_t(std::max(n, 1u))), "alloc")))
     return rc;
-  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 0, dt.p, dtt.p,
+  DevScene sv = sc->view();
+  sv.wide = c->params.traversal == DSPBR_TRAVERSAL_WIDE;
+  launch_trace_rays(sv, reinterpret_cast<const float4*>(r.p), n, 0, dt.p, dtt.p,
                     reinterpret_cast<float2*>(duv.p), nullptr, c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "trace")) || (rc = down(s, tri, dt, n, c->stream)) ||
       (rc = down(s, t, dtt, n, c->stream)) || (rc = down(s, uv, duv, 2 * size_t(n), c->stream)))
@@ -888,7 +930,9 @@ int dspbr_trace_occluded(dspbr_ctx* c, const dspbr_scene* sc, const float* rays,
   DevBuf<int32_t> o;
   int rc;
   if ((rc = up(s, r, rays, size_t(n) * 8, c->stream)) || (rc = s.cuda(o.alloc(std::max(n, 1u)), "alloc"))) return rc;
-  launch_trace_rays(sc->view(), reinterpret_cast<const float4*>(r.p), n, 1, nullptr, nullptr, nullptr, o.p,
+  DevScene sv = sc->view();
+  sv.wide = c->params.traversal == DSPBR_TRAVERSAL_WIDE;
+  launch_trace_rays(sv, reinterpret_cast<const float4*>(r.p), n, 1, nullptr, nullptr, nullptr, o.p,
                     c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "occluded")) || (rc = down(s, occ, o, n, c->stream))) return rc;
   return s.cuda(cudaStreamSynchronize(c->stream), "occluded");

@@ -31,8 +31,12 @@ struct DevScene {
   const uint32_t* __restrict__ indices;  // 3 per triangle
   const float4* __restrict__ materials;  // 17 float4 per material (68 floats)
   const uint8_t* __restrict__ tri_class;  // shading class per mesh triangle
+  const float4* __restrict__ wnodes;      // 4-wide BVH: 8 float4 per node (bvh_wide.h WideNode4)
+  const int2* __restrict__ wleaves;       // leaf-slot range [x, y) per wide leaf
+  int wroot;                              // >= 0: wide node; < 0: ~leaf (the binary root is a leaf)
   int num_nodes, num_slots, num_tris, num_materials;
   int boxes_finite;  // every node bound is finite (checked at upload)
+  int wide;          // closest-hit / any-hit queries of paths use the wide BVH
 };
 
 struct DevIbl {
@@ -212,6 +216,101 @@ DEV bool traverse_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfar, Hi
 }
 
 DEV bool finite3(v3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+// ---- 4-wide traversal ------------------------------------------------------------------
+// Same boxes, same slab arithmetic and same triangle test as the binary
+// traversal above, over the collapsed 4-wide tree: the children hit by the ray
+// are pushed far to near, so the nearest is visited first.  The closest t is
+// the same as the binary traversal's; when two triangles hit at exactly the
+// same t, the one tested first is kept, and the order of the tests differs.
+constexpr int kWideStack = 96;
+
+DEV void cswap(float& da, int& ca, float& db, int& cb) {
+  if (db < da) {
+    float t = da; da = db; db = t;
+    int c = ca; ca = cb; cb = c;
+  }
+}
+
+template <bool kAny, bool kExactNaN>
+DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfar, Hit& hit, bool& aborted) {
+  hit.t = tfar;
+  hit.tri = -1;
+  hit.u = hit.v = 0.f;
+  int stack[kWideStack];
+  int top = 0;
+  int cur = s.wroot;  // the next entry to visit is kept in a register
+  bool have = true;
+  int step = 0;
+  bool overflow = false;
+  for (; step < kMaxSteps && have; ++step) {
+    const int e = cur;
+    if (e < 0) {
+      const int2 lf = __ldg(s.wleaves + ~e);
+      for (int i = lf.x; i < lf.y; ++i) {
+        const float4* tp = s.tris + 3 * size_t(i);
+        float4 a = __ldg(tp);
+        int id = __float_as_int(a.w);
+        if (id < 0) continue;
+        float t, u, v;
+        if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
+          hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
+          if (kAny) { aborted = false; return true; }
+        }
+      }
+    } else {
+      const float4* nd = s.wnodes + 8 * size_t(e);
+      const float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+      const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+      const int4 ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
+      const int n = __ldg(reinterpret_cast<const int*>(nd + 7));
+      float d0 = n > 0 ? slab<kExactNaN>(make_float4(lx.x, ly.x, lz.x, 0.f), make_float4(hx.x, hy.x, hz.x, 0.f), org,
+                                         inv, hit.t)
+                       : kBvhFar;
+      float d1 = n > 1 ? slab<kExactNaN>(make_float4(lx.y, ly.y, lz.y, 0.f), make_float4(hx.y, hy.y, hz.y, 0.f), org,
+                                         inv, hit.t)
+                       : kBvhFar;
+      float d2 = n > 2 ? slab<kExactNaN>(make_float4(lx.z, ly.z, lz.z, 0.f), make_float4(hx.z, hy.z, hz.z, 0.f), org,
+                                         inv, hit.t)
+                       : kBvhFar;
+      float d3 = n > 3 ? slab<kExactNaN>(make_float4(lx.w, ly.w, lz.w, 0.f), make_float4(hx.w, hy.w, hz.w, 0.f), org,
+                                         inv, hit.t)
+                       : kBvhFar;
+      int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+      // ascending order of entry distance (5-comparator network)
+      cswap(d0, c0, d1, c1);
+      cswap(d2, c2, d3, c3);
+      cswap(d0, c0, d2, c2);
+      cswap(d1, c1, d3, c3);
+      cswap(d1, c1, d2, c2);
+      auto push = [&](float d, int c) {
+        if (d < kBvhFar) {
+          if (top < kWideStack) stack[top++] = c;
+          else overflow = true;
+        }
+      };
+      push(d3, c3);
+      push(d2, c2);
+      push(d1, c1);
+      if (d0 < kBvhFar) {  // nearest child next, without a trip through the stack
+        cur = c0;
+        continue;
+      }
+    }
+    if (top > 0) cur = stack[--top];
+    else have = false;
+  }
+  aborted = overflow || (have && step >= kMaxSteps);
+  return hit.tri >= 0;
+}
+
+template <bool kAny>
+DEV bool traverse_wide(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted) {
+  v3 inv = inv_dir(dir);
+  if (s.boxes_finite && finite3(org) && finite3(inv))
+    return traverse_wide_impl<kAny, false>(s, org, inv, dir, tfar, hit, aborted);
+  return traverse_wide_impl<kAny, true>(s, org, inv, dir, tfar, hit, aborted);
+}
 
 template <bool kAny>
 DEV bool traverse(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted, uint32_t* nodes_visited = nullptr,

@@ -122,7 +122,9 @@ void Engine::set_launch(const LaunchCfg& lc) {
     return;
   cudaStreamSynchronize(stream_);
   drop_graph();
+  const int trav = lc_.traversal;
   lc_ = lc;
+  lc_.traversal = trav;
 }
 
 Sched Engine::sched() const {
@@ -152,6 +154,7 @@ int Engine::set_job(int slot, const Job& job, unsigned long long items_total) {
   Status s{err_};
   if (slot < 0 || slot >= kMaxJobs) return s.fail(DSPBR_ERR_INVALID, "job slot %d out of range", slot);
   k_set_job<<<1, 32, 0, stream_>>>(job, items_total, slot, jobs_.p, js_.p, d_status_);
+  slot_traversal_[slot] = job.s.wide ? kTravWide : kTravReference;
   ++kind_launches[3];
   return s.cuda(cudaGetLastError(), "set job");
 }
@@ -172,6 +175,15 @@ int Engine::set_active(const std::vector<int>& order) {
   for (int i = 0; i < kMaxJobs; ++i) list.slot[i] = i < list.n ? order[i] : -1;
   k_set_active<<<1, kMaxJobs, 0, stream_>>>(list, active_.p);
   ++kind_launches[3];
+  // one traversal kind for all active jobs: launch the kernels specialised for it
+  int trav = order.empty() ? lc_.traversal : slot_traversal_[order[0]];
+  for (int k : order)
+    if (slot_traversal_[k] != trav) trav = kTravPerPath;
+  if (trav != lc_.traversal) {
+    TRY_CUDA(s, cudaStreamSynchronize(stream_), "sync");
+    drop_graph();
+    lc_.traversal = trav;
+  }
   return s.cuda(cudaGetLastError(), "set active jobs");
 }
 

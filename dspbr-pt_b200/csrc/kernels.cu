@@ -269,8 +269,20 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
 }
 
 // ---- extend: closest hit ------------------------------------------------------------------------
-template <bool kCount>
-__global__ void __launch_bounds__(256) k_extend(Sched sc, PathBuf b, int cur) {
+// Closest hit / any hit of one path ray with the traversal the variant names:
+// counting frames take the reference's binary traversal, whose node and
+// triangle counts define the algorithmic bytes of the roofline.
+template <bool kAny, bool kCount, int kTrav>
+DEV bool trace_path_ray(const DevScene& s, v3 org, v3 dir, float tfar, Hit& h, bool& aborted, uint32_t* nodes,
+                        uint32_t* tris) {
+  if (!kCount && (kTrav == kTravWide || (kTrav == kTravPerPath && s.wide)))
+    return traverse_wide<kAny>(s, org, dir, tfar, h, aborted);
+  return traverse<kAny>(s, org, dir, tfar, h, aborted, kCount ? nodes : nullptr, kCount ? tris : nullptr);
+}
+
+// 256 threads x 4 blocks per SM: at most 64 registers, 32 warps resident
+template <bool kCount, int kTrav>
+__global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -283,7 +295,7 @@ __global__ void __launch_bounds__(256) k_extend(Sched sc, PathBuf b, int cur) {
       const DevScene s = sc.jobs[b.job[slot]].s;
       float4 o = b.org[slot], d = b.dir[slot];
       Hit h;
-      traverse<false>(s, mk(o), mk(d), kTfarMax, h, aborted, kCount ? &nodes : nullptr, kCount ? &tris : nullptr);
+      trace_path_ray<false, kCount, kTrav>(s, mk(o), mk(d), kTfarMax, h, aborted, &nodes, &tris);
       b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
@@ -303,8 +315,8 @@ __global__ void __launch_bounds__(256) k_extend(Sched sc, PathBuf b, int cur) {
 }
 
 // ---- connect: NEE shadow rays (bvh.glsl:218-229) ---------------------------------------------
-template <bool kCount>
-__global__ void __launch_bounds__(256) k_connect(Sched sc, PathBuf b, int cur) {
+template <bool kCount, int kTrav>
+__global__ void __launch_bounds__(256, 4) k_connect(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[kCntShadow0 + cur];
   const uint32_t* qs = b.qs[cur];
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
@@ -323,8 +335,7 @@ __global__ void __launch_bounds__(256) k_connect(Sched sc, PathBuf b, int cur) {
         Hit h;
         bool ab = false;
         // isOccluded normalises the light direction (bvh.glsl:225-229)
-        if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
-                            kCount ? &tris : nullptr))
+        if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, &nodes, &tris))
           add = mk(b.sh_c[slot]);
         aborted |= ab;
         ++nrays;
@@ -333,8 +344,7 @@ __global__ void __launch_bounds__(256) k_connect(Sched sc, PathBuf b, int cur) {
         float4 d = b.pl_dir[slot];
         Hit h;
         bool ab = false;
-        if (!traverse<true>(s, org, normalize_rn(mk(d)), d.w, h, ab, kCount ? &nodes : nullptr,
-                            kCount ? &tris : nullptr))
+        if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, &nodes, &tris))
           add = add + mk(b.pl_c[slot]);
         aborted |= ab;
         ++nrays;
@@ -578,9 +588,11 @@ __global__ void __launch_bounds__(128) k_trace_rays(DevScene s, const float4* ra
     bool ab = false;
     if (any) {
       // isOccluded (bvh.glsl:225-229) normalises the direction first
-      occ[i] = traverse<true>(s, org, normalize_rn(dir), c.z, h, ab) ? 1 : 0;
+      const v3 nd = normalize_rn(dir);
+      occ[i] = (s.wide ? traverse_wide<true>(s, org, nd, c.z, h, ab) : traverse<true>(s, org, nd, c.z, h, ab)) ? 1 : 0;
     } else {
-      traverse<false>(s, org, dir, c.z, h, ab);
+      if (s.wide) traverse_wide<false>(s, org, dir, c.z, h, ab);
+      else traverse<false>(s, org, dir, c.z, h, ab);
       tri[i] = h.tri;
       t[i] = h.t;
       uv[i] = make_float2(h.u, h.v);
@@ -678,12 +690,18 @@ void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st) 
   k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur);
 }
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
-  if (count) k_extend<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
-  else k_extend<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
+  const dim3 g(lc.trace_blocks), t(lc.trace_threads);
+  if (count) k_extend<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_extend<false, kTravWide><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravReference) k_extend<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
+  else k_extend<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
-  if (count) k_connect<true><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
-  else k_connect<false><<<lc.trace_blocks, lc.trace_threads, 0, st>>>(sc, b, cur);
+  const dim3 g(lc.trace_blocks), t(lc.trace_threads);
+  if (count) k_connect<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_connect<false, kTravWide><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravReference) k_connect<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
+  else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st) {
   k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);

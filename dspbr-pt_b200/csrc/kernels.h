@@ -119,9 +119,14 @@ struct Sched {
   unsigned long long* iteration;
 };
 
+// Traversal of the path kernels: per path (the job's DevScene::wide), or one
+// kind for every path when all active jobs use the same (smaller kernels).
+enum : int { kTravPerPath = 0, kTravWide = 1, kTravReference = 2 };
+
 struct LaunchCfg {
   int trace_blocks = 148 * 16, trace_threads = 128;
   int shade_blocks = 148 * 8, shade_threads = 128;
+  int traversal = kTravPerPath;
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);

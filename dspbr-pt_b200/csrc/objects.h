@@ -19,6 +19,9 @@ struct dspbr_scene {
   dspbr::DevBuf<float4> nodes, tris, verts, materials;
   dspbr::DevBuf<uint32_t> indices;
   dspbr::DevBuf<uint8_t> tri_class;
+  dspbr::DevBuf<float4> wnodes;  // 4-wide BVH (8 float4 per node)
+  dspbr::DevBuf<int2> wleaves;
+  int wroot = 0;
   uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
   std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
   std::vector<float> host_materials;
@@ -31,11 +34,16 @@ struct dspbr_scene {
     s.num_nodes = int(num_nodes); s.num_slots = int(num_slots); s.num_tris = int(num_tris);
     s.num_materials = int(num_materials);
     s.tri_class = tri_class.p;
+    s.wnodes = wnodes.p;
+    s.wleaves = wleaves.p;
+    s.wroot = wroot;
+    s.wide = 1;
     s.boxes_finite = boxes_finite ? 1 : 0;
     return s;
   }
   uint64_t bytes() const {
-    return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes();
+    return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes() +
+           wnodes.bytes() + wleaves.bytes();
   }
 };
 

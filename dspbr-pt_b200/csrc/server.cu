@@ -127,6 +127,7 @@ Job job_of(const dspbr_request& r, double4* accum) {
   Job j{};
   j.p = make_job_params(r.params, r.camera, r.fov_deg, r.near_plane, r.width, r.height, r.ibl != nullptr, 1);
   j.s = r.scene->view();
+  j.s.wide = r.params.traversal == DSPBR_TRAVERSAL_WIDE;
   if (r.ibl) j.e = r.ibl->view();
   j.accum = reinterpret_cast<double*>(accum);
   return j;

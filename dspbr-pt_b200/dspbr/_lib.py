@@ -19,6 +19,7 @@ ERR = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", -4:
 PROFILE_FULL, PROFILE_LEAN = 0, 1
 RNG_MWC, RNG_PCG = 0, 1
 ENV_ALIAS, ENV_CDF = 0, 1
+TRAVERSAL_WIDE, TRAVERSAL_REFERENCE = 0, 1
 
 
 class DspbrError(RuntimeError):
@@ -34,7 +35,7 @@ class Params(C.Structure):
         ("clamp_threshold", C.c_float), ("point_light_position", C.c_float * 4),
         ("point_light_emission", C.c_float * 4), ("rr_start_depth", C.c_int32), ("rr_termination_prob", C.c_float),
         ("profile", C.c_int32), ("rng", C.c_int32), ("seed", C.c_uint64), ("env_sampling", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("traversal", C.c_int32), ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -125,6 +126,7 @@ SIGNATURES = {
     "dspbr_bvh_copy": (C.c_int, [_V, _F, _I]),
     "dspbr_bvh_error": (C.c_int, [_V, C.c_char_p, C.c_size_t]),
     "dspbr_bvh_free": (None, [_V]),
+    "dspbr_bvh_wide": (C.c_int, [_F, C.c_uint32, C.c_uint32, _U, _U, _I, _F, _I]),
     "dspbr_scene_create": (C.c_int, [_V, _F, C.c_uint32, _U, C.c_uint32, _F, C.c_uint32, _F, C.c_uint32, _I,
                                       C.c_uint32, _PV]),
     "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),

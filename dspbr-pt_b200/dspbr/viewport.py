@@ -219,6 +219,8 @@ def apply_settings(p, settings: dict, display: dict | None = None) -> None:
             p.env_sampling = _lib.ENV_CDF if v == "cdf" else _lib.ENV_ALIAS
         elif k == "russianRouletteStartDepth":
             p.rr_start_depth = int(v)
+        elif k == "traversal":
+            p.traversal = _lib.TRAVERSAL_REFERENCE if v == "reference" else _lib.TRAVERSAL_WIDE
         elif k == "materialProfile":
             p.profile = _lib.PROFILE_LEAN if v == "webgl-lean" else _lib.PROFILE_FULL
         else:

@@ -38,6 +38,7 @@ enum {
 
 enum { DSPBR_PROFILE_FULL = 0, DSPBR_PROFILE_LEAN = 1 };
 enum { DSPBR_RNG_MWC = 0, DSPBR_RNG_PCG = 1 };
+enum { DSPBR_TRAVERSAL_WIDE = 0, DSPBR_TRAVERSAL_REFERENCE = 1 };
 enum { DSPBR_ENV_ALIAS = 0, DSPBR_ENV_CDF = 1 };
 
 typedef struct dspbr_ctx dspbr_ctx;
@@ -64,7 +65,9 @@ typedef struct dspbr_params {
   int32_t rng;                    /* DSPBR_RNG_MWC = rng.glsl sequence; DSPBR_RNG_PCG = PCG32 per pixel/sample */
   uint64_t seed;                  /* PCG seed */
   int32_t env_sampling;           /* DSPBR_ENV_ALIAS (O(1), same pmf) or DSPBR_ENV_CDF (reference's binary search) */
-  int32_t reserved[7];
+  int32_t traversal;              /* DSPBR_TRAVERSAL_WIDE (4-wide BVH collapsed from the binary one) or
+                                     DSPBR_TRAVERSAL_REFERENCE (the binary traversal of bvh.glsl:149-229, bit for bit) */
+  int32_t reserved[6];
 } dspbr_params;
 
 /* PathtracingRendererDiagnostics (renderer.ts:79-110) plus throughput counters. */
@@ -105,6 +108,14 @@ int dspbr_bvh_info(const dspbr_bvh* bvh, uint32_t* num_nodes, uint32_t* num_indi
 int dspbr_bvh_copy(const dspbr_bvh* bvh, float* nodes, int32_t* indices);
 /* _get_last_error_ptr / _get_last_error_len */
 int dspbr_bvh_error(const dspbr_bvh* bvh, char* buf, size_t size);
+/* The 4-wide BVH the path kernels traverse (DSPBR_TRAVERSAL_WIDE), collapsed
+ * from a reference-layout BVH (16 floats per node): 32 words per wide node
+ * (float lo_x[4], lo_y[4], lo_z[4], hi_x[4], hi_y[4], hi_z[4]; int child[4];
+ * int count, pad[3]; child >= 0 wide node, < 0 ~leaf) and 2 ints per leaf
+ * (leaf-slot range [begin, end)).  root >= 0: wide node; < 0: ~leaf.  Call
+ * with NULL outputs for the sizes.  No context needed (host only). */
+int dspbr_bvh_wide(const float* nodes, uint32_t num_nodes, uint32_t num_indices, uint32_t* num_wide_nodes,
+                   uint32_t* num_wide_leaves, int32_t* root, float* wide_nodes, int32_t* wide_leaves);
 void dspbr_bvh_free(dspbr_bvh* bvh);
 
 /* ---- scene: replaces PathtracingSceneDataWebGL2.init + initBvh

@@ -27,9 +27,34 @@ def g():
     return helpers.load_golden()
 
 
+def ref_params():
+    """Default settings with the reference's binary traversal (the bit-exact suite's context)."""
+    p = _lib.default_params()
+    p.traversal = _lib.TRAVERSAL_REFERENCE
+    return p
+
+
+def set_traversal(ctx, mode):
+    import ctypes as C
+    p = _lib.default_params()
+    ctx.check(ctx.lib.dspbr_get_params(ctx.h, C.byref(p)))
+    p.traversal = mode
+    ctx.check(ctx.lib.dspbr_set_params(ctx.h, C.byref(p)))
+
+
 @pytest.fixture(scope="module")
 def ctx():
-    return Context(0)
+    """Bit-exact suite: the reference's binary traversal (bvh.glsl:149-229)."""
+    c = Context(0)
+    set_traversal(c, _lib.TRAVERSAL_REFERENCE)
+    return c
+
+
+@pytest.fixture(scope="module")
+def ctx_wide():
+    c = Context(0)
+    set_traversal(c, _lib.TRAVERSAL_WIDE)
+    return c
 
 
 @pytest.fixture(scope="module")
@@ -93,6 +118,39 @@ def test_closest_hit_bitexact_large_scene(ctx, ntris):
     np.testing.assert_array_equal(occ, (o.trace(rays, mode=2)[0] >= 0).astype(np.int32))
 
 
+@pytest.mark.parametrize("ntris", [20_000, 1_000_000])
+def test_wide_traversal_same_closest_t_as_reference(ctx, ctx_wide, ntris):
+    """DSPBR_TRAVERSAL_WIDE (the path kernels' default): same closest t and
+    hit/miss as the reference's binary traversal; the triangle differs only
+    when two triangles hit at exactly that t (the one tested first is kept)."""
+    sc = synth.make_sized(23, ntris, env_size=(16, 8))
+    bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    ds = DeviceScene(ctx, sc.vertices, sc.indices, sc.materials, bvh)
+    dsw = DeviceScene(ctx_wide, sc.vertices, sc.indices, sc.materials, bvh)
+    rays = helpers.random_rays(sc.vertices, 200_000, seed=24)
+    tri, t, uv = trace_gpu(ctx, ds, rays)
+    wtri, wt, wuv = trace_gpu(ctx_wide, dsw, rays)
+    assert (tri >= 0).sum() > 500  # sparse scenes: most random rays leave the scene
+    np.testing.assert_array_equal(wtri >= 0, tri >= 0)
+    np.testing.assert_array_equal(wt.view(np.uint32), t.view(np.uint32))
+    differ = wtri != tri
+    assert differ.mean() < 1e-3, differ.mean()
+    same = ~differ
+    np.testing.assert_array_equal(wuv[same].view(np.uint32), uv[same].view(np.uint32))
+    np.testing.assert_array_equal(trace_gpu(ctx_wide, dsw, rays, True), trace_gpu(ctx, ds, rays, True))
+
+
+def test_wide_traversal_golden(ctx_wide, g):
+    bvh = Bvh(g["bvh_nodes"], g["bvh_indices"], 0, g["indices"].size // 3)
+    ds = DeviceScene(ctx_wide, g["vertices"], g["indices"], g["materials"], bvh)
+    tri, t, uv = trace_gpu(ctx_wide, ds, g["rays"])
+    np.testing.assert_array_equal(t.view(np.uint32), g["hit_t"].view(np.uint32))
+    # the boxes stand on the floor: coplanar overlapping faces hit at exactly
+    # the same t, and the triangle kept is the one tested first
+    assert (tri != g["hit_tri"]).mean() < 0.01
+    np.testing.assert_array_equal(trace_gpu(ctx_wide, ds, g["rays"], True), g["occluded"])
+
+
 def test_empty_and_degenerate_rays(ctx, gscene, g):
     rays = np.zeros((6, 8), np.float32)
     rays[:, 6] = 1e5
@@ -145,13 +203,13 @@ def test_bsdf_matches_reference_golden(ctx, gscene, g):
 def test_bsdf_matches_oracle_many(ctx, gscene, g, lean):
     hit, wo, rnd = helpers.bsdf_queries(100_000, g["materials"].shape[0], seed=31 + lean)
     if lean:
-        p = _lib.default_params()
+        p = ref_params()
         p.profile = _lib.PROFILE_LEAN
         ctx.check(ctx.lib.dspbr_set_params(ctx.h, p))
     try:
         ev, sm, fl = bsdf_gpu(ctx, gscene, hit, wo, rnd)
     finally:
-        ctx.check(ctx.lib.dspbr_set_params(ctx.h, _lib.default_params()))
+        ctx.check(ctx.lib.dspbr_set_params(ctx.h, ref_params()))
     o = oracle_lib.Oracle()
     o.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
     rev, rsm, rfl = o.bsdf(hit, wo, rnd, "f32", lean)
@@ -208,14 +266,14 @@ def test_ibl_tables_large_env_bitexact(ctx):
 
 
 def _ibl_query(ctx, ibl, r2, dirs, mode):
-    p = _lib.default_params()
+    p = ref_params()
     p.env_sampling = mode
     ctx.check(ctx.lib.dspbr_set_params(ctx.h, p))
     n = r2.shape[0]
     sdp, pdf, rgb = np.zeros((n, 4), np.float32), np.zeros(n, np.float32), np.zeros((n, 3), np.float32)
     ctx.check(ctx.lib.dspbr_ibl_query(ctx.h, ibl.h, n, _lib.fptr(r2), _lib.fptr(dirs), _lib.fptr(sdp),
                                       _lib.fptr(pdf), _lib.fptr(rgb)))
-    ctx.check(ctx.lib.dspbr_set_params(ctx.h, _lib.default_params()))
+    ctx.check(ctx.lib.dspbr_set_params(ctx.h, ref_params()))
     return sdp, pdf, rgb
 
 
@@ -263,13 +321,14 @@ def _viewport(sc, W, H, settings):
     return v
 
 
-def test_image_matches_golden_path_for_path(g):
+@pytest.mark.parametrize("traversal", ["reference", "wide"])
+def test_image_matches_golden_path_for_path(g, traversal):
     sc = synth.Scene("golden", g["vertices"], g["indices"], g["image_scene_materials"],
                      synth.Camera(g["cam_matrix"], float(g["cam_fov_near_wh"][0]), float(g["cam_fov_near_wh"][1])),
                      env=g["image_env"])
     sc.bvh = Bvh(g["bvh_nodes"], g["bvh_indices"], 0, 0)
     W, H, F = (int(x) for x in g["image_whf"])
-    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf"})
+    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf", "traversal": traversal})
     v.start(F)
     img = v.readAccumulation()
     v.dispose()
@@ -279,11 +338,12 @@ def test_image_matches_golden_path_for_path(g):
     assert np.abs(img - g["image"]).mean() < 0.01 * g["image"][..., :3].mean()
 
 
-def test_image_mwc_matches_oracle_per_pixel():
+@pytest.mark.parametrize("traversal", ["reference", "wide"])
+def test_image_mwc_matches_oracle_per_pixel(traversal):
     sc = synth.make_small(0)
     sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
     W, H, F = 128, 128, 8
-    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf"})
+    v = _viewport(sc, W, H, {"maxBounces": 8, "envSampling": "cdf", "traversal": traversal})
     v.start(F)
     img = v.readAccumulation()
     d = v.diagnostics
