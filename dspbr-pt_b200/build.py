@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "dspbr", "libdspbr_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["api.cu", "engine.cu", "server.cu", "display.cu", "kernels.cu", "ibl.cu", "ibl_noalloc.cu", "bvh_build.cpp", "bvh_wide.cpp"]
+SOURCES = ["api.cu", "engine.cu", "server.cu", "display.cu", "kernels.cu", "ibl.cu", "ibl_noalloc.cu", "bvh_build.cpp", "bvh_wide.cpp", "bvh_gpu.cu"]
 
 
 # files whose arithmetic must round every operation like the shader it restates

@@ -14,6 +14,7 @@
 #include <thread>
 #include <vector>
 
+#include "bvh_gpu.h"
 #include "bvh_wide.h"
 #include "display.h"
 #include "dspbr.h"
@@ -136,6 +137,57 @@ static int classify_triangles(Status& s, dspbr_scene* sc, cudaStream_t st) {
   return s.cuda(cudaStreamSynchronize(st), "upload classes");
 }
 
+// Scene creation with the BVH built and collapsed on the device.
+static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t num_vertices,
+                                   const uint32_t* indices, uint32_t num_indices, const float* materials,
+                                   uint32_t num_materials, dspbr_scene** out) {
+  Status s = c->st();
+  std::unique_ptr<dspbr_scene> sc(new dspbr_scene());
+  sc->ctx = c;
+  sc->num_tris = num_indices / 3;
+  sc->num_verts = num_vertices;
+  sc->num_materials = num_materials;
+  double t0 = now_ms();
+  int rc;
+  if ((rc = s.cuda(sc->verts.alloc(size_t(num_vertices) * 5), "alloc vertices")) ||
+      (rc = s.cuda(sc->indices.alloc(num_indices), "alloc indices")) ||
+      (rc = s.cuda(sc->materials.alloc(size_t(num_materials) * 17), "alloc materials")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->verts.p, vertices, size_t(num_vertices) * 80, cudaMemcpyHostToDevice, c->stream), "upload vertices")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->indices.p, indices, size_t(num_indices) * 4, cudaMemcpyHostToDevice, c->stream), "upload indices")) ||
+      (rc = s.cuda(cudaMemcpyAsync(sc->materials.p, materials, size_t(num_materials) * 272, cudaMemcpyHostToDevice, c->stream), "upload materials")))
+    return rc;
+  DeviceBvh bin;
+  if ((rc = build_bvh_device(sc->verts.p, sc->indices.p, sc->num_tris, c->stream, &bin, s))) return rc;
+  DeviceWideBvh wide;
+  if ((rc = collapse_bvh4_device(bin, c->stream, &wide, s))) return rc;
+  sc->bvh_build_ms = now_ms() - t0;
+  t0 = now_ms();
+  sc->nodes.swap(bin.nodes);
+  sc->num_nodes = bin.num_nodes;
+  sc->num_slots = bin.num_slots;
+  sc->wnodes.swap(wide.nodes);
+  sc->wleaves.swap(wide.leaves);
+  sc->wroot = wide.root;
+  // the builder's boxes are unions of vertex positions: finite iff they are
+  for (uint32_t v = 0; v < num_vertices && sc->boxes_finite; ++v)
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(vertices[size_t(v) * 20 + k])) sc->boxes_finite = false;
+  sc->host_materials.assign(materials, materials + size_t(num_materials) * 68);
+  sc->tri_material.resize(sc->num_tris);
+  for (uint32_t t = 0; t < sc->num_tris; ++t)
+    sc->tri_material[t] = uint32_t(vertices[size_t(indices[3 * size_t(t)]) * 20 + 3]);
+  if ((rc = classify_triangles(s, sc.get(), c->stream))) return rc;
+  if ((rc = s.cuda(sc->tris.alloc(size_t(sc->num_slots) * 3), "alloc tris"))) return rc;
+  launch_gather_tris(sc->verts.p, sc->indices.p, bin.remap.p, sc->num_slots, sc->num_tris, sc->tris.p, c->stream);
+  if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) ||
+      (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload")))
+    return rc;
+  sc->device_remap.swap(bin.remap);
+  sc->upload_ms = now_ms() - t0;
+  *out = sc.release();
+  return DSPBR_OK;
+}
+
 extern "C" {
 
 void dspbr_params_default(dspbr_params* p) {
@@ -239,6 +291,9 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
       if (materials[size_t(m) * 68 + k] >= 0.f)
         return s.fail(DSPBR_ERR_INVALID, "scene: material %u uses a texture (record slot %d); textured materials are not supported", m, k);
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  if ((!bvh_nodes || !bvh_indices) && c->bvh_builder == DSPBR_BVH_BUILD_DEVICE)
+    return scene_create_device_bvh(c, vertices, num_vertices, indices, num_indices, materials, num_materials, out);
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   auto* sc = new dspbr_scene();
   sc->ctx = c;
   std::vector<float> host_nodes;
@@ -322,6 +377,38 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
   }
   sc->upload_ms = now_ms() - t0;
   *out = sc;
+  return DSPBR_OK;
+}
+
+int dspbr_set_bvh_builder(dspbr_ctx* c, int builder) {
+  if (!c || (builder != DSPBR_BVH_BUILD_HOST && builder != DSPBR_BVH_BUILD_DEVICE)) return DSPBR_ERR_INVALID;
+  c->bvh_builder = builder;
+  return DSPBR_OK;
+}
+
+int dspbr_scene_bvh(const dspbr_scene* sc, float* nodes, int32_t* remap, uint32_t* num_nodes, uint32_t* num_indices) {
+  if (!sc) return DSPBR_ERR_INVALID;
+  if (num_nodes) *num_nodes = sc->num_nodes;
+  if (num_indices) *num_indices = sc->num_slots;
+  Status s = sc->ctx->st();
+  TRY_CUDA(s, cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+  if (nodes) {
+    TRY_CUDA(s, cudaMemcpy(nodes, sc->nodes.p, size_t(sc->num_nodes) * 64, cudaMemcpyDeviceToHost), "read BVH");
+    for (size_t i = 0; i < size_t(sc->num_nodes) * 16; i += 4) {  // int bits back to the reference's floats
+      int32_t v;
+      std::memcpy(&v, nodes + i + 3, 4);
+      nodes[i + 3] = float(v);
+    }
+  }
+  if (remap) {
+    if (sc->device_remap.p) {
+      TRY_CUDA(s, cudaMemcpy(remap, sc->device_remap.p, size_t(sc->num_slots) * 4, cudaMemcpyDeviceToHost), "read remap");
+    } else {
+      std::vector<float4> t(size_t(sc->num_slots) * 3);
+      TRY_CUDA(s, cudaMemcpy(t.data(), sc->tris.p, t.size() * 16, cudaMemcpyDeviceToHost), "read remap");
+      for (size_t i = 0; i < sc->num_slots; ++i) std::memcpy(remap + i, &t[3 * i].w, 4);
+    }
+  }
   return DSPBR_OK;
 }
 

@@ -1,0 +1,425 @@
+// BVH construction on the device (linear BVH), emitting the reference's
+// binary node layout (bvh.glsl:1-6) so that every later stage -- the leaf
+// triangle gather, the 4-wide collapse, both traversals -- is unchanged.
+//
+// The reference builds its BVH on the host with TinyBVH (tinybvh_builder.ts);
+// the host binned-SAH builder here (bvh_build.cpp) plays that role and is the
+// default.  For large scenes admitted while others render, a host build of
+// seconds dominates the time to the first frame, so this builder trades some
+// tree quality for speed:
+//   1. per triangle: bounds and centroid; centroid bounds of the scene;
+//   2. 63-bit Morton codes of the centroids (21 bits per axis), sorted with
+//      the triangle index (CUB radix sort);
+//   3. the radix tree over the sorted codes (Karras, "Maximizing parallelism
+//      in the construction of BVHs, octrees, and k-d trees", HPG 2012), equal
+//      codes ordered by position;
+//   4. bounds and triangle counts bottom-up: each leaf walks towards the root,
+//      the second child to arrive at a node computes its union;
+//   5. output: subtrees of at most kLeafMax triangles become leaves (a
+//      subtree is a contiguous range of the sorted triangles); the other
+//      nodes store the boxes of their two children.
+// Node ids: internal node i -> i, triangle leaf j -> (n - 1) + j, so the root
+// is node 0 as the reference requires; nodes inside collapsed subtrees are
+// unreachable and stay zero.
+#include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "bvh_gpu.h"
+
+namespace dspbr {
+
+namespace {
+
+constexpr int kLeafMax = 4;
+
+__device__ __forceinline__ uint64_t spread21(uint32_t v) {
+  uint64_t x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
+struct Box {
+  float lo[3], hi[3];
+};
+
+__global__ void k_tri_bounds(const float4* __restrict__ verts, const uint32_t* __restrict__ idx, uint32_t n,
+                             float4* __restrict__ lo, float4* __restrict__ hi, float* __restrict__ block_bounds) {
+  __shared__ float red[6][256];
+  float c_lo[3] = {3.4e38f, 3.4e38f, 3.4e38f}, c_hi[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    float4 a = verts[5 * size_t(idx[3 * size_t(t)])], b = verts[5 * size_t(idx[3 * size_t(t) + 1])],
+           c = verts[5 * size_t(idx[3 * size_t(t) + 2])];
+    float4 l = make_float4(fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z)), 0.f);
+    float4 h = make_float4(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z)), 0.f);
+    lo[t] = l;
+    hi[t] = h;
+    float cx = 0.5f * (l.x + h.x), cy = 0.5f * (l.y + h.y), cz = 0.5f * (l.z + h.z);
+    c_lo[0] = fminf(c_lo[0], cx); c_lo[1] = fminf(c_lo[1], cy); c_lo[2] = fminf(c_lo[2], cz);
+    c_hi[0] = fmaxf(c_hi[0], cx); c_hi[1] = fmaxf(c_hi[1], cy); c_hi[2] = fmaxf(c_hi[2], cz);
+  }
+  for (int k = 0; k < 3; ++k) {
+    red[k][threadIdx.x] = c_lo[k];
+    red[3 + k][threadIdx.x] = c_hi[k];
+  }
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int k = 0; k < 3; ++k) {
+        red[k][threadIdx.x] = fminf(red[k][threadIdx.x], red[k][threadIdx.x + s]);
+        red[3 + k][threadIdx.x] = fmaxf(red[3 + k][threadIdx.x], red[3 + k][threadIdx.x + s]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) block_bounds[6 * blockIdx.x + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, uint32_t n,
+                         const float* __restrict__ block_bounds, int nblocks, uint64_t* __restrict__ keys,
+                         uint32_t* __restrict__ ids) {
+  __shared__ float sb[6];
+  if (threadIdx.x < 6) {
+    float v = threadIdx.x < 3 ? 3.4e38f : -3.4e38f;
+    for (int b = 0; b < nblocks; ++b) {
+      float x = block_bounds[6 * b + threadIdx.x];
+      v = threadIdx.x < 3 ? fminf(v, x) : fmaxf(v, x);
+    }
+    sb[threadIdx.x] = v;
+  }
+  __syncthreads();
+  const float ex = fmaxf(sb[3] - sb[0], 1e-30f), ey = fmaxf(sb[4] - sb[1], 1e-30f), ez = fmaxf(sb[5] - sb[2], 1e-30f);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    float4 l = lo[t], h = hi[t];
+    float cx = (0.5f * (l.x + h.x) - sb[0]) / ex, cy = (0.5f * (l.y + h.y) - sb[1]) / ey,
+          cz = (0.5f * (l.z + h.z) - sb[2]) / ez;
+    const float m = 2097151.f;  // 2^21 - 1
+    uint32_t ix = uint32_t(fminf(fmaxf(cx * m, 0.f), m)), iy = uint32_t(fminf(fmaxf(cy * m, 0.f), m)),
+             iz = uint32_t(fminf(fmaxf(cz * m, 0.f), m));
+    keys[t] = spread21(ix) << 2 | spread21(iy) << 1 | spread21(iz);
+    ids[t] = t;
+  }
+}
+
+// common prefix length of keys i and j, extended by the index for equal keys
+__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint64_t a = keys[i], b = keys[j];
+  if (a == b) return 64 + __clz(uint32_t(i ^ j));
+  return __clzll(a ^ b);
+}
+
+// Karras 2012: internal node i covers [first, last] of the sorted leaves and
+// splits after `split`.  child >= 0: internal node; child < 0: leaf ~index.
+__global__ void k_radix_tree(const uint64_t* __restrict__ keys, int n, int2* __restrict__ child,
+                             int2* __restrict__ range, int* __restrict__ parent) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;  // bounded: lmax <= 2n
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+      if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int len = l;
+    for (int t = (len + 1) >> 1;; t = (t + 1) >> 1) {
+      if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+      if (t == 1) break;
+    }
+    int split = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    int left = (first == split) ? ~split : split;
+    int right = (last == split + 1) ? ~(split + 1) : split + 1;
+    child[i] = make_int2(left, right);
+    range[i] = make_int2(first, last);
+    if (left >= 0) parent[left] = i;
+    else parent[(n - 1) + ~left] = i;
+    if (right >= 0) parent[right] = i;
+    else parent[(n - 1) + ~right] = i;
+  }
+}
+
+// Bounds and triangle counts bottom-up.  node_lo/hi/count index: internal i,
+// leaf j at (n - 1) + j.  flags: one arrival counter per internal node.
+__global__ void k_bounds_up(const float4* __restrict__ tlo, const float4* __restrict__ thi,
+                            const uint32_t* __restrict__ ids, int n, const int2* __restrict__ child,
+                            const int* __restrict__ parent, float4* node_lo, float4* node_hi, int* count,
+                            int* flags) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int leaf = (n - 1) + j;
+    node_lo[leaf] = tlo[ids[j]];
+    node_hi[leaf] = thi[ids[j]];
+    count[leaf] = 1;
+    __threadfence();
+    int p = parent[leaf];
+    // at most depth <= n - 1 steps; the second arrival at a node continues
+    for (int steps = 0; p >= 0 && steps < n; ++steps) {
+      if (atomicAdd(&flags[p], 1) == 0) break;
+      __threadfence();
+      const int2 c = child[p];
+      const int a = c.x >= 0 ? c.x : (n - 1) + ~c.x, b = c.y >= 0 ? c.y : (n - 1) + ~c.y;
+      const float4 la = __ldcg(node_lo + a), ha = __ldcg(node_hi + a), lb = __ldcg(node_lo + b),
+                   hb = __ldcg(node_hi + b);
+      node_lo[p] = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), 0.f);
+      node_hi[p] = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.f);
+      count[p] = __ldcg(count + a) + __ldcg(count + b);
+      __threadfence();
+      p = p == 0 ? -1 : parent[p];
+    }
+  }
+}
+
+__device__ __forceinline__ float ibits(int v) { return __int_as_float(v); }
+
+// Reference-layout nodes (int bits in lanes 3, 7, 11, 15) and the leaf-slot
+// remap (sorted triangle ids).
+__global__ void k_emit(int n, const int2* __restrict__ child, const int2* __restrict__ range,
+                       const float4* __restrict__ node_lo, const float4* __restrict__ node_hi,
+                       const int* __restrict__ count, const uint32_t* __restrict__ ids, float4* __restrict__ nodes,
+                       int32_t* __restrict__ remap) {
+  const int total = 2 * n - 1;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+    if (v < n) remap[v] = int32_t(ids[v]);
+    float4* o = nodes + 4 * size_t(v);
+    const bool is_leaf_prim = v >= n - 1;
+    const int cnt = count[v];
+    // a node is emitted as a leaf when its subtree is small (or it is a triangle)
+    const bool as_leaf = is_leaf_prim || cnt <= kLeafMax;
+    if (as_leaf) {
+      const int first = is_leaf_prim ? v - (n - 1) : range[v].x;
+      o[0] = make_float4(0.f, 0.f, 0.f, ibits(0));
+      o[1] = make_float4(0.f, 0.f, 0.f, ibits(0));
+      o[2] = make_float4(0.f, 0.f, 0.f, ibits(cnt));
+      o[3] = make_float4(0.f, 0.f, 0.f, ibits(first));
+      continue;
+    }
+    const int2 c = child[v];
+    const int a = c.x >= 0 ? c.x : (n - 1) + ~c.x, b = c.y >= 0 ? c.y : (n - 1) + ~c.y;
+    const float4 la = node_lo[a], ha = node_hi[a], lb = node_lo[b], hb = node_hi[b];
+    o[0] = make_float4(la.x, la.y, la.z, ibits(a));
+    o[1] = make_float4(ha.x, ha.y, ha.z, ibits(b));
+    o[2] = make_float4(lb.x, lb.y, lb.z, ibits(0));
+    o[3] = make_float4(hb.x, hb.y, hb.z, ibits(0));
+  }
+}
+
+// ---- 4-wide collapse, one frontier level per launch ---------------------------------------
+struct WideCounters {
+  int nodes, leaves, next;  // wide nodes and leaves allocated, entries of the next frontier
+};
+
+__device__ __forceinline__ int bin_int(const float4* nodes, int n, int lane) {
+  return __float_as_int(reinterpret_cast<const float*>(nodes + 4 * size_t(n))[lane]);
+}
+
+__device__ __forceinline__ float box_area(float lx, float ly, float lz, float hx, float hy, float hz) {
+  float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+  if (!(dx >= 0.f) || !(dy >= 0.f) || !(dz >= 0.f)) return 0.f;
+  return dx * dy + dy * dz + dz * dx;
+}
+
+struct WChild {
+  int node;
+  float lo[3], hi[3];
+};
+
+// children of binary inner node n, as bvh_push_child would push them
+__device__ int bin_children(const float4* nodes, uint32_t num_nodes, int n, WChild* out) {
+  const float4 n0 = nodes[4 * size_t(n)], n1 = nodes[4 * size_t(n) + 1], n2 = nodes[4 * size_t(n) + 2],
+               n3 = nodes[4 * size_t(n) + 3];
+  const int l = __float_as_int(n0.w), r = __float_as_int(n1.w);
+  int m = 0;
+  if (l >= 0 && uint32_t(l) < num_nodes && l != n) out[m++] = {l, {n0.x, n0.y, n0.z}, {n1.x, n1.y, n1.z}};
+  if (r >= 0 && uint32_t(r) < num_nodes && r != n) out[m++] = {r, {n2.x, n2.y, n2.z}, {n3.x, n3.y, n3.z}};
+  return m;
+}
+
+__global__ void k_collapse_level(const float4* __restrict__ bin, uint32_t num_nodes, uint32_t num_slots,
+                                 const int2* __restrict__ frontier, int count, int2* __restrict__ next,
+                                 float4* __restrict__ wnodes, int2* __restrict__ wleaves, WideCounters* ctr) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < count; f += gridDim.x * blockDim.x) {
+    const int2 e = frontier[f];  // (binary inner node, wide slot)
+    WChild kids[4];
+    int nk = bin_children(bin, num_nodes, e.x, kids);
+    for (int guard = 0; guard < 4; ++guard) {  // open the largest inner child while there is room
+      int best = -1;
+      float best_area = -1.f;
+      WChild grand[2];
+      for (int k = 0; k < nk; ++k) {
+        if (bin_int(bin, kids[k].node, 11) > 0) continue;  // a leaf
+        if (nk - 1 + bin_children(bin, num_nodes, kids[k].node, grand) > 4) continue;
+        float a = box_area(kids[k].lo[0], kids[k].lo[1], kids[k].lo[2], kids[k].hi[0], kids[k].hi[1], kids[k].hi[2]);
+        if (a > best_area) {
+          best_area = a;
+          best = k;
+        }
+      }
+      if (best < 0) break;
+      const int ng = bin_children(bin, num_nodes, kids[best].node, grand);
+      for (int k = best; k + 1 < nk; ++k) kids[k] = kids[k + 1];
+      --nk;
+      for (int k = 0; k < ng; ++k) kids[nk++] = grand[k];
+    }
+    float lo[3][4], hi[3][4];
+    int ch[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 4; ++k)
+      for (int a = 0; a < 3; ++a) lo[a][k] = hi[a][k] = 0.f;
+    for (int k = 0; k < nk; ++k) {
+      for (int a = 0; a < 3; ++a) {
+        lo[a][k] = kids[k].lo[a];
+        hi[a][k] = kids[k].hi[a];
+      }
+      const int c = kids[k].node;
+      const int cnt = bin_int(bin, c, 11);
+      if (cnt > 0) {  // a leaf: the slot range the reference's leaf loop tests
+        const int first = bin_int(bin, c, 15);
+        long long b0 = first > 0 ? first : 0;
+        long long b1 = (long long)first + (cnt < 64 ? cnt : 64);
+        if (b1 > (long long)num_slots) b1 = num_slots;
+        if (b1 < b0) b1 = b0;
+        const int li = atomicAdd(&ctr->leaves, 1);
+        wleaves[li] = make_int2(int(b0), int(b1));
+        ch[k] = ~li;
+      } else {
+        const int wi = atomicAdd(&ctr->nodes, 1);
+        next[atomicAdd(&ctr->next, 1)] = make_int2(c, wi);
+        ch[k] = wi;
+      }
+    }
+    float4* o = wnodes + 8 * size_t(e.y);
+    o[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    o[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    o[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    o[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    o[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    o[6] = make_float4(__int_as_float(ch[0]), __int_as_float(ch[1]), __int_as_float(ch[2]), __int_as_float(ch[3]));
+    o[7] = make_float4(__int_as_float(nk), 0.f, 0.f, 0.f);
+  }
+}
+
+int grid(size_t n, int threads, int cap) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  return int(b < size_t(cap) ? b : size_t(cap));
+}
+
+}  // namespace
+
+int build_bvh_device(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st, DeviceBvh* out,
+                     Status& s) {
+  if (ntris == 0) return s.fail(DSPBR_ERR_INVALID, "device BVH: no triangles");
+  if (ntris > (1u << 28)) return s.fail(DSPBR_ERR_INVALID, "device BVH: too many triangles");
+  const int n = int(ntris);
+  const int total = 2 * n - 1;
+  DevBuf<float4> tlo, thi, nlo, nhi;
+  DevBuf<float> bb;
+  DevBuf<uint64_t> keys, keys2;
+  DevBuf<uint32_t> ids, ids2;
+  DevBuf<int2> child, range;
+  DevBuf<int> parent, count, flags;
+  const int nb = grid(ntris, 256, 148 * 4);
+  TRY_CUDA(s, tlo.alloc(n), "device BVH");
+  TRY_CUDA(s, thi.alloc(n), "device BVH");
+  TRY_CUDA(s, bb.alloc(6 * size_t(nb)), "device BVH");
+  TRY_CUDA(s, keys.alloc(n), "device BVH");
+  TRY_CUDA(s, keys2.alloc(n), "device BVH");
+  TRY_CUDA(s, ids.alloc(n), "device BVH");
+  TRY_CUDA(s, ids2.alloc(n), "device BVH");
+  TRY_CUDA(s, nlo.alloc(total), "device BVH");
+  TRY_CUDA(s, nhi.alloc(total), "device BVH");
+  TRY_CUDA(s, count.alloc(total), "device BVH");
+  TRY_CUDA(s, parent.alloc(total), "device BVH");
+  TRY_CUDA(s, child.alloc(std::max(n - 1, 1)), "device BVH");
+  TRY_CUDA(s, range.alloc(std::max(n - 1, 1)), "device BVH");
+  TRY_CUDA(s, flags.alloc(std::max(n - 1, 1)), "device BVH");
+  TRY_CUDA(s, out->nodes.alloc(size_t(total) * 4), "device BVH");
+  TRY_CUDA(s, out->remap.alloc(n), "device BVH");
+  k_tri_bounds<<<nb, 256, 0, st>>>(verts, indices, ntris, tlo.p, thi.p, bb.p);
+  k_morton<<<grid(ntris, 256, 148 * 8), 256, 0, st>>>(tlo.p, thi.p, ntris, bb.p, nb, keys.p, ids.p);
+  size_t temp = 0;
+  TRY_CUDA(s, cub::DeviceRadixSort::SortPairs(nullptr, temp, keys.p, keys2.p, ids.p, ids2.p, n, 0, 63, st),
+           "device BVH sort");
+  DevBuf<unsigned char> tmp;
+  TRY_CUDA(s, tmp.alloc(std::max<size_t>(temp, 1)), "device BVH");
+  TRY_CUDA(s, cub::DeviceRadixSort::SortPairs(tmp.p, temp, keys.p, keys2.p, ids.p, ids2.p, n, 0, 63, st),
+           "device BVH sort");
+  TRY_CUDA(s, cudaMemsetAsync(parent.p, 0xff, parent.bytes(), st), "device BVH");
+  TRY_CUDA(s, cudaMemsetAsync(flags.p, 0, flags.bytes(), st), "device BVH");
+  if (n > 1) k_radix_tree<<<grid(n - 1, 256, 148 * 8), 256, 0, st>>>(keys2.p, n, child.p, range.p, parent.p);
+  k_bounds_up<<<grid(n, 256, 148 * 8), 256, 0, st>>>(tlo.p, thi.p, ids2.p, n, child.p, parent.p, nlo.p, nhi.p,
+                                                      count.p, flags.p);
+  TRY_CUDA(s, cudaMemsetAsync(out->nodes.p, 0, out->nodes.bytes(), st), "device BVH");
+  k_emit<<<grid(total, 256, 148 * 8), 256, 0, st>>>(n, child.p, range.p, nlo.p, nhi.p, count.p, ids2.p, out->nodes.p,
+                                                    out->remap.p);
+  TRY_CUDA(s, cudaGetLastError(), "device BVH");
+  // the temporaries are freed at return: wait for the kernels that use them
+  TRY_CUDA(s, cudaStreamSynchronize(st), "device BVH");
+  out->num_nodes = uint32_t(total);
+  out->num_slots = uint32_t(n);
+  return DSPBR_OK;
+}
+
+int collapse_bvh4_device(const DeviceBvh& bin, cudaStream_t st, DeviceWideBvh* out, Status& s) {
+  const uint32_t nn = bin.num_nodes;
+  if (nn == 0) return s.fail(DSPBR_ERR_INVALID, "wide BVH: empty tree");
+  // the root: a leaf root is tested without a box; otherwise wide node 0
+  int32_t root_cnt = 0, root_first = 0;
+  TRY_CUDA(s, cudaMemcpyAsync(&root_cnt, reinterpret_cast<const char*>(bin.nodes.p) + 44, 4, cudaMemcpyDeviceToHost, st),
+           "wide BVH");
+  TRY_CUDA(s, cudaMemcpyAsync(&root_first, reinterpret_cast<const char*>(bin.nodes.p) + 60, 4, cudaMemcpyDeviceToHost,
+                              st), "wide BVH");
+  TRY_CUDA(s, cudaStreamSynchronize(st), "wide BVH");
+  TRY_CUDA(s, out->leaves.alloc(nn), "wide BVH");
+  if (root_cnt > 0) {
+    long long b0 = root_first > 0 ? root_first : 0;
+    long long b1 = (long long)root_first + (root_cnt < 64 ? root_cnt : 64);
+    if (b1 > (long long)bin.num_slots) b1 = bin.num_slots;
+    if (b1 < b0) b1 = b0;
+    int2 lf = make_int2(int(b0), int(b1));
+    TRY_CUDA(s, cudaMemcpyAsync(out->leaves.p, &lf, sizeof lf, cudaMemcpyHostToDevice, st), "wide BVH");
+    TRY_CUDA(s, out->nodes.alloc(8), "wide BVH");
+    TRY_CUDA(s, cudaStreamSynchronize(st), "wide BVH");
+    out->root = ~0;
+    out->num_nodes = 0;
+    out->num_leaves = 1;
+    return DSPBR_OK;
+  }
+  // each wide node holds >= 2 children, so there are fewer wide nodes than binary inner nodes
+  TRY_CUDA(s, out->nodes.alloc(size_t(nn) * 8), "wide BVH");
+  DevBuf<int2> fa, fb;
+  DevBuf<WideCounters> ctr;
+  TRY_CUDA(s, fa.alloc(nn), "wide BVH");
+  TRY_CUDA(s, fb.alloc(nn), "wide BVH");
+  TRY_CUDA(s, ctr.alloc(1), "wide BVH");
+  WideCounters h{1, 0, 0};  // wide node 0 is the root
+  int2 first = make_int2(0, 0);
+  TRY_CUDA(s, cudaMemcpyAsync(ctr.p, &h, sizeof h, cudaMemcpyHostToDevice, st), "wide BVH");
+  TRY_CUDA(s, cudaMemcpyAsync(fa.p, &first, sizeof first, cudaMemcpyHostToDevice, st), "wide BVH");
+  int count = 1;
+  int2* cur = fa.p;
+  int2* nxt = fb.p;
+  for (uint32_t level = 0; count > 0 && level <= nn; ++level) {
+    TRY_CUDA(s, cudaMemsetAsync(&ctr.p->next, 0, sizeof(int), st), "wide BVH");
+    k_collapse_level<<<grid(count, 128, 148 * 8), 128, 0, st>>>(bin.nodes.p, nn, bin.num_slots, cur, count, nxt,
+                                                               out->nodes.p, out->leaves.p, ctr.p);
+    TRY_CUDA(s, cudaGetLastError(), "wide BVH");
+    TRY_CUDA(s, cudaMemcpyAsync(&h, ctr.p, sizeof h, cudaMemcpyDeviceToHost, st), "wide BVH");
+    TRY_CUDA(s, cudaStreamSynchronize(st), "wide BVH");
+    count = h.next;
+    std::swap(cur, nxt);
+  }
+  if (count != 0) return s.fail(DSPBR_ERR_INVALID, "wide BVH: the tree does not end (cyclic input)");
+  out->root = 0;
+  out->num_nodes = uint32_t(h.nodes);
+  out->num_leaves = uint32_t(h.leaves);
+  return DSPBR_OK;
+}
+
+}  // namespace dspbr

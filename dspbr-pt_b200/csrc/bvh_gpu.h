@@ -1,0 +1,33 @@
+// BVH construction and 4-wide collapse on the device (bvh_gpu.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "host.h"
+
+namespace dspbr {
+
+// A binary BVH in the device layout of DevScene::nodes (reference layout,
+// child / count / first as int bits) and its leaf-slot remap.
+struct DeviceBvh {
+  DevBuf<float4> nodes;  // 4 float4 per node
+  DevBuf<int32_t> remap;
+  uint32_t num_nodes = 0, num_slots = 0;
+};
+
+// Linear BVH over the triangles (verts: 5 float4 per vertex, position in the
+// first; indices: 3 per triangle).  Synchronises `st` before returning.
+int build_bvh_device(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st, DeviceBvh* out,
+                     Status& s);
+
+// 4-wide collapse of a well-formed binary BVH already on the device (the same
+// rule as collapse_bvh4, level by level).  wnodes: 8 float4 per wide node.
+struct DeviceWideBvh {
+  DevBuf<float4> nodes;
+  DevBuf<int2> leaves;
+  int32_t root = 0;
+  uint32_t num_nodes = 0, num_leaves = 0;
+};
+int collapse_bvh4_device(const DeviceBvh& bin, cudaStream_t st, DeviceWideBvh* out, Status& s);
+
+}  // namespace dspbr

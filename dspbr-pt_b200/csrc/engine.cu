@@ -303,6 +303,21 @@ int Engine::iterate(int n, bool counting, int* done) {
 
 bool Engine::job_done(int slot) const { return h_status_ && h_status_->job[slot].done != 0u; }
 
+int Engine::drain() {
+  const Sched sc = sched();
+  const PathBuf b = paths();
+  const int cur = cur_;
+  mark_begin(2);
+  launch_connect(sc, b, cur, false, lc_, stream_);
+  launch_drain(sc, b, cur, stream_);
+  launch_commit(sc, b, cur, stream_, false);
+  mark_end();
+  kind_launches[1] += 1;
+  kind_launches[3] += 2;
+  cur_ ^= 1;
+  return Status{err_}.cuda(cudaGetLastError(), "drain");
+}
+
 int Engine::run_until_done(int slot, unsigned long long max_iter, bool counting) {
   Status s{err_};
   unsigned long long it = 0;
@@ -317,6 +332,14 @@ int Engine::run_until_done(int slot, unsigned long long max_iter, bool counting)
     if (k > kLookahead) {
       TRY_CUDA(s, cudaEventSynchronize(ring_[(k - 1 - kLookahead) % kRing]), "render");
       if (job_done(slot)) return DSPBR_OK;
+      // the tail: every work item started and few paths left
+      const volatile JobStatus& js = h_status_->job[slot];
+      if (!counting && js.items_next >= js.items_total && h_status_->live_paths < kDrainBelow) {
+        int rc2 = drain();
+        if (rc2) return rc2;
+        TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");
+        if (job_done(slot)) return DSPBR_OK;
+      }
     }
   }
   TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");

@@ -49,6 +49,10 @@ class Engine {
   // Runs iterations until job `slot` has started all items and has no live
   // path, keeping `lookahead` steps queued; `max_iter` bounds the loop.
   int run_until_done(int slot, unsigned long long max_iter, bool counting);
+  // Finishes every path in the pool in one launch (connect of the pending
+  // shadow rays, then each path run to its end).  Only when no active job has
+  // unstarted work items.
+  int drain();
   bool job_done(int slot) const;
   const volatile HostStatus* status() const { return h_status_; }
 
@@ -99,6 +103,7 @@ class Engine {
   cudaGraphExec_t graph_ = nullptr;
   // loop events and profiling events
   static constexpr int kRing = 8, kLookahead = 4;
+  static constexpr unsigned kDrainBelow = 1u << 16;  // live paths below which a render call drains
   cudaEvent_t ring_[kRing] = {};
   std::vector<cudaEvent_t> ev_pool_;
   std::vector<std::pair<int, int>> ev_marks_;

@@ -34,6 +34,10 @@ struct DevBuf {
     return e;
   }
   size_t bytes() const { return n * sizeof(T); }
+  void swap(DevBuf& o) {
+    T* tp = p; p = o.p; o.p = tp;
+    size_t tn = n; n = o.n; o.n = tn;
+  }
 };
 
 // Error reporting into a context's last-error string.

@@ -223,14 +223,16 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
 }
 
 // ---- commit: book-keeping of one iteration (one block of kMaxJobs threads) -----------------
-__global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cur) {
+// regen_ran = false (after a drain): no work item was handed out, only the
+// counters and the status are updated.
+__global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cur, int regen_ran) {
   __shared__ unsigned long long scan[kMaxJobs];
   const int n = min(*sc.nactive, kMaxJobs);
   int j;
   unsigned long long rem = remaining(sc, threadIdx.x, n, j), total;
   unsigned long long pre = block_scan(rem, scan, total, n);
   const unsigned long long head = *b.free_head;
-  const unsigned long long avail = min(*b.free_tail - head, total);
+  const unsigned long long avail = regen_ran ? min(*b.free_tail - head, total) : 0ull;
   // the regen that just ran gave job a the items [pre, pre + rem) clipped to avail
   if (j >= 0 && avail > pre) {
     unsigned long long took = min(avail - pre, rem);
@@ -315,6 +317,38 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
 }
 
 // ---- connect: NEE shadow rays (bvh.glsl:218-229) ---------------------------------------------
+// The NEE shadow rays of one path vertex (IBL and point light): visible
+// contributions are added to the path radiance.
+template <bool kCount, int kTrav>
+DEV void connect_slot(const Sched& sc, const PathBuf& b, uint32_t slot, bool& aborted, int& nrays, uint32_t* nodes,
+                      uint32_t* tris) {
+  const DevScene s = sc.jobs[b.job[slot]].s;
+  int flags = b.sh_flags[slot];
+  v3 org = mk(b.org[slot]);
+  v3 add = mk(0.f);
+  if (flags & 1) {
+    float4 d = b.sh_dir[slot];
+    Hit h;
+    bool ab = false;
+    // isOccluded normalises the light direction (bvh.glsl:225-229)
+    if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, nodes, tris))
+      add = mk(b.sh_c[slot]);
+    aborted |= ab;
+    ++nrays;
+  }
+  if (flags & 2) {
+    float4 d = b.pl_dir[slot];
+    Hit h;
+    bool ab = false;
+    if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, nodes, tris))
+      add = add + mk(b.pl_c[slot]);
+    aborted |= ab;
+    ++nrays;
+  }
+  float4 L = b.rad[slot];
+  b.rad[slot] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+}
+
 template <bool kCount, int kTrav>
 __global__ void __launch_bounds__(256, 4) k_connect(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[kCntShadow0 + cur];
@@ -324,34 +358,7 @@ __global__ void __launch_bounds__(256, 4) k_connect(Sched sc, PathBuf b, int cur
     bool aborted = false;
     int nrays = 0;
     uint32_t nodes = 0, tris = 0;
-    if (i < count) {
-      uint32_t slot = qs[i];
-      const DevScene s = sc.jobs[b.job[slot]].s;
-      int flags = b.sh_flags[slot];
-      v3 org = mk(b.org[slot]);
-      v3 add = mk(0.f);
-      if (flags & 1) {
-        float4 d = b.sh_dir[slot];
-        Hit h;
-        bool ab = false;
-        // isOccluded normalises the light direction (bvh.glsl:225-229)
-        if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, &nodes, &tris))
-          add = mk(b.sh_c[slot]);
-        aborted |= ab;
-        ++nrays;
-      }
-      if (flags & 2) {
-        float4 d = b.pl_dir[slot];
-        Hit h;
-        bool ab = false;
-        if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, &nodes, &tris))
-          add = add + mk(b.pl_c[slot]);
-        aborted |= ab;
-        ++nrays;
-      }
-      float4 L = b.rad[slot];
-      b.rad[slot] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
-    }
+    if (i < count) connect_slot<kCount, kTrav>(sc, b, qs[i], aborted, nrays, &nodes, &tris);
     unsigned m1 = __ballot_sync(0xffffffffu, nrays >= 1), m2 = __ballot_sync(0xffffffffu, nrays >= 2);
     if ((threadIdx.x & 31) == 0 && (m1 | m2)) atomicAdd(b.stats + 1, (unsigned long long)(__popc(m1) + __popc(m2)));
     count_warp(b.stats + 2, aborted);
@@ -551,6 +558,54 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
   }
 }
 
+// ---- drain: the last paths of a render call, each run to completion ---------------------
+// Once every work item has started and few paths are left, the remaining
+// bounces are latency-bound: each wavefront iteration costs about the latency
+// of its slowest ray whatever the number of paths.  This kernel takes the
+// paths queued for the next extend (their pending shadow rays were connected
+// by the k_connect launched before it) and runs every path through extend ->
+// shade_miss / shade -> connect until it ends: the same device functions in
+// the same order per path, so each path's result is unchanged.
+__global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
+  const uint32_t count = b.counts[cur];
+  const uint32_t* q = b.q[cur];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    uint32_t slot = 0, job = 0, closest = 0, shadow_rays = 0;
+    bool aborted = false;
+    if (i < count) {
+      slot = q[i];
+      job = b.job[slot];
+      for (int guard = 0; guard < 4 * kMaxSteps; ++guard) {
+        const DevScene s = sc.jobs[job].s;
+        float4 o = b.org[slot], d = b.dir[slot];
+        Hit h;
+        bool ab = false;
+        trace_path_ray<false, false, kTravPerPath>(s, mk(o), mk(d), kTfarMax, h, ab, nullptr, nullptr);
+        aborted |= ab;
+        ++closest;
+        b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+        if (h.tri < 0) {
+          shade_miss_path(sc, b, slot);
+          break;
+        }
+        bool shadow = false;
+        const bool cont = shade_path(sc, b, slot, shadow);
+        if (shadow) {
+          int nrays = 0;
+          connect_slot<false, kTravPerPath>(sc, b, slot, aborted, nrays, nullptr, nullptr);
+          shadow_rays += uint32_t(nrays);
+        }
+        if (!cont) break;
+      }
+    }
+    free_slots(sc, b, i < count, slot, job);
+    add_warp(b.stats + 0, closest);
+    add_warp(b.stats + 1, shadow_rays);
+    count_warp(b.stats + 2, aborted);
+  }
+}
+
 __global__ void k_mean(const double4* accum, double inv, float4* out, int npix) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
     double4 a = accum[i];
@@ -686,8 +741,8 @@ void launch_init_pool(const PathBuf& b, cudaStream_t st) {
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st) {
   k_regen<<<grid_for(b.capacity, kMaxJobs, 148 * 8), kMaxJobs, 0, st>>>(sc, b, next);
 }
-void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st) {
-  k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur);
+void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran) {
+  k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur, regen_ran ? 1 : 0);
 }
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
@@ -705,6 +760,9 @@ void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, cons
 }
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st) {
   k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
+}
+void launch_drain(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st) {
+  k_drain<<<148 * 4, 128, 0, st>>>(sc, b, cur);
 }
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
   k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(sc, b);

@@ -135,7 +135,9 @@ void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st);
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
-void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st);
+void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
+// runs every path queued in q[cur] to its end (call after connect(cur), when no work item is left)
+void launch_drain(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
 
 // kernel-level queries (device buffers)

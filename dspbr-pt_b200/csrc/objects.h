@@ -22,6 +22,7 @@ struct dspbr_scene {
   dspbr::DevBuf<float4> wnodes;  // 4-wide BVH (8 float4 per node)
   dspbr::DevBuf<int2> wleaves;
   int wroot = 0;
+  dspbr::DevBuf<int32_t> device_remap;  // leaf-slot remap of a device-built BVH
   uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
   std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
   std::vector<float> host_materials;
@@ -43,7 +44,7 @@ struct dspbr_scene {
   }
   uint64_t bytes() const {
     return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes() +
-           wnodes.bytes() + wleaves.bytes();
+           wnodes.bytes() + wleaves.bytes() + device_remap.bytes();
   }
 };
 
@@ -76,6 +77,7 @@ struct dspbr_ctx {
   dspbr_scene* scene = nullptr;
   dspbr_ibl* ibl = nullptr;
   uint32_t wave_paths = 1u << 21;
+  int bvh_builder = DSPBR_BVH_BUILD_HOST;  // for scenes created without a BVH
   std::unique_ptr<dspbr::Engine> eng;  // path pool + job table; this context's render is job slot 0
   // render_async: the iteration loop runs on a worker thread
   std::thread worker;

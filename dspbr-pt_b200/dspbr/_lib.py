@@ -20,6 +20,7 @@ PROFILE_FULL, PROFILE_LEAN = 0, 1
 RNG_MWC, RNG_PCG = 0, 1
 ENV_ALIAS, ENV_CDF = 0, 1
 TRAVERSAL_WIDE, TRAVERSAL_REFERENCE = 0, 1
+BVH_BUILD_HOST, BVH_BUILD_DEVICE = 0, 1
 
 
 class DspbrError(RuntimeError):
@@ -129,6 +130,8 @@ SIGNATURES = {
     "dspbr_bvh_wide": (C.c_int, [_F, C.c_uint32, C.c_uint32, _U, _U, _I, _F, _I]),
     "dspbr_scene_create": (C.c_int, [_V, _F, C.c_uint32, _U, C.c_uint32, _F, C.c_uint32, _F, C.c_uint32, _I,
                                       C.c_uint32, _PV]),
+    "dspbr_set_bvh_builder": (C.c_int, [_V, C.c_int]),
+    "dspbr_scene_bvh": (C.c_int, [_V, _F, _I, _U, _U]),
     "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),
     "dspbr_scene_device_bytes": (C.c_int, [_V, C.POINTER(C.c_uint64)]),
     "dspbr_scene_destroy": (C.c_int, [_V]),

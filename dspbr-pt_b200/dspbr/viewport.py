@@ -79,6 +79,11 @@ class Context:
     def check(self, rc):
         check(rc, self.h)
 
+    def set_bvh_builder(self, builder: str) -> None:
+        """BVH builder of scenes created without one: "host" (binned SAH) or "device" (linear BVH)."""
+        self.check(self.lib.dspbr_set_bvh_builder(self.h, _lib.BVH_BUILD_DEVICE if builder == "device"
+                                                  else _lib.BVH_BUILD_HOST))
+
     def host_array(self, shape, dtype=np.float32) -> np.ndarray:
         """numpy array over page-locked host memory (dspbr_host_alloc)."""
         import weakref
@@ -114,6 +119,15 @@ class DeviceScene:
     def update_materials(self, materials, first: int = 0):
         m = f32(materials).reshape(-1, MATERIAL_STRIDE)
         self.ctx.check(self.ctx.lib.dspbr_scene_update_materials(self.h, fptr(m), first, m.shape[0]))
+
+    def bvh(self) -> "Bvh":
+        """The scene's binary BVH in the reference layout, read back from the device."""
+        nn, ni = C.c_uint32(), C.c_uint32()
+        self.ctx.check(self.ctx.lib.dspbr_scene_bvh(self.h, None, None, C.byref(nn), C.byref(ni)))
+        nodes = np.zeros(nn.value * 16, np.float32)
+        remap = np.zeros(ni.value, np.int32)
+        self.ctx.check(self.ctx.lib.dspbr_scene_bvh(self.h, fptr(nodes), iptr(remap), None, None))
+        return Bvh(nodes, remap, 0, self.num_triangles)
 
     def device_bytes(self) -> int:
         b = C.c_uint64()
@@ -182,7 +196,7 @@ def look_at_matrix(position, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
     return e
 
 
-DISPLAY_SETTINGS = ("exposure", "toneMapping", "pixelRatio", "interactionPixelRatio", "enableGamma", "enableFxaa",
+DISPLAY_SETTINGS = ("bvhBuilder", "exposure", "toneMapping", "pixelRatio", "interactionPixelRatio", "enableGamma", "enableFxaa",
                     "tileResolution", "debugMode")
 
 
@@ -221,6 +235,9 @@ def apply_settings(p, settings: dict, display: dict | None = None) -> None:
             p.rr_start_depth = int(v)
         elif k == "traversal":
             p.traversal = _lib.TRAVERSAL_REFERENCE if v == "reference" else _lib.TRAVERSAL_WIDE
+        elif k == "bvhBuilder":
+            if display is not None:
+                display[k] = v
         elif k == "materialProfile":
             p.profile = _lib.PROFILE_LEAN if v == "webgl-lean" else _lib.PROFILE_FULL
         else:
@@ -281,6 +298,7 @@ class PathtracingViewport:
     def setScene(self, scene) -> None:
         """scene: a synth.Scene or any object with vertices / indices / materials arrays."""
         try:
+            self.ctx.set_bvh_builder(self._display.get("bvhBuilder", "host"))
             ds = DeviceScene(self.ctx, scene.vertices, scene.indices, scene.materials, getattr(scene, "bvh", None))
         except Exception as e:
             self._emit("sceneLoadFailed", {"error": e})
