@@ -249,6 +249,34 @@ def _pct(v, q):
     return float(v[min(len(v) - 1, int(round(q * (len(v) - 1))))]) if v else None
 
 
+def scene_build_section(local, sc, args):
+    """Scene creation (BVH build, 4-wide collapse, upload) of the workload with
+    the host binned-SAH builder and the device LBVH builder, and the render
+    throughput over each tree."""
+    from dspbr.viewport import PathtracingCamera, PathtracingViewport
+    out = {}
+    for builder in ("host", "device"):
+        v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
+                                settings={"maxBounces": sc.max_bounces, "bvhBuilder": builder})
+        scene = type(sc)(sc.name, sc.vertices, sc.indices, sc.materials, sc.camera, sc.width, sc.height,
+                         env=sc.env)  # no prebuilt BVH: the library builds it
+        t0 = time.perf_counter()
+        v.setScene(scene)
+        t1 = time.perf_counter()
+        v.setIBL(sc.env)
+        v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
+        lib, h = v.ctx.lib, v.ctx.h
+        v.ctx.check(lib.dspbr_render(h, 2))
+        d0 = v.diagnostics
+        v.ctx.check(lib.dspbr_render(h, max(2, min(args.steps, 10))))
+        d1 = v.diagnostics
+        rays = sum(d1[k] - d0[k] for k in ("rays_primary", "rays_extension", "rays_shadow"))
+        out[builder] = {"scene_create_ms": 1e3 * (t1 - t0), "bvh_build_ms": d1["bvh_build_ms"],
+                        "mrays_per_s": rays / (d1["last_render_ms"] * 1e-3) / 1e6, "bvh_nodes": d1["bvh_nodes"]}
+        v.dispose()
+    return out
+
+
 def serving_section(local, quick=False):
     """Batching (64 viewports over 8 scenes of 10k-2M triangles, 128^2-1024^2,
     1-64 spp) and serving (Poisson arrivals over 16 scenes of 50k-4M
@@ -461,6 +489,7 @@ def run_gpu_arm(args):
                  "read_accumulation_ms": 1e3 * parts[2] / e2e_steps}
     cs = clocks.summary()
     v.dispose()
+    build = scene_build_section(local, sc, args) if ws == 1 and not args.no_serving else None
     serving = None
     if ws == 1 and not args.no_serving:
         serving = serving_section(local, quick=args.quick_serving)
@@ -499,6 +528,8 @@ def run_gpu_arm(args):
             "rays_per_step": rays / max(1, args.steps),
             "traversal_aborted": d1["traversal_aborted"],
         }
+        if build is not None:
+            line["scene_build"] = build
         if serving is not None:
             line.update(serving)
         print(json.dumps(line))
