@@ -76,6 +76,18 @@ static int settle(dspbr_ctx* c) {
   return rc;
 }
 
+// Texture slots of the material record (material.ts layout): 39, 44-59, 63.
+static const int kTexSlots[] = {39, 44, 45, 46, 47, 48, 49, 50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 63};
+static int32_t max_texture_id(const float* materials, uint32_t num_materials) {
+  int32_t mx = -1;
+  for (uint32_t m = 0; m < num_materials; ++m)
+    for (int k : kTexSlots) {
+      float id = materials[size_t(m) * 68 + k];
+      if (id >= 0.f) mx = std::max(mx, id < 2147483520.f ? int32_t(id) : INT32_MAX);
+    }
+  return mx;
+}
+
 // Reference-layout nodes for the device: child index / count / first become
 // the shader's int() of the stored floats (int bits in lanes 3, 7, 11, 15).
 // Returns whether every box bound is finite.
@@ -113,6 +125,8 @@ static uint32_t material_signature(const float* m) {
   if (m[26] > 0.f) sig |= 128u;                                // diffuse transmission
   if (m[5] != 0.f) sig |= 256u;                                // anisotropy
   if (m[8] < 1.f || m[27] > 0.f) sig |= 512u;                  // cutout
+  for (int k : kTexSlots)
+    if (m[k] >= 0.f) sig |= 1024u;                             // textured
   return sig;
 }
 
@@ -173,6 +187,7 @@ static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(vertices[size_t(v) * 20 + k])) sc->boxes_finite = false;
   sc->host_materials.assign(materials, materials + size_t(num_materials) * 68);
+  sc->max_tex_id = max_texture_id(materials, num_materials);
   sc->tri_material.resize(sc->num_tris);
   for (uint32_t t = 0; t < sc->num_tris; ++t)
     sc->tri_material[t] = uint32_t(vertices[size_t(indices[3 * size_t(t)]) * 20 + 3]);
@@ -284,12 +299,6 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     if (!(m >= 0.f) || uint32_t(m) >= num_materials)
       return s.fail(DSPBR_ERR_INVALID, "scene: vertex %u references material %g of %u", v, m, num_materials);
   }
-  // texture ids (material.ts: slots 39, 44-59, 63); textures are not supported yet
-  static const int kTexSlots[] = {39, 44, 45, 46, 47, 48, 49, 50, 51, 52, 53, 54, 55, 56, 57, 58, 59, 63};
-  for (uint32_t m = 0; m < num_materials; ++m)
-    for (int k : kTexSlots)
-      if (materials[size_t(m) * 68 + k] >= 0.f)
-        return s.fail(DSPBR_ERR_INVALID, "scene: material %u uses a texture (record slot %d); textured materials are not supported", m, k);
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   if ((!bvh_nodes || !bvh_indices) && c->bvh_builder == DSPBR_BVH_BUILD_DEVICE)
     return scene_create_device_bvh(c, vertices, num_vertices, indices, num_indices, materials, num_materials, out);
@@ -362,6 +371,7 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     }
   }
   sc->host_materials.assign(materials, materials + size_t(num_materials) * 68);
+  sc->max_tex_id = max_texture_id(materials, num_materials);
   sc->tri_material.resize(sc->num_tris);
   for (uint32_t t = 0; t < sc->num_tris; ++t)
     sc->tri_material[t] = uint32_t(vertices[size_t(indices[3 * size_t(t)]) * 20 + 3]);
@@ -412,6 +422,53 @@ int dspbr_scene_bvh(const dspbr_scene* sc, float* nodes, int32_t* remap, uint32_
   return DSPBR_OK;
 }
 
+int dspbr_scene_set_textures(dspbr_scene* sc, const float* tex_infos, uint32_t num_tex_infos,
+                             const dspbr_texture_array* arrays, uint32_t num_arrays) {
+  if (!sc || (num_tex_infos && !tex_infos) || (num_arrays && !arrays)) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(sc->ctx); if (rc_) return rc_; }
+  Status s = sc->ctx->st();
+  if (int64_t(sc->max_tex_id) >= int64_t(num_tex_infos))
+    return s.fail(DSPBR_ERR_INVALID, "set_textures: the materials use texture id %d, %u texture infos given",
+                  sc->max_tex_id, num_tex_infos);
+  for (uint32_t a = 0; a < num_arrays; ++a) {
+    const dspbr_texture_array& t = arrays[a];
+    if (t.width <= 0 || t.height <= 0 || t.layers <= 0 || !t.rgba8 || int64_t(t.width) * t.height * t.layers > (int64_t(1) << 31))
+      return s.fail(DSPBR_ERR_INVALID, "set_textures: texture array %u is malformed", a);
+  }
+  TRY_CUDA(s, cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+  cudaStream_t st = sc->ctx->stream;
+  TRY_CUDA(s, cudaStreamSynchronize(st), "set textures");
+  std::vector<std::unique_ptr<DevBuf<uchar4>>> data;
+  std::vector<DevTexArray> desc(num_arrays);
+  for (uint32_t a = 0; a < num_arrays; ++a) {
+    const dspbr_texture_array& t = arrays[a];
+    const size_t n = size_t(t.width) * t.height * t.layers;
+    data.emplace_back(new DevBuf<uchar4>());
+    TRY_CUDA(s, data.back()->alloc(n), "alloc texture array");
+    TRY_CUDA(s, cudaMemcpyAsync(data.back()->p, t.rgba8, n * 4, cudaMemcpyHostToDevice, st), "upload texture array");
+    desc[a] = DevTexArray{data.back()->p, t.width, t.height, t.layers};
+  }
+  DevBuf<DevTexArray> dt;
+  DevBuf<float4> di;
+  if (num_arrays) {
+    TRY_CUDA(s, dt.alloc(num_arrays), "alloc texture arrays");
+    TRY_CUDA(s, cudaMemcpyAsync(dt.p, desc.data(), desc.size() * sizeof(DevTexArray), cudaMemcpyHostToDevice, st),
+             "upload texture arrays");
+  }
+  if (num_tex_infos) {
+    TRY_CUDA(s, di.alloc(size_t(num_tex_infos) * 2), "alloc texture infos");
+    TRY_CUDA(s, cudaMemcpyAsync(di.p, tex_infos, size_t(num_tex_infos) * 32, cudaMemcpyHostToDevice, st),
+             "upload texture infos");
+  }
+  TRY_CUDA(s, cudaStreamSynchronize(st), "set textures");
+  sc->tex_data.swap(data);
+  sc->tex_arrays.swap(dt);
+  sc->texinfo.swap(di);
+  sc->num_texinfo = num_tex_infos;
+  sc->num_tex_arrays = num_arrays;
+  return dspbr_reset(sc->ctx);
+}
+
 int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32_t first, uint32_t count) {
   if (!sc || !materials || first + count > sc->num_materials) return DSPBR_ERR_INVALID;
   { int rc_ = settle(sc->ctx); if (rc_) return rc_; }
@@ -421,6 +478,7 @@ int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32
                               cudaMemcpyHostToDevice, sc->ctx->stream), "update materials");
   TRY_CUDA(s, cudaStreamSynchronize(sc->ctx->stream), "update materials");
   std::copy(materials, materials + size_t(count) * 68, sc->host_materials.begin() + size_t(first) * 68);
+  sc->max_tex_id = max_texture_id(sc->host_materials.data(), sc->num_materials);
   { int rc_ = classify_triangles(s, sc, sc->ctx->stream); if (rc_) return rc_; }
   dspbr_reset(sc->ctx);
   return DSPBR_OK;
@@ -632,6 +690,8 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
   if (rc) return rc;
   if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
   if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
+  if (int64_t(c->scene->max_tex_id) >= int64_t(c->scene->num_texinfo))
+    return s.fail(DSPBR_ERR_STATE, "render: the scene's materials use textures; call dspbr_scene_set_textures");
   if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
   if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
@@ -1030,6 +1090,8 @@ int dspbr_bsdf_query(dspbr_ctx* c, const dspbr_scene* sc, uint32_t n, const floa
   if (!c || !sc || !hit || !wo || !rnd || !eval4 || !sample10 || !flags) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
   Status s = c->st();
+  if (int64_t(sc->max_tex_id) >= int64_t(sc->num_texinfo))
+    return s.fail(DSPBR_ERR_STATE, "bsdf_query: the scene's materials use textures; call dspbr_scene_set_textures");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   DevBuf<float> dh, dw, dr, de, ds;
   DevBuf<int32_t> df;

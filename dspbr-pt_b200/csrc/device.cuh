@@ -24,6 +24,12 @@ constexpr int kMaxLeafTris = 64;
 // same truncating conversion the shader's int() performs).  tris: 3 float4 per
 // BVH leaf slot, pre-gathered in leaf order: (p0.xyz, mesh triangle id bits),
 // (p1 - p0, 0), (p2 - p0, 0); id -1 marks a remap entry the reference skips.
+// One RGBA8 texture array (all layers share a resolution; scene_data_webgl2.ts:266-300).
+struct DevTexArray {
+  const uchar4* __restrict__ data;  // layers x h x w
+  int w, h, layers;
+};
+
 struct DevScene {
   const float4* __restrict__ nodes;
   const float4* __restrict__ tris;
@@ -37,6 +43,9 @@ struct DevScene {
   int num_nodes, num_slots, num_tris, num_materials;
   int boxes_finite;  // every node bound is finite (checked at upload)
   int wide;          // closest-hit / any-hit queries of paths use the wide BVH
+  const float4* __restrict__ texinfo;         // 2 float4 per TexInfo (material.ts:483-523)
+  const DevTexArray* __restrict__ tex_arrays;
+  int num_texinfo, num_tex_arrays;
 };
 
 struct DevIbl {
@@ -455,8 +464,166 @@ DEV float4 vtx(const DevScene& s, uint32_t vi, int slot) { return __ldg(s.verts 
 // get_onb(n) (utils.glsl:97-102): Spencer & Jones basis, first column
 DEV v3 onb_tangent(v3 n) { return normalize(cross(n, mk(-n.z, n.x, -n.y))); }
 
-NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
+// ---- material textures (the reference's generated texture accessor,
+// scene_data_webgl2.ts:318-363) -------------------------------------------------------
+// texture(sampler2DArray, vec3) with LINEAR + REPEAT filtering on UNORM8
+// texels: the texel coordinates use IEEE-rounded operations so that the
+// texels chosen are those of the reference arithmetic.
+DEV float4 texel8(const DevTexArray& t, int i, int j, int l) {
+  uchar4 c = __ldg(t.data + (size_t(l) * t.h + j) * t.w + i);
+  return make_float4(__fdiv_rn(float(c.x), 255.f), __fdiv_rn(float(c.y), 255.f), __fdiv_rn(float(c.z), 255.f),
+                     __fdiv_rn(float(c.w), 255.f));
+}
+DEV int wrap_repeat(int i, int n) {
+  int m = i % n;
+  return m < 0 ? m + n : m;
+}
+DEV float4 tex_array_sample(const DevTexArray& t, float u, float v, float layer) {
+  float lf = floorf(__fadd_rn(layer, 0.5f));
+  int l = lf < 0.f ? 0 : (lf > float(t.layers - 1) ? t.layers - 1 : int(lf));
+  float uu = __fsub_rn(__fmul_rn(u, float(t.w)), 0.5f), vv = __fsub_rn(__fmul_rn(v, float(t.h)), 0.5f);
+  float fu = floorf(uu), fv = floorf(vv);
+  float a = __fsub_rn(uu, fu), b = __fsub_rn(vv, fv);
+  int iu = int(fu), iv = int(fv);
+  int i0 = wrap_repeat(iu, t.w), j0 = wrap_repeat(iv, t.h), i1 = wrap_repeat(iu + 1, t.w), j1 = wrap_repeat(iv + 1, t.h);
+  float4 t00 = texel8(t, i0, j0, l), t10 = texel8(t, i1, j0, l), t01 = texel8(t, i0, j1, l), t11 = texel8(t, i1, j1, l);
+  float w00 = __fmul_rn(__fsub_rn(1.f, a), __fsub_rn(1.f, b)), w10 = __fmul_rn(a, __fsub_rn(1.f, b));
+  float w01 = __fmul_rn(__fsub_rn(1.f, a), b), w11 = __fmul_rn(a, b);
+  auto mix4 = [&](float x00, float x10, float x01, float x11) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(w00, x00), __fmul_rn(w10, x10)), __fmul_rn(w01, x01)),
+                     __fmul_rn(w11, x11));
+  };
+  return make_float4(mix4(t00.x, t10.x, t01.x, t11.x), mix4(t00.y, t10.y, t01.y, t11.y),
+                     mix4(t00.z, t10.z, t01.z, t11.z), mix4(t00.w, t10.w, t01.w, t11.w));
+}
+// get_texture_value(id, uv0, uv1); uv1 is never filled by the reference
+// (RenderState.uv1 stays zero).
+NOINL float4 texture_value(const DevScene& s, float id, float u0, float v0) {
+  const int idx = int(id);
+  float4 i0 = make_float4(0.f, 0.f, 0.f, 0.f), i1 = i0;  // a TexInfo beyond the table reads as zeros
+  if (idx >= 0 && idx < s.num_texinfo) {
+    i0 = __ldg(s.texinfo + 2 * size_t(idx));
+    i1 = __ldg(s.texinfo + 2 * size_t(idx) + 1);
+  }
+  const float u = i1.z > 0.5f ? 0.f : u0, v = i1.z > 0.5f ? 0.f : v0;
+  const int arr = int(i0.z);
+  if (arr < 0 || arr >= s.num_tex_arrays) return make_float4(1.f, 1.f, 1.f, 1.f);
+  return tex_array_sample(s.tex_arrays[arr], __fadd_rn(__fmul_rn(u, i1.x), i0.x), __fadd_rn(__fmul_rn(v, i1.y), i0.y),
+                          i0.w);
+}
+DEV v3 to_linear_rgb(float4 c) { return mk(powf(c.x, 2.2f), powf(c.y, 2.2f), powf(c.z, 2.2f)); }
+
+// configure_gltf_material (material.glsl:5-110) from the interpolated render
+// state: material record, textures, vertex colour, normal map, fix_normals,
+// anisotropy rotation, closure.  n / ng / tangent as fillRenderState leaves
+// them (not yet flipped to the incident side).
+NOINL Surface configure_gltf(const DevScene& s, int mat, v3 n, v3 ng, float4 tangent, v3 wi, float u0, float v0,
+                             float4 vcol, bool lean) {
   Surface S;
+  mat = min(max(mat, 0), s.num_materials - 1);
+  const float4* m = s.materials + 17 * size_t(mat);
+  float4 m0 = __ldg(m + 0), m1 = __ldg(m + 1), m2 = __ldg(m + 2), m3 = __ldg(m + 3), m4 = __ldg(m + 4),
+         m5 = __ldg(m + 5), m6 = __ldg(m + 6), m7 = __ldg(m + 7), m8 = __ldg(m + 8), m9 = __ldg(m + 9),
+         m10 = __ldg(m + 10), m15 = __ldg(m + 15), m16 = __ldg(m + 16);
+  // texture ids (material.ts layout): 39 diffuseTransmission, 44 baseColor,
+  // 45 metallicRoughness, 46 normal, 47 emissive, 48 specular, 49 specularColor,
+  // 50 transmission, 51 clearcoat, 52 clearcoatRoughness, 54 sheenColor,
+  // 55 sheenRoughness, 56 anisotropy, 57 anisotropyDirection, 58 iridescence,
+  // 59 iridescenceThickness, 63 diffuseTransmissionColor
+  const bool textured = s.num_texinfo > 0;
+  const float4 one = make_float4(1.f, 1.f, 1.f, 1.f);
+  float4 m11 = one, m12 = one, m13 = one, m14 = one;
+  if (textured) {
+    m11 = __ldg(m + 11); m12 = __ldg(m + 12); m13 = __ldg(m + 13); m14 = __ldg(m + 14);
+  } else {
+    m11 = m12 = m13 = m14 = make_float4(-1.f, -1.f, -1.f, -1.f);
+    m9.w = -1.f;
+    m15.w = -1.f;
+  }
+  auto tex = [&](float id) { return id < 0.f ? one : texture_value(s, id, u0, v0); };
+  GltfMaterial g;
+  float4 bc = tex(m11.x);
+  g.base_color = m11.x < 0.f ? mk(m0) : mk(m0) * to_linear_rgb(bc);
+  float opacity = bc.w;
+  if (sqrtf(vcol.x * vcol.x + vcol.y * vcol.y + vcol.z * vcol.z + vcol.w * vcol.w) > 0.f) {
+    g.base_color = g.base_color * mk(vcol);
+    opacity = opacity * vcol.w;
+  }
+  float cutout = m2.x * opacity;
+  if (m6.w > 0.f) cutout = cutout < m6.w ? 0.f : 1.f;
+  if (m6.w == 1.f) cutout = 1.f;
+  g.transmission = m12.z < 0.f ? m1.w : m1.w * tex(m12.z).x;
+  g.diffuse_transmission = m9.w < 0.f ? m6.z : m6.z * tex(m9.w).x;
+  g.diffuse_transmission_color = m15.w < 0.f ? mk(m15) : mk(m15) * to_linear_rgb(tex(m15.w));
+  bool thin = m8.w > 0.5f;
+  g.ior = m2.w;
+  float4 orm = tex(m11.y);
+  g.metallic = m11.y < 0.f ? m0.w : m0.w * orm.z;
+  g.roughness = m11.y < 0.f ? m1.x : m1.x * orm.y;
+  float4 aniso = tex(m14.x);
+  g.anisotropy = m14.x < 0.f ? m1.y : m1.y * aniso.z;
+  if (m12.y < 0.f) {
+    g.specular_color = mk(m3);
+  } else {
+    float4 sc = tex(m12.y);
+    g.specular_color = mk(m3) * mk(powf(sc.x, 2.2f), powf(sc.y, 2.2f), powf(sc.z, 2.2f));
+  }
+  g.specular = m12.x < 0.f ? m3.w : m3.w * tex(m12.x).w;
+  g.sheen_roughness = m13.w < 0.f ? m4.w : m4.w * tex(m13.w).x;
+  g.sheen_color = m13.z < 0.f ? mk(m4) : mk(m4) * to_linear_rgb(tex(m13.z));
+  v3 t3 = mk(tangent.x, tangent.y, tangent.z);
+  if (m11.z >= 0.f) {  // normal map (material.glsl:55-64)
+    v3 b = normalize(cross(n, t3));
+    v3 tt = cross(b, n);
+    float4 tn = tex(m11.z);
+    v3 nt = normalize(mk(tn.x, tn.y, tn.z) * 2.0f - mk(1.f));
+    nt = normalize(nt * mk(m2.z, m2.z, 1.f));
+    n = tt * nt.x + b * nt.y + n * nt.z;
+    v3 b2 = normalize(cross(n, t3)) * tangent.w;
+    t3 = cross(b2, n);
+  }
+  // fix_normals (utils.glsl:88-98)
+  bool back = false;
+  if (dot(wi, ng) < 0.f) { ng = -ng; back = true; }
+  if (dot(ng, n) < 0.f) n = -n;
+  // anisotropy direction -> rotation -> tangent (material.glsl:71-82, utils.glsl:183-190)
+  float ax = m9.x, ay = m9.y;
+  if (m14.y >= 0.f) {
+    float4 ad = tex(m14.y);
+    ax = ad.x * 2.0f - 1.f;
+    ay = ad.y * 2.0f - 1.f;
+  } else if (m14.x >= 0.f) {
+    ax = aniso.x * 2.0f - 1.f;
+    ay = aniso.y * 2.0f - 1.f;
+  }
+  float rot = atan2f(ay, ax) + kGlslPi;
+  if (rot > 0.f) {
+    v3 b = cross(n, t3) * tangent.w;
+    float sr, cr;
+    sincosf(rot, &sr, &cr);
+    t3 = t3 * cr + b * sr;
+  }
+  g.clearcoat = m12.w < 0.f ? m6.x : m6.x * tex(m12.w).x;
+  g.clearcoat_roughness = m13.x < 0.f ? m6.y : m6.y * tex(m13.x).x;
+  g.thickness = thin ? 0.f : 1.f;
+  g.iridescence = m14.z < 0.f ? m10.x : m10.x * tex(m14.z).x;
+  g.iridescence_ior = m10.y;
+  g.iridescence_thickness = mixf(m10.z, m10.w, m14.w < 0.f ? 1.f : tex(m14.w).y);
+  g.dispersion = m16.x;
+  S.c = build_closure(g, t3, lean);
+  S.n = n;
+  S.ng = ng;
+  S.emissive = m11.w < 0.f ? mk(m5) : mk(m5) * to_linear_rgb(tex(m11.w));
+  S.att_color = mk(m7);
+  S.att_dist = m7.w;
+  S.cutout = cutout;
+  S.backside = back;
+  S.thin_walled = thin;
+  return S;
+}
+
+// fillRenderState (renderer.frag:72-91, bvh.glsl:84-134) + configure_gltf.
+NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
   uint32_t i0 = __ldg(s.indices + 3 * size_t(tri)), i1 = __ldg(s.indices + 3 * size_t(tri) + 1),
            i2 = __ldg(s.indices + 3 * size_t(tri) + 2);
   float4 q0 = vtx(s, i0, 0), q1 = vtx(s, i1, 0), q2 = vtx(s, i2, 0);
@@ -473,63 +640,13 @@ NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hi
   float4 c0 = vtx(s, i0, 4), c1 = vtx(s, i1, 4), c2 = vtx(s, i2, 4);
   float4 vcol = make_float4(w0 * c0.x + bu * c1.x + bv * c2.x, w0 * c0.y + bu * c1.y + bv * c2.y,
                             w0 * c0.z + bu * c1.z + bv * c2.z, w0 * c0.w + bu * c1.w + bv * c2.w);
-  int mat = int(uint32_t(q0.w));
-  mat = min(max(mat, 0), s.num_materials - 1);
-  const float4* m = s.materials + 17 * size_t(mat);
-  float4 m0 = __ldg(m + 0), m1 = __ldg(m + 1), m2 = __ldg(m + 2), m3 = __ldg(m + 3), m4 = __ldg(m + 4),
-         m5 = __ldg(m + 5), m6 = __ldg(m + 6), m7 = __ldg(m + 7), m8 = __ldg(m + 8), m9 = __ldg(m + 9),
-         m10 = __ldg(m + 10), m15 = __ldg(m + 15), m16 = __ldg(m + 16);
-  GltfMaterial g;
-  g.base_color = mk(m0);
-  float opacity = 1.f;
-  if (sqrtf(vcol.x * vcol.x + vcol.y * vcol.y + vcol.z * vcol.z + vcol.w * vcol.w) > 0.f) {
-    g.base_color = g.base_color * mk(vcol);
-    opacity = opacity * vcol.w;
+  float u0 = 0.f, v0 = 0.f;
+  if (s.num_texinfo > 0) {  // compute_interpolated_uv(set 0) (bvh.glsl:108-116)
+    float4 a = vtx(s, i0, 2), b = vtx(s, i1, 2), c = vtx(s, i2, 2);
+    u0 = w0 * a.x + bu * b.x + bv * c.x;
+    v0 = w0 * a.y + bu * b.y + bv * c.y;
   }
-  float cutout = m2.x * opacity;
-  if (m6.w > 0.f) cutout = cutout < m6.w ? 0.f : 1.f;
-  if (m6.w == 1.f) cutout = 1.f;
-  g.metallic = m0.w;
-  g.roughness = m1.x;
-  g.anisotropy = m1.y;
-  g.transmission = m1.w;
-  g.ior = m2.w;
-  g.specular_color = mk(m3);
-  g.specular = m3.w;
-  g.sheen_color = mk(m4);
-  g.sheen_roughness = m4.w;
-  g.clearcoat = m6.x;
-  g.clearcoat_roughness = m6.y;
-  g.diffuse_transmission = m6.z;
-  g.diffuse_transmission_color = mk(m15);
-  bool thin = m8.w > 0.5f;
-  g.thickness = thin ? 0.f : 1.f;
-  g.iridescence = m10.x;
-  g.iridescence_ior = m10.y;
-  g.iridescence_thickness = mixf(m10.z, m10.w, 1.f);
-  g.dispersion = m16.x;
-  // fix_normals
-  bool back = false;
-  if (dot(wi, ng) < 0.f) { ng = -ng; back = true; }
-  if (dot(ng, n) < 0.f) n = -n;
-  // anisotropy rotation -> tangent (material.glsl:84-93, utils.glsl:179-186)
-  float rot = atan2f(m9.y, m9.x) + kGlslPi;
-  v3 t3 = mk(tangent.x, tangent.y, tangent.z);
-  if (rot > 0.f) {
-    v3 b = cross(n, t3) * tangent.w;
-    float sr, cr;
-    sincosf(rot, &sr, &cr);
-    t3 = t3 * cr + b * sr;
-  }
-  S.c = build_closure(g, t3, lean);
-  S.n = n;
-  S.ng = ng;
-  S.emissive = mk(m5);
-  S.att_color = mk(m7);
-  S.att_dist = m7.w;
-  S.cutout = cutout;
-  S.backside = back;
-  S.thin_walled = thin;
+  Surface S = configure_gltf(s, int(uint32_t(q0.w)), n, ng, tangent, wi, u0, v0, vcol, lean);
   S.pos = hit_pos;
   return S;
 }

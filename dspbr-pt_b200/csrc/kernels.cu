@@ -665,33 +665,10 @@ __global__ void k_bsdf_query(DevScene s, uint32_t n, const float* hit20, const f
     float4 tangent = make_float4(h[6], h[7], h[8], h[9]);
     v3 wi = mk(h[10], h[11], h[12]);
     float4 vcol = make_float4(h[15], h[16], h[17], h[18]);
-    int mat = min(max(int(uint32_t(h[19])), 0), s.num_materials - 1);
-    const float4* m = s.materials + 17 * size_t(mat);
-    float4 m0 = m[0], m1 = m[1], m2 = m[2], m3 = m[3], m4 = m[4], m6 = m[6], m8 = m[8], m9 = m[9], m10 = m[10],
-           m15 = m[15], m16 = m[16];
-    GltfMaterial g;
-    g.base_color = mk(m0);
-    if (sqrtf(vcol.x * vcol.x + vcol.y * vcol.y + vcol.z * vcol.z + vcol.w * vcol.w) > 0.f)
-      g.base_color = g.base_color * mk(vcol);
-    g.metallic = m0.w; g.roughness = m1.x; g.anisotropy = m1.y; g.transmission = m1.w; g.ior = m2.w;
-    g.specular_color = mk(m3); g.specular = m3.w; g.sheen_color = mk(m4); g.sheen_roughness = m4.w;
-    g.clearcoat = m6.x; g.clearcoat_roughness = m6.y; g.diffuse_transmission = m6.z;
-    g.diffuse_transmission_color = mk(m15);
-    g.thickness = m8.w > 0.5f ? 0.f : 1.f;
-    g.iridescence = m10.x; g.iridescence_ior = m10.y; g.iridescence_thickness = mixf(m10.z, m10.w, 1.f);
-    g.dispersion = m16.x;
-    bool back = false;
-    if (dot(wi, ng) < 0.f) { ng = -ng; back = true; }
-    if (dot(ng, n0) < 0.f) n0 = -n0;
-    float rot = atan2f(m9.y, m9.x) + kGlslPi;
-    v3 t3 = mk(tangent.x, tangent.y, tangent.z);
-    if (rot > 0.f) {
-      v3 bt = cross(n0, t3) * tangent.w;
-      float sr, cr;
-      sincosf(rot, &sr, &cr);
-      t3 = t3 * cr + bt * sr;
-    }
-    Closure c = build_closure(g, t3, lean != 0);
+    Surface S = configure_gltf(s, int(uint32_t(h[19])), n0, ng, tangent, wi, h[13], h[14], vcol, lean != 0);
+    const Closure& c = S.c;
+    n0 = S.n;
+    const bool back = S.backside;
     v3 wo = mk(wo3[3 * i], wo3[3 * i + 1], wo3[3 * i + 2]);
     v3 ev = bsdf_eval(c, n0, wi, wo);
     float pd = bsdf_pdf(c, n0, wi, wo);

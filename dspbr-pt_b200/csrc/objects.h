@@ -23,6 +23,12 @@ struct dspbr_scene {
   dspbr::DevBuf<int2> wleaves;
   int wroot = 0;
   dspbr::DevBuf<int32_t> device_remap;  // leaf-slot remap of a device-built BVH
+  // material textures
+  std::vector<std::unique_ptr<dspbr::DevBuf<uchar4>>> tex_data;
+  dspbr::DevBuf<dspbr::DevTexArray> tex_arrays;
+  dspbr::DevBuf<float4> texinfo;
+  uint32_t num_texinfo = 0, num_tex_arrays = 0;
+  int32_t max_tex_id = -1;  // largest texture id the materials use
   uint32_t num_nodes = 0, num_slots = 0, num_tris = 0, num_verts = 0, num_materials = 0;
   std::vector<uint32_t> tri_material;  // host copy, for re-classing after material edits
   std::vector<float> host_materials;
@@ -39,12 +45,22 @@ struct dspbr_scene {
     s.wleaves = wleaves.p;
     s.wroot = wroot;
     s.wide = 1;
+    s.texinfo = texinfo.p;
+    s.tex_arrays = tex_arrays.p;
+    s.num_texinfo = int(num_texinfo);
+    s.num_tex_arrays = int(num_tex_arrays);
     s.boxes_finite = boxes_finite ? 1 : 0;
     return s;
   }
   uint64_t bytes() const {
     return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes() +
-           wnodes.bytes() + wleaves.bytes() + device_remap.bytes();
+           wnodes.bytes() + wleaves.bytes() + device_remap.bytes() + texinfo.bytes() + tex_arrays.bytes() +
+           tex_bytes();
+  }
+  uint64_t tex_bytes() const {
+    uint64_t b = 0;
+    for (auto& t : tex_data) b += t->bytes();
+    return b;
   }
 };
 

@@ -406,6 +406,8 @@ int dspbr_server_submit(dspbr_server* s, const dspbr_request* req, uint64_t* id)
   Status st = s->st();
   if (!req->scene || req->scene->ctx != s->ctx || (req->ibl && req->ibl->ctx != s->ctx))
     return st.fail(DSPBR_ERR_INVALID, "submit: scene / IBL of another context");
+  if (int64_t(req->scene->max_tex_id) >= int64_t(req->scene->num_texinfo))
+    return st.fail(DSPBR_ERR_STATE, "submit: the scene's materials use textures; call dspbr_scene_set_textures");
   if (req->width <= 0 || req->height <= 0 || int64_t(req->width) * req->height > (int64_t(1) << 28) ||
       req->spp <= 0 || !req->out_rgba || !(req->fov_deg > 0.f && req->fov_deg < 180.f) || !(req->near_plane > 0.f) ||
       req->params.max_bounces < 0 || req->params.max_bounces > 4096)

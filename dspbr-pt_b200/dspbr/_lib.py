@@ -57,6 +57,10 @@ class Diag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TextureArray(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("layers", C.c_int32), ("rgba8", C.c_void_p)]
+
+
 class Display(C.Structure):
     _fields_ = [("exposure", C.c_float), ("tonemapping", C.c_int32), ("gamma", C.c_int32), ("fxaa", C.c_int32),
                 ("reserved", C.c_int32 * 4)]
@@ -131,6 +135,7 @@ SIGNATURES = {
     "dspbr_scene_create": (C.c_int, [_V, _F, C.c_uint32, _U, C.c_uint32, _F, C.c_uint32, _F, C.c_uint32, _I,
                                       C.c_uint32, _PV]),
     "dspbr_set_bvh_builder": (C.c_int, [_V, C.c_int]),
+    "dspbr_scene_set_textures": (C.c_int, [_V, _F, C.c_uint32, C.POINTER(TextureArray), C.c_uint32]),
     "dspbr_scene_bvh": (C.c_int, [_V, _F, _I, _U, _U]),
     "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),
     "dspbr_scene_device_bytes": (C.c_int, [_V, C.POINTER(C.c_uint64)]),

@@ -427,6 +427,93 @@ def make_sized(seed: int, target_tris: int, env_size=(1024, 512)) -> Scene:
     return Scene(f"sized{target_tris}", verts, idx, mats, cam, 512, 512, 16, 12, 2, env, seed)
 
 
+# ---- material textures --------------------------------------------------------
+TEXTURE_SLOTS = ["baseColorTextureId", "metallicRoughnessTextureId", "normalTextureId", "emissiveTextureId",
+                 "specularTextureId", "specularColorTextureId", "transmissionTextureId", "clearcoatTextureId",
+                 "clearcoatRoughnessTextureId", "sheenColorTextureId", "sheenRoughnessTextureId",
+                 "anisotropyTextureId", "anisotropyDirectionTextureId", "iridescenceTextureId",
+                 "iridescenceThicknessTextureId", "diffuseTransmissionTextureId",
+                 "diffuseTransmissionColorTextureId"]
+
+
+def texture_set(seed: int = 0):
+    """Seeded material textures as the reference packs them (scene_data.ts:71-100):
+    RGBA8 arrays grouped by resolution, and TexInfo records (offset.xy, array,
+    layer, scale.xy, uv set, pad; material.ts:483-523).  Array 0 is 32x32 with
+    5 layers (colour checker with alpha, occlusion-roughness-metallic noise,
+    normal-map bumps, emissive dots, masks); array 1 is 16x8 with 2 layers."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:32, 0:32]
+    a0 = np.zeros((5, 32, 32, 4), np.uint8)
+    chk = ((x // 8 + y // 8) % 2).astype(bool)
+    a0[0, ..., 0] = np.where(chk, 220, 40)
+    a0[0, ..., 1] = np.where(chk, 180, 90)
+    a0[0, ..., 2] = rng.integers(30, 230, (32, 32))
+    a0[0, ..., 3] = np.where((x + y) % 11 == 0, 60, 255)
+    a0[1, ..., 0] = 255
+    a0[1, ..., 1] = rng.integers(10, 255, (32, 32))
+    a0[1, ..., 2] = rng.integers(0, 255, (32, 32))
+    a0[1, ..., 3] = 255
+    bump = np.sin(x / 32 * 2 * np.pi * 3)[..., None] * np.array([0.4, 0.0, 0.0]) + \
+        np.cos(y / 32 * 2 * np.pi * 2)[..., None] * np.array([0.0, 0.3, 0.0])
+    nrm = bump + np.array([0.0, 0.0, 1.0])
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    a0[2, ..., 0:3] = np.round((nrm * 0.5 + 0.5) * 255).astype(np.uint8)
+    a0[2, ..., 3] = 255
+    dots = ((x % 9 == 4) & (y % 7 == 3))
+    a0[3, ..., 0:3] = np.where(dots[..., None], np.array([255, 200, 120]), 0)
+    a0[3, ..., 3] = 255
+    a0[4] = rng.integers(0, 256, (32, 32, 4))
+    y1, x1 = np.mgrid[0:8, 0:16]
+    a1 = np.zeros((2, 8, 16, 4), np.uint8)
+    a1[0, ..., 0:3] = rng.integers(60, 256, (8, 16, 3))
+    a1[0, ..., 3] = rng.integers(0, 256, (8, 16))
+    ang = np.arctan2(y1 - 3.5, x1 - 7.5)
+    a1[1, ..., 0] = np.round((np.cos(ang) * 0.5 + 0.5) * 255)
+    a1[1, ..., 1] = np.round((np.sin(ang) * 0.5 + 0.5) * 255)
+    a1[1, ..., 2] = rng.integers(0, 256, (8, 16))
+    a1[1, ..., 3] = 255
+    # (array, layer, scale, offset, uv set)
+    refs = [(0, 0, (1, 1), (0, 0), 0), (0, 1, (2.5, 1.5), (0.3, -0.2), 0), (0, 2, (1, 1), (0, 0), 0),
+            (0, 3, (3, 3), (0.1, 0.7), 0), (0, 4, (0.5, 2), (0.25, 0), 0), (1, 0, (1, 1), (0, 0), 0),
+            (1, 1, (1.7, 0.9), (-0.4, 0.15), 0), (0, 0, (4, 4), (0.5, 0.5), 1), (1, 0, (6, 2), (0, 0), 0)]
+    infos = np.zeros((len(refs), 8), np.float32)
+    for k, (arr, layer, sc, off, uvset) in enumerate(refs):
+        infos[k] = [off[0], off[1], arr, layer, sc[0], sc[1], uvset, 0]
+    return infos, [a0, a1]
+
+
+def texture_materials(materials: np.ndarray, seed: int = 0) -> np.ndarray:
+    """Copies of the material records with texture references on every texture
+    slot over the set (each material gets about half of the slots)."""
+    rng = np.random.default_rng(seed)
+    out = np.array(materials, np.float32, copy=True)
+    fixed = {"baseColorTextureId": 0, "metallicRoughnessTextureId": 1, "normalTextureId": 2, "emissiveTextureId": 3,
+             "specularColorTextureId": 5, "anisotropyDirectionTextureId": 6, "sheenColorTextureId": 8}
+    for m in range(out.shape[0]):
+        for slot in TEXTURE_SLOTS:
+            if rng.uniform() < 0.5:
+                tid = fixed.get(slot, int(rng.integers(0, 9)))
+                out[m, MAT[slot]] = tid
+        out[m, MAT["emissiveFactor"]:MAT["emissiveFactor"] + 3] = np.maximum(
+            out[m, MAT["emissiveFactor"]:MAT["emissiveFactor"] + 3], 0.5 if rng.uniform() < 0.25 else 0.0)
+    return out
+
+
+def make_textured_small(seed: int = 0) -> Scene:
+    """The small scene with planar uvs on every vertex and textured materials."""
+    sc = make_small(seed)
+    v = sc.vertices.copy()
+    p = v[:, 0:3]
+    v[:, 8] = p[:, 0] * 0.9 + p[:, 1] * 0.35
+    v[:, 9] = p[:, 2] * 0.8 + p[:, 1] * 0.55
+    sc.vertices = v
+    sc.materials = texture_materials(sc.materials, seed + 1)
+    sc.name = "small-textured"
+    sc.tex_infos, sc.tex_arrays = texture_set(seed + 2)
+    return sc
+
+
 WORKLOADS = {"small": make_small, "large": make_large, "divergence": make_divergence}
 
 

@@ -120,6 +120,17 @@ class DeviceScene:
         m = f32(materials).reshape(-1, MATERIAL_STRIDE)
         self.ctx.check(self.ctx.lib.dspbr_scene_update_materials(self.h, fptr(m), first, m.shape[0]))
 
+    def set_textures(self, tex_infos, arrays) -> None:
+        """Material textures: (N, 8) TexInfo records and RGBA8 arrays of shape
+        (layers, height, width, 4) (dspbr_scene_set_textures)."""
+        infos = f32(tex_infos).reshape(-1, 8)
+        arrs = [np.ascontiguousarray(a, np.uint8) for a in arrays]
+        desc = (_lib.TextureArray * max(len(arrs), 1))()
+        for k, a in enumerate(arrs):
+            desc[k].layers, desc[k].height, desc[k].width = a.shape[0], a.shape[1], a.shape[2]
+            desc[k].rgba8 = a.ctypes.data
+        self.ctx.check(self.ctx.lib.dspbr_scene_set_textures(self.h, fptr(infos), infos.shape[0], desc, len(arrs)))
+
     def bvh(self) -> "Bvh":
         """The scene's binary BVH in the reference layout, read back from the device."""
         nn, ni = C.c_uint32(), C.c_uint32()
@@ -300,6 +311,8 @@ class PathtracingViewport:
         try:
             self.ctx.set_bvh_builder(self._display.get("bvhBuilder", "host"))
             ds = DeviceScene(self.ctx, scene.vertices, scene.indices, scene.materials, getattr(scene, "bvh", None))
+            if getattr(scene, "tex_infos", None) is not None:
+                ds.set_textures(scene.tex_infos, scene.tex_arrays)
         except Exception as e:
             self._emit("sceneLoadFailed", {"error": e})
             raise

@@ -133,6 +133,19 @@ int dspbr_scene_create(dspbr_ctx* ctx, const float* vertices, uint32_t num_verti
                        uint32_t num_bvh_indices, dspbr_scene** out);
 /* material edits (dirty materials re-uploaded, renderer.ts:440-448) */
 int dspbr_set_bvh_builder(dspbr_ctx* ctx, int builder);
+/* Material textures (scene_data.ts:71-100, scene_data_webgl2.ts:233-363):
+ * textures of one resolution form an RGBA8 texture array sampled LINEAR +
+ * REPEAT; tex_infos holds 8 floats per texture reference (TexInfo,
+ * material.ts:483-523: offset.xy, array index, layer, scale.xy, uv set, pad),
+ * the ids the material records' texture slots name.  Every id a material uses
+ * must be below num_tex_infos; a scene whose materials use textures renders
+ * only once this was called.  The data is copied. */
+typedef struct dspbr_texture_array {
+  int32_t width, height, layers;
+  const uint8_t* rgba8;       /* layers x height x width x 4 bytes, row 0 first */
+} dspbr_texture_array;
+int dspbr_scene_set_textures(dspbr_scene* scene, const float* tex_infos, uint32_t num_tex_infos,
+                             const dspbr_texture_array* arrays, uint32_t num_arrays);
 /* The scene's binary BVH in the reference layout (16 floats per node, child /
  * count / first as floats) and its leaf-slot remap; NULL arrays query the sizes. */
 int dspbr_scene_bvh(const dspbr_scene* scene, float* nodes, int32_t* remap, uint32_t* num_nodes,

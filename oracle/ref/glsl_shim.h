@@ -237,6 +237,31 @@ static inline vec4 texture(const sampler2D& s, vec2 uv) {
   return (real(1) - a) * (real(1) - b) * t00 + a * (real(1) - b) * t10 + (real(1) - a) * b * t01 + a * b * t11;
 }
 
+// sampler2DArray of RGBA8 layers (material texture arrays,
+// scene_data_webgl2.ts:266-300): UNORM texels c / 255, LINEAR + REPEAT within
+// the layer round(layer) clamped to the array (GLSL ES 3.00 8.9, GL ES 3.0 3.8.10).
+struct sampler2DArray {
+  const uint8_t* data = nullptr;  // layers x h x w x 4
+  int w = 0, h = 0, layers = 0;
+};
+static inline vec4 glsl_texel8(const sampler2DArray& s, int i, int j, int l) {
+  const uint8_t* t = s.data + ((size_t(l) * s.h + j) * s.w + i) * 4;
+  return vec4(real(t[0]) / real(255), real(t[1]) / real(255), real(t[2]) / real(255), real(t[3]) / real(255));
+}
+static inline vec4 texture(const sampler2DArray& s, vec3 uvl) {
+  if (!s.data || s.layers <= 0) return vec4(0, 0, 0, 0);
+  real lf = std::floor(uvl.z + real(0.5));
+  int l = lf < real(0) ? 0 : (lf > real(s.layers - 1) ? s.layers - 1 : int(lf));
+  real u = uvl.x * real(s.w) - real(0.5), v = uvl.y * real(s.h) - real(0.5);
+  real fu = std::floor(u), fv = std::floor(v);
+  real a = u - fu, b = v - fv;
+  int i0 = glsl_wrap_repeat(int(fu), s.w), j0 = glsl_wrap_repeat(int(fv), s.h);
+  int i1 = glsl_wrap_repeat(int(fu) + 1, s.w), j1 = glsl_wrap_repeat(int(fv) + 1, s.h);
+  vec4 t00 = glsl_texel8(s, i0, j0, l), t10 = glsl_texel8(s, i1, j0, l);
+  vec4 t01 = glsl_texel8(s, i0, j1, l), t11 = glsl_texel8(s, i1, j1, l);
+  return (real(1) - a) * (real(1) - b) * t00 + a * (real(1) - b) * t10 + (real(1) - a) * b * t01 + a * b * t11;
+}
+
 // Fragment-stage built-ins (per host thread).
 extern thread_local vec4 gl_FragCoord;
 extern thread_local vec2 v_uv;

@@ -121,6 +121,26 @@ int REF(set_scene)(const float* vertices, int nverts, const uint32_t* indices, i
 }
 
 // renderer.ts:802-838 (luminance 0.299/0.587/0.114, per-row then marginal).
+// Material textures (scene_data_webgl2.ts:233-363): `infos` holds 8 floats per
+// TexInfo, `data[i]` the RGBA8 layers of texture array i, whl[3 i..3 i+2] its
+// width, height and layer count.  The harness keeps copies.
+int REF(set_textures)(const float* infos, int ninfos, int narrays, const uint8_t* const* data, const int* whl) {
+  if (ninfos < 0 || narrays < 0 || narrays > kGlslMaxTexArrays) return -1;
+  static std::vector<float> info_copy;
+  static std::vector<std::vector<uint8_t>> array_copy;
+  info_copy.assign(infos, infos + 8 * size_t(ninfos));
+  array_copy.assign(size_t(narrays), {});
+  for (int i = 0; i < narrays; ++i) {
+    size_t bytes = size_t(whl[3 * i]) * whl[3 * i + 1] * whl[3 * i + 2] * 4;
+    array_copy[i].assign(data[i], data[i] + bytes);
+    glsl_tex_arrays[i] = sampler2DArray{array_copy[i].data(), whl[3 * i], whl[3 * i + 1], whl[3 * i + 2]};
+  }
+  glsl_tex_infos = info_copy.data();
+  glsl_num_tex_infos = ninfos;
+  glsl_num_tex_arrays = narrays;
+  return 0;
+}
+
 int REF(set_ibl)(const float* rgba, int w, int h) {
   if (w <= 0 || h <= 0) return -1;
   HostIbl& I = g_ibl;

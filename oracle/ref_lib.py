@@ -56,6 +56,18 @@ class GlslReference:
         if rc != 0:
             raise ValueError("reference harness rejected the scene")
 
+    def set_textures(self, infos, arrays):
+        """infos: (N, 8) TexInfo records; arrays: list of uint8 (layers, h, w, 4) texture arrays."""
+        inf = np.ascontiguousarray(infos, np.float32).reshape(-1, 8)
+        arrs = [np.ascontiguousarray(a, np.uint8) for a in arrays]
+        ptrs = (C.c_void_p * max(len(arrs), 1))(*[a.ctypes.data for a in arrs])
+        whl = np.array([[a.shape[2], a.shape[1], a.shape[0]] for a in arrs] or [[0, 0, 0]], np.int32).reshape(-1)
+        self._tex_keep = [inf, arrs, ptrs, whl]
+        fn = self.fn("set_textures")
+        fn.argtypes = [_F, C.c_int, C.c_int, C.POINTER(C.c_void_p), _I]
+        if fn(inf.ctypes.data_as(_F), inf.shape[0], len(arrs), ptrs, whl.ctypes.data_as(_I)) != 0:
+            raise ValueError("reference harness rejected the textures")
+
     def set_ibl(self, rgba):
         img = np.ascontiguousarray(rgba, np.float32)
         self._env = img
@@ -82,7 +94,7 @@ class GlslReference:
         assert accum.dtype == np.float32 and accum.flags.c_contiguous and accum.shape == (height, width, 4)
         rc = self.fn("render")(width, height, accum.ctypes.data_as(_F), threads)
         if rc != 0:
-            raise ValueError("reference render failed (textured material?)")
+            raise ValueError("reference render failed (a texture id beyond the TexInfo table)")
         return accum
 
     def render_pixels(self, xy, width, height, threads: int = 0):

@@ -106,6 +106,33 @@ def main():
     g["display_fxaa_in"] = tm
     g["display_fxaa"] = r32.fxaa(tm)
     g["display_image_aces_fxaa"] = r32.fxaa(r32.tonemap(acc, 1.0, 1, 3))
+    # material textures (scene_data_webgl2.ts:233-363, material.glsl:5-110):
+    # BSDF queries over textured feature materials, and a textured image
+    tinfos, tarrays = synth.texture_set(3)
+    tmats = synth.texture_materials(mats, 4)
+    g["tex_infos"] = tinfos
+    g["tex_array0"], g["tex_array1"] = tarrays
+    g["tex_materials"] = tmats
+    for r in (r32, r64):
+        r.set_scene(sc.vertices, sc.indices, tmats, bvh.nodes, bvh.indices)
+        r.set_textures(tinfos, tarrays)
+    thit, two, trnd = helpers.bsdf_queries(3000, tmats.shape[0], seed=16)
+    thit[:, 13:15] = np.random.default_rng(17).uniform(-1.5, 2.5, size=(3000, 2))  # wrap-around uvs
+    g["tex_bsdf_hit"], g["tex_bsdf_wo"], g["tex_bsdf_rnd"] = thit, two, trnd
+    g["tex_bsdf_eval32"], g["tex_bsdf_sample32"], g["tex_bsdf_flags"] = r32.bsdf(thit, two, trnd)
+    g["tex_bsdf_eval64"], g["tex_bsdf_sample64"], _ = r64.bsdf(thit, two, trnd)
+    ts = synth.make_textured_small(0)
+    tbvh = Bvh.build(ts.vertices, ts.indices, 20)
+    r32.set_scene(ts.vertices, ts.indices, ts.materials, tbvh.nodes, tbvh.indices)
+    r32.set_textures(ts.tex_infos, ts.tex_arrays)
+    r32.set_ibl(ts.env)
+    W, H, F = 32, 32, 4
+    acc = np.zeros((H, W, 4), np.float32)
+    for f in range(1, F + 1):
+        r32.set_uniforms(ref_lib.uniform_block(ts.camera.matrix_world, ts.camera.fov, ts.camera.near, W, H, f, 8))
+        assert r32.render(W, H, acc) is not None
+    g["tex_image"] = acc
+    g["tex_image_whf"] = np.array([W, H, F], np.int32)
     np.savez_compressed(os.path.join(OUT, "reference_small.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_small.npz"))
 

@@ -136,3 +136,19 @@ def test_display_golden_reproduces_from_reference_build(g):
             np.testing.assert_array_equal(r.tonemap(g["display_hdr"], 1.7, gamma, int(mode)),
                                           g[f"display_tonemap_g{gamma}"][k])
     np.testing.assert_array_equal(r.fxaa(g["display_fxaa_in"]), g["display_fxaa"])
+
+
+def test_textured_golden_reproduces_from_reference_build(g):
+    from oracle import ref_lib
+    if not ref_lib.available("f32"):
+        pytest.skip("oracle/_ref not built (reference checkout absent)")
+    r = ref_lib.GlslReference("f32")
+    r.set_scene(g["vertices"], g["indices"], g["tex_materials"], g["bvh_nodes"], g["bvh_indices"])
+    r.set_textures(g["tex_infos"], [g["tex_array0"], g["tex_array1"]])
+    ev, sm, fl = r.bsdf(g["tex_bsdf_hit"], g["tex_bsdf_wo"], g["tex_bsdf_rnd"])
+    np.testing.assert_array_equal(ev, g["tex_bsdf_eval32"])
+    np.testing.assert_array_equal(sm, g["tex_bsdf_sample32"])
+    # the textures matter: the same queries without them differ
+    r.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
+    ev0, _, _ = r.bsdf(g["tex_bsdf_hit"], g["tex_bsdf_wo"], g["tex_bsdf_rnd"])
+    assert (np.abs(ev0 - ev).max(1) > 1e-6).mean() > 0.3
