@@ -516,7 +516,10 @@ DEV v3 to_linear_rgb(float4 c) { return mk(powf(c.x, 2.2f), powf(c.y, 2.2f), pow
 // configure_gltf_material (material.glsl:5-110) from the interpolated render
 // state: material record, textures, vertex colour, normal map, fix_normals,
 // anisotropy rotation, closure.  n / ng / tangent as fillRenderState leaves
-// them (not yet flipped to the incident side).
+// them (not yet flipped to the incident side).  kTextured = false is the
+// variant for scenes without textures: every texture id reads as unset (-1),
+// which is what those scenes' materials hold.
+template <bool kTextured>
 NOINL Surface configure_gltf(const DevScene& s, int mat, v3 n, v3 ng, float4 tangent, v3 wi, float u0, float v0,
                              float4 vcol, bool lean) {
   Surface S;
@@ -530,10 +533,9 @@ NOINL Surface configure_gltf(const DevScene& s, int mat, v3 n, v3 ng, float4 tan
   // 50 transmission, 51 clearcoat, 52 clearcoatRoughness, 54 sheenColor,
   // 55 sheenRoughness, 56 anisotropy, 57 anisotropyDirection, 58 iridescence,
   // 59 iridescenceThickness, 63 diffuseTransmissionColor
-  const bool textured = s.num_texinfo > 0;
   const float4 one = make_float4(1.f, 1.f, 1.f, 1.f);
   float4 m11 = one, m12 = one, m13 = one, m14 = one;
-  if (textured) {
+  if (kTextured) {
     m11 = __ldg(m + 11); m12 = __ldg(m + 12); m13 = __ldg(m + 13); m14 = __ldg(m + 14);
   } else {
     m11 = m12 = m13 = m14 = make_float4(-1.f, -1.f, -1.f, -1.f);
@@ -623,7 +625,8 @@ NOINL Surface configure_gltf(const DevScene& s, int mat, v3 n, v3 ng, float4 tan
 }
 
 // fillRenderState (renderer.frag:72-91, bvh.glsl:84-134) + configure_gltf.
-NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
+template <bool kTextured>
+NOINL Surface make_surface_t(const DevScene& s, int tri, float bu, float bv, v3 hit_pos, v3 wi, bool lean) {
   uint32_t i0 = __ldg(s.indices + 3 * size_t(tri)), i1 = __ldg(s.indices + 3 * size_t(tri) + 1),
            i2 = __ldg(s.indices + 3 * size_t(tri) + 2);
   float4 q0 = vtx(s, i0, 0), q1 = vtx(s, i1, 0), q2 = vtx(s, i2, 0);
@@ -641,14 +644,15 @@ NOINL Surface make_surface(const DevScene& s, int tri, float bu, float bv, v3 hi
   float4 vcol = make_float4(w0 * c0.x + bu * c1.x + bv * c2.x, w0 * c0.y + bu * c1.y + bv * c2.y,
                             w0 * c0.z + bu * c1.z + bv * c2.z, w0 * c0.w + bu * c1.w + bv * c2.w);
   float u0 = 0.f, v0 = 0.f;
-  if (s.num_texinfo > 0) {  // compute_interpolated_uv(set 0) (bvh.glsl:108-116)
+  if (kTextured) {  // compute_interpolated_uv(set 0) (bvh.glsl:108-116)
     float4 a = vtx(s, i0, 2), b = vtx(s, i1, 2), c = vtx(s, i2, 2);
     u0 = w0 * a.x + bu * b.x + bv * c.x;
     v0 = w0 * a.y + bu * b.y + bv * c.y;
   }
-  Surface S = configure_gltf(s, int(uint32_t(q0.w)), n, ng, tangent, wi, u0, v0, vcol, lean);
+  Surface S = configure_gltf<kTextured>(s, int(uint32_t(q0.w)), n, ng, tangent, wi, u0, v0, vcol, lean);
   S.pos = hit_pos;
   return S;
 }
+
 
 }  // namespace dspbr

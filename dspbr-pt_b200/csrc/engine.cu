@@ -123,8 +123,10 @@ void Engine::set_launch(const LaunchCfg& lc) {
   cudaStreamSynchronize(stream_);
   drop_graph();
   const int trav = lc_.traversal;
+  const bool tex = lc_.textured;
   lc_ = lc;
   lc_.traversal = trav;
+  lc_.textured = tex;
 }
 
 Sched Engine::sched() const {
@@ -155,6 +157,7 @@ int Engine::set_job(int slot, const Job& job, unsigned long long items_total) {
   if (slot < 0 || slot >= kMaxJobs) return s.fail(DSPBR_ERR_INVALID, "job slot %d out of range", slot);
   k_set_job<<<1, 32, 0, stream_>>>(job, items_total, slot, jobs_.p, js_.p, d_status_);
   slot_traversal_[slot] = job.s.wide ? kTravWide : kTravReference;
+  slot_textured_[slot] = job.s.num_texinfo > 0;
   ++kind_launches[3];
   return s.cuda(cudaGetLastError(), "set job");
 }
@@ -179,10 +182,14 @@ int Engine::set_active(const std::vector<int>& order) {
   int trav = order.empty() ? lc_.traversal : slot_traversal_[order[0]];
   for (int k : order)
     if (slot_traversal_[k] != trav) trav = kTravPerPath;
-  if (trav != lc_.traversal) {
+  // the shade kernels without the texture code when no active job samples textures
+  bool tex = false;
+  for (int k : order) tex = tex || slot_textured_[k];
+  if (trav != lc_.traversal || tex != lc_.textured) {
     TRY_CUDA(s, cudaStreamSynchronize(stream_), "sync");
     drop_graph();
     lc_.traversal = trav;
+    lc_.textured = tex;
   }
   return s.cuda(cudaGetLastError(), "set active jobs");
 }
@@ -309,7 +316,7 @@ int Engine::drain() {
   const int cur = cur_;
   mark_begin(2);
   launch_connect(sc, b, cur, false, lc_, stream_);
-  launch_drain(sc, b, cur, stream_);
+  launch_drain(sc, b, cur, lc_, stream_);
   launch_commit(sc, b, cur, stream_, false);
   mark_end();
   kind_launches[1] += 1;

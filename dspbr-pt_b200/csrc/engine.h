@@ -84,6 +84,7 @@ class Engine {
   uint32_t capacity_ = 0;
   int cur_ = 0;  // parity of the next iteration
   int slot_traversal_[kMaxJobs] = {};  // kTravWide / kTravReference of each job slot
+  bool slot_textured_[kMaxJobs] = {};  // the job's scene samples material textures
   LaunchCfg lc_;
   // pool
   DevBuf<float4> org_, dir_, weight_, rad_, hit_, sh_dir_, sh_c_, pl_dir_, pl_c_;

@@ -427,6 +427,7 @@ __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
 // Surface hit.  Returns true if the path continues with an extension ray and
 // sets `shadow` when NEE shadow rays were emitted; otherwise the path's sample
 // has been accumulated.
+template <bool kTextured>
 DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shadow) {
   shadow = false;
   const uint32_t j = b.job[slot];
@@ -453,7 +454,7 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
   v3 org = mk(o4);
   v3 wi = -dir;
   v3 pos = org + dir * hit.x;
-  Surface S = make_surface(J.s, tri, hit.y, hit.z, pos, wi, p.lean != 0);
+  Surface S = make_surface_t<kTextured>(J.s, tri, hit.y, hit.z, pos, wi, p.lean != 0);
   if (S.backside && !S.thin_walled) {  // Beer-Lambert absorption (misptdl.glsl:60-63)
     v3 sigma = -vlog(S.att_color) / S.att_dist;
     w = w * vexp(-sigma * hit.x);
@@ -525,6 +526,8 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
   return true;
 }
 
+// kTextured = false: no active job's scene has textures (their texture ids are all unset)
+template <bool kTextured>
 __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
   // the class queues, read as one sequence in class order
   __shared__ uint32_t start[kNumClasses + 1];
@@ -550,7 +553,7 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
       for (int jk = 1; jk < kNumClasses; ++jk) k += i >= start[jk] ? 1 : 0;
       slot = b.qh[size_t(k) * b.capacity + (i - start[k])];
       job = b.job[slot];
-      cont = shade_path(sc, b, slot, shadow);
+      cont = shade_path<kTextured>(sc, b, slot, shadow);
     }
     enqueue(qn, cn, cont, slot);
     enqueue(b.qs[next], b.counts + kCntShadow0 + next, shadow, slot);
@@ -566,6 +569,7 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
 // by the k_connect launched before it) and runs every path through extend ->
 // shade_miss / shade -> connect until it ends: the same device functions in
 // the same order per path, so each path's result is unchanged.
+template <bool kTextured>
 __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
@@ -590,7 +594,7 @@ __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
           break;
         }
         bool shadow = false;
-        const bool cont = shade_path(sc, b, slot, shadow);
+        const bool cont = shade_path<kTextured>(sc, b, slot, shadow);
         if (shadow) {
           int nrays = 0;
           connect_slot<false, kTravPerPath>(sc, b, slot, aborted, nrays, nullptr, nullptr);
@@ -665,7 +669,9 @@ __global__ void k_bsdf_query(DevScene s, uint32_t n, const float* hit20, const f
     float4 tangent = make_float4(h[6], h[7], h[8], h[9]);
     v3 wi = mk(h[10], h[11], h[12]);
     float4 vcol = make_float4(h[15], h[16], h[17], h[18]);
-    Surface S = configure_gltf(s, int(uint32_t(h[19])), n0, ng, tangent, wi, h[13], h[14], vcol, lean != 0);
+    const int mat = int(uint32_t(h[19]));
+    Surface S = s.num_texinfo > 0 ? configure_gltf<true>(s, mat, n0, ng, tangent, wi, h[13], h[14], vcol, lean != 0)
+                                  : configure_gltf<false>(s, mat, n0, ng, tangent, wi, h[13], h[14], vcol, lean != 0);
     const Closure& c = S.c;
     n0 = S.n;
     const bool back = S.backside;
@@ -736,10 +742,12 @@ void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, cons
   else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st) {
-  k_shade<<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
+  if (lc.textured) k_shade<true><<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
+  else k_shade<false><<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
 }
-void launch_drain(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st) {
-  k_drain<<<148 * 4, 128, 0, st>>>(sc, b, cur);
+void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st) {
+  if (lc.textured) k_drain<true><<<148 * 4, 128, 0, st>>>(sc, b, cur);
+  else k_drain<false><<<148 * 4, 128, 0, st>>>(sc, b, cur);
 }
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
   k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(sc, b);

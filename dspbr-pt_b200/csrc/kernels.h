@@ -127,6 +127,7 @@ struct LaunchCfg {
   int trace_blocks = 148 * 16, trace_threads = 128;
   int shade_blocks = 148 * 8, shade_threads = 128;
   int traversal = kTravPerPath;
+  bool textured = false;  // some active job samples material textures
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
@@ -137,7 +138,7 @@ void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& 
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
 // runs every path queued in q[cur] to its end (call after connect(cur), when no work item is left)
-void launch_drain(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st);
+void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
 
 // kernel-level queries (device buffers)

@@ -66,3 +66,42 @@ def test_textured_image_matches_golden_path_for_path(g, traversal):
     print("textured pixels equal to the reference path for path:", close.mean())
     assert close.mean() > 0.95
     assert np.abs(img - ref).mean() < 0.01 * ref[..., :3].mean()
+
+
+def test_server_mixes_textured_and_untextured_requests():
+    from dspbr.server import Server
+    from dspbr.viewport import DeviceIbl
+    ctx = Context(0)
+    tex, plain = synth.make_textured_small(0), synth.make_small(0)
+    scenes, ibls = [], []
+    for sc in (tex, plain):
+        sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+        ds = DeviceScene(ctx, sc.vertices, sc.indices, sc.materials, sc.bvh)
+        if getattr(sc, "tex_infos", None) is not None:
+            ds.set_textures(sc.tex_infos, sc.tex_arrays)
+        scenes.append(ds)
+        ibls.append(DeviceIbl(ctx, sc.env))
+    reqs = [(0, 48, 40, 3), (1, 40, 32, 4), (0, 17, 9, 2)]
+
+    def submit(srv, r):
+        k, w, h, spp = r
+        sc = (tex, plain)[k]
+        return srv.submit(scenes[k], ibls[k], helpers.camera_of(sc), w, h, spp, {"maxBounces": 6})
+
+    alone = []
+    for r in reqs:
+        srv = Server(ctx, path_pool=1 << 16)
+        img, info = srv.wait(submit(srv, r))
+        srv.close()
+        assert info["state"] == "done"
+        alone.append(img.copy())
+    srv = Server(ctx, path_pool=3000)
+    ids = [submit(srv, r) for r in reqs]
+    mix = [srv.wait(i, timeout_ms=120000)[0].copy() for i in ids]
+    srv.close()
+    for a, m in zip(alone, mix):
+        np.testing.assert_allclose(m, a, rtol=1e-6, atol=1e-7)
+    assert all(np.isfinite(a).all() and a[..., :3].max() > 0 for a in alone)
+    for o in scenes + ibls:
+        o.close()
+    ctx.close()
