@@ -277,6 +277,72 @@ def scene_build_section(local, sc, args):
     return out
 
 
+def configs_section(local, args):
+    """The other two scene configurations at one progressive frame (1 spp) per
+    step: "small" (1,324 triangles, 512x512, 8 bounces: BVH and triangles sit
+    in L2) and "divergence" (4M triangles, 60% transmissive / volume /
+    dispersive and 20% iridescent materials, 4096x2048 env, 1280x720, 32
+    bounces, Russian roulette after bounce 4).  PCG32 per pixel sample and the
+    alias-table environment sampling; the BVH is built by the library (host
+    binned SAH).  Device time of K frames in one render call, the k_extend
+    time of the same frames, and the reference traversal's node / triangle
+    counts of one more frame for the traversal roofline."""
+    from dspbr import synth
+    from dspbr.viewport import PathtracingCamera, PathtracingViewport
+    out = {}
+    peak, peak_kind = peaks()
+    for name in ("small", "divergence"):
+        t0 = time.perf_counter()
+        sc = synth.WORKLOADS[name](0)
+        t1 = time.perf_counter()
+        v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
+                                settings={"maxBounces": sc.max_bounces,
+                                          "russianRouletteStartDepth": sc.rr_start_depth,
+                                          "rng": "pcg", "envSampling": "alias"})
+        v.setScene(sc)
+        v.setIBL(sc.env)
+        v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
+        t2 = time.perf_counter()
+        lib, h = v.ctx.lib, v.ctx.h
+        k = max(2, min(args.steps, 10))
+        v.ctx.check(lib.dspbr_render(h, max(3, args.warmup)))
+        d0 = v.diagnostics
+        v.ctx.check(lib.dspbr_render(h, k))
+        d1 = v.diagnostics
+        rays = sum(d1[f] - d0[f] for f in ("rays_primary", "rays_extension", "rays_shadow"))
+        ms = d1["last_render_ms"]
+        v.ctx.check(lib.dspbr_set_profiling(h, 1))
+        v.ctx.check(lib.dspbr_render(h, k))
+        dp = v.diagnostics
+        v.ctx.check(lib.dspbr_set_profiling(h, 0))
+        v.ctx.check(lib.dspbr_set_counting(h, 1))
+        dc0 = v.diagnostics
+        v.ctx.check(lib.dspbr_render(h, 1))
+        dc1 = v.diagnostics
+        v.ctx.check(lib.dspbr_set_counting(h, 0))
+        alg = 64.0 * dc1["nodes_closest"] + 40.0 * dc1["tris_closest"]
+        closest = (dc1["rays_primary"] + dc1["rays_extension"]) - (dc0["rays_primary"] + dc0["rays_extension"])
+        ext_ms = dp["extend_ms"] / k
+        achieved = alg / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
+        out[name] = {
+            "triangles": int(sc.num_triangles), "width": sc.width, "height": sc.height,
+            "max_bounces": sc.max_bounces, "rr_start_depth": sc.rr_start_depth, "frames": k,
+            "mrays_per_s": rays / (ms * 1e-3) / 1e6, "ms_per_frame": ms / k,
+            "samples_per_s": sc.width * sc.height * k / (ms * 1e-3),
+            "rays_per_frame": rays / k, "traversal_aborted": d1["traversal_aborted"] - d0["traversal_aborted"],
+            "extend_roofline": {"achieved": achieved, "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+                                "frac": achieved / peak if achieved else None, "bytes_per_frame": alg,
+                                "nodes_per_ray": dc1["nodes_closest"] / max(1, closest),
+                                "tris_per_ray": dc1["tris_closest"] / max(1, closest),
+                                "extend_ms_per_frame": ext_ms},
+            "connect_ms_per_frame": dp["connect_ms"] / k, "shade_ms_per_frame": dp["shade_ms"] / k,
+            "scene_gen_s": t1 - t0, "scene_load_s": t2 - t1,
+            "full_config_estimate_s": ms / k * sc.spp / 1e3,
+        }
+        v.dispose()
+    return out
+
+
 def serving_section(local, quick=False):
     """Batching (64 viewports over 8 scenes of 10k-2M triangles, 128^2-1024^2,
     1-64 spp) and serving (Poisson arrivals over 16 scenes of 50k-4M
@@ -490,6 +556,7 @@ def run_gpu_arm(args):
     cs = clocks.summary()
     v.dispose()
     build = scene_build_section(local, sc, args) if ws == 1 and not args.no_serving else None
+    other = configs_section(local, args) if ws == 1 and not args.no_serving else None
     serving = None
     if ws == 1 and not args.no_serving:
         serving = serving_section(local, quick=args.quick_serving)
@@ -530,6 +597,8 @@ def run_gpu_arm(args):
         }
         if build is not None:
             line["scene_build"] = build
+        if other is not None:
+            line["configs"] = other
         if serving is not None:
             line.update(serving)
         print(json.dumps(line))

@@ -402,7 +402,9 @@ def make_large(seed: int = 0, target_tris: int = 1_000_000, n_inst: int = 256) -
     return Scene("large", verts, idx, mats, cam, 1920, 1080, 256, 12, 2, env, seed)
 
 
-def make_divergence(seed: int = 0, target_tris: int = 4_000_000, n_inst: int = 400) -> Scene:
+def make_divergence(seed: int = 0, n_inst: int = 536, tris_per_inst: int = 10_000) -> Scene:
+    """~4.0M triangles: 536 instances alternating 9,800-triangle displaced grids
+    and 5,120-triangle icospheres."""
     rng = np.random.default_rng(seed)
 
     def kind(i):  # 60% transmissive/volume (dispersive), 20% iridescent, 20% base
@@ -411,7 +413,7 @@ def make_divergence(seed: int = 0, target_tris: int = 4_000_000, n_inst: int = 4
             return ["transmission", "volume", "dispersion"][r % 3]
         return "iridescence" if r < 8 else "base"
 
-    verts, idx, mats = _instances(rng, n_inst, target_tris // n_inst, kind)
+    verts, idx, mats = _instances(rng, n_inst, tris_per_inst, kind)
     env = env_lognormal(4096, 2048, rng, 1.5, 1e4)
     cam = Camera.look_at((0, 15, 135), (0, 0, 0), fov=45.0, near=0.1)
     return Scene("divergence", verts, idx, mats, cam, 1280, 720, 512, 32, 4, env, seed)
