@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, f32
-from .viewport import Context, DeviceIbl, DeviceScene, PathtracingCamera, apply_settings
+from .viewport import Context, DeviceIbl, DeviceScene, PathtracingCamera, apply_scene_lights, apply_settings
 
 STATES = {_lib.REQ_QUEUED: "queued", _lib.REQ_RUNNING: "running", _lib.REQ_DONE: "done",
           _lib.REQ_CANCELLED: "cancelled", _lib.REQ_FAILED: "failed"}
@@ -57,6 +57,7 @@ class Server:
         r.fov_deg, r.near_plane = float(camera.fov), float(camera.near)
         r.width, r.height, r.spp = int(width), int(height), int(spp)
         self.lib.dspbr_params_default(C.byref(r.params))
+        apply_scene_lights(r.params, getattr(scene, "lights", None))
         if settings:
             apply_settings(r.params, settings)
         if out is None:

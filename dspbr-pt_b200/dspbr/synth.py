@@ -126,6 +126,9 @@ class Scene:
     env: np.ndarray | None = None  # (H, W, 4) float32
     seed: int = 0
     meta: dict = field(default_factory=dict)
+    # KHR_lights_punctual lights on mesh nodes, as scene_loader.ts:187-199 adds
+    # them: {"position": (x, y, z), "type": 0 point / 1 other, "emission": (r, g, b)}
+    lights: list = field(default_factory=list)
 
     @property
     def num_triangles(self) -> int:

@@ -96,11 +96,27 @@ class Context:
         return np.frombuffer(raw, dtype=dtype).reshape(shape)
 
 
+def apply_scene_lights(params, lights) -> bool:
+    """The first scene light drives u_point_light_* whatever its type
+    (renderer.ts:424-430); no light disables it (w = 0).  Returns whether the
+    parameters changed."""
+    pos, emis = (0.0, 0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 0.0)
+    if lights:
+        pos = (*[float(x) for x in lights[0]["position"]], 1.0)
+        emis = (*[float(x) for x in lights[0]["emission"]], 1.0)
+    changed = tuple(params.point_light_position) != pos or tuple(params.point_light_emission) != emis
+    for k in range(4):
+        params.point_light_position[k] = pos[k]
+        params.point_light_emission[k] = emis[k]
+    return changed
+
+
 class DeviceScene:
     """Scene resident on the device (dspbr_scene)."""
 
-    def __init__(self, ctx: Context, vertices, indices, materials, bvh: Bvh | None = None):
+    def __init__(self, ctx: Context, vertices, indices, materials, bvh: Bvh | None = None, lights=None):
         self.ctx = ctx
+        self.lights = list(lights or [])  # host-side: requests on this scene take their point light from it
         v = f32(vertices).reshape(-1, VERTEX_STRIDE)
         i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         m = f32(materials).reshape(-1, MATERIAL_STRIDE)
@@ -319,6 +335,9 @@ class PathtracingViewport:
         if self._scene is not None:
             self._scene.close()
         self._scene = ds
+        ds.lights = list(getattr(scene, "lights", None) or [])
+        if apply_scene_lights(self.params, ds.lights):
+            self._apply_params()
         self.ctx.check(self.ctx.lib.dspbr_set_scene(self.ctx.h, ds.h))
         self._emit("sceneLoaded", {"scene": scene})
         self._emit_diag()

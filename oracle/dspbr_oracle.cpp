@@ -1080,6 +1080,7 @@ struct Params {
   int max_bounces, use_ibl, bg_from_ibl, rr_start, env_mode, lean, pcg;
   float ibl_rot_deg, bg[4], ray_eps, clamp, rr_prob;
   uint64_t seed;
+  float pl_pos[4], pl_emis[4];  // u_point_light_position / _emission; w > 0.5 enables
 };
 
 template <class R> V<R> rot_phi(V<R> d, R a) {
@@ -1248,6 +1249,22 @@ void trace_path(const Scene& s, const Ibl* I, const Params& P, int px, int py, u
           Ld = ibl_eval(*I, rot, ld) * f * cnl / ip;
           if (bp > K<R>::EPS_PDF) Ld = Ld * (ip / (ip + bp));
         }
+      }
+    }
+    // sampleAndEvaluatePointLight (lighting.glsl:2-22): visibility by a
+    // nearest-hit ray bounded by the light distance (bvh.glsl:218-223)
+    if (P.pl_pos[3] > 0.5f) {
+      V<R> lp = v3<R>(R(P.pl_pos[0]), R(P.pl_pos[1]), R(P.pl_pos[2]));
+      V<R> ld = lp - pos;
+      R dist2 = dot(ld, ld);
+      V<R> ldn = nrm(ld);
+      R cnl = sat(dot(ldn, nn));
+      Hit<R> sh;
+      bool visible = !closest_hit(s, pos, ldn, std::sqrt(dist2), sh, ts, true);
+      if (cnl > K<R>::EPS_COS && visible) {
+        V<R> f = eval(S.c, S.n, wi, ldn) / gmax(std::fabs(dot(S.n, ldn)), K<R>::EPS);
+        V<R> e = v3<R>(R(P.pl_emis[0]), R(P.pl_emis[1]), R(P.pl_emis[2]));
+        Ld = Ld + f * (e / dist2) * cnl;
       }
     }
     L = L + Ld * w;

@@ -27,7 +27,7 @@ class Params(C.Structure):
                 ("height", C.c_int), ("max_bounces", C.c_int), ("use_ibl", C.c_int), ("bg_from_ibl", C.c_int),
                 ("rr_start", C.c_int), ("env_mode", C.c_int), ("lean", C.c_int), ("pcg", C.c_int),
                 ("ibl_rot_deg", C.c_float), ("bg", C.c_float * 4), ("ray_eps", C.c_float), ("clamp", C.c_float),
-                ("rr_prob", C.c_float), ("seed", C.c_uint64)]
+                ("rr_prob", C.c_float), ("seed", C.c_uint64), ("pl_pos", C.c_float * 4), ("pl_emis", C.c_float * 4)]
 
 
 def build() -> str:
@@ -38,7 +38,8 @@ def build() -> str:
 
 
 def make_params(matrix, fov, near, width, height, max_bounces=8, use_ibl=1, bg_from_ibl=1, rr_start=2, env_mode=1,
-                lean=0, pcg=0, ibl_rot_deg=0.0, bg=(0, 0, 0, 1), ray_eps=1e-4, clamp=3.0, rr_prob=0.1, seed=0):
+                lean=0, pcg=0, ibl_rot_deg=0.0, bg=(0, 0, 0, 1), ray_eps=1e-4, clamp=3.0, rr_prob=0.1, seed=0,
+                point_light=None):
     p = Params()
     for i, x in enumerate(np.asarray(matrix, np.float32).reshape(16)):
         p.view[i] = float(x)
@@ -48,6 +49,10 @@ def make_params(matrix, fov, near, width, height, max_bounces=8, use_ibl=1, bg_f
     for i in range(4):
         p.bg[i] = bg[i]
     p.ray_eps, p.clamp, p.rr_prob, p.seed = ray_eps, clamp, rr_prob, seed
+    if point_light is not None:  # ((x, y, z), (r, g, b))
+        for i in range(3):
+            p.pl_pos[i], p.pl_emis[i] = float(point_light[0][i]), float(point_light[1][i])
+        p.pl_pos[3] = p.pl_emis[3] = 1.0
     return p
 
 

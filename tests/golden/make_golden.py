@@ -133,6 +133,23 @@ def main():
         assert r32.render(W, H, acc) is not None
     g["tex_image"] = acc
     g["tex_image_whf"] = np.array([W, H, F], np.int32)
+    # the point light (lighting.glsl:2-22, misptdl.glsl:24-30): the small scene
+    # with a light under the ceiling, as the first scene light sets it
+    # (renderer.ts:424-430)
+    ps = synth.make_small(0)
+    pbvh = Bvh.build(ps.vertices, ps.indices, 20)
+    r32.set_scene(ps.vertices, ps.indices, ps.materials, pbvh.nodes, pbvh.indices)
+    r32.set_ibl(ps.env)
+    light = ((0.2, 1.7, 0.3), (6.0, 5.0, 4.0))
+    W, H, F = 32, 32, 4
+    acc = np.zeros((H, W, 4), np.float32)
+    for f in range(1, F + 1):
+        r32.set_uniforms(ref_lib.uniform_block(ps.camera.matrix_world, ps.camera.fov, ps.camera.near, W, H, f, 8,
+                                               point_light=light))
+        assert r32.render(W, H, acc) is not None
+    g["pl_image"] = acc
+    g["pl_light"] = np.array(light, np.float32)
+    g["pl_image_whf"] = np.array([W, H, F], np.int32)
     np.savez_compressed(os.path.join(OUT, "reference_small.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_small.npz"))
 

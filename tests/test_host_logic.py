@@ -97,3 +97,14 @@ def test_bench_replica_reductions_gloo_world_size_2():
         p.join(timeout=60)
     assert [r[:3] for r in res] == [(0, 2, 0), (1, 2, 1)]
     assert all(r[3] == 2.5 and r[4] == 3.0 for r in res)
+
+
+def test_first_scene_light_sets_the_point_light():
+    # renderer.ts:424-430: lights[0] of any type, w = 1; no light: w = 0
+    p = _lib.default_params()
+    assert viewport.apply_scene_lights(p, [{"position": (1, 2, 3), "type": 1, "emission": (4, 5, 6)},
+                                           {"position": (9, 9, 9), "type": 0, "emission": (1, 1, 1)}])
+    assert tuple(p.point_light_position) == (1, 2, 3, 1) and tuple(p.point_light_emission) == (4, 5, 6, 1)
+    assert not viewport.apply_scene_lights(p, [{"position": (1, 2, 3), "type": 0, "emission": (4, 5, 6)}])
+    assert viewport.apply_scene_lights(p, [])
+    assert tuple(p.point_light_position) == (0, 0, 0, 0)

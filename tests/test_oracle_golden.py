@@ -152,3 +152,18 @@ def test_textured_golden_reproduces_from_reference_build(g):
     r.set_scene(g["vertices"], g["indices"], g["materials"], g["bvh_nodes"], g["bvh_indices"])
     ev0, _, _ = r.bsdf(g["tex_bsdf_hit"], g["tex_bsdf_wo"], g["tex_bsdf_rnd"])
     assert (np.abs(ev0 - ev).max(1) > 1e-6).mean() > 0.3
+
+
+def test_point_light_image_matches_reference(g):
+    from dspbr import synth
+    from dspbr.viewport import Bvh
+    sc = synth.make_small(0)
+    bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    o = oracle_lib.Oracle()
+    o.set_scene(sc.vertices, sc.indices, sc.materials, bvh.nodes, bvh.indices)
+    o.set_ibl(sc.env)
+    W, H, F = (int(x) for x in g["pl_image_whf"])
+    p = oracle_lib.make_params(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, W, H, max_bounces=8,
+                               point_light=g["pl_light"])
+    img = o.render_image(p, F)
+    assert helpers.close_mask(img, g["pl_image"], 1e-5, 1e-6).mean() > 0.999
