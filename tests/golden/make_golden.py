@@ -9,6 +9,7 @@ Inputs are stored beside the outputs so that the fixtures stand alone.
 Run from the repository root where the reference checkout is available:
     python tests/golden/make_golden.py
 """
+import hashlib
 import os
 import sys
 
@@ -150,6 +151,26 @@ def main():
     g["pl_image"] = acc
     g["pl_light"] = np.array(light, np.float32)
     g["pl_image_whf"] = np.array([W, H, F], np.int32)
+    # a glTF asset packed by dspbr.gltf (scene_loader.ts), rendered by the
+    # reference shaders with its textures
+    from tests.gltf_writer import sample_camera, sample_scene
+    from dspbr import gltf
+    gs = gltf.load_gltf(sample_scene().glb_bytes())
+    cam = sample_camera()
+    gbvh = Bvh.build(gs.vertices, gs.indices, 20)
+    r32.set_scene(gs.vertices, gs.indices, gs.materials, gbvh.nodes, gbvh.indices)
+    r32.set_textures(gs.tex_infos, gs.tex_arrays)
+    r32.set_ibl(ps.env)
+    W, H, F = 48, 36, 4
+    acc = np.zeros((H, W, 4), np.float32)
+    for f in range(1, F + 1):
+        r32.set_uniforms(ref_lib.uniform_block(cam.matrix_world, cam.fov, cam.near, W, H, f, 8))
+        assert r32.render(W, H, acc) is not None
+    g["gltf_image"] = acc
+    g["gltf_image_whf"] = np.array([W, H, F], np.int32)
+    g["gltf_vertices_sha"] = np.frombuffer(hashlib.sha256(gs.vertices.tobytes() + gs.indices.tobytes() +
+                                                          gs.materials.tobytes() + gs.tex_infos.tobytes()).digest(),
+                                           np.uint8)
     np.savez_compressed(os.path.join(OUT, "reference_small.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_small.npz"))
 
