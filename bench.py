@@ -343,6 +343,41 @@ def configs_section(local, args):
     return out
 
 
+def gltf_section(local, args):
+    """glTF asset to first frame: a ~1.9M-triangle .glb (256 instancing nodes,
+    four materials, four 1024x1024 PNG textures) packed by dspbr.gltf
+    (scene_loader.ts), then setScene (host binned-SAH BVH, 4-wide collapse,
+    upload, textures) and setIBL, then frames at 1280x720."""
+    from dspbr import gltf, synth
+    from dspbr.viewport import PathtracingCamera, PathtracingViewport
+    from tests.gltf_writer import large_asset
+    glb = large_asset().glb_bytes()
+    t0 = time.perf_counter()
+    sc = gltf.load_gltf(glb)
+    t1 = time.perf_counter()
+    v = PathtracingViewport(device=local, width=1280, height=720, settings={"maxBounces": 8})
+    v.setScene(sc)
+    t2 = time.perf_counter()
+    env = synth.make_small(0).env
+    v.setIBL(env)
+    cam = synth.Camera.look_at((0, 20, 120), (0, 0, 0), fov=45.0, near=0.1)
+    v.setCamera(PathtracingCamera(cam.matrix_world, cam.fov, cam.near))
+    lib, h = v.ctx.lib, v.ctx.h
+    v.ctx.check(lib.dspbr_render(h, 1))
+    t3 = time.perf_counter()
+    d0 = v.diagnostics
+    k = max(2, min(args.steps, 10))
+    v.ctx.check(lib.dspbr_render(h, k))
+    d1 = v.diagnostics
+    v.dispose()
+    rays = sum(d1[f] - d0[f] for f in ("rays_primary", "rays_extension", "rays_shadow"))
+    return {"file_mb": len(glb) / 1e6, "triangles": int(sc.num_triangles), "materials": int(sc.materials.shape[0]),
+            "texture_layers": int(sum(a.shape[0] for a in sc.tex_arrays)),
+            "load_gltf_ms": 1e3 * (t1 - t0), "set_scene_ms": 1e3 * (t2 - t1),
+            "to_first_frame_ms": 1e3 * (t3 - t0), "mrays_per_s": rays / (d1["last_render_ms"] * 1e-3) / 1e6,
+            "ms_per_frame": d1["last_render_ms"] / k}
+
+
 def serving_section(local, quick=False):
     """Batching (64 viewports over 8 scenes of 10k-2M triangles, 128^2-1024^2,
     1-64 spp) and serving (Poisson arrivals over 16 scenes of 50k-4M
@@ -553,10 +588,20 @@ def run_gpu_arm(args):
     e2e_value = e2e_rays / e2e_t / 1e6
     e2e_parts = {"set_camera_ms": 1e3 * parts[0] / e2e_steps, "render_1_frame_ms": 1e3 * parts[1] / e2e_steps,
                  "read_accumulation_ms": 1e3 * parts[2] / e2e_steps}
+    # the iterations of one more single-frame call (untimed): device clock at
+    # the end of each iteration from the first one's end, and the paths left
+    last = v.timeline(1)
+    v.setCamera(cam)
+    v.start(1)
+    tl = v.timeline(256)
+    tl = tl[tl[:, 0] > (last[-1, 0] if len(last) else -1)]
+    if len(tl):
+        e2e_parts["one_frame_iterations"] = [[round(float(r[1] - tl[0, 1]), 4), int(r[2])] for r in tl]
     cs = clocks.summary()
     v.dispose()
     build = scene_build_section(local, sc, args) if ws == 1 and not args.no_serving else None
     other = configs_section(local, args) if ws == 1 and not args.no_serving else None
+    gltf_load = gltf_section(local, args) if ws == 1 and not args.no_serving else None
     serving = None
     if ws == 1 and not args.no_serving:
         serving = serving_section(local, quick=args.quick_serving)
@@ -599,6 +644,8 @@ def run_gpu_arm(args):
             line["scene_build"] = build
         if other is not None:
             line["configs"] = other
+        if gltf_load is not None:
+            line["gltf"] = gltf_load
         if serving is not None:
             line.update(serving)
         print(json.dumps(line))

@@ -652,6 +652,13 @@ int dspbr_set_wave_paths(dspbr_ctx* c, uint32_t paths) {
   return DSPBR_OK;
 }
 
+int dspbr_set_drain_threshold(dspbr_ctx* c, uint32_t paths) {
+  if (!c) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  c->eng->set_drain_below(paths);
+  return DSPBR_OK;
+}
+
 int dspbr_resize(dspbr_ctx* c, int w, int h) {
   if (!c || w <= 0 || h <= 0 || int64_t(w) * h > (int64_t(1) << 28)) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
@@ -988,6 +995,24 @@ int dspbr_host_free(dspbr_ctx* c, void* ptr) {
   if (c) return c->st().cuda(e, "host free");
   cudaGetLastError();
   return DSPBR_ERR_CUDA;
+}
+
+int dspbr_get_timeline(dspbr_ctx* c, uint32_t max_entries, uint64_t* iteration, uint64_t* t_ns, uint32_t* live,
+                       uint32_t* count) {
+  if (!c || !count) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  std::vector<TimelineEntry> tl;
+  int rc = c->eng->timeline(max_entries, tl);
+  if (rc) return rc;
+  for (size_t k = 0; k < tl.size(); ++k) {
+    if (iteration) iteration[k] = tl[k].iteration;
+    if (t_ns) t_ns[k] = tl[k].t_ns;
+    if (live) live[k] = tl[k].live;
+  }
+  *count = uint32_t(tl.size());
+  return DSPBR_OK;
 }
 
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {

@@ -47,6 +47,9 @@ Engine::~Engine() {
   for (auto e : ring_)
     if (e) cudaEventDestroy(e);
   for (auto e : ev_pool_) cudaEventDestroy(e);
+  if (fork_) cudaEventDestroy(fork_);
+  if (join_) cudaEventDestroy(join_);
+  if (side_) cudaStreamDestroy(side_);
   if (h_status_) cudaFreeHost(h_status_);
 }
 
@@ -60,6 +63,11 @@ int Engine::init() {
   TRY_CUDA(s, counts_.alloc(kCntNum), "counters");
   TRY_CUDA(s, cursors_.alloc(3), "counters");
   TRY_CUDA(s, stats_.alloc(8), "stats");
+  TRY_CUDA(s, timeline_.alloc(kTimeline), "timeline");
+  TRY_CUDA(s, cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "stream");
+  TRY_CUDA(s, cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
+  TRY_CUDA(s, cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "event");
+  TRY_CUDA(s, cudaMemsetAsync(timeline_.p, 0, timeline_.bytes(), stream_), "timeline");
   TRY_CUDA(s, cudaMemsetAsync(js_.p, 0, js_.bytes(), stream_), "job table");
   TRY_CUDA(s, cudaMemsetAsync(active_.p, 0, active_.bytes(), stream_), "job table");
   TRY_CUDA(s, cudaMemsetAsync(counts_.p, 0, counts_.bytes(), stream_), "counters");
@@ -137,6 +145,7 @@ Sched Engine::sched() const {
   sc.nactive = active_.p + kMaxJobs;
   sc.status = d_status_;
   sc.iteration = cursors_.p + 2;
+  sc.timeline = timeline_.p;
   return sc;
 }
 
@@ -247,9 +256,129 @@ int Engine::one_iteration(bool counting) {
   return Status{err_}.cuda(cudaGetLastError(), "render launch");
 }
 
+// In a captured iteration the closest-hit launch (q[cur]) and the shadow-ray
+// launch (qs[cur]) run as parallel branches: extend writes the hit records,
+// hit / miss queues and their counters, connect adds to the path radiance;
+// neither reads what the other writes.  When few paths are left, each is
+// bound by the latency of its slowest ray, and the two overlap.
+void Engine::extend_and_connect(const Sched& sc, const PathBuf& b, int cur) {
+  cudaEventRecord(fork_, stream_);
+  cudaStreamWaitEvent(side_, fork_, 0);
+  launch_connect(sc, b, cur, false, lc_, side_);
+  launch_extend(sc, b, cur, false, lc_, stream_);
+  cudaEventRecord(join_, side_);
+  cudaStreamWaitEvent(stream_, join_, 0);
+}
+
 void Engine::drop_graph() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
+  if (loop_graph_) cudaGraphExecDestroy(loop_graph_);
+  loop_graph_ = nullptr;
+}
+
+// while (cond) { iteration(0); iteration(1) + loop decision }; connect(0);
+// drain(0); commit(0).  The condition starts at 1 on every launch; the
+// commit kernel of the second iteration sets it (kernels.cu, k_commit), and
+// LoopCtl::pairs_left bounds the number of pairs.
+int Engine::capture_loop_graph() {
+  Status s{err_};
+  const Sched sc = sched();
+  const PathBuf b = paths();
+  if (!loop_ctl_.p) TRY_CUDA(s, loop_ctl_.alloc(1), "loop control");
+  cudaGraph_t g = nullptr;
+  TRY_CUDA(s, cudaGraphCreate(&g, 0), "loop graph");
+  auto fail = [&](cudaError_t e, const char* what) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return s.cuda(e, what);
+  };
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return fail(e, "loop graph condition");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop_node;
+  e = cudaGraphAddNode(&loop_node, g, nullptr, 0, &cp);
+  if (e != cudaSuccess) return fail(e, "loop graph node");
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(e, "loop body capture");
+  for (int cur = 0; cur < 2; ++cur) {
+    extend_and_connect(sc, b, cur);
+    launch_shade_miss(sc, b, lc_, stream_);
+    launch_shade(sc, b, cur ^ 1, lc_, stream_);
+    launch_regen(sc, b, cur ^ 1, stream_);
+    if (cur == 0) launch_commit(sc, b, cur, stream_);
+    else launch_commit_loop(sc, b, cur, h, loop_ctl_.p, stream_);
+  }
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(stream_, &captured);
+  if (e != cudaSuccess) return fail(e, "loop body capture");
+  e = cudaStreamBeginCaptureToGraph(stream_, g, &loop_node, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(e, "loop tail capture");
+  launch_connect(sc, b, 0, false, lc_, stream_);
+  launch_drain(sc, b, 0, lc_, stream_);
+  launch_commit(sc, b, 0, stream_, false);
+  e = cudaStreamEndCapture(stream_, &captured);
+  if (e != cudaSuccess) return fail(e, "loop tail capture");
+  e = cudaGraphInstantiate(&loop_graph_, g, 0);
+  cudaGraphDestroy(g);
+  g = nullptr;
+  if (e != cudaSuccess) {
+    loop_graph_ = nullptr;
+    return fail(e, "loop graph instantiate");
+  }
+  return DSPBR_OK;
+}
+
+int Engine::timeline(uint32_t max_entries, std::vector<TimelineEntry>& out) {
+  Status s{err_};
+  out.clear();
+  if (!timeline_.p) return DSPBR_OK;
+  std::vector<TimelineEntry> all(kTimeline);
+  TRY_CUDA(s, cudaStreamSynchronize(stream_), "timeline");
+  TRY_CUDA(s, cudaMemcpy(all.data(), timeline_.p, timeline_.bytes(), cudaMemcpyDeviceToHost), "timeline");
+  const unsigned long long last = h_status_->iteration;
+  const unsigned long long n = std::min<unsigned long long>({max_entries, last, kTimeline});
+  for (unsigned long long it = last + 1 - n; it <= last && n; ++it) {
+    const TimelineEntry& e = all[it % kTimeline];
+    if (e.iteration == it) out.push_back(e);
+  }
+  return DSPBR_OK;
+}
+
+int Engine::run_loop(int slot, unsigned long long max_iter) {
+  Status s{err_};
+  const volatile HostStatus* hs = h_status_;
+  const unsigned long long it0 = hs->iteration;  // every earlier launch has completed
+  unsigned long long eager = 0;
+  if (cur_ == 1) {  // the loop body starts at parity 0
+    int rc = one_iteration(false);
+    if (rc) return rc;
+    eager = 1;
+    max_iter = max_iter > 1 ? max_iter - 1 : 1;
+  }
+  if (!loop_graph_) {
+    int rc = capture_loop_graph();
+    if (rc) return rc;
+  }
+  launch_set_loop(loop_ctl_.p, (max_iter + 1) / 2, drain_below_, stream_);
+  TRY_CUDA(s, cudaGetLastError(), "loop control");
+  TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+  TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");
+  // the tail's commit counts as one more iteration
+  const unsigned long long body = hs->iteration - it0 - 1 - eager;
+  kind_launches[0] += body;
+  kind_launches[1] += body + 1;
+  kind_launches[2] += 4 * body;
+  kind_launches[3] += 3;
+  cur_ = 0;  // the tail drained every path: both queues are empty
+  if (job_done(slot)) return DSPBR_OK;
+  return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: job not finished after %llu iterations", max_iter);
 }
 
 // Two iterations (parity 0, then 1) captured from the stream.  Every argument
@@ -262,8 +391,7 @@ int Engine::capture_graph() {
   cudaGraph_t g = nullptr;
   TRY_CUDA(s, cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
   for (int cur = 0; cur < 2; ++cur) {
-    launch_extend(sc, b, cur, false, lc_, stream_);
-    launch_connect(sc, b, cur, false, lc_, stream_);
+    extend_and_connect(sc, b, cur);
     launch_shade_miss(sc, b, lc_, stream_);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
@@ -327,6 +455,7 @@ int Engine::drain() {
 
 int Engine::run_until_done(int slot, unsigned long long max_iter, bool counting) {
   Status s{err_};
+  if (!counting && !profiling) return run_loop(slot, max_iter);
   unsigned long long it = 0;
   long k = 0;
   while (it < max_iter) {
@@ -341,7 +470,7 @@ int Engine::run_until_done(int slot, unsigned long long max_iter, bool counting)
       if (job_done(slot)) return DSPBR_OK;
       // the tail: every work item started and few paths left
       const volatile JobStatus& js = h_status_->job[slot];
-      if (!counting && js.items_next >= js.items_total && h_status_->live_paths < kDrainBelow) {
+      if (!counting && js.items_next >= js.items_total && h_status_->live_paths < drain_below_) {
         int rc2 = drain();
         if (rc2) return rc2;
         TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");

@@ -49,6 +49,13 @@ class Engine {
   // Runs iterations until job `slot` has started all items and has no live
   // path, keeping `lookahead` steps queued; `max_iter` bounds the loop.
   int run_until_done(int slot, unsigned long long max_iter, bool counting);
+  // The same as one graph launch: a device-side while loop over pairs of
+  // iterations (the commit kernel decides whether another pair runs), then
+  // the tail drain; the host waits once.  Not while profiling or counting.
+  int run_loop(int slot, unsigned long long max_iter);
+  void set_drain_below(uint32_t paths) { drain_below_ = paths ? paths : kDrainBelow; }
+  // The last (up to max_entries, at most kTimeline) iterations' records, oldest first.
+  int timeline(uint32_t max_entries, std::vector<TimelineEntry>& out);
   // Finishes every path in the pool in one launch (connect of the pending
   // shadow rays, then each path run to its end).  Only when no active job has
   // unstarted work items.
@@ -72,6 +79,8 @@ class Engine {
  private:
   int one_iteration(bool counting);
   int capture_graph();
+  int capture_loop_graph();
+  void extend_and_connect(const Sched& sc, const PathBuf& b, int cur);
   void drop_graph();
   cudaEvent_t next_event();
   void mark_begin(int kind);
@@ -98,13 +107,23 @@ class Engine {
   DevBuf<uint32_t> counts_;
   DevBuf<unsigned long long> cursors_;  // free head, free tail, iteration
   DevBuf<unsigned long long> stats_;
+  DevBuf<TimelineEntry> timeline_;
   HostStatus* h_status_ = nullptr;
   HostStatus* d_status_ = nullptr;
   // two iterations (parity 0 then 1) captured once
   cudaGraphExec_t graph_ = nullptr;
+  // a render call: while (device condition) { two iterations }, then the tail
+  cudaGraphExec_t loop_graph_ = nullptr;
+  // fork / join of the parallel extend and connect branches during capture
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  DevBuf<LoopCtl> loop_ctl_;
   // loop events and profiling events
   static constexpr int kRing = 8, kLookahead = 4;
-  static constexpr unsigned kDrainBelow = 1u << 16;  // live paths below which a render call drains
+  // default: live paths below which a render call drains (single-frame 1080p
+  // calls of the large workload: 2^15 fastest of 2^8..2^16)
+  static constexpr unsigned kDrainBelow = 1u << 15;
+  unsigned drain_below_ = kDrainBelow;
   cudaEvent_t ring_[kRing] = {};
   std::vector<cudaEvent_t> ev_pool_;
   std::vector<std::pair<int, int>> ev_marks_;

@@ -110,6 +110,14 @@ struct PathBuf {
 };
 
 // The job table as the kernels see it.
+// Per-iteration record written by k_commit (a ring of kTimeline entries,
+// indexed by iteration number): device clock and paths queued afterwards.
+constexpr int kTimeline = 1024;
+struct TimelineEntry {
+  unsigned long long iteration, t_ns;
+  unsigned int live, pad;
+};
+
 struct Sched {
   const Job* jobs;        // kMaxJobs slots
   JobState* js;           // kMaxJobs slots
@@ -117,6 +125,7 @@ struct Sched {
   const int* nactive;
   HostStatus* status;     // mapped host memory (device pointer)
   unsigned long long* iteration;
+  TimelineEntry* timeline;  // kTimeline entries
 };
 
 // Traversal of the path kernels: per path (the job's DevScene::wide), or one
@@ -137,6 +146,17 @@ void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, cons
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st);
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
+
+// Device-side loop control of a render call run as one graph: after each pair
+// of iterations k_commit keeps the loop going while pairs remain and either a
+// work item has not started or at least drain_below paths are alive.
+struct LoopCtl {
+  unsigned long long pairs_left;
+  unsigned long long drain_below;
+};
+void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, cudaGraphConditionalHandle h, LoopCtl* ctl,
+                        cudaStream_t st);
+void launch_set_loop(LoopCtl* ctl, unsigned long long pairs, unsigned long long drain_below, cudaStream_t st);
 // runs every path queued in q[cur] to its end (call after connect(cur), when no work item is left)
 void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);

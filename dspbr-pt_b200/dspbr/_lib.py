@@ -164,7 +164,10 @@ SIGNATURES = {
     "dspbr_display_image": (C.c_int, [_V, _F, C.c_int, C.c_int, C.POINTER(Display), _F, C.POINTER(C.c_uint8)]),
     "dspbr_host_free": (C.c_int, [_V, _V]),
     "dspbr_get_diagnostics": (C.c_int, [_V, C.POINTER(Diag)]),
+    "dspbr_get_timeline": (C.c_int, [_V, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "dspbr_set_wave_paths": (C.c_int, [_V, C.c_uint32]),
+    "dspbr_set_drain_threshold": (C.c_int, [_V, C.c_uint32]),
     "dspbr_set_counting": (C.c_int, [_V, C.c_int]),
     "dspbr_set_profiling": (C.c_int, [_V, C.c_int]),
     "dspbr_trace_closest": (C.c_int, [_V, _V, _F, C.c_uint32, _I, _F, _F]),

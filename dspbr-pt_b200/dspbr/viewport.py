@@ -451,6 +451,18 @@ class PathtracingViewport:
         out["display"] = dict(self._display)
         return out
 
+    def timeline(self, max_entries: int = 1024) -> np.ndarray:
+        """(n, 3) float64: iteration, device clock (ms), paths queued after it;
+        the last iterations of the path engine, oldest first."""
+        n = max(1, min(int(max_entries), 1024))
+        it, t, live = np.zeros(n, np.uint64), np.zeros(n, np.uint64), np.zeros(n, np.uint32)
+        cnt = C.c_uint32()
+        self.ctx.check(self.ctx.lib.dspbr_get_timeline(
+            self.ctx.h, n, it.ctypes.data_as(C.POINTER(C.c_uint64)), t.ctypes.data_as(C.POINTER(C.c_uint64)),
+            live.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(cnt)))
+        k = cnt.value
+        return np.stack([it[:k].astype(np.float64), t[:k].astype(np.float64) * 1e-6, live[:k].astype(np.float64)], 1)
+
     def _emit_diag(self):
         if self._listeners["diagnosticsChanged"]:
             self._emit("diagnosticsChanged", {"diagnostics": self.diagnostics})

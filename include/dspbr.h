@@ -232,9 +232,19 @@ int dspbr_display_image(dspbr_ctx* ctx, const float* rgba, int width, int height
 int dspbr_host_alloc(dspbr_ctx* ctx, size_t bytes, void** out);
 int dspbr_host_free(dspbr_ctx* ctx, void* ptr);
 int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
+/* The last iterations of the path engine (at most max_entries, at most 1024),
+ * oldest first: iteration number, device clock (ns) at its end and the paths
+ * queued for the next one.  New: the reference renders one full-screen pass
+ * per frame and has no iterations to report (renderer.ts:512-565). */
+int dspbr_get_timeline(dspbr_ctx* ctx, uint32_t max_entries, uint64_t* iteration, uint64_t* t_ns, uint32_t* live,
+                       uint32_t* count);
 /* paths per wave (0 = default 2^21); the wave covers min(frames, paths/pixels)
  * samples of every pixel.  Set by the autotuner. */
 int dspbr_set_wave_paths(dspbr_ctx* ctx, uint32_t paths);
+/* live paths below which a render call, once every sample has started,
+ * finishes the remaining paths in one launch (each path run to its end by
+ * one thread) instead of more wavefront iterations.  0 = the default. */
+int dspbr_set_drain_threshold(dspbr_ctx* ctx, uint32_t paths);
 /* count BVH node visits and triangle tests of every traced ray (diagnostics) */
 int dspbr_set_counting(dspbr_ctx* ctx, int enable);
 /* time every extend / connect / shade launch with CUDA events (diagnostics) */

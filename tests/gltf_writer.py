@@ -252,3 +252,51 @@ def sample_scene() -> GltfBuilder:
 def sample_camera():
     from dspbr import synth
     return synth.Camera.look_at((0.0, 1.6, 4.2), (0.0, 0.4, 0.0), fov=45.0, near=0.05)
+
+
+def large_asset(n_nodes: int = 256, seed: int = 0) -> GltfBuilder:
+    """~1.9M triangles as glTF instancing: n_nodes nodes over four meshes (a
+    9,800-triangle displaced grid and a 5,120-triangle icosphere, twice each,
+    with normals, uvs and tangents), four 1024x1024 textures shared by four
+    materials, random translation / rotation / scale per node."""
+    from dspbr import synth
+    rng = np.random.default_rng(seed)
+    b = GltfBuilder()
+    gp, gn, guv, gi = quad_grid(70, 1.0)
+    gp[:, 2] = 0.08 * np.sin(6 * gp[:, 0]) * np.cos(5 * gp[:, 1])
+    gtan = np.tile(np.array([1, 0, 0, 1], np.float32), (gp.shape[0], 1))
+    sv, sf = synth.icosphere(4)
+    sv = sv.astype(np.float32)
+    suv = (0.5 + 0.5 * sv[:, :2]).astype(np.float32)
+    stan = np.tile(np.array([0, 0, 1, 1], np.float32), (sv.shape[0], 1))
+    tex = []
+    for k in range(4):
+        img = rng.integers(0, 256, (1024, 1024, 4), dtype=np.uint8)
+        img[..., 3] = 255
+        tex.append(b.texture(b.image(png_bytes(img), name=f"t{k}")))
+    mats = []
+    for k in range(4):
+        mats.append(b.material({"pbrMetallicRoughness": {"baseColorTexture": {"index": tex[k]},
+                                                         "metallicRoughnessTexture": {"index": tex[(k + 1) % 4]}},
+                                "normalTexture": {"index": tex[(k + 2) % 4]},
+                                "extensions": {"KHR_materials_clearcoat": {"clearcoatFactor": 0.3 * k}}}))
+    meshes = []
+    for k in range(4):
+        if k % 2 == 0:
+            attrs = {"POSITION": b.accessor(gp), "NORMAL": b.accessor(gn), "TEXCOORD_0": b.accessor(guv),
+                     "TANGENT": b.accessor(gtan)}
+            idx = gi
+        else:
+            attrs = {"POSITION": b.accessor(sv), "NORMAL": b.accessor(sv), "TEXCOORD_0": b.accessor(suv),
+                     "TANGENT": b.accessor(stan)}
+            idx = np.asarray(sf, np.uint32).reshape(-1)
+        meshes.append(b.mesh([{"attributes": attrs, "indices": b.accessor(idx), "material": mats[k]}]))
+    roots = []
+    for i in range(n_nodes):
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        s = float(rng.uniform(2, 8))
+        roots.append(b.node(mesh=meshes[i % 4], translation=rng.uniform(-50, 50, 3).tolist(),
+                            rotation=q.tolist(), scale=[s, s, s]))
+    b.scene(roots)
+    return b

@@ -1,0 +1,54 @@
+"""The engine's render loop on the GPU: a render call runs as one graph (a
+device-side while loop over pairs of iterations, then the tail drain), with
+the same image as the host-driven loop of the profiling mode, and the
+per-iteration timeline it records."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from dspbr import synth
+from dspbr.viewport import Bvh, PathtracingViewport
+from tests import helpers
+
+pytestmark = pytest.mark.gpu
+
+
+def _viewport(settings):
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    v = PathtracingViewport(width=96, height=64, settings=settings)
+    v.setScene(sc)
+    v.setIBL(sc.env)
+    v.setCamera(helpers.camera_of(sc))
+    return v
+
+
+@pytest.mark.parametrize("pool", [0, 997, 20000])
+def test_device_loop_equals_host_loop(pool):
+    imgs = []
+    for profiling in (0, 1):
+        v = _viewport({"maxBounces": 8})
+        if pool:
+            v.ctx.check(v.ctx.lib.dspbr_set_wave_paths(v.ctx.h, pool))
+        v.ctx.check(v.ctx.lib.dspbr_set_profiling(v.ctx.h, profiling))
+        v.start(3)
+        v.start(5)  # a second call continues the accumulation up to 5 samples
+        imgs.append(v.readAccumulation())
+        d = v.diagnostics
+        v.dispose()
+        assert d["sample_count"] == 5 and d["traversal_aborted"] == 0
+    np.testing.assert_allclose(imgs[0], imgs[1], rtol=1e-6, atol=1e-7)
+
+
+def test_timeline_of_a_render_call():
+    v = _viewport({"maxBounces": 8})
+    v.start(1)
+    first = v.timeline(1)
+    v.start(5)
+    tl = v.timeline(1024)
+    v.dispose()
+    tl = tl[tl[:, 0] > first[-1, 0]]
+    assert len(tl) >= 2
+    assert (np.diff(tl[:, 0]) == 1).all() and (np.diff(tl[:, 1]) >= 0).all()
+    assert tl[-1, 2] == 0  # the tail left no path
