@@ -241,76 +241,112 @@ DEV void cswap(float& da, int& ca, float& db, int& cb) {
   }
 }
 
+// Resumable state of one 4-wide traversal: the traversal is a sequence of
+// steps (one node or one leaf each), so a kernel can run rays of different
+// lengths side by side and start a new ray in a lane whose ray has finished.
+struct WideTrav {
+  int cur;        // the entry visited next (kept out of the stack)
+  int top, step;
+  bool have;      // an entry is left to visit
+  bool overflow;  // a push found the stack full
+  bool any_hit;   // kAny: a triangle was accepted
+};
+
+DEV void wide_begin(WideTrav& w, int root) {
+  w.cur = root;
+  w.top = 0;
+  w.step = 0;
+  w.have = true;
+  w.overflow = false;
+  w.any_hit = false;
+}
+
+// One step; returns whether another step is due (entries left, step cap not
+// reached, no accepted triangle for kAny).
+template <bool kAny, bool kExactNaN>
+DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
+                   const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack) {
+  const int e = w.cur;
+  bool next_in_register = false;
+  if (e < 0) {
+    const int2 lf = __ldg(wleaves + ~e);
+    for (int i = lf.x; i < lf.y; ++i) {
+      const float4* tp = tris + 3 * size_t(i);
+      float4 a = __ldg(tp);
+      int id = __float_as_int(a.w);
+      if (id < 0) continue;
+      float t, u, v;
+      if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
+        hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
+        if (kAny) {
+          w.any_hit = true;
+          return false;
+        }
+      }
+    }
+  } else {
+    const float4* nd = wnodes + 8 * size_t(e);
+    const float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+    const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
+    const int n = __ldg(reinterpret_cast<const int*>(nd + 7));
+    float d0 = n > 0 ? slab<kExactNaN>(make_float4(lx.x, ly.x, lz.x, 0.f), make_float4(hx.x, hy.x, hz.x, 0.f), org,
+                                       inv, hit.t)
+                     : kBvhFar;
+    float d1 = n > 1 ? slab<kExactNaN>(make_float4(lx.y, ly.y, lz.y, 0.f), make_float4(hx.y, hy.y, hz.y, 0.f), org,
+                                       inv, hit.t)
+                     : kBvhFar;
+    float d2 = n > 2 ? slab<kExactNaN>(make_float4(lx.z, ly.z, lz.z, 0.f), make_float4(hx.z, hy.z, hz.z, 0.f), org,
+                                       inv, hit.t)
+                     : kBvhFar;
+    float d3 = n > 3 ? slab<kExactNaN>(make_float4(lx.w, ly.w, lz.w, 0.f), make_float4(hx.w, hy.w, hz.w, 0.f), org,
+                                       inv, hit.t)
+                     : kBvhFar;
+    int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+    // ascending order of entry distance (5-comparator network)
+    cswap(d0, c0, d1, c1);
+    cswap(d2, c2, d3, c3);
+    cswap(d0, c0, d2, c2);
+    cswap(d1, c1, d3, c3);
+    cswap(d1, c1, d2, c2);
+    auto push = [&](float d, int c) {
+      if (d < kBvhFar) {
+        if (w.top < kWideStack) stack[w.top++] = c;
+        else w.overflow = true;
+      }
+    };
+    push(d3, c3);
+    push(d2, c2);
+    push(d1, c1);
+    if (d0 < kBvhFar) {  // nearest child next, without a trip through the stack
+      w.cur = c0;
+      next_in_register = true;
+    }
+  }
+  if (!next_in_register) {
+    if (w.top > 0) w.cur = stack[--w.top];
+    else w.have = false;
+  }
+  ++w.step;
+  return w.have && w.step < kMaxSteps;
+}
+
+// `aborted`: the stack overflowed or the step cap ended the traversal with
+// entries left (not when kAny accepted a triangle).
+DEV bool wide_aborted(const WideTrav& w) { return !w.any_hit && (w.overflow || (w.have && w.step >= kMaxSteps)); }
+
 template <bool kAny, bool kExactNaN>
 DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfar, Hit& hit, bool& aborted) {
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
   int stack[kWideStack];
-  int top = 0;
-  int cur = s.wroot;  // the next entry to visit is kept in a register
-  bool have = true;
-  int step = 0;
-  bool overflow = false;
-  for (; step < kMaxSteps && have; ++step) {
-    const int e = cur;
-    if (e < 0) {
-      const int2 lf = __ldg(s.wleaves + ~e);
-      for (int i = lf.x; i < lf.y; ++i) {
-        const float4* tp = s.tris + 3 * size_t(i);
-        float4 a = __ldg(tp);
-        int id = __float_as_int(a.w);
-        if (id < 0) continue;
-        float t, u, v;
-        if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
-          hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
-          if (kAny) { aborted = false; return true; }
-        }
-      }
-    } else {
-      const float4* nd = s.wnodes + 8 * size_t(e);
-      const float4 lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
-      const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
-      const int4 ch = __ldg(reinterpret_cast<const int4*>(nd + 6));
-      const int n = __ldg(reinterpret_cast<const int*>(nd + 7));
-      float d0 = n > 0 ? slab<kExactNaN>(make_float4(lx.x, ly.x, lz.x, 0.f), make_float4(hx.x, hy.x, hz.x, 0.f), org,
-                                         inv, hit.t)
-                       : kBvhFar;
-      float d1 = n > 1 ? slab<kExactNaN>(make_float4(lx.y, ly.y, lz.y, 0.f), make_float4(hx.y, hy.y, hz.y, 0.f), org,
-                                         inv, hit.t)
-                       : kBvhFar;
-      float d2 = n > 2 ? slab<kExactNaN>(make_float4(lx.z, ly.z, lz.z, 0.f), make_float4(hx.z, hy.z, hz.z, 0.f), org,
-                                         inv, hit.t)
-                       : kBvhFar;
-      float d3 = n > 3 ? slab<kExactNaN>(make_float4(lx.w, ly.w, lz.w, 0.f), make_float4(hx.w, hy.w, hz.w, 0.f), org,
-                                         inv, hit.t)
-                       : kBvhFar;
-      int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
-      // ascending order of entry distance (5-comparator network)
-      cswap(d0, c0, d1, c1);
-      cswap(d2, c2, d3, c3);
-      cswap(d0, c0, d2, c2);
-      cswap(d1, c1, d3, c3);
-      cswap(d1, c1, d2, c2);
-      auto push = [&](float d, int c) {
-        if (d < kBvhFar) {
-          if (top < kWideStack) stack[top++] = c;
-          else overflow = true;
-        }
-      };
-      push(d3, c3);
-      push(d2, c2);
-      push(d1, c1);
-      if (d0 < kBvhFar) {  // nearest child next, without a trip through the stack
-        cur = c0;
-        continue;
-      }
-    }
-    if (top > 0) cur = stack[--top];
-    else have = false;
+  WideTrav w;
+  wide_begin(w, s.wroot);
+  while (wide_step<kAny, kExactNaN>(s.wnodes, s.wleaves, s.tris, org, inv, dir, hit, w, stack)) {
   }
-  aborted = overflow || (have && step >= kMaxSteps);
-  return hit.tri >= 0;
+  aborted = wide_aborted(w);
+  return kAny ? (w.any_hit || hit.tri >= 0) : hit.tri >= 0;
 }
 
 template <bool kAny>

@@ -247,6 +247,8 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
     b.counts[cur] = 0;                 // q[cur]: consumed by this iteration's extend
     b.counts[kCntShadow0 + cur] = 0;   // qs[cur]: consumed by this iteration's connect
     b.counts[kCntMiss] = 0;
+    b.counts[kCntFetchExt] = 0;
+    b.counts[kCntFetchShadow] = 0;
   }
   if (t < kNumClasses) b.counts[kCntHit0 + t] = 0;
   // status for the host (mapped memory)
@@ -340,6 +342,52 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
   }
 }
 
+// Persistent warps (one grid of resident blocks) that take 32 consecutive
+// queue entries at a time from a cursor (one atomic per warp), instead of a
+// fixed share of the queue each: a warp that drew short rays takes more.
+// Starting rays one lane at a time as lanes finish balanced the lanes better
+// but was slower (each start pays the latency of a ray's first loads) and
+// lost the queue order the shading kernels' memory accesses benefit from.
+DEV bool next_warp_batch(uint32_t* cursor, uint32_t count, uint32_t& i) {
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(cursor, 32u);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  i = base + uint32_t(lane);
+  return base < count;
+}
+
+// closest hits of q[cur], 4-wide traversal
+__global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int cur) {
+  const uint32_t count = b.counts[cur];
+  const uint32_t* q = b.q[cur];
+  uint32_t rays = 0, aborted_n = 0;
+  uint32_t i;
+  while (next_warp_batch(b.counts + kCntFetchExt, count, i)) {
+    bool is_hit = false, is_miss = false;
+    uint32_t slot = 0;
+    int cls = 0;
+    if (i < count) {
+      slot = q[i];
+      const DevScene s = sc.jobs[b.job[slot]].s;
+      float4 o = b.org[slot], d = b.dir[slot];
+      Hit h;
+      bool aborted = false;
+      traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
+      b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+      is_hit = h.tri >= 0;
+      is_miss = !is_hit;
+      if (is_hit) cls = __ldg(s.tri_class + h.tri);
+      ++rays;
+      aborted_n += aborted ? 1u : 0u;
+    }
+    enqueue_keyed(b.qh, b.counts + kCntHit0, b.capacity, is_hit, cls, slot);
+    enqueue(b.qm, b.counts + kCntMiss, is_miss, slot);
+  }
+  add_warp(b.stats + 0, rays);
+  add_warp(b.stats + 2, aborted_n);
+}
+
 // ---- connect: NEE shadow rays (bvh.glsl:218-229) ---------------------------------------------
 // The NEE shadow rays of one path vertex (IBL and point light): visible
 // contributions are added to the path radiance.
@@ -391,6 +439,25 @@ __global__ void __launch_bounds__(256, 4) k_connect(Sched sc, PathBuf b, int cur
       add_warp(b.stats + 6, tris);
     }
   }
+}
+
+// the shadow rays of qs[cur] by persistent warps (see next_warp_batch), 4-wide traversal
+__global__ void __launch_bounds__(128, 8) k_connect_dyn(Sched sc, PathBuf b, int cur) {
+  const uint32_t count = b.counts[kCntShadow0 + cur];
+  const uint32_t* qs = b.qs[cur];
+  uint32_t rays = 0, aborted_n = 0;
+  uint32_t i;
+  while (next_warp_batch(b.counts + kCntFetchShadow, count, i)) {
+    if (i < count) {
+      bool aborted = false;
+      int nrays = 0;
+      connect_slot<false, kTravWide>(sc, b, qs[i], aborted, nrays, nullptr, nullptr);
+      rays += uint32_t(nrays);
+      aborted_n += aborted ? 1u : 0u;
+    }
+  }
+  add_warp(b.stats + 1, rays);
+  add_warp(b.stats + 2, aborted_n);
 }
 
 // ---- shade ------------------------------------------------------------------------------------
@@ -761,14 +828,14 @@ void launch_set_loop(LoopCtl* ctl, unsigned long long pairs, unsigned long long 
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
   if (count) k_extend<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
-  else if (lc.traversal == kTravWide) k_extend<false, kTravWide><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_extend_dyn<<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
   else if (lc.traversal == kTravReference) k_extend<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
   else k_extend<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
   if (count) k_connect<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
-  else if (lc.traversal == kTravWide) k_connect<false, kTravWide><<<g, t, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_connect_dyn<<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
   else if (lc.traversal == kTravReference) k_connect<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
   else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }

@@ -70,6 +70,8 @@ enum : int {
   kCntShadow0 = 2,  // NEE shadow queues (ping-pong)
   kCntShadow1 = 3,
   kCntMiss = 4,     // paths whose extension ray left the scene
+  kCntFetchExt = 5,     // next q[cur] entry a k_extend warp starts (dynamic fetch)
+  kCntFetchShadow = 6,  // next qs[cur] entry a k_connect warp starts
   kCntHit0 = 8,     // paths whose extension ray hit a triangle, one queue per shading class
   kCntNum = 32
 };
@@ -137,6 +139,7 @@ struct LaunchCfg {
   int shade_blocks = 148 * 8, shade_threads = 128;
   int traversal = kTravPerPath;
   bool textured = false;  // some active job samples material textures
+  int dyn_blocks = 148 * 8;  // k_extend_dyn: blocks of 128 threads (resident ones at 64 registers)
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
