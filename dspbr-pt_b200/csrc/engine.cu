@@ -65,6 +65,7 @@ int Engine::init() {
   TRY_CUDA(s, stats_.alloc(8), "stats");
   TRY_CUDA(s, timeline_.alloc(kTimeline), "timeline");
   TRY_CUDA(s, cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking), "stream");
+  init_launch_sizes(lc_);
   TRY_CUDA(s, cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
   TRY_CUDA(s, cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "event");
   TRY_CUDA(s, cudaMemsetAsync(timeline_.p, 0, timeline_.bytes(), stream_), "timeline");

@@ -151,7 +151,9 @@ __global__ void k_init_pool(PathBuf b) {
 
 // ---- regen: new samples in free slots (renderer.frag:146-150) ----------------------------
 // Free slot i (in free-list order) takes the i-th unstarted work item of the
-// active jobs in priority order.
+// active jobs in priority order and entry base + i of q[next], where base is
+// the queue's length after this iteration's shade (no atomic: k_commit adds
+// the number of new paths to the queue counter).
 __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int next) {
   __shared__ unsigned long long scan[kMaxJobs];
   __shared__ unsigned long long pre[kMaxJobs];
@@ -166,13 +168,11 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
   const unsigned long long nfree = *b.free_tail - head;
   const uint32_t avail = uint32_t(min(nfree, total));
   const uint32_t head_pos = uint32_t(head % b.capacity);
-  uint32_t* q = b.q[next];
-  uint32_t* cnt = b.counts + next;
+  uint32_t* q = b.q[next] + b.counts[next];
   for (uint32_t base = blockIdx.x * blockDim.x; base < avail; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
-    bool valid = i < avail;
-    uint32_t slot = 0;
-    if (valid) {
+    if (i < avail) {
+      uint32_t slot = 0;
       int lo = 0, hi = n - 1;  // last active job whose range starts at or before i
       while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
       b.frame[slot] = frame;
       b.bounce[slot] = 0;
       b.job[slot] = uint32_t(jj);
+      q[i] = slot;
     }
-    enqueue(q, cnt, valid, slot);
   }
 }
 
@@ -244,11 +244,14 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
   const int t = threadIdx.x;
   if (t == 0) {
     *b.free_head = head + avail;
+    b.counts[cur ^ 1] += uint32_t(avail);  // q[next]: the paths the regen that just ran appended
     b.counts[cur] = 0;                 // q[cur]: consumed by this iteration's extend
     b.counts[kCntShadow0 + cur] = 0;   // qs[cur]: consumed by this iteration's connect
     b.counts[kCntMiss] = 0;
     b.counts[kCntFetchExt] = 0;
     b.counts[kCntFetchShadow] = 0;
+    b.counts[kCntFetchShade] = 0;
+    b.counts[kCntFetchMiss] = 0;
   }
   if (t < kNumClasses) b.counts[kCntHit0 + t] = 0;
   // status for the host (mapped memory)
@@ -342,19 +345,28 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
   }
 }
 
-// Persistent warps (one grid of resident blocks) that take 32 consecutive
-// queue entries at a time from a cursor (one atomic per warp), instead of a
-// fixed share of the queue each: a warp that drew short rays takes more.
-// Starting rays one lane at a time as lanes finish balanced the lanes better
-// but was slower (each start pays the latency of a ray's first loads) and
-// lost the queue order the shading kernels' memory accesses benefit from.
-DEV bool next_warp_batch(uint32_t* cursor, uint32_t count, uint32_t& i) {
+// Persistent warps (one grid of resident blocks) that take batches of 32
+// consecutive queue entries: the first batch of a warp is its own index, the
+// later ones come from a cursor (one atomic per batch), so a warp that drew
+// short work takes more and a short queue costs no atomic at all.  Starting
+// rays one lane at a time as lanes finish balanced the lanes better but was
+// slower (each start pays the latency of a ray's first loads) and lost the
+// queue order the shading kernels' memory accesses benefit from.
+DEV bool next_warp_batch(uint32_t* cursor, uint32_t count, uint32_t& i, bool& first) {
   const int lane = threadIdx.x & 31;
-  uint32_t base = 0;
-  if (lane == 0) base = atomicAdd(cursor, 32u);
-  base = __shfl_sync(0xffffffffu, base, 0);
-  i = base + uint32_t(lane);
-  return base < count;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t batch;
+  if (first) {
+    batch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    first = false;
+  } else {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(cursor, 1u);
+    batch = warps + __shfl_sync(0xffffffffu, c, 0);
+  }
+  if (batch >= (count + 31u) / 32u) return false;
+  i = batch * 32u + uint32_t(lane);
+  return true;
 }
 
 // closest hits of q[cur], 4-wide traversal
@@ -363,7 +375,8 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
   const uint32_t* q = b.q[cur];
   uint32_t rays = 0, aborted_n = 0;
   uint32_t i;
-  while (next_warp_batch(b.counts + kCntFetchExt, count, i)) {
+  bool first = true;
+  while (next_warp_batch(b.counts + kCntFetchExt, count, i, first)) {
     bool is_hit = false, is_miss = false;
     uint32_t slot = 0;
     int cls = 0;
@@ -447,7 +460,8 @@ __global__ void __launch_bounds__(128, 8) k_connect_dyn(Sched sc, PathBuf b, int
   const uint32_t* qs = b.qs[cur];
   uint32_t rays = 0, aborted_n = 0;
   uint32_t i;
-  while (next_warp_batch(b.counts + kCntFetchShadow, count, i)) {
+  bool first = true;
+  while (next_warp_batch(b.counts + kCntFetchShadow, count, i, first)) {
     if (i < count) {
       bool aborted = false;
       int nrays = 0;
@@ -502,8 +516,9 @@ DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
 
 __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
   const uint32_t count = b.counts[kCntMiss];
-  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
-    uint32_t i = base + threadIdx.x;
+  uint32_t i;
+  bool first = true;
+  while (next_warp_batch(b.counts + kCntFetchMiss, count, i, first)) {
     uint32_t slot = 0;
     uint32_t job = 0;
     if (i < count) {
@@ -634,8 +649,9 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
   const uint32_t count = start[kNumClasses];
   uint32_t* qn = b.q[next];
   uint32_t* cn = b.counts + next;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
-    uint32_t i = base + threadIdx.x;
+  uint32_t i;
+  bool first = true;
+  while (next_warp_batch(b.counts + kCntFetchShade, count, i, first)) {
     bool cont = false, shadow = false;
     uint32_t slot = 0, job = 0;
     if (i < count) {
@@ -809,6 +825,23 @@ static int grid_for(uint64_t n, int threads, int cap) {
   return int(b < uint64_t(cap) ? b : uint64_t(cap));
 }
 
+void init_launch_sizes(LaunchCfg& lc) {
+  int dev = 0, sms = 148, n = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto resident = [&](const void* fn, int threads, int fallback) {
+    n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess || n <= 0) {
+      cudaGetLastError();
+      n = fallback;
+    }
+    return n * sms;
+  };
+  lc.dyn_blocks = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
+  lc.shade_dyn_blocks[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 3);
+  lc.shade_dyn_blocks[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 2);
+  lc.miss_dyn_blocks = resident(reinterpret_cast<const void*>(k_shade_miss), 256, 6);
+}
+
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
   k_init_pool<<<grid_for(b.capacity, 256, 148 * 8), 256, 0, st>>>(b);
 }
@@ -840,15 +873,15 @@ void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, cons
   else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st) {
-  if (lc.textured) k_shade<true><<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
-  else k_shade<false><<<lc.shade_blocks, lc.shade_threads, 0, st>>>(sc, b, next);
+  if (lc.textured) k_shade<true><<<lc.shade_dyn_blocks[1], 128, 0, st>>>(sc, b, next);
+  else k_shade<false><<<lc.shade_dyn_blocks[0], 128, 0, st>>>(sc, b, next);
 }
 void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st) {
   if (lc.textured) k_drain<true><<<148 * 4, 128, 0, st>>>(sc, b, cur);
   else k_drain<false><<<148 * 4, 128, 0, st>>>(sc, b, cur);
 }
 void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
-  k_shade_miss<<<lc.shade_blocks, 256, 0, st>>>(sc, b);
+  k_shade_miss<<<lc.miss_dyn_blocks, 256, 0, st>>>(sc, b);
 }
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st) {
   k_mean<<<grid_for(npix, 256, 148 * 8), 256, 0, st>>>(accum, inv_count, out, npix);

@@ -73,6 +73,8 @@ enum : int {
   kCntFetchExt = 5,     // next q[cur] entry a k_extend warp starts (dynamic fetch)
   kCntFetchShadow = 6,  // next qs[cur] entry a k_connect warp starts
   kCntHit0 = 8,     // paths whose extension ray hit a triangle, one queue per shading class
+  kCntFetchShade = 24,  // next hit-queue entry a k_shade warp starts
+  kCntFetchMiss = 25,   // next miss-queue entry a k_shade_miss warp starts
   kCntNum = 32
 };
 constexpr int kNumClasses = 16;
@@ -139,10 +141,15 @@ struct LaunchCfg {
   int shade_blocks = 148 * 8, shade_threads = 128;
   int traversal = kTravPerPath;
   bool textured = false;  // some active job samples material textures
-  int dyn_blocks = 148 * 8;  // k_extend_dyn: blocks of 128 threads (resident ones at 64 registers)
+  int dyn_blocks = 148 * 8;  // k_extend / k_connect: resident blocks of 128 threads (64 registers)
+  // resident blocks of the persistent shading kernels (set by init_launch_sizes)
+  int shade_dyn_blocks[2] = {148 * 3, 148 * 2};  // k_shade<false>, k_shade<true>, 128 threads
+  int miss_dyn_blocks = 148 * 6;                 // k_shade_miss, 256 threads
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
+// resident-block counts of the persistent kernels on this device (occupancy API)
+void init_launch_sizes(LaunchCfg& lc);
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
