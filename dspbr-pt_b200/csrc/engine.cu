@@ -85,8 +85,7 @@ int Engine::init() {
 }
 
 size_t Engine::pool_bytes() const {
-  return org_.bytes() * 9 + rng_.bytes() + sh_flags_.bytes() + bounce_.bytes() + pixel_.bytes() + frame_.bytes() +
-         job_.bytes() + q0_.bytes() * 6 + qh_.bytes();
+  return st_.bytes() + hits_.bytes() + sh_.bytes() + q0_.bytes() * 6 + qh_.bytes();
 }
 
 int Engine::ensure_pool(uint32_t cap) {
@@ -98,14 +97,8 @@ int Engine::ensure_pool(uint32_t cap) {
   TRY_CUDA(s, cudaStreamSynchronize(stream_), "sync");
   drop_graph();
   capacity_ = 0;
-  if ((rc = s.cuda(org_.alloc(cap), "paths")) || (rc = s.cuda(dir_.alloc(cap), "paths")) ||
-      (rc = s.cuda(weight_.alloc(cap), "paths")) || (rc = s.cuda(rad_.alloc(cap), "paths")) ||
-      (rc = s.cuda(hit_.alloc(cap), "paths")) || (rc = s.cuda(sh_dir_.alloc(cap), "paths")) ||
-      (rc = s.cuda(sh_c_.alloc(cap), "paths")) || (rc = s.cuda(pl_dir_.alloc(cap), "paths")) ||
-      (rc = s.cuda(pl_c_.alloc(cap), "paths")) || (rc = s.cuda(rng_.alloc(cap), "paths")) ||
-      (rc = s.cuda(sh_flags_.alloc(cap), "paths")) || (rc = s.cuda(bounce_.alloc(cap), "paths")) ||
-      (rc = s.cuda(pixel_.alloc(cap), "paths")) || (rc = s.cuda(frame_.alloc(cap), "paths")) ||
-      (rc = s.cuda(job_.alloc(cap), "paths")) || (rc = s.cuda(q0_.alloc(cap), "queues")) ||
+  if ((rc = s.cuda(st_.alloc(cap), "paths")) || (rc = s.cuda(hits_.alloc(cap), "paths")) ||
+      (rc = s.cuda(sh_.alloc(cap), "paths")) || (rc = s.cuda(q0_.alloc(cap), "queues")) ||
       (rc = s.cuda(q1_.alloc(cap), "queues")) || (rc = s.cuda(qs0_.alloc(cap), "queues")) ||
       (rc = s.cuda(qs1_.alloc(cap), "queues")) || (rc = s.cuda(qh_.alloc(size_t(cap) * kNumClasses), "queues")) ||
       (rc = s.cuda(qm_.alloc(cap), "queues")) || (rc = s.cuda(qfree_.alloc(cap), "queues")))
@@ -152,9 +145,7 @@ Sched Engine::sched() const {
 
 PathBuf Engine::paths() const {
   PathBuf b{};
-  b.org = org_.p; b.dir = dir_.p; b.weight = weight_.p; b.rad = rad_.p; b.rng = rng_.p; b.hit = hit_.p;
-  b.sh_dir = sh_dir_.p; b.sh_c = sh_c_.p; b.pl_dir = pl_dir_.p; b.pl_c = pl_c_.p; b.sh_flags = sh_flags_.p;
-  b.pixel = pixel_.p; b.frame = frame_.p; b.bounce = bounce_.p; b.job = job_.p;
+  b.st = st_.p; b.hits = hits_.p; b.sh = sh_.p;
   b.q[0] = q0_.p; b.q[1] = q1_.p; b.qs[0] = qs0_.p; b.qs[1] = qs1_.p; b.qh = qh_.p; b.qm = qm_.p;
   b.qfree = qfree_.p; b.free_head = cursors_.p; b.free_tail = cursors_.p + 1;
   b.counts = counts_.p; b.stats = stats_.p;

@@ -96,10 +96,10 @@ class Engine {
   bool slot_textured_[kMaxJobs] = {};  // the job's scene samples material textures
   LaunchCfg lc_;
   // pool
-  DevBuf<float4> org_, dir_, weight_, rad_, hit_, sh_dir_, sh_c_, pl_dir_, pl_c_;
-  DevBuf<uint64_t> rng_;
-  DevBuf<int> sh_flags_, bounce_;
-  DevBuf<uint32_t> pixel_, frame_, job_, q0_, q1_, qs0_, qs1_, qh_, qm_, qfree_;
+  DevBuf<PathState> st_;
+  DevBuf<PathHit> hits_;
+  DevBuf<PathShadow> sh_;
+  DevBuf<uint32_t> q0_, q1_, qs0_, qs1_, qh_, qm_, qfree_;
   // job table and counters
   DevBuf<Job> jobs_;
   DevBuf<JobState> js_;

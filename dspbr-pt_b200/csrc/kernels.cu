@@ -65,17 +65,10 @@ DEV void add_warp(unsigned long long* ctr, uint32_t v) {
 
 DEV float4 f4(v3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
 
-DEV Rng load_rng(const WaveParams& p, const PathBuf& b, uint32_t slot) {
-  Rng r;
-  r.state = b.rng[slot];
-  r.inc = p.rng_pcg ? pcg_inc(uint64_t(b.frame[slot]) * uint64_t(p.npix) + b.pixel[slot]) : 0;
-  return r;
-}
-
 // A terminated path adds its sample to its job's pixel sums; the caller
 // frees the slot (free_slots).
-DEV void finish_path(const Job& J, const PathBuf& b, uint32_t slot, float4 c) {
-  double* a = J.accum + 4 * size_t(b.pixel[slot]);
+DEV void finish_path(const Job& J, uint32_t pixel, float4 c) {
+  double* a = J.accum + 4 * size_t(pixel);
   atomicAdd(a + 0, double(c.x));
   atomicAdd(a + 1, double(c.y));
   atomicAdd(a + 2, double(c.z));
@@ -208,15 +201,16 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
       float r1 = r.next();
       v3 org, dir;
       camera_ray(p.cam, px, py, r0, r1, org, dir);
-      b.org[slot] = f4(org, 0.f);
-      b.dir[slot] = f4(dir, 0.f);
-      b.weight[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-      b.rad[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-      b.rng[slot] = r.state;
-      b.pixel[slot] = pixel;
-      b.frame[slot] = frame;
-      b.bounce[slot] = 0;
-      b.job[slot] = uint32_t(jj);
+      PathState ps;
+      ps.org = f4(org, __int_as_float(0));
+      ps.dir = f4(dir, __uint_as_float(uint32_t(jj)));
+      ps.weight = make_float4(1.f, 1.f, 1.f, 0.f);
+      ps.rad = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+      ps.rng = r.state;
+      ps.pixel = pixel;
+      ps.frame = frame;
+      ps.pad[0] = ps.pad[1] = ps.pad[2] = ps.pad[3] = 0u;
+      b.st[slot] = ps;
       q[i] = slot;
     }
   }
@@ -323,11 +317,11 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
     int cls = 0;
     if (i < count) {
       slot = q[i];
-      const DevScene s = sc.jobs[b.job[slot]].s;
-      float4 o = b.org[slot], d = b.dir[slot];
+      const float4 o = b.st[slot].org, d = b.st[slot].dir;
+      const DevScene s = sc.jobs[__float_as_uint(d.w)].s;
       Hit h;
       trace_path_ray<false, kCount, kTrav>(s, mk(o), mk(d), kTfarMax, h, aborted, &nodes, &tris);
-      b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
       if (is_hit) cls = __ldg(s.tri_class + h.tri);
@@ -382,12 +376,12 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
     int cls = 0;
     if (i < count) {
       slot = q[i];
-      const DevScene s = sc.jobs[b.job[slot]].s;
-      float4 o = b.org[slot], d = b.dir[slot];
+      const float4 o = b.st[slot].org, d = b.st[slot].dir;
+      const DevScene s = sc.jobs[__float_as_uint(d.w)].s;
       Hit h;
       bool aborted = false;
       traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
-      b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
       if (is_hit) cls = __ldg(s.tri_class + h.tri);
@@ -407,31 +401,34 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
 template <bool kCount, int kTrav>
 DEV void connect_slot(const Sched& sc, const PathBuf& b, uint32_t slot, bool& aborted, int& nrays, uint32_t* nodes,
                       uint32_t* tris) {
-  const DevScene s = sc.jobs[b.job[slot]].s;
-  int flags = b.sh_flags[slot];
-  v3 org = mk(b.org[slot]);
+  const float4 o4 = b.st[slot].org, d4 = b.st[slot].dir;
+  const DevScene s = sc.jobs[__float_as_uint(d4.w)].s;
+  const float4 w4 = b.st[slot].weight, L = b.st[slot].rad;
+  const int flags = __float_as_int(L.w);
+  v3 org = mk(o4);
   v3 add = mk(0.f);
   if (flags & 1) {
-    float4 d = b.sh_dir[slot];
+    float4 d = b.sh[slot].sh_dir;
     Hit h;
     bool ab = false;
     // isOccluded normalises the light direction (bvh.glsl:225-229)
     if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, nodes, tris))
-      add = mk(b.sh_c[slot]);
+      add = mk(b.sh[slot].sh_c);
     aborted |= ab;
     ++nrays;
   }
   if (flags & 2) {
-    float4 d = b.pl_dir[slot];
+    float4 d = b.sh[slot].pl_dir;
     Hit h;
     bool ab = false;
     if (!trace_path_ray<true, kCount, kTrav>(s, org, normalize_rn(mk(d)), d.w, h, ab, nodes, tris))
-      add = add + mk(b.pl_c[slot]);
+      add = add + mk(b.sh[slot].pl_c);
     aborted |= ab;
     ++nrays;
   }
-  float4 L = b.rad[slot];
-  b.rad[slot] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+  // the whole sector (weight, radiance) written back
+  b.st[slot].weight = w4;
+  b.st[slot].rad = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
 }
 
 template <bool kCount, int kTrav>
@@ -487,20 +484,19 @@ DEV float4 clamp_result(const WaveParams& p, v3 L) {
 // A path whose ray left the scene: background for camera rays
 // (misptdl.glsl:41-46), MIS-weighted environment otherwise (misptdl.glsl:84-88).
 DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
-  const uint32_t j = b.job[slot];
-  const Job& J = sc.jobs[j];
+  const PathState ps = b.st[slot];
+  const Job& J = sc.jobs[path_job(ps)];
   const WaveParams p = J.p;  // local copy: the outlined material calls would force reloads
-  float4 d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
-  v3 dir = mk(d4);
-  v3 w = mk(w4);
-  float last_pdf = w4.w;
-  v3 L = mk(l4);
-  if (b.bounce[slot] == 0) {
+  v3 dir = mk(ps.dir);
+  v3 w = mk(ps.weight);
+  float last_pdf = ps.weight.w;
+  v3 L = mk(ps.rad);
+  if (path_bounce(ps) == 0) {
     if (p.bg_from_ibl > 0) {
       v3 env = p.has_ibl ? ibl_eval(J.e, p.ibl_rot, dir) : mk(0.f);
-      finish_path(J, b, slot, f4(env * w, 1.f));
+      finish_path(J, ps.pixel, f4(env * w, 1.f));
     } else {
-      finish_path(J, b, slot,
+      finish_path(J, ps.pixel,
                   make_float4(powf(p.bg_color.x, 2.2f), powf(p.bg_color.y, 2.2f), powf(p.bg_color.z, 2.2f),
                               p.bg_color.w));
     }
@@ -511,7 +507,7 @@ DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
     float mis = mis_balance(last_pdf, ipdf);
     L = L + ibl_eval(J.e, p.ibl_rot, dir) * w * mis * float(p.use_ibl);
   }
-  finish_path(J, b, slot, clamp_result(p, L));
+  finish_path(J, ps.pixel, clamp_result(p, L));
 }
 
 __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
@@ -523,7 +519,7 @@ __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
     uint32_t job = 0;
     if (i < count) {
       slot = b.qm[i];
-      job = b.job[slot];
+      job = __float_as_uint(b.st[slot].dir.w);
       shade_miss_path(sc, b, slot);
     }
     free_slots(sc, b, i < count, slot, job);
@@ -536,25 +532,30 @@ __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
 template <bool kTextured>
 DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shadow) {
   shadow = false;
-  const uint32_t j = b.job[slot];
-  const Job& J = sc.jobs[j];
+  PathState& ps = b.st[slot];
+  const float4 o4 = ps.org, d4 = ps.dir, w4 = ps.weight, l4 = ps.rad;
+  const Job& J = sc.jobs[__float_as_uint(d4.w)];
   const WaveParams p = J.p;  // local copy: the outlined material calls would force reloads
-  float4 hit = b.hit[slot];
+  float4 hit = b.hits[slot].h;
   int tri = __float_as_int(hit.w);
-  float4 o4 = b.org[slot], d4 = b.dir[slot], w4 = b.weight[slot], l4 = b.rad[slot];
   v3 dir = mk(d4);
   v3 w = mk(w4);
   v3 L = mk(l4);
-  int bounce = b.bounce[slot];
+  const int bounce = __float_as_int(o4.w);
   if (!(bounce < p.max_bounces)) {  // loop condition (misptdl.glsl:54)
-    finish_path(J, b, slot, clamp_result(p, L));
+    finish_path(J, ps.pixel, clamp_result(p, L));
     return false;
   }
-  Rng rng = load_rng(p, b, slot);
+  Rng rng;
+  {
+    const uint4 aux = *reinterpret_cast<const uint4*>(&ps.rng);  // rng (2 words), pixel, frame
+    rng.state = uint64_t(aux.x) | (uint64_t(aux.y) << 32);
+    rng.inc = p.rng_pcg ? pcg_inc(uint64_t(aux.w) * uint64_t(p.npix) + aux.z) : 0;
+  }
   // Russian roulette (renderer.frag:119-123): weight boost every bounce
   w = w * p.rr_factor;
   if (bounce > p.rr_start && rng.next() <= p.rr_prob) {
-    finish_path(J, b, slot, clamp_result(p, L));
+    finish_path(J, ps.pixel, clamp_result(p, L));
     return false;
   }
   v3 org = mk(o4);
@@ -581,7 +582,7 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
     pdf = bs.pdf;
     bw = bs.weight;
     if (pdf < kEpsPdf) {  // absorbed: returns L without the clamp
-      finish_path(J, b, slot, f4(L, 1.f));
+      finish_path(J, ps.pixel, f4(L, 1.f));
       return false;
     }
   }
@@ -600,8 +601,8 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
       float bpdf = bsdf_pdf(S.c, S.n, wi, ld);
       v3 c = ibl_eval(J.e, p.ibl_rot, ld) * f * cosnl / ipdf;
       if (bpdf > kEpsPdf) c = c * mis_balance(ipdf, bpdf);
-      b.sh_dir[slot] = f4(ld, kTfarMax);
-      b.sh_c[slot] = f4(c * w, 0.f);
+      b.sh[slot].sh_dir = f4(ld, kTfarMax);  // one whole sector
+      b.sh[slot].sh_c = f4(c * w, 0.f);
       flags |= 1;
     }
   }
@@ -614,21 +615,23 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
     if (cosnl > kEpsCos) {
       v3 f = bsdf_eval(S.c, S.n, wi, ldn) / fmaxf(fabsf(dot(S.n, ldn)), kEps);
       v3 c = f * (mk(p.pl_emis.x, p.pl_emis.y, p.pl_emis.z) / dist2) * cosnl;
-      b.pl_dir[slot] = f4(ldn, sqrtf(dist2));
-      b.pl_c[slot] = f4(c * w, 0.f);
+      b.sh[slot].pl_dir = f4(ldn, sqrtf(dist2));  // one whole sector
+      b.sh[slot].pl_c = f4(c * w, 0.f);
       flags |= 2;
     }
   }
-  b.sh_flags[slot] = flags;
   shadow = flags != 0;
 
   w = w * bw;
-  b.org[slot] = f4(pos, 0.f);
-  b.dir[slot] = f4(wo, 0.f);
-  b.weight[slot] = f4(w, pdf);
-  b.rad[slot] = f4(L, 0.f);
-  b.rng[slot] = rng.state;
-  b.bounce[slot] = bounce + 1;
+  // the whole record: three sectors (job, pixel and frame read back, not kept live)
+  const float job_bits = ps.dir.w;
+  const uint2 pf = *reinterpret_cast<const uint2*>(&ps.pixel);
+  ps.org = f4(pos, __int_as_float(bounce + 1));
+  ps.dir = f4(wo, job_bits);
+  ps.weight = f4(w, pdf);
+  ps.rad = f4(L, __int_as_float(flags));
+  *reinterpret_cast<uint4*>(&ps.rng) = make_uint4(uint32_t(rng.state), uint32_t(rng.state >> 32), pf.x, pf.y);
+  *reinterpret_cast<uint4*>(ps.pad) = make_uint4(0u, 0u, 0u, 0u);
   return true;
 }
 
@@ -659,7 +662,7 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
 #pragma unroll
       for (int jk = 1; jk < kNumClasses; ++jk) k += i >= start[jk] ? 1 : 0;
       slot = b.qh[size_t(k) * b.capacity + (i - start[k])];
-      job = b.job[slot];
+      job = __float_as_uint(b.st[slot].dir.w);
       cont = shade_path<kTextured>(sc, b, slot, shadow);
     }
     enqueue(qn, cn, cont, slot);
@@ -686,16 +689,16 @@ __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
     bool aborted = false;
     if (i < count) {
       slot = q[i];
-      job = b.job[slot];
+      job = __float_as_uint(b.st[slot].dir.w);
       for (int guard = 0; guard < 4 * kMaxSteps; ++guard) {
         const DevScene s = sc.jobs[job].s;
-        float4 o = b.org[slot], d = b.dir[slot];
+        float4 o = b.st[slot].org, d = b.st[slot].dir;
         Hit h;
         bool ab = false;
         trace_path_ray<false, false, kTravPerPath>(s, mk(o), mk(d), kTfarMax, h, ab, nullptr, nullptr);
         aborted |= ab;
         ++closest;
-        b.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+        b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
         if (h.tri < 0) {
           shade_miss_path(sc, b, slot);
           break;

@@ -83,22 +83,43 @@ static_assert(kCntHit0 + kNumClasses <= kCntNum, "counter block too small");
 // Structure-of-arrays state of a pool of path slots.  Jobs stream their work
 // items through the pool: a path that terminates accumulates its sample into
 // its job's image and frees its slot, and the next work item takes it.
+// Path state of one slot, 96 B: three 32 B sectors that every kernel reads
+// and writes whole.  Slots are visited through queues in no particular
+// order, so a record per slot (not one array per field) keeps each access to
+// whole sectors: a partly written sector costs the memory system a read of
+// the rest.
+struct __align__(32) PathState {
+  float4 org;     // ray origin (the shadow rays of the vertex share it); w: bounces so far (int bits)
+  float4 dir;     // xyz; w: job slot (uint bits)
+  float4 weight;  // path_weight.xyz, last_bounce_pdf
+  float4 rad;     // L.xyz; w: shadow rays pending (int bits: 1 IBL, 2 point light)
+  uint64_t rng;
+  uint32_t pixel;  // pixel index of the slot's sample
+  uint32_t frame;  // progressive frame number of the slot's sample
+  uint32_t pad[4];
+};
+static_assert(sizeof(PathState) == 96, "PathState is three sectors");
+// closest hit of the slot's extension ray: t, u, v, triangle id bits (+ pad to a sector)
+struct __align__(32) PathHit {
+  float4 h;
+  float4 pad;
+};
+// NEE shadow rays of the slot's last vertex, 64 B
+struct __align__(32) PathShadow {
+  float4 sh_dir;  // IBL shadow ray dir.xyz, tfar
+  float4 sh_c;    // IBL NEE contribution * path weight
+  float4 pl_dir;  // point-light shadow ray dir.xyz, tfar
+  float4 pl_c;
+};
+
+__device__ __forceinline__ int path_bounce(const PathState& s) { return __float_as_int(s.org.w); }
+__device__ __forceinline__ uint32_t path_job(const PathState& s) { return __float_as_uint(s.dir.w); }
+__device__ __forceinline__ int path_flags(const PathState& s) { return __float_as_int(s.rad.w); }
+
 struct PathBuf {
-  float4* org;      // ray origin (shadow rays of the same vertex share it)
-  float4* dir;
-  float4* weight;   // path_weight.xyz, last_bounce_pdf
-  float4* rad;      // L.xyz
-  uint64_t* rng;
-  float4* hit;      // t, u, v, triangle id bits
-  float4* sh_dir;   // IBL shadow ray dir.xyz, tfar
-  float4* sh_c;     // IBL NEE contribution * path weight
-  float4* pl_dir;   // point-light shadow ray dir.xyz, tfar
-  float4* pl_c;
-  int* sh_flags;    // bit0: IBL shadow ray, bit1: point-light shadow ray
-  uint32_t* pixel;  // pixel index of the slot's sample
-  uint32_t* frame;  // progressive frame number of the slot's sample
-  int* bounce;      // bounces so far (misptdl.glsl `bounce`)
-  uint32_t* job;    // job slot of the path
+  PathState* st;
+  PathHit* hits;
+  PathShadow* sh;
   uint32_t* q[2];   // extension queues (slot ids)
   uint32_t* qs[2];  // shadow queues
   uint32_t* qh;     // hit queues: class k at qh + k * capacity
