@@ -93,6 +93,73 @@ DEV void free_slots(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot,
   if (pred && lane == __ffs(peers) - 1) atomicSub(&sc.js[job].live, uint32_t(__popc(peers)));
 }
 
+// The same for persistent warps, batched: freed slots collect in a per-warp
+// shared-memory buffer and go to the free list with one atomic on its tail
+// per kFreeBuf slots; live-path decrements collect per job in a register.
+// Per batch of 32 paths, free_slots costs two atomics on two addresses that
+// every warp of the kernel updates; here a warp flushes a few times per
+// launch.  flush() must run before the warp exits.
+constexpr int kFreeBuf = 256;
+struct WarpFree {
+  uint32_t* buf;  // this warp's kFreeBuf entries (shared memory)
+  uint32_t n;     // entries held (warp-uniform)
+  int job;        // job of the pending live decrement (warp-uniform), -1: none
+  uint32_t dec;
+  DEV void init(uint32_t* warp_buf) {
+    buf = warp_buf;
+    n = 0;
+    job = -1;
+    dec = 0;
+  }
+  DEV void flush_slots(const PathBuf& b) {
+    if (!n) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(b.free_tail, (unsigned long long)n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const uint32_t pos0 = uint32_t(base % b.capacity);
+    __syncwarp();
+    for (uint32_t k = uint32_t(lane); k < n; k += 32u) {
+      uint32_t pos = pos0 + k;
+      if (pos >= b.capacity) pos -= b.capacity;
+      b.qfree[pos] = buf[k];
+    }
+    __syncwarp();
+    n = 0;
+  }
+  DEV void flush_live(const Sched& sc) {
+    if (job >= 0 && dec && (threadIdx.x & 31) == 0) atomicSub(&sc.js[job].live, dec);
+    job = -1;
+    dec = 0;
+  }
+  DEV void flush(const Sched& sc, const PathBuf& b) {
+    flush_slots(b);
+    flush_live(sc);
+  }
+  DEV void add(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot, uint32_t jb) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    if (n + uint32_t(__popc(m)) > uint32_t(kFreeBuf)) flush_slots(b);
+    if (pred) buf[n + uint32_t(__popc(m & ((1u << lane) - 1u)))] = slot;
+    n += uint32_t(__popc(m));
+    __syncwarp();
+    // live counts: one job for every freed path of the batch (the usual case) or several
+    const int first_job = __shfl_sync(0xffffffffu, int(jb), __ffs(m) - 1);
+    const bool one_job = __all_sync(0xffffffffu, !pred || int(jb) == first_job);
+    if (one_job) {
+      if (first_job != job) {
+        flush_live(sc);
+        job = first_job;
+      }
+      dec += uint32_t(__popc(m));
+    } else {
+      const unsigned peers = __match_any_sync(0xffffffffu, pred ? int(jb) : -1);
+      if (pred && lane == __ffs(peers) - 1) atomicSub(&sc.js[jb].live, uint32_t(__popc(peers)));
+    }
+  }
+};
+
 // Exclusive prefix sum over the block (blockDim.x == kMaxJobs threads); `n`
 // values are non-zero at most (a single active job needs no scan).
 DEV unsigned long long block_scan(unsigned long long v, unsigned long long* sh, unsigned long long& total, int n) {
@@ -511,6 +578,9 @@ DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
 }
 
 __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
+  __shared__ uint32_t freed[256 / 32][kFreeBuf];
+  WarpFree wf;
+  wf.init(freed[threadIdx.x >> 5]);
   const uint32_t count = b.counts[kCntMiss];
   uint32_t i;
   bool first = true;
@@ -522,8 +592,9 @@ __global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
       job = __float_as_uint(b.st[slot].dir.w);
       shade_miss_path(sc, b, slot);
     }
-    free_slots(sc, b, i < count, slot, job);
+    wf.add(sc, b, i < count, slot, job);
   }
+  wf.flush(sc, b);
 }
 
 // Surface hit.  Returns true if the path continues with an extension ray and
@@ -637,7 +708,7 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
 
 // kTextured = false: no active job's scene has textures (their texture ids are all unset)
 template <bool kTextured>
-__global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
+__global__ void __launch_bounds__(128) k_shade(Sched sc, PathBuf b, int next) {
   // the class queues, read as one sequence in class order
   __shared__ uint32_t start[kNumClasses + 1];
   if (threadIdx.x == 0) {
@@ -652,6 +723,9 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
   const uint32_t count = start[kNumClasses];
   uint32_t* qn = b.q[next];
   uint32_t* cn = b.counts + next;
+  __shared__ uint32_t freed[128 / 32][kFreeBuf];
+  WarpFree wf;
+  wf.init(freed[threadIdx.x >> 5]);
   uint32_t i;
   bool first = true;
   while (next_warp_batch(b.counts + kCntFetchShade, count, i, first)) {
@@ -667,8 +741,9 @@ __global__ void __launch_bounds__(256) k_shade(Sched sc, PathBuf b, int next) {
     }
     enqueue(qn, cn, cont, slot);
     enqueue(b.qs[next], b.counts + kCntShadow0 + next, shadow, slot);
-    free_slots(sc, b, i < count && !cont, slot, job);
+    wf.add(sc, b, i < count && !cont, slot, job);
   }
+  wf.flush(sc, b);
 }
 
 // ---- drain: the last paths of a render call, each run to completion ---------------------
