@@ -37,7 +37,7 @@ METRIC = "Mrays/s"
 
 def extend_traffic():
     """DRAM bytes per frame of the k_extend launches, from the committed ncu
-    summary (profiles/k_extend_wide_large_1080p.md), or None."""
+    summary (profiles/k_extend_dyn_large_1080p.md), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "k_extend_traffic.json")) as f:
             return int(json.load(f)["dram_bytes_per_frame"])
@@ -626,7 +626,7 @@ def run_gpu_arm(args):
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": extend_traffic(),
                          "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_extend "
-                                          "launches per frame (profiles/k_extend_wide_large_1080p.md); achieved "
+                                          "launches per frame (profiles/k_extend_dyn_large_1080p.md); achieved "
                                           "and bytes_per_frame use the reference traversal's node/triangle counts",
                          "bytes_per_frame": alg_bytes_frame, "closest_rays_per_frame": rays_closest_frame,
                          "nodes_per_ray": d2["nodes_closest"] / max(1, rays_closest_frame),
