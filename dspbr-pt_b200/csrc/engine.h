@@ -54,6 +54,7 @@ class Engine {
   // the tail drain; the host waits once.  Not while profiling or counting.
   int run_loop(int slot, unsigned long long max_iter);
   void set_drain_below(uint32_t paths) { drain_below_ = paths ? paths : kDrainBelow; }
+  unsigned drain_below() const { return drain_below_; }
   // The last (up to max_entries, at most kTimeline) iterations' records, oldest first.
   int timeline(uint32_t max_entries, std::vector<TimelineEntry>& out);
   // Finishes every path in the pool in one launch (connect of the pending

@@ -266,6 +266,7 @@ void driver_loop(dspbr_server* s) {
   cudaEvent_t after;
   cudaEventCreateWithFlags(&after, cudaEventDisableTiming);
   long k = 0;
+  long drained = -1;  // events up to this index were recorded before the last drain
   int rc = DSPBR_OK;
   for (;;) {
     bool have_jobs;
@@ -339,6 +340,23 @@ void driver_loop(dspbr_server* s) {
         if (r.cancel && !r.cancel_sent && r.slot >= 0) {
           s->eng->cancel_job(r.slot);
           r.cancel_sent = true;
+        }
+      }
+      // the tail: nothing waits for admission, every active request's work
+      // items have started and few paths are left: finish them in one drain
+      // launch instead of iterations bound by the latency of the longest path
+      if (rc == DSPBR_OK && synced > drained && s->queue.empty() && !s->order.empty() &&
+          done.size() < s->order.size()) {
+        const volatile HostStatus* hs = s->eng->status();
+        bool started = hs->live_paths < s->eng->drain_below();
+        for (uint64_t id : s->order) {
+          const ReqRec& r = s->reqs[id];
+          const volatile JobStatus& js = hs->job[r.slot];
+          if (r.admit_seq > synced || js.items_next < js.items_total) started = false;
+        }
+        if (started) {
+          rc = s->eng->drain();
+          drained = k;  // the statuses of later events include the drain
         }
       }
     }
