@@ -279,6 +279,20 @@ def scene_build_section(local, sc, args):
         rays = sum(d1[k] - d0[k] for k in ("rays_primary", "rays_extension", "rays_shadow"))
         out[builder] = {"scene_create_ms": 1e3 * (t1 - t0), "bvh_build_ms": d1["bvh_build_ms"],
                         "mrays_per_s": rays / (d1["last_render_ms"] * 1e-3) / 1e6, "bvh_nodes": d1["bvh_nodes"]}
+        if builder == "device":
+            # animated geometry: every vertex moved, the BVH refitted on the device
+            moved = sc.vertices.copy()
+            moved[:, 1] += (0.5 * np.sin(0.05 * moved[:, 0])).astype(np.float32)
+            t2 = time.perf_counter()
+            v._scene.update_vertices(moved)
+            t3 = time.perf_counter()
+            v.ctx.check(lib.dspbr_render(h, 2))
+            d2 = v.diagnostics
+            v.ctx.check(lib.dspbr_render(h, max(2, min(args.steps, 10))))
+            d3 = v.diagnostics
+            rays = sum(d3[k] - d2[k] for k in ("rays_primary", "rays_extension", "rays_shadow"))
+            out["refit"] = {"update_vertices_ms": 1e3 * (t3 - t2), "vertices": int(moved.shape[0]),
+                            "mrays_per_s_after": rays / (d3["last_render_ms"] * 1e-3) / 1e6}
         v.dispose()
     return out
 

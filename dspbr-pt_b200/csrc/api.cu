@@ -182,6 +182,7 @@ static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t
   sc->wnodes.swap(wide.nodes);
   sc->wleaves.swap(wide.leaves);
   sc->wroot = wide.root;
+  sc->num_wnodes = wide.num_nodes;
   // the builder's boxes are unions of vertex positions: finite iff they are
   for (uint32_t v = 0; v < num_vertices && sc->boxes_finite; ++v)
     for (int k = 0; k < 3; ++k)
@@ -359,6 +360,7 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     // the 4-wide BVH for the path kernels, collapsed from the same binary tree
     WideBvh wb = collapse_bvh4(conv.data(), num_bvh_nodes, num_bvh_indices);
     sc->wroot = wb.root;
+    sc->num_wnodes = uint32_t(wb.nodes.size());
     if ((rc = s.cuda(sc->wnodes.alloc(std::max<size_t>(wb.nodes.size(), 1) * 8), "alloc wide nodes")) ||
         (rc = s.cuda(sc->wleaves.alloc(std::max<size_t>(wb.leaves.size(), 1)), "alloc wide leaves")) ||
         (rc = s.cuda(cudaMemcpyAsync(sc->wnodes.p, wb.nodes.data(), wb.nodes.size() * sizeof(WideNode4),
@@ -480,6 +482,33 @@ int dspbr_scene_update_materials(dspbr_scene* sc, const float* materials, uint32
   std::copy(materials, materials + size_t(count) * 68, sc->host_materials.begin() + size_t(first) * 68);
   sc->max_tex_id = max_texture_id(sc->host_materials.data(), sc->num_materials);
   { int rc_ = classify_triangles(s, sc, sc->ctx->stream); if (rc_) return rc_; }
+  dspbr_reset(sc->ctx);
+  return DSPBR_OK;
+}
+
+int dspbr_scene_update_vertices(dspbr_scene* sc, const float* vertices, uint32_t first, uint32_t count) {
+  if (!sc || (count && !vertices) || uint64_t(first) + count > sc->num_verts) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(sc->ctx); if (rc_) return rc_; }
+  Status s = sc->ctx->st();
+  for (uint32_t v = 0; v < count; ++v) {
+    const float m = vertices[size_t(v) * 20 + 3];
+    if (!(m >= 0.f) || m >= float(sc->num_materials))
+      return s.fail(DSPBR_ERR_INVALID, "update vertices: vertex %u references material %g of %u", first + v, m,
+                    sc->num_materials);
+  }
+  TRY_CUDA(s, cudaSetDevice(sc->ctx->device), "cudaSetDevice");
+  cudaStream_t st = sc->ctx->stream;
+  TRY_CUDA(s, cudaStreamSynchronize(st), "update vertices");
+  TRY_CUDA(s, cudaMemcpyAsync(sc->verts.p + size_t(first) * 5, vertices, size_t(count) * 80, cudaMemcpyHostToDevice, st),
+           "update vertices");
+  const double t0 = now_ms();
+  int rc = refit_scene_device(sc->nodes.p, sc->num_nodes, sc->num_slots, sc->wnodes.p, sc->num_wnodes, sc->wleaves.p,
+                              sc->tris.p, sc->device_remap.p, sc->verts.p, sc->indices.p, sc->num_tris, st, s);
+  if (rc) return rc;
+  sc->refit_ms = now_ms() - t0;
+  for (uint32_t v = 0; v < count && sc->boxes_finite; ++v)
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(vertices[size_t(v) * 20 + k])) sc->boxes_finite = false;
   dspbr_reset(sc->ctx);
   return DSPBR_OK;
 }

@@ -23,9 +23,12 @@
 // unreachable and stay zero.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include "bvh_gpu.h"
+#include "kernels.h"
 
 namespace dspbr {
 
@@ -304,6 +307,180 @@ __global__ void k_collapse_level(const float4* __restrict__ bin, uint32_t num_no
   }
 }
 
+// ---- refit: the same trees over moved vertices --------------------------------------------
+constexpr int kMaxLeaf = 64;  // MAX_TRIANGLES_PER_LEAF (bvh.glsl:10): the slots a leaf test visits
+
+// A box over the triangles of leaf slots [b0, b1); ids from the leaf-ordered
+// triangle records (w = mesh triangle id bits, -1: a slot the traversal skips).
+__device__ bool slot_box(const float4* __restrict__ tris, int b0, int b1, const float4* __restrict__ verts,
+                         const uint32_t* __restrict__ idx, uint32_t ntris, float4& lo, float4& hi) {
+  bool any = false;
+  lo = make_float4(0.f, 0.f, 0.f, 0.f);
+  hi = lo;
+  for (int i = b0; i < b1; ++i) {
+    const int id = __float_as_int(tris[3 * size_t(i)].w);
+    if (id < 0 || uint32_t(id) >= ntris) continue;
+    for (int k = 0; k < 3; ++k) {
+      const float4 p = verts[5 * size_t(idx[3 * size_t(id) + k])];
+      if (!any) {
+        lo = make_float4(p.x, p.y, p.z, 0.f);
+        hi = lo;
+        any = true;
+      } else {
+        lo = make_float4(fminf(lo.x, p.x), fminf(lo.y, p.y), fminf(lo.z, p.z), 0.f);
+        hi = make_float4(fmaxf(hi.x, p.x), fmaxf(hi.y, p.y), fmaxf(hi.z, p.z), 0.f);
+      }
+    }
+  }
+  return any;
+}
+
+__device__ __forceinline__ void box_union(float4& lo, float4& hi, bool& any, float4 l, float4 h) {
+  if (!any) {
+    lo = l;
+    hi = h;
+    any = true;
+  } else {
+    lo = make_float4(fminf(lo.x, l.x), fminf(lo.y, l.y), fminf(lo.z, l.z), 0.f);
+    hi = make_float4(fmaxf(hi.x, h.x), fmaxf(hi.y, h.y), fmaxf(hi.z, h.z), 0.f);
+  }
+}
+
+// Binary tree (reference layout: an inner node stores its children's boxes):
+// parent links of valid children (child in range, not the node itself).
+__global__ void k_refit_bin_parents(const float4* __restrict__ nodes, uint32_t nn, int* __restrict__ parent) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    const float4* o = nodes + 4 * size_t(i);
+    if (__float_as_int(o[2].w) > 0) continue;  // leaf
+    const int l = __float_as_int(o[0].w), r = __float_as_int(o[1].w);
+    if (l >= 0 && uint32_t(l) < nn && uint32_t(l) != i) parent[l] = int(i);
+    if (r >= 0 && uint32_t(r) < nn && uint32_t(r) != i) parent[r] = int(i);
+  }
+}
+
+// Leaf boxes from their triangles (the slots the reference's leaf loop
+// visits), then unions towards the root: the second child to arrive at an
+// inner node writes both children's boxes into it.  A child without any
+// triangle keeps the box its parent had.  Each walk is bounded by nn steps.
+__global__ void k_refit_bin_up(float4* nodes, uint32_t nn, uint32_t nslots, const float4* __restrict__ tris,
+                               const float4* __restrict__ verts, const uint32_t* __restrict__ idx, uint32_t ntris,
+                               const int* __restrict__ parent, float4* box_lo, float4* box_hi, int* has_box,
+                               int* flags) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+    const float4* o = nodes + 4 * size_t(i);
+    const int cnt = __float_as_int(o[2].w);
+    if (cnt <= 0) continue;
+    const int first = __float_as_int(o[3].w);
+    const int b0 = max(first, 0);
+    const long long end = (long long)first + (long long)min(cnt, kMaxLeaf);
+    const int b1 = int(end < (long long)nslots ? end : (long long)nslots);
+    float4 lo, hi;
+    const bool any = slot_box(tris, b0, b1, verts, idx, ntris, lo, hi);
+    box_lo[i] = lo;
+    box_hi[i] = hi;
+    has_box[i] = any ? 1 : 0;
+    __threadfence();
+    int p = parent[i];
+    for (uint32_t steps = 0; p >= 0 && steps < nn; ++steps) {
+      if (atomicAdd(&flags[p], 1) == 0) break;  // the sibling finishes this node
+      __threadfence();
+      float4* q = nodes + 4 * size_t(p);
+      const int a = __float_as_int(q[0].w), c = __float_as_int(q[1].w);
+      bool anyp = false;
+      float4 plo = make_float4(0.f, 0.f, 0.f, 0.f), phi = plo;
+      if (__ldcg(has_box + a)) {
+        const float4 l = __ldcg(box_lo + a), h = __ldcg(box_hi + a);
+        q[0] = make_float4(l.x, l.y, l.z, q[0].w);
+        q[1] = make_float4(h.x, h.y, h.z, q[1].w);
+        box_union(plo, phi, anyp, l, h);
+      }
+      if (__ldcg(has_box + c)) {
+        const float4 l = __ldcg(box_lo + c), h = __ldcg(box_hi + c);
+        q[2] = make_float4(l.x, l.y, l.z, q[2].w);
+        q[3] = make_float4(h.x, h.y, h.z, q[3].w);
+        box_union(plo, phi, anyp, l, h);
+      }
+      box_lo[p] = plo;
+      box_hi[p] = phi;
+      has_box[p] = anyp ? 1 : 0;
+      __threadfence();
+      p = parent[p];
+    }
+  }
+}
+
+// 4-wide tree: parent (node, child slot) of each wide node and the number of
+// wide-node children of each node.
+__global__ void k_refit_wide_parents(const float4* __restrict__ wnodes, uint32_t nw, int2* __restrict__ parent,
+                                     int* __restrict__ inner) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    const float4* o = wnodes + 8 * size_t(i);
+    const int4 ch = *reinterpret_cast<const int4*>(o + 6);
+    const int n = min(max(__float_as_int(o[7].x), 0), 4);
+    const int c[4] = {ch.x, ch.y, ch.z, ch.w};
+    int k_inner = 0;
+    for (int k = 0; k < n; ++k)
+      if (c[k] >= 0 && uint32_t(c[k]) < nw && uint32_t(c[k]) != i) {
+        parent[c[k]] = make_int2(int(i), k);
+        ++k_inner;
+      }
+    inner[i] = k_inner;
+  }
+}
+
+__device__ __forceinline__ void wide_set_box(float4* o, int k, float4 lo, float4 hi) {
+  float* f = reinterpret_cast<float*>(o);
+  f[0 * 4 + k] = lo.x; f[1 * 4 + k] = lo.y; f[2 * 4 + k] = lo.z;
+  f[3 * 4 + k] = hi.x; f[4 * 4 + k] = hi.y; f[5 * 4 + k] = hi.z;
+}
+
+// A wide node whose children are all leaves starts a walk: its leaf boxes,
+// its own box into its parent's slot; the last wide-node child to arrive at a
+// node finishes it (its leaf children, then its own box) and goes on.
+__global__ void k_refit_wide_up(float4* wnodes, uint32_t nw, const int2* __restrict__ wleaves,
+                                const float4* __restrict__ tris, const float4* __restrict__ verts,
+                                const uint32_t* __restrict__ idx, uint32_t ntris, const int2* __restrict__ parent,
+                                const int* __restrict__ inner, int* flags) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    if (inner[i] != 0) continue;
+    int v = int(i);
+    for (uint32_t steps = 0; steps <= nw; ++steps) {
+      float4* o = wnodes + 8 * size_t(v);
+      const int4 ch = *reinterpret_cast<const int4*>(o + 6);
+      const int n = min(max(__float_as_int(o[7].x), 0), 4);
+      const int c[4] = {ch.x, ch.y, ch.z, ch.w};
+      bool any = false;
+      float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
+      for (int k = 0; k < n; ++k) {
+        float4 l, h;
+        if (c[k] < 0) {  // leaf child: its triangles
+          const int2 r = wleaves[~c[k]];
+          if (!slot_box(tris, r.x, r.y, verts, idx, ntris, l, h)) continue;
+          wide_set_box(o, k, l, h);
+        } else {  // wide child: the box its walk left in this slot
+          const float* f = reinterpret_cast<const float*>(o);
+          l = make_float4(__ldcg(f + 0 * 4 + k), __ldcg(f + 1 * 4 + k), __ldcg(f + 2 * 4 + k), 0.f);
+          h = make_float4(__ldcg(f + 3 * 4 + k), __ldcg(f + 4 * 4 + k), __ldcg(f + 5 * 4 + k), 0.f);
+        }
+        box_union(lo, hi, any, l, h);
+      }
+      const int2 pk = parent[v];
+      if (pk.x < 0) break;  // the root
+      if (any) wide_set_box(wnodes + 8 * size_t(pk.x), pk.y, lo, hi);
+      __threadfence();
+      if (atomicAdd(&flags[pk.x], 1) + 1 != inner[pk.x]) break;  // other children still to come
+      __threadfence();
+      v = pk.x;
+    }
+  }
+}
+
+// leaf-slot remap recovered from the leaf-ordered triangle records
+__global__ void k_remap_from_tris(const float4* __restrict__ tris, uint32_t nslots, int32_t* __restrict__ remap) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += gridDim.x * blockDim.x)
+    remap[i] = __float_as_int(tris[3 * size_t(i)].w);
+}
+
 int grid(size_t n, int threads, int cap) {
   size_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -311,6 +488,48 @@ int grid(size_t n, int threads, int cap) {
 }
 
 }  // namespace
+
+int refit_scene_device(float4* nodes, uint32_t num_nodes, uint32_t num_slots, float4* wnodes, uint32_t num_wide,
+                       const int2* wleaves, float4* tris, const int32_t* remap, const float4* verts,
+                       const uint32_t* indices, uint32_t ntris, cudaStream_t st, Status& s) {
+  DevBuf<int> parent, flags, has_box, inner;
+  DevBuf<float4> lo, hi;
+  DevBuf<int2> wparent;
+  DevBuf<int32_t> own_remap;
+  TRY_CUDA(s, parent.alloc(std::max<uint32_t>(num_nodes, 1)), "refit");
+  TRY_CUDA(s, flags.alloc(std::max<uint32_t>(std::max(num_nodes, num_wide), 1)), "refit");
+  TRY_CUDA(s, has_box.alloc(std::max<uint32_t>(num_nodes, 1)), "refit");
+  TRY_CUDA(s, lo.alloc(std::max<uint32_t>(num_nodes, 1)), "refit");
+  TRY_CUDA(s, hi.alloc(std::max<uint32_t>(num_nodes, 1)), "refit");
+  // binary tree
+  TRY_CUDA(s, cudaMemsetAsync(parent.p, 0xff, parent.bytes(), st), "refit");
+  TRY_CUDA(s, cudaMemsetAsync(flags.p, 0, flags.bytes(), st), "refit");
+  k_refit_bin_parents<<<grid(num_nodes, 256, 148 * 8), 256, 0, st>>>(nodes, num_nodes, parent.p);
+  k_refit_bin_up<<<grid(num_nodes, 256, 148 * 8), 256, 0, st>>>(nodes, num_nodes, num_slots, tris, verts, indices,
+                                                                ntris, parent.p, lo.p, hi.p, has_box.p, flags.p);
+  TRY_CUDA(s, cudaGetLastError(), "refit");
+  // 4-wide tree
+  if (num_wide) {
+    TRY_CUDA(s, wparent.alloc(num_wide), "refit");
+    TRY_CUDA(s, inner.alloc(num_wide), "refit");
+    TRY_CUDA(s, cudaMemsetAsync(wparent.p, 0xff, wparent.bytes(), st), "refit");
+    TRY_CUDA(s, cudaMemsetAsync(flags.p, 0, flags.bytes(), st), "refit");
+    k_refit_wide_parents<<<grid(num_wide, 256, 148 * 8), 256, 0, st>>>(wnodes, num_wide, wparent.p, inner.p);
+    k_refit_wide_up<<<grid(num_wide, 256, 148 * 8), 256, 0, st>>>(wnodes, num_wide, wleaves, tris, verts, indices,
+                                                                  ntris, wparent.p, inner.p, flags.p);
+    TRY_CUDA(s, cudaGetLastError(), "refit");
+  }
+  // the leaf-ordered triangle records over the new positions
+  if (!remap) {
+    TRY_CUDA(s, own_remap.alloc(std::max<uint32_t>(num_slots, 1)), "refit");
+    k_remap_from_tris<<<grid(num_slots, 256, 148 * 8), 256, 0, st>>>(tris, num_slots, own_remap.p);
+    remap = own_remap.p;
+  }
+  if (num_slots) launch_gather_tris(verts, indices, remap, num_slots, ntris, tris, st);
+  TRY_CUDA(s, cudaGetLastError(), "refit");
+  TRY_CUDA(s, cudaStreamSynchronize(st), "refit");
+  return DSPBR_OK;
+}
 
 int build_bvh_device(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st, DeviceBvh* out,
                      Status& s) {

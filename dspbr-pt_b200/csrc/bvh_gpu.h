@@ -30,4 +30,13 @@ struct DeviceWideBvh {
 };
 int collapse_bvh4_device(const DeviceBvh& bin, cudaStream_t st, DeviceWideBvh* out, Status& s);
 
+// Refit after the vertices moved (indices unchanged): the boxes of the binary
+// tree (reference layout) and of the 4-wide tree are recomputed bottom-up from
+// their leaves' triangles, keeping both topologies, and the leaf-ordered
+// triangle records are gathered again.  remap: the leaf-slot remap, or null to
+// recover it from the records.  Synchronises `st`.
+int refit_scene_device(float4* nodes, uint32_t num_nodes, uint32_t num_slots, float4* wnodes, uint32_t num_wide,
+                       const int2* wleaves, float4* tris, const int32_t* remap, const float4* verts,
+                       const uint32_t* indices, uint32_t ntris, cudaStream_t st, Status& s);
+
 }  // namespace dspbr

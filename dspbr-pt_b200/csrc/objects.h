@@ -22,6 +22,8 @@ struct dspbr_scene {
   dspbr::DevBuf<float4> wnodes;  // 4-wide BVH (8 float4 per node)
   dspbr::DevBuf<int2> wleaves;
   int wroot = 0;
+  uint32_t num_wnodes = 0;  // wide nodes in use
+  double refit_ms = 0.0;    // the last dspbr_scene_update_vertices
   dspbr::DevBuf<int32_t> device_remap;  // leaf-slot remap of a device-built BVH
   // material textures
   std::vector<std::unique_ptr<dspbr::DevBuf<uchar4>>> tex_data;

@@ -138,6 +138,7 @@ SIGNATURES = {
     "dspbr_scene_set_textures": (C.c_int, [_V, _F, C.c_uint32, C.POINTER(TextureArray), C.c_uint32]),
     "dspbr_scene_bvh": (C.c_int, [_V, _F, _I, _U, _U]),
     "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),
+    "dspbr_scene_update_vertices": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),
     "dspbr_scene_device_bytes": (C.c_int, [_V, C.POINTER(C.c_uint64)]),
     "dspbr_scene_destroy": (C.c_int, [_V]),
     "dspbr_ibl_create": (C.c_int, [_V, _F, C.c_int, C.c_int, _PV]),

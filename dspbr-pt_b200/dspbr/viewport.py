@@ -136,6 +136,12 @@ class DeviceScene:
         m = f32(materials).reshape(-1, MATERIAL_STRIDE)
         self.ctx.check(self.ctx.lib.dspbr_scene_update_materials(self.h, fptr(m), first, m.shape[0]))
 
+    def update_vertices(self, vertices, first: int = 0) -> None:
+        """New 20-float records for vertices [first, first + n) (same triangles); the
+        BVH is refitted on the device (dspbr_scene_update_vertices)."""
+        v = f32(vertices).reshape(-1, VERTEX_STRIDE)
+        self.ctx.check(self.ctx.lib.dspbr_scene_update_vertices(self.h, fptr(v), int(first), v.shape[0]))
+
     def set_textures(self, tex_infos, arrays) -> None:
         """Material textures: (N, 8) TexInfo records and RGBA8 arrays of shape
         (layers, height, width, 4) (dspbr_scene_set_textures)."""

@@ -151,6 +151,16 @@ int dspbr_scene_set_textures(dspbr_scene* scene, const float* tex_infos, uint32_
 int dspbr_scene_bvh(const dspbr_scene* scene, float* nodes, int32_t* remap, uint32_t* num_nodes,
                     uint32_t* num_indices);
 int dspbr_scene_update_materials(dspbr_scene* scene, const float* materials, uint32_t first, uint32_t count);
+/* Moves vertices [first, first + count) to new 20-float records (same
+ * triangles): the BVH keeps its topology and its boxes are refitted on the
+ * device, bottom-up from the leaves' triangles (the binary tree of
+ * dspbr_scene_bvh and the 4-wide tree of the path kernels), then the
+ * leaf-ordered triangle records are gathered again.  New: the reference
+ * rebuilds its BVH on every setScene (tinybvh_builder.ts:43-256); a refit is
+ * the animated-geometry step of a device BVH.  Resets the accumulation of the
+ * scene's context; not while a server request renders the scene.  Shading
+ * classes stay those of the creation (they only group hits for speed). */
+int dspbr_scene_update_vertices(dspbr_scene* scene, const float* vertices, uint32_t first, uint32_t count);
 int dspbr_scene_device_bytes(const dspbr_scene* scene, uint64_t* bytes);
 int dspbr_scene_destroy(dspbr_scene* scene);
 
