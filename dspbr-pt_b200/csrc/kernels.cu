@@ -708,7 +708,9 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
 
 // kTextured = false: no active job's scene has textures (their texture ids are all unset)
 template <bool kTextured>
-__global__ void __launch_bounds__(128) k_shade(Sched sc, PathBuf b, int next) {
+// 5 blocks of 128 threads per SM (96 registers, some spilled): of 3..8 blocks
+// per SM the fastest frames (3: 168 registers, no spills; 4 and 6..8 slower)
+__global__ void __launch_bounds__(128, 5) k_shade(Sched sc, PathBuf b, int next) {
   // the class queues, read as one sequence in class order
   __shared__ uint32_t start[kNumClasses + 1];
   if (threadIdx.x == 0) {
@@ -915,8 +917,8 @@ void init_launch_sizes(LaunchCfg& lc) {
     return n * sms;
   };
   lc.dyn_blocks = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
-  lc.shade_dyn_blocks[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 3);
-  lc.shade_dyn_blocks[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 2);
+  lc.shade_dyn_blocks[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 5);
+  lc.shade_dyn_blocks[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 5);
   lc.miss_dyn_blocks = resident(reinterpret_cast<const void*>(k_shade_miss), 256, 6);
 }
 

@@ -164,7 +164,7 @@ struct LaunchCfg {
   bool textured = false;  // some active job samples material textures
   int dyn_blocks = 148 * 8;  // k_extend / k_connect: resident blocks of 128 threads (64 registers)
   // resident blocks of the persistent shading kernels (set by init_launch_sizes)
-  int shade_dyn_blocks[2] = {148 * 3, 148 * 2};  // k_shade<false>, k_shade<true>, 128 threads
+  int shade_dyn_blocks[2] = {148 * 5, 148 * 5};  // k_shade<false>, k_shade<true>, 128 threads
   int miss_dyn_blocks = 148 * 6;                 // k_shade_miss, 256 threads
 };
 
