@@ -262,10 +262,13 @@ DEV void wide_begin(WideTrav& w, int root) {
 }
 
 // One step; returns whether another step is due (entries left, step cap not
-// reached, no accepted triangle for kAny).
-template <bool kAny, bool kExactNaN>
-DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
-                   const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack) {
+// reached, no accepted triangle for an any-hit ray).  `any` is a run-time
+// flag so that closest-hit and any-hit rays can share one instruction stream;
+// the callers with a constant get the specialised code.
+template <bool kExactNaN>
+DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
+                      const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack,
+                      bool any) {
   const int e = w.cur;
   bool next_in_register = false;
   if (e < 0) {
@@ -278,7 +281,7 @@ DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ w
       float t, u, v;
       if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
         hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
-        if (kAny) {
+        if (any) {
           w.any_hit = true;
           return false;
         }
@@ -331,6 +334,12 @@ DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ w
   return w.have && w.step < kMaxSteps;
 }
 
+template <bool kAny, bool kExactNaN>
+DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
+                   const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack) {
+  return wide_step_rt<kExactNaN>(wnodes, wleaves, tris, org, inv, dir, hit, w, stack, kAny);
+}
+
 // `aborted`: the stack overflowed or the step cap ended the traversal with
 // entries left (not when kAny accepted a triangle).
 DEV bool wide_aborted(const WideTrav& w) { return !w.any_hit && (w.overflow || (w.have && w.step >= kMaxSteps)); }
@@ -347,6 +356,27 @@ DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfa
   }
   aborted = wide_aborted(w);
   return kAny ? (w.any_hit || hit.tri >= 0) : hit.tri >= 0;
+}
+
+// closest hit (any = false) or any hit (any = true) chosen at run time
+DEV bool traverse_wide_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool any, Hit& hit, bool& aborted) {
+  v3 inv = inv_dir(dir);
+  const bool exact = !(s.boxes_finite && finite3(org) && finite3(inv));
+  hit.t = tfar;
+  hit.tri = -1;
+  hit.u = hit.v = 0.f;
+  int stack[kWideStack];
+  WideTrav w;
+  wide_begin(w, s.wroot);
+  if (exact) {
+    while (wide_step_rt<true>(s.wnodes, s.wleaves, s.tris, org, inv, dir, hit, w, stack, any)) {
+    }
+  } else {
+    while (wide_step_rt<false>(s.wnodes, s.wleaves, s.tris, org, inv, dir, hit, w, stack, any)) {
+    }
+  }
+  aborted = wide_aborted(w);
+  return w.any_hit || hit.tri >= 0;
 }
 
 template <bool kAny>

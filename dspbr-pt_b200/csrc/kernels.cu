@@ -758,39 +758,105 @@ __global__ void __launch_bounds__(128, 5) k_shade(Sched sc, PathBuf b, int next)
 // the same order per path, so each path's result is unchanged.
 template <bool kTextured>
 __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
+  // two lanes per path: the even lane runs the path (extension ray, shading),
+  // the odd lane the NEE shadow rays of the path's last vertex.  The shadow
+  // rays of vertex k and the extension ray of vertex k + 1 start at the same
+  // point and are independent, so the two lanes trace them side by side
+  // (one traversal routine, any-hit chosen at run time); the shadow
+  // contribution reaches the path radiance before the next shading reads it,
+  // the order of the one-lane loop, so each path's result is unchanged.
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
-  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool helper = (lane & 1) != 0;
+  const unsigned pair = 3u << (lane & ~1);
+  const uint32_t per_round = (gridDim.x * blockDim.x) >> 1;
+  for (uint32_t base = (blockIdx.x * blockDim.x) >> 1; base < count; base += per_round) {
+    const uint32_t i = base + (threadIdx.x >> 1);
     uint32_t slot = 0, job = 0, closest = 0, shadow_rays = 0;
     bool aborted = false;
     if (i < count) {
       slot = q[i];
       job = __float_as_uint(b.st[slot].dir.w);
+      bool pending = false;  // shadow rays of the last vertex not yet traced (pair-uniform)
       for (int guard = 0; guard < 4 * kMaxSteps; ++guard) {
         const DevScene s = sc.jobs[job].s;
-        float4 o = b.st[slot].org, d = b.st[slot].dir;
         Hit h;
-        bool ab = false;
-        trace_path_ray<false, false, kTravPerPath>(s, mk(o), mk(d), kTfarMax, h, ab, nullptr, nullptr);
-        aborted |= ab;
-        ++closest;
-        b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
-        if (h.tri < 0) {
-          shade_miss_path(sc, b, slot);
-          break;
+        h.tri = -1;
+        h.t = h.u = h.v = 0.f;
+        if (s.wide) {
+          // extension ray (even lane) and IBL shadow ray (odd lane) in one pass
+          const float4 o = b.st[slot].org;
+          float4 d = b.st[slot].dir;
+          float tfar = kTfarMax;
+          bool trace = !helper;
+          int flags = 0;
+          if (helper && pending) {
+            flags = __float_as_int(b.st[slot].rad.w);
+            if (flags & 1) {
+              const float4 sd = b.sh[slot].sh_dir;
+              d = make_float4(sd.x, sd.y, sd.z, 0.f);
+              tfar = sd.w;
+              trace = true;
+            }
+          }
+          bool ab = false, occluded = false;
+          if (trace) {
+            // isOccluded normalises the light direction (bvh.glsl:225-229)
+            const v3 dir = helper ? normalize_rn(mk(d)) : mk(d);
+            occluded = traverse_wide_rt(s, mk(o), dir, tfar, helper, h, ab);
+            aborted |= ab;
+          }
+          if (helper && pending) {
+            v3 add = mk(0.f);
+            if (flags & 1) {
+              if (!occluded) add = mk(b.sh[slot].sh_c);
+              ++shadow_rays;
+            }
+            if (flags & 2) {  // the point-light ray, after
+              const float4 pd = b.sh[slot].pl_dir;
+              Hit hp;
+              bool abp = false;
+              if (!traverse_wide_rt(s, mk(o), normalize_rn(mk(pd)), pd.w, true, hp, abp))
+                add = add + mk(b.sh[slot].pl_c);
+              aborted |= abp;
+              ++shadow_rays;
+            }
+            const float4 w4 = b.st[slot].weight, L = b.st[slot].rad;
+            b.st[slot].weight = w4;
+            b.st[slot].rad = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+          }
+        } else {
+          // the reference's binary traversal: shadow rays, then the extension ray
+          if (helper && pending) {
+            int nrays = 0;
+            connect_slot<false, kTravPerPath>(sc, b, slot, aborted, nrays, nullptr, nullptr);
+            shadow_rays += uint32_t(nrays);
+          }
+          __syncwarp(pair);
+          if (!helper) {
+            const float4 o = b.st[slot].org, d = b.st[slot].dir;
+            bool ab = false;
+            trace_path_ray<false, false, kTravPerPath>(s, mk(o), mk(d), kTfarMax, h, ab, nullptr, nullptr);
+            aborted |= ab;
+          }
         }
-        bool shadow = false;
-        const bool cont = shade_path<kTextured>(sc, b, slot, shadow);
-        if (shadow) {
-          int nrays = 0;
-          connect_slot<false, kTravPerPath>(sc, b, slot, aborted, nrays, nullptr, nullptr);
-          shadow_rays += uint32_t(nrays);
+        __syncwarp(pair);  // the shadow contribution is in the record before the shading reads it
+        bool cont = false, shadow = false;
+        if (!helper) {
+          ++closest;
+          b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
+          if (h.tri < 0) shade_miss_path(sc, b, slot);
+          else cont = shade_path<kTextured>(sc, b, slot, shadow);
         }
-        if (!cont) break;
+        cont = __shfl_sync(pair, cont, lane & ~1);
+        pending = __shfl_sync(pair, shadow, lane & ~1);
+        __syncwarp(pair);  // the shading's records are written before the helper reads them
+        if (!cont) break;  // a path that ends emits no shadow ray
       }
     }
-    free_slots(sc, b, i < count, slot, job);
+    // one free per path (even lanes)
+    free_slots(sc, b, i < count && !helper, slot, job);
     add_warp(b.stats + 0, closest);
     add_warp(b.stats + 1, shadow_rays);
     count_warp(b.stats + 2, aborted);
