@@ -405,21 +405,33 @@ def make_large(seed: int = 0, target_tris: int = 1_000_000, n_inst: int = 256) -
     return Scene("large", verts, idx, mats, cam, 1920, 1080, 256, 12, 2, env, seed)
 
 
+def _divergence_kind(i):
+    """60% transmissive / volume / dispersive, 20% iridescent, 20% base materials."""
+    r = (i * 7919) % 10
+    if r < 6:
+        return ["transmission", "volume", "dispersion"][r % 3]
+    return "iridescence" if r < 8 else "base"
+
+
 def make_divergence(seed: int = 0, n_inst: int = 536, tris_per_inst: int = 10_000) -> Scene:
     """~4.0M triangles: 536 instances alternating 9,800-triangle displaced grids
     and 5,120-triangle icospheres."""
     rng = np.random.default_rng(seed)
-
-    def kind(i):  # 60% transmissive/volume (dispersive), 20% iridescent, 20% base
-        r = (i * 7919) % 10
-        if r < 6:
-            return ["transmission", "volume", "dispersion"][r % 3]
-        return "iridescence" if r < 8 else "base"
-
-    verts, idx, mats = _instances(rng, n_inst, tris_per_inst, kind)
+    verts, idx, mats = _instances(rng, n_inst, tris_per_inst, _divergence_kind)
     env = env_lognormal(4096, 2048, rng, 1.5, 1e4)
     cam = Camera.look_at((0, 15, 135), (0, 0, 0), fov=45.0, near=0.1)
     return Scene("divergence", verts, idx, mats, cam, 1280, 720, 512, 32, 4, env, seed)
+
+
+def make_divergence_small(seed: int = 0) -> Scene:
+    """The divergence configuration's material mix on a small scene for
+    path-level parity: 24 instances (~5.4k triangles) packed in a 12 m cube,
+    128x64 environment, 32 bounces."""
+    rng = np.random.default_rng(seed)
+    verts, idx, mats = _instances(rng, 24, 320, _divergence_kind, cube=12.0)
+    env = env_lognormal(128, 64, rng, 1.5, 1e3)
+    cam = Camera.look_at((0, 4, 18), (0, 0, 0), fov=50.0, near=0.05)
+    return Scene("divergence-small", verts, idx, mats, cam, 48, 36, 16, 32, 2, env, seed)
 
 
 def make_sized(seed: int, target_tris: int, env_size=(1024, 512)) -> Scene:

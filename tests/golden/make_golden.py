@@ -168,6 +168,20 @@ def main():
         assert r32.render(W, H, acc) is not None
     g["gltf_image"] = acc
     g["gltf_image_whf"] = np.array([W, H, F], np.int32)
+    # the divergence configuration's materials (transmission, volume absorption,
+    # dispersion, iridescence) at 32 bounces, path for path
+    dv = synth.make_divergence_small(0)
+    dbvh = Bvh.build(dv.vertices, dv.indices, 20)
+    r32.set_scene(dv.vertices, dv.indices, dv.materials, dbvh.nodes, dbvh.indices)
+    r32.set_textures(gltf.DEFAULT_TEX_INFO.reshape(1, 8), [])
+    r32.set_ibl(dv.env)
+    W, H, F = dv.width, dv.height, 4
+    acc = np.zeros((H, W, 4), np.float32)
+    for f in range(1, F + 1):
+        r32.set_uniforms(ref_lib.uniform_block(dv.camera.matrix_world, dv.camera.fov, dv.camera.near, W, H, f, 32))
+        assert r32.render(W, H, acc) is not None
+    g["div_image"] = acc
+    g["div_image_whf"] = np.array([W, H, F], np.int32)
     g["gltf_vertices_sha"] = np.frombuffer(hashlib.sha256(gs.vertices.tobytes() + gs.indices.tobytes() +
                                                           gs.materials.tobytes() + gs.tex_infos.tobytes()).digest(),
                                            np.uint8)

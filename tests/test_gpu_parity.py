@@ -480,3 +480,23 @@ def test_reference_shader_direct_when_available(ctx, g, gscene):
     rtri, rt, ruv = ref.trace(rays)
     np.testing.assert_array_equal(tri, rtri)
     np.testing.assert_array_equal(t.view(np.uint32), rt.view(np.uint32))
+
+
+@pytest.mark.parametrize("traversal", ["reference", "wide"])
+def test_divergence_materials_image_matches_golden_path_for_path(g, traversal):
+    """The divergence configuration's material mix (transmission, volume
+    absorption, dispersion, iridescence) at 32 bounces."""
+    sc = synth.make_divergence_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    W, H, F = (int(x) for x in g["div_image_whf"])
+    v = _viewport(sc, W, H, {"maxBounces": 32, "envSampling": "cdf", "traversal": traversal})
+    v.start(F)
+    img = v.readAccumulation()
+    d = v.diagnostics
+    v.dispose()
+    assert d["traversal_aborted"] == 0
+    ref = g["div_image"]
+    close = helpers.close_mask(img[..., :3], ref[..., :3], 1e-3, 1e-4).all(-1)
+    print("divergence materials: pixels equal to the reference path for path:", close.mean())
+    assert close.mean() > 0.95
+    assert np.abs(img - ref).mean() < 0.01 * ref[..., :3].mean()

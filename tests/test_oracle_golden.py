@@ -167,3 +167,19 @@ def test_point_light_image_matches_reference(g):
                                point_light=g["pl_light"])
     img = o.render_image(p, F)
     assert helpers.close_mask(img, g["pl_image"], 1e-5, 1e-6).mean() > 0.999
+
+
+def test_divergence_materials_image_matches_reference(g):
+    """Transmission, volume absorption, dispersion and iridescence at 32 bounces."""
+    from dspbr import synth
+    from dspbr.viewport import Bvh
+    dv = synth.make_divergence_small(0)
+    bvh = Bvh.build(dv.vertices, dv.indices, 20)
+    o = oracle_lib.Oracle()
+    o.set_scene(dv.vertices, dv.indices, dv.materials, bvh.nodes, bvh.indices)
+    o.set_ibl(dv.env)
+    W, H, F = (int(x) for x in g["div_image_whf"])
+    p = oracle_lib.make_params(dv.camera.matrix_world, dv.camera.fov, dv.camera.near, W, H, max_bounces=32)
+    img = o.render_image(p, F)
+    close = helpers.close_mask(img, g["div_image"], 1e-4, 1e-5).all(-1)
+    assert close.mean() > 0.99
