@@ -391,7 +391,7 @@ int dspbr_server_create(dspbr_ctx* ctx, const dspbr_server_config* cfg, dspbr_se
   s->ctx = ctx;
   s->device = ctx->device;
   if (cfg) s->cfg = *cfg;
-  if (s->cfg.path_pool == 0) s->cfg.path_pool = 1u << 21;
+  if (s->cfg.path_pool == 0) s->cfg.path_pool = 1u << 23;
   if (s->cfg.max_active <= 0 || s->cfg.max_active > kMaxJobs) s->cfg.max_active = kMaxJobs;
   if (s->cfg.hbm_budget_bytes == 0) s->cfg.hbm_budget_bytes = kDefaultBudget;
   Status st = ctx->st();
@@ -646,24 +646,10 @@ int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, 
     }
     return DSPBR_OK;
   };
-  for (uint32_t pool : {1u << 20, 1u << 21, 1u << 22})
+  // the path kernels size their grids from the occupancy API: the pool size is
+  // what is left to choose
+  for (uint32_t pool : {1u << 20, 1u << 21, 1u << 22, 1u << 23})
     if (!rc && pool != best_pool) rc = consider(pool, best);
-  for (int tt : {64, 128, 256})
-    for (int per_sm : {8, 16, 32}) {
-      LaunchCfg lc = best;
-      lc.trace_threads = tt;
-      lc.trace_blocks = 148 * per_sm * 128 / tt;
-      if (!rc && !(lc.trace_threads == best.trace_threads && lc.trace_blocks == best.trace_blocks))
-        rc = consider(best_pool, lc);
-    }
-  for (int tt : {64, 128, 256})
-    for (int per_sm : {4, 8, 16}) {
-      LaunchCfg lc = best;
-      lc.shade_threads = tt;
-      lc.shade_blocks = 148 * per_sm * 128 / tt;
-      if (!rc && !(lc.shade_threads == best.shade_threads && lc.shade_blocks == best.shade_blocks))
-        rc = consider(best_pool, lc);
-    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // leave an empty pool of the chosen size with the chosen launch sizes

@@ -248,7 +248,7 @@ int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
  * per frame and has no iterations to report (renderer.ts:512-565). */
 int dspbr_get_timeline(dspbr_ctx* ctx, uint32_t max_entries, uint64_t* iteration, uint64_t* t_ns, uint32_t* live,
                        uint32_t* count);
-/* paths per wave (0 = default 2^21); the wave covers min(frames, paths/pixels)
+/* paths per wave (0 = default 2^23); the wave covers min(frames, paths/pixels)
  * samples of every pixel.  Set by the autotuner. */
 int dspbr_set_wave_paths(dspbr_ctx* ctx, uint32_t paths);
 /* live paths below which a render call, once every sample has started,
@@ -292,7 +292,7 @@ int dspbr_camera_rays(dspbr_ctx* ctx, uint32_t n, const int32_t* xy, const float
  * driver thread owns the server's CUDA stream; the calls below are
  * thread-safe. */
 typedef struct dspbr_server_config {
-  uint32_t path_pool;         /* path slots (0: 2^21) */
+  uint32_t path_pool;         /* path slots (0: 2^23) */
   int max_active;             /* requests in flight at once, 1..256 (0: 256) */
   uint64_t hbm_budget_bytes;  /* path pool + scenes in use + request buffers (0: 120 GB) */
   int reserved[8];
@@ -349,8 +349,8 @@ int dspbr_server_cancel(dspbr_server* srv, uint64_t id);
 int dspbr_server_release(dspbr_server* srv, uint64_t id);
 int dspbr_server_get_stats(dspbr_server* srv, dspbr_server_stats* stats);
 /* Autotuner: renders the sample requests (results discarded) under candidate
- * path-pool sizes and extend/connect/shade block sizes, keeps the fastest in
- * rays per second.  Call while the server is idle.  seconds bounds the time. */
+ * path-pool sizes (2^20..2^23, within half the HBM budget), keeps the fastest
+ * in rays per second.  Call while the server is idle.  seconds bounds the time. */
 int dspbr_server_autotune(dspbr_server* srv, const dspbr_request* samples, int n, double seconds);
 int dspbr_server_destroy(dspbr_server* srv);
 

@@ -137,7 +137,7 @@ def test_autotune_then_serve(world):
     srv = Server(ctx)
     samples = [srv.request(scenes[i], ibls[i], _cam(hosts[i]), 256, 256, 4)[0] for i in (0, 1)]
     st = srv.autotune(samples, seconds=5.0)
-    assert st["path_pool"] in (1 << 20, 1 << 21, 1 << 22)
+    assert st["path_pool"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
     assert st["trace_threads"] in (64, 128, 256) and st["shade_threads"] in (64, 128, 256)
     r = _requests(world)[0]
     img, info = srv.wait(_submit(srv, world, r))
