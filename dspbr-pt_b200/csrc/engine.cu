@@ -236,14 +236,13 @@ int Engine::one_iteration(bool counting) {
   launch_connect(sc, b, cur, counting, lc_, stream_);
   mark_end();
   mark_begin(2);
-  launch_shade_miss(sc, b, lc_, stream_);
   launch_shade(sc, b, cur ^ 1, lc_, stream_);
   launch_regen(sc, b, cur ^ 1, stream_);
   launch_commit(sc, b, cur, stream_);
   mark_end();
   kind_launches[0] += 1;
   kind_launches[1] += 1;
-  kind_launches[2] += 4;
+  kind_launches[2] += 3;
   cur_ ^= 1;
   return Status{err_}.cuda(cudaGetLastError(), "render launch");
 }
@@ -301,7 +300,6 @@ int Engine::capture_loop_graph() {
   if (e != cudaSuccess) return fail(e, "loop body capture");
   for (int cur = 0; cur < 2; ++cur) {
     extend_and_connect(sc, b, cur);
-    launch_shade_miss(sc, b, lc_, stream_);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     if (cur == 0) launch_commit(sc, b, cur, stream_);
@@ -366,7 +364,7 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
   const unsigned long long body = hs->iteration - it0 - 1 - eager;
   kind_launches[0] += body;
   kind_launches[1] += body + 1;
-  kind_launches[2] += 4 * body;
+  kind_launches[2] += 3 * body;
   kind_launches[3] += 3;
   cur_ = 0;  // the tail drained every path: both queues are empty
   if (job_done(slot)) return DSPBR_OK;
@@ -384,7 +382,6 @@ int Engine::capture_graph() {
   TRY_CUDA(s, cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "graph capture");
   for (int cur = 0; cur < 2; ++cur) {
     extend_and_connect(sc, b, cur);
-    launch_shade_miss(sc, b, lc_, stream_);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     launch_commit(sc, b, cur, stream_);
@@ -416,7 +413,7 @@ int Engine::iterate(int n, bool counting, int* done) {
       TRY_CUDA(s, cudaGraphLaunch(graph_, stream_), "graph launch");
       kind_launches[0] += 2;
       kind_launches[1] += 2;
-      kind_launches[2] += 8;
+      kind_launches[2] += 6;
       k += 2;
     } else {
       int rc = one_iteration(counting);

@@ -312,7 +312,6 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
     b.counts[kCntFetchExt] = 0;
     b.counts[kCntFetchShadow] = 0;
     b.counts[kCntFetchShade] = 0;
-    b.counts[kCntFetchMiss] = 0;
   }
   if (t < kNumClasses) b.counts[kCntHit0 + t] = 0;
   // status for the host (mapped memory)
@@ -577,25 +576,6 @@ DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot) {
   finish_path(J, ps.pixel, clamp_result(p, L));
 }
 
-__global__ void __launch_bounds__(256) k_shade_miss(Sched sc, PathBuf b) {
-  __shared__ uint32_t freed[256 / 32][kFreeBuf];
-  WarpFree wf;
-  wf.init(freed[threadIdx.x >> 5]);
-  const uint32_t count = b.counts[kCntMiss];
-  uint32_t i;
-  bool first = true;
-  while (next_warp_batch(b.counts + kCntFetchMiss, count, i, first)) {
-    uint32_t slot = 0;
-    uint32_t job = 0;
-    if (i < count) {
-      slot = b.qm[i];
-      job = __float_as_uint(b.st[slot].dir.w);
-      shade_miss_path(sc, b, slot);
-    }
-    wf.add(sc, b, i < count, slot, job);
-  }
-  wf.flush(sc, b);
-}
 
 // Surface hit.  Returns true if the path continues with an extension ray and
 // sets `shadow` when NEE shadow rays were emitted; otherwise the path's sample
@@ -711,8 +691,10 @@ template <bool kTextured>
 // 5 blocks of 128 threads per SM (96 registers, some spilled): of 3..8 blocks
 // per SM the fastest frames (3: 168 registers, no spills; 4 and 6..8 slower)
 __global__ void __launch_bounds__(128, 5) k_shade(Sched sc, PathBuf b, int next) {
-  // the class queues, read as one sequence in class order
-  __shared__ uint32_t start[kNumClasses + 1];
+  // the class queues, then the miss queue, read as one sequence: the misses
+  // (environment, background) are shaded by the same persistent warps after
+  // the surface hits, with no launch of their own
+  __shared__ uint32_t start[kNumClasses + 2];
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
     for (int k = 0; k < kNumClasses; ++k) {
@@ -720,9 +702,11 @@ __global__ void __launch_bounds__(128, 5) k_shade(Sched sc, PathBuf b, int next)
       acc += b.counts[kCntHit0 + k];
     }
     start[kNumClasses] = acc;
+    start[kNumClasses + 1] = acc + b.counts[kCntMiss];
   }
   __syncthreads();
-  const uint32_t count = start[kNumClasses];
+  const uint32_t hits = start[kNumClasses];
+  const uint32_t count = start[kNumClasses + 1];
   uint32_t* qn = b.q[next];
   uint32_t* cn = b.counts + next;
   __shared__ uint32_t freed[128 / 32][kFreeBuf];
@@ -733,13 +717,17 @@ __global__ void __launch_bounds__(128, 5) k_shade(Sched sc, PathBuf b, int next)
   while (next_warp_batch(b.counts + kCntFetchShade, count, i, first)) {
     bool cont = false, shadow = false;
     uint32_t slot = 0, job = 0;
-    if (i < count) {
+    if (i < hits) {
       int k = 0;
 #pragma unroll
       for (int jk = 1; jk < kNumClasses; ++jk) k += i >= start[jk] ? 1 : 0;
       slot = b.qh[size_t(k) * b.capacity + (i - start[k])];
       job = __float_as_uint(b.st[slot].dir.w);
       cont = shade_path<kTextured>(sc, b, slot, shadow);
+    } else if (i < count) {
+      slot = b.qm[i - hits];
+      job = __float_as_uint(b.st[slot].dir.w);
+      shade_miss_path(sc, b, slot);
     }
     enqueue(qn, cn, cont, slot);
     enqueue(b.qs[next], b.counts + kCntShadow0 + next, shadow, slot);
@@ -985,7 +973,6 @@ void init_launch_sizes(LaunchCfg& lc) {
   lc.dyn_blocks = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
   lc.shade_dyn_blocks[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 5);
   lc.shade_dyn_blocks[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 5);
-  lc.miss_dyn_blocks = resident(reinterpret_cast<const void*>(k_shade_miss), 256, 6);
 }
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
@@ -1025,9 +1012,6 @@ void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& 
 void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st) {
   if (lc.textured) k_drain<true><<<148 * 4, 128, 0, st>>>(sc, b, cur);
   else k_drain<false><<<148 * 4, 128, 0, st>>>(sc, b, cur);
-}
-void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st) {
-  k_shade_miss<<<lc.miss_dyn_blocks, 256, 0, st>>>(sc, b);
 }
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st) {
   k_mean<<<grid_for(npix, 256, 148 * 8), 256, 0, st>>>(accum, inv_count, out, npix);

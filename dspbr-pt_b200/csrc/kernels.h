@@ -74,7 +74,6 @@ enum : int {
   kCntFetchShadow = 6,  // next qs[cur] entry a k_connect warp starts
   kCntHit0 = 8,     // paths whose extension ray hit a triangle, one queue per shading class
   kCntFetchShade = 24,  // next hit-queue entry a k_shade warp starts
-  kCntFetchMiss = 25,   // next miss-queue entry a k_shade_miss warp starts
   kCntNum = 32
 };
 constexpr int kNumClasses = 16;
@@ -165,7 +164,6 @@ struct LaunchCfg {
   int dyn_blocks = 148 * 8;  // k_extend / k_connect: resident blocks of 128 threads (64 registers)
   // resident blocks of the persistent shading kernels (set by init_launch_sizes)
   int shade_dyn_blocks[2] = {148 * 5, 148 * 5};  // k_shade<false>, k_shade<true>, 128 threads
-  int miss_dyn_blocks = 148 * 6;                 // k_shade_miss, 256 threads
 };
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
@@ -175,7 +173,6 @@ void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st);
-void launch_shade_miss(const Sched& sc, const PathBuf& b, const LaunchCfg& lc, cudaStream_t st);
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
 
 // Device-side loop control of a render call run as one graph: after each pair
