@@ -694,10 +694,12 @@ int dspbr_resize(dspbr_ctx* c, int w, int h) {
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "resize");
+  // the image buffers only grow: a viewport that changes size request by
+  // request keeps its allocations (a fresh cudaMalloc of tens of MB after
+  // other allocations were freed costs milliseconds)
   size_t npix = size_t(w) * h;
-  TRY_CUDA(s, c->accum.alloc(npix), "alloc accumulation");
-  TRY_CUDA(s, c->mean.alloc(npix), "alloc readback");
-  c->display.reset();
+  if (c->accum.n < npix) TRY_CUDA(s, c->accum.alloc(npix), "alloc accumulation");
+  if (c->mean.n < npix) TRY_CUDA(s, c->mean.alloc(npix), "alloc readback");
   c->width = w;
   c->height = h;
   return dspbr_reset(c);
@@ -710,7 +712,8 @@ int dspbr_reset(dspbr_ctx* c) {
   c->sample_count = 0;
   if (c->accum.p) {
     TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-    TRY_CUDA(s, cudaMemsetAsync(c->accum.p, 0, c->accum.bytes(), c->stream), "clear accumulation");
+    TRY_CUDA(s, cudaMemsetAsync(c->accum.p, 0, size_t(c->width) * c->height * sizeof(double4), c->stream),
+             "clear accumulation");
   }
   return DSPBR_OK;
 }
@@ -911,7 +914,7 @@ static int display_pass(dspbr_ctx* c, const dspbr_display* d, bool bytes8, void*
   if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_display: no image");
   if (!(d->exposure == d->exposure)) return s.fail(DSPBR_ERR_INVALID, "read_display: exposure is NaN");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  if (!c->display.p) TRY_CUDA(s, c->display.alloc(npix), "alloc display buffer");
+  if (c->display.n < npix) TRY_CUDA(s, c->display.alloc(npix), "alloc display buffer");
   DisplayParams p;
   p.exposure = d->exposure;
   p.mode = d->tonemapping;

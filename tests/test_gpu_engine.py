@@ -52,3 +52,26 @@ def test_timeline_of_a_render_call():
     assert len(tl) >= 2
     assert (np.diff(tl[:, 0]) == 1).all() and (np.diff(tl[:, 1]) >= 0).all()
     assert tl[-1, 2] == 0  # the tail left no path
+
+
+def test_resize_keeps_larger_buffers_and_images_match_a_fresh_viewport():
+    """A viewport that grows, then shrinks, keeps its image buffers (they only
+    grow) and renders what a viewport created at each size renders."""
+    sizes = [(96, 64), (160, 100), (48, 32)]
+    v = _viewport({"maxBounces": 8})
+    got, disp = [], []
+    for w, h in sizes:
+        v.resize(w, h)
+        v.start(3)
+        got.append(v.readAccumulation().copy())
+        disp.append(v.readDisplay().copy())
+    v.dispose()
+    for (w, h), img, d in zip(sizes, got, disp):
+        f = _viewport({"maxBounces": 8})
+        f.resize(w, h)
+        f.start(3)
+        assert img.shape[:2] == (h, w)
+        # samples of one pixel are summed by atomics in completion order
+        np.testing.assert_allclose(img, f.readAccumulation(), rtol=1e-6, atol=1e-7)
+        assert np.abs(d.astype(np.int16) - f.readDisplay().astype(np.int16)).max() <= 1
+        f.dispose()
