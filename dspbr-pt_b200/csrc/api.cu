@@ -247,7 +247,10 @@ int dspbr_create(int device, dspbr_ctx** out) {
   dspbr_params_default(&c->params);
   Status s = c->st();
   if (s.cuda(cudaSetDevice(device), "cudaSetDevice") || s.cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream") ||
-      s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event")) {
+      s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event") ||
+      s.cuda(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "stream") ||
+      s.cuda(cudaEventCreateWithFlags(&c->ev_mean, cudaEventDisableTiming), "event") ||
+      s.cuda(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming), "event")) {
     dspbr_destroy(c);
     return DSPBR_ERR_CUDA;
   }
@@ -265,10 +268,14 @@ int dspbr_destroy(dspbr_ctx* c) {
   settle(c);
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->ev_mean) cudaEventDestroy(c->ev_mean);
+  if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   c->eng.reset();
   if (c->stage) cudaFreeHost(c->stage);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DSPBR_OK;
@@ -694,6 +701,7 @@ int dspbr_resize(dspbr_ctx* c, int w, int h) {
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   TRY_CUDA(s, cudaStreamSynchronize(c->stream), "resize");
+  { int rc_ = dspbr_read_wait(c); if (rc_) return rc_; }  // a pending copy reads the mean buffer
   // the image buffers only grow: a viewport that changes size request by
   // request keeps its allocations (a fresh cudaMalloc of tens of MB after
   // other allocations were freed costs milliseconds)
@@ -871,6 +879,12 @@ static void parallel_copy(void* dst, const void* src, size_t bytes) {
 
 // Device-to-host copy of a result: one DMA into page-locked memory, else
 // through the context's page-locked staging buffer and a parallel host copy.
+// A copy of read_accum_async still reading the mean buffer: the stream's
+// next writes to it wait for that copy.
+static cudaError_t after_pending_copy(dspbr_ctx* c) {
+  return c->copy_pending ? cudaStreamWaitEvent(c->stream, c->ev_copied, 0) : cudaSuccess;
+}
+
 static int copy_out(dspbr_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
   Status s = c->st();
   cudaPointerAttributes attr{};
@@ -903,8 +917,44 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_accum: no image");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
+  TRY_CUDA(s, after_pending_copy(c), "read accumulation");
   launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
   return copy_out(c, rgba, c->mean.p, npix * 16, "read accumulation");
+}
+
+int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
+  if (!c || !rgba) return DSPBR_ERR_INVALID;
+  { int rc_ = settle(c); if (rc_) return rc_; }
+  Status s = c->st();
+  size_t npix = size_t(c->width) * c->height;
+  if (num_floats < npix * 4)
+    return s.fail(DSPBR_ERR_INVALID, "read_accum_async: buffer holds %zu floats, need %zu", num_floats, npix * 4);
+  if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_accum_async: no image");
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();
+  if (!pinned) return s.fail(DSPBR_ERR_INVALID, "read_accum_async: the buffer is not page-locked (dspbr_host_alloc)");
+  double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
+  TRY_CUDA(s, after_pending_copy(c), "read accumulation");
+  launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
+  TRY_CUDA(s, cudaGetLastError(), "read accumulation");
+  TRY_CUDA(s, cudaEventRecord(c->ev_mean, c->stream), "event");
+  TRY_CUDA(s, cudaStreamWaitEvent(c->copy_stream, c->ev_mean, 0), "read accumulation");
+  TRY_CUDA(s, cudaMemcpyAsync(rgba, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->copy_stream), "read accumulation");
+  TRY_CUDA(s, cudaEventRecord(c->ev_copied, c->copy_stream), "event");
+  c->copy_pending = true;
+  return DSPBR_OK;
+}
+
+int dspbr_read_wait(dspbr_ctx* c) {
+  if (!c) return DSPBR_ERR_INVALID;
+  if (!c->copy_pending) return DSPBR_OK;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  c->copy_pending = false;
+  TRY_CUDA(s, cudaEventSynchronize(c->ev_copied), "read accumulation");
+  return DSPBR_OK;
 }
 
 // tonemap (+ FXAA) of the running mean into `out` (float4 or uchar4 per pixel)
@@ -915,6 +965,7 @@ static int display_pass(dspbr_ctx* c, const dspbr_display* d, bool bytes8, void*
   if (!(d->exposure == d->exposure)) return s.fail(DSPBR_ERR_INVALID, "read_display: exposure is NaN");
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   if (c->display.n < npix) TRY_CUDA(s, c->display.alloc(npix), "alloc display buffer");
+  TRY_CUDA(s, after_pending_copy(c), "read display");  // the mean buffer is the epilogue's scratch
   DisplayParams p;
   p.exposure = d->exposure;
   p.mode = d->tonemapping;
@@ -1054,8 +1105,7 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   std::memset(d, 0, sizeof *d);
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  TRY_CUDA(s, cudaMemcpyAsync(st, c->eng->stats(), sizeof st, cudaMemcpyDeviceToHost, c->stream), "read stats");
-  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "read stats");
+  if (int rc = c->eng->read_stats(st)) return rc;
   d->sample_count = c->sample_count;
   d->width = c->width;
   d->height = c->height;

@@ -33,6 +33,12 @@ __global__ void k_set_active(ActiveList list, int* active) {
 }
 
 // Cancel: no further work items start; paths in flight finish normally.
+// The ray counters into mapped host memory by one warp: a copy-engine
+// transfer would queue behind a pending device-to-host copy of an image.
+__global__ void k_read_stats(const unsigned long long* stats, HostStatus* out) {
+  if (threadIdx.x < 8) out->stats[threadIdx.x] = stats[threadIdx.x];
+}
+
 __global__ void k_cancel_job(int slot, JobState* js) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   if (js[slot].items_total > js[slot].items_next) js[slot].items_total = js[slot].items_next;
@@ -422,6 +428,16 @@ int Engine::iterate(int n, bool counting, int* done) {
     }
   }
   if (done) *done = k;
+  return DSPBR_OK;
+}
+
+int Engine::read_stats(unsigned long long out[8]) {
+  Status s{err_};
+  k_read_stats<<<1, 32, 0, stream_>>>(stats_.p, d_status_);
+  ++kind_launches[3];
+  TRY_CUDA(s, cudaGetLastError(), "read stats");
+  TRY_CUDA(s, cudaStreamSynchronize(stream_), "read stats");
+  for (int i = 0; i < 8; ++i) out[i] = h_status_->stats[i];
   return DSPBR_OK;
 }
 

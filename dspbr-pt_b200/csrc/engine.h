@@ -73,6 +73,8 @@ class Engine {
   void clear_marks();
 
   unsigned long long* stats() const { return stats_.p; }
+  // the eight ray counters, read through the mapped status record (no copy engine)
+  int read_stats(unsigned long long out[8]);
   Sched sched() const;
   PathBuf paths() const;
   cudaStream_t stream() const { return stream_; }

@@ -59,6 +59,7 @@ struct HostStatus {
   unsigned int live_paths;          // paths queued for the next extend
   unsigned int nactive;
   JobStatus job[kMaxJobs];          // by job slot
+  unsigned long long stats[8];      // ray counters, stored on request (Engine::read_stats)
 };
 
 // Queue counters (uint32 slots of PathBuf::counts).  Iteration i works on

@@ -108,6 +108,10 @@ struct dspbr_ctx {
   dspbr::DevBuf<float4> display;  // display epilogue output (allocated on first use)
   float* stage = nullptr;  // page-locked staging for readback into pageable memory
   size_t stage_bytes = 0;
+  // read_accum_async: the mean is computed on `stream`, copied on `copy_stream`
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_mean = nullptr, ev_copied = nullptr;
+  bool copy_pending = false;
   uint64_t sample_count = 0;
   uint64_t rays_primary = 0;
   double last_render_ms = 0;

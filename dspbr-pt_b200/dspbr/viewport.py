@@ -428,6 +428,21 @@ class PathtracingViewport:
         self.ctx.check(self.ctx.lib.dspbr_read_accum(self.ctx.h, fptr(out), out.size))
         return out
 
+    def readAccumulationAsync(self, out: np.ndarray) -> np.ndarray:
+        """Pipelined readAccumulation into `out` (from allocReadbackBuffer():
+        page-locked, (height, width, 4) float32): enqueues the mean and its
+        copy and returns; the next start() overlaps the copy.  `out` holds
+        the image after readWait()."""
+        shape = (self.height, self.width, 4)
+        if out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError(f"readAccumulationAsync: out must be a C-contiguous float32 array of shape {shape}")
+        self.ctx.check(self.ctx.lib.dspbr_read_accum_async(self.ctx.h, fptr(out), out.size))
+        return out
+
+    def readWait(self) -> None:
+        """Waits for the copies of readAccumulationAsync."""
+        self.ctx.check(self.ctx.lib.dspbr_read_wait(self.ctx.h))
+
     def readDisplay(self, rgba8: bool = True) -> np.ndarray:
         """The presented frame: the running mean through the reference's
         tone-mapping / gamma / FXAA passes with the viewport's display

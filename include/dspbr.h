@@ -210,6 +210,14 @@ int dspbr_wait(dspbr_ctx* ctx);
 /* readAccumulation (absent in the reference, which only displays): running
  * mean RGBA32F, width*height*4 floats, row 0 = bottom row (gl_FragCoord.y 0.5). */
 int dspbr_read_accum(dspbr_ctx* ctx, float* rgba, size_t num_floats);
+/* Pipelined readAccumulation: enqueues the running mean of the frames rendered
+ * so far and its device-to-host copy (on a copy stream of the context), and
+ * returns.  The next render can start at once and overlaps the copy.  `rgba`
+ * is page-locked (dspbr_host_alloc; else DSPBR_ERR_INVALID) and is complete
+ * when dspbr_read_wait returns.  Later calls that write the mean (another
+ * read, a display read, a resize) are ordered after the pending copy. */
+int dspbr_read_accum_async(dspbr_ctx* ctx, float* rgba, size_t num_floats);
+int dspbr_read_wait(dspbr_ctx* ctx);
 /* Display epilogue (renderer.ts:666-700): the accumulation mean through
  * tonemap.frag (exposure, operator, gamma) and optionally fxaa.frag -- the
  * reference's "postprocess" buffer -- as RGBA32F, or converted to the 8-bit

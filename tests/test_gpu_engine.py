@@ -75,3 +75,30 @@ def test_resize_keeps_larger_buffers_and_images_match_a_fresh_viewport():
         np.testing.assert_allclose(img, f.readAccumulation(), rtol=1e-6, atol=1e-7)
         assert np.abs(d.astype(np.int16) - f.readDisplay().astype(np.int16)).max() <= 1
         f.dispose()
+
+
+def test_async_readback_overlapping_the_next_render():
+    """read_accum_async: the mean of the frames rendered before the call,
+    bit-equal to read_accum, although the next render runs during the copy;
+    a read that follows is ordered after the pending copy; pageable memory is
+    refused."""
+    v = _viewport({"maxBounces": 8})
+    v.start(3)
+    ref3 = v.readAccumulation()
+    bufs = [v.allocReadbackBuffer(), v.allocReadbackBuffer()]
+    v.readAccumulationAsync(bufs[0])
+    v.start(5)  # two more frames while the copy runs
+    ref5 = v.readAccumulation()  # writes the mean buffer after the pending copy
+    v.readWait()
+    np.testing.assert_array_equal(bufs[0], ref3)
+    v.readAccumulationAsync(bufs[1])
+    v.readAccumulationAsync(bufs[0])  # a second pending copy of the same frames
+    v.readWait()
+    np.testing.assert_array_equal(bufs[1], ref5)
+    np.testing.assert_array_equal(bufs[0], ref5)
+    with pytest.raises(RuntimeError):
+        v.readAccumulationAsync(np.empty_like(ref5))
+    v.readAccumulationAsync(bufs[1])
+    v.resize(48, 32)  # waits for the copy before the buffers can change
+    np.testing.assert_array_equal(bufs[1], ref5)
+    v.dispose()
