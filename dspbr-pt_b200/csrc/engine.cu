@@ -274,10 +274,28 @@ void Engine::drop_graph() {
   loop_graph_ = nullptr;
 }
 
-// while (cond) { iteration(0); iteration(1) + loop decision }; connect(0);
-// drain(0); commit(0).  The condition starts at 1 on every launch; the
-// commit kernel of the second iteration sets it (kernels.cu, k_commit), and
-// LoopCtl::pairs_left bounds the number of pairs.
+// Nodes of `g` that no other node depends on.
+static cudaError_t graph_sinks(cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+  size_t n = 0;
+  cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+  if (e != cudaSuccess) return e;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if ((e = cudaGraphGetNodes(g, nodes.data(), &n)) != cudaSuccess) return e;
+  for (size_t i = 0; i < n; ++i) {
+    size_t k = 0;
+    if ((e = cudaGraphNodeGetDependentNodes(nodes[i], nullptr, &k)) != cudaSuccess) return e;
+    if (k == 0) out.push_back(nodes[i]);
+  }
+  return cudaSuccess;
+}
+
+// while (loop) { iteration(0); if (second) iteration(1) }; if (tail[1])
+// { connect(1); drain(1); commit(1) }; if (tail[0]) { connect(0); drain(0);
+// commit(0) }.  The loop condition starts at 1 on every launch; each
+// iteration's commit (kernels.cu, k_commit) decides whether the next one
+// runs, so the tail starts after the first iteration that leaves fewer than
+// the drain threshold of paths, at either parity.  LoopCtl::iters_left
+// bounds the number of iterations.
 int Engine::capture_loop_graph() {
   Status s{err_};
   const Sched sc = sched();
@@ -290,37 +308,66 @@ int Engine::capture_loop_graph() {
     cudaGetLastError();
     return s.cuda(e, what);
   };
-  cudaGraphConditionalHandle h;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+  // handles: the while loop (entered), iteration B's IF (set by A), one IF
+  // per tail parity (set by the commit that stops the loop)
+  cudaGraphConditionalHandle h_loop, h_second, h_tail[2];
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h_loop, g, 1u, cudaGraphCondAssignDefault);
+  for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+    e = cudaGraphConditionalHandleCreate(&h_tail[k], g, 0u, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return fail(e, "loop graph condition");
-  cudaGraphNodeParams cp = {};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t loop_node;
-  e = cudaGraphAddNode(&loop_node, g, nullptr, 0, &cp);
-  if (e != cudaSuccess) return fail(e, "loop graph node");
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return fail(e, "loop body capture");
-  for (int cur = 0; cur < 2; ++cur) {
+  auto add_cond = [&](cudaGraph_t parent, const cudaGraphNode_t* deps, size_t ndeps, cudaGraphConditionalHandle h,
+                      cudaGraphConditionalNodeType type, cudaGraphNode_t& node, cudaGraph_t& body) {
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaError_t r = cudaGraphAddNode(&node, parent, deps, ndeps, &cp);
+    if (r == cudaSuccess) body = cp.conditional.phGraph_out[0];
+    return r;
+  };
+  auto iteration = [&](int cur, const LoopHandles& lh) {
     extend_and_connect(sc, b, cur);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
-    if (cur == 0) launch_commit(sc, b, cur, stream_);
-    else launch_commit_loop(sc, b, cur, h, loop_ctl_.p, stream_);
-  }
+    launch_commit_loop(sc, b, cur, lh, loop_ctl_.p, stream_);
+  };
+  cudaGraphNode_t loop_node, second_node, tail_node[2];
+  cudaGraph_t body = nullptr, body_b = nullptr, tail_body[2] = {nullptr, nullptr};
   cudaGraph_t captured = nullptr;
+  e = add_cond(g, nullptr, 0, h_loop, cudaGraphCondTypeWhile, loop_node, body);
+  if (e != cudaSuccess) return fail(e, "loop graph node");
+  e = cudaGraphConditionalHandleCreate(&h_second, body, 0u, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return fail(e, "loop graph condition");
+  // iteration A (parity 0)
+  e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(e, "loop body capture");
+  iteration(0, LoopHandles{h_loop, h_second, h_tail[1], 1});
   e = cudaStreamEndCapture(stream_, &captured);
   if (e != cudaSuccess) return fail(e, "loop body capture");
-  e = cudaStreamBeginCaptureToGraph(stream_, g, &loop_node, nullptr, 1, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return fail(e, "loop tail capture");
-  launch_connect(sc, b, 0, false, lc_, stream_);
-  launch_drain(sc, b, 0, lc_, stream_);
-  launch_commit(sc, b, 0, stream_, false);
+  // iteration B (parity 1) after A's commit, the only node of the body without dependents
+  std::vector<cudaGraphNode_t> sinks;
+  if ((e = graph_sinks(body, sinks)) != cudaSuccess) return fail(e, "loop body");
+  e = add_cond(body, sinks.data(), sinks.size(), h_second, cudaGraphCondTypeIf, second_node, body_b);
+  if (e != cudaSuccess) return fail(e, "loop graph node");
+  e = cudaStreamBeginCaptureToGraph(stream_, body_b, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return fail(e, "loop body capture");
+  iteration(1, LoopHandles{h_loop, cudaGraphConditionalHandle(0), h_tail[0], 0});
   e = cudaStreamEndCapture(stream_, &captured);
-  if (e != cudaSuccess) return fail(e, "loop tail capture");
+  if (e != cudaSuccess) return fail(e, "loop body capture");
+  // the tails: connect, drain and commit of the parity the loop stopped at
+  for (int k = 0; k < 2; ++k) {
+    const cudaGraphNode_t dep = k == 0 ? loop_node : tail_node[0];
+    e = add_cond(g, &dep, 1, h_tail[k], cudaGraphCondTypeIf, tail_node[k], tail_body[k]);
+    if (e != cudaSuccess) return fail(e, "loop graph node");
+    e = cudaStreamBeginCaptureToGraph(stream_, tail_body[k], nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(e, "loop tail capture");
+    launch_connect(sc, b, k, false, lc_, stream_);
+    launch_drain(sc, b, k, lc_, stream_);
+    launch_commit(sc, b, k, stream_, false);
+    e = cudaStreamEndCapture(stream_, &captured);
+    if (e != cudaSuccess) return fail(e, "loop tail capture");
+  }
   e = cudaGraphInstantiate(&loop_graph_, g, 0);
   cudaGraphDestroy(g);
   g = nullptr;
@@ -362,7 +409,7 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
     int rc = capture_loop_graph();
     if (rc) return rc;
   }
-  launch_set_loop(loop_ctl_.p, (max_iter + 1) / 2, drain_below_, stream_);
+  launch_set_loop(loop_ctl_.p, max_iter, drain_below_, stream_);
   TRY_CUDA(s, cudaGetLastError(), "loop control");
   TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
   TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");

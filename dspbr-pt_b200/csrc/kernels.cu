@@ -286,8 +286,8 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
 // ---- commit: book-keeping of one iteration (one block of kMaxJobs threads) -----------------
 // regen_ran = false (after a drain): no work item was handed out, only the
 // counters and the status are updated.
-__global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cur, int regen_ran,
-                                                     cudaGraphConditionalHandle loop, LoopCtl* ctl) {
+__global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cur, int regen_ran, LoopHandles lh,
+                                                     LoopCtl* ctl) {
   __shared__ unsigned long long scan[kMaxJobs];
   const int n = min(*sc.nactive, kMaxJobs);
   int j;
@@ -342,19 +342,25 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
     te.live = live;
     te.pad = 0;
     sc.timeline[it % kTimeline] = te;
-    if (ctl) {  // the render loop's next pair of iterations, or the tail
+    if (ctl) {  // the render loop's next iteration, or the tail
       const bool started = total <= avail;  // the regen that just ran placed every remaining work item
-      const unsigned long long pairs = ctl->pairs_left;
-      const bool go = pairs > 1 && !(started && live < ctl->drain_below);
-      ctl->pairs_left = pairs ? pairs - 1 : 0;
-      cudaGraphSetConditional(loop, go ? 1u : 0u);
+      const unsigned long long left = ctl->iters_left;
+      const bool go = left > 1 && !(started && live < ctl->drain_below);
+      ctl->iters_left = left ? left - 1 : 0;
+      if (lh.first) {
+        cudaGraphSetConditional(lh.second, go ? 1u : 0u);
+        if (!go) cudaGraphSetConditional(lh.loop, 0u);
+      } else {
+        cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
+      }
+      if (!go) cudaGraphSetConditional(lh.tail, 1u);
     }
   }
 }
 
-__global__ void k_set_loop(LoopCtl* ctl, unsigned long long pairs, unsigned long long drain_below) {
+__global__ void k_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    ctl->pairs_left = pairs;
+    ctl->iters_left = iterations;
     ctl->drain_below = drain_below;
   }
 }
@@ -982,14 +988,14 @@ void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st) 
   k_regen<<<grid_for(b.capacity, kMaxJobs, 148 * 8), kMaxJobs, 0, st>>>(sc, b, next);
 }
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran) {
-  k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur, regen_ran ? 1 : 0, cudaGraphConditionalHandle(0), nullptr);
+  k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur, regen_ran ? 1 : 0, LoopHandles{}, nullptr);
 }
-void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, cudaGraphConditionalHandle h, LoopCtl* ctl,
+void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, const LoopHandles& h, LoopCtl* ctl,
                         cudaStream_t st) {
   k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur, 1, h, ctl);
 }
-void launch_set_loop(LoopCtl* ctl, unsigned long long pairs, unsigned long long drain_below, cudaStream_t st) {
-  k_set_loop<<<1, 32, 0, st>>>(ctl, pairs, drain_below);
+void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, cudaStream_t st) {
+  k_set_loop<<<1, 32, 0, st>>>(ctl, iterations, drain_below);
 }
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);

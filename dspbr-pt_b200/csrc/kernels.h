@@ -176,16 +176,24 @@ void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, cons
 void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& lc, cudaStream_t st);
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
 
-// Device-side loop control of a render call run as one graph: after each pair
-// of iterations k_commit keeps the loop going while pairs remain and either a
-// work item has not started or at least drain_below paths are alive.
+// Device-side loop control of a render call run as one graph.  The loop body
+// is iteration A (parity 0), then iteration B (parity 1) under an IF node;
+// after each iteration k_commit keeps going while iterations remain and either
+// a work item has not started or at least drain_below paths are alive.  The
+// commit that stops selects the tail of its parity (an IF node each).
 struct LoopCtl {
-  unsigned long long pairs_left;
+  unsigned long long iters_left;
   unsigned long long drain_below;
 };
-void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, cudaGraphConditionalHandle h, LoopCtl* ctl,
+struct LoopHandles {
+  cudaGraphConditionalHandle loop;    // the while node
+  cudaGraphConditionalHandle second;  // iteration B's IF node (set by A)
+  cudaGraphConditionalHandle tail;    // the IF node of the tail that follows this iteration
+  int first;                          // 1: iteration A
+};
+void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, const LoopHandles& h, LoopCtl* ctl,
                         cudaStream_t st);
-void launch_set_loop(LoopCtl* ctl, unsigned long long pairs, unsigned long long drain_below, cudaStream_t st);
+void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, cudaStream_t st);
 // runs every path queued in q[cur] to its end (call after connect(cur), when no work item is left)
 void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);
