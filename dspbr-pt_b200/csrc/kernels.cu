@@ -857,10 +857,13 @@ __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
   }
 }
 
+// Streaming (evict-first) loads and stores: the 48 bytes per pixel it moves
+// would otherwise push the scene's BVH out of L2 before the next frame.
 __global__ void k_mean(const double4* accum, double inv, float4* out, int npix) {
+  const double2* a2 = reinterpret_cast<const double2*>(accum);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
-    double4 a = accum[i];
-    out[i] = make_float4(float(a.x * inv), float(a.y * inv), float(a.z * inv), float(a.w * inv));
+    const double2 lo = __ldcs(a2 + 2 * size_t(i)), hi = __ldcs(a2 + 2 * size_t(i) + 1);
+    __stcs(out + i, make_float4(float(lo.x * inv), float(lo.y * inv), float(hi.x * inv), float(hi.y * inv)));
   }
 }
 

@@ -102,3 +102,29 @@ def test_async_readback_overlapping_the_next_render():
     v.resize(48, 32)  # waits for the copy before the buffers can change
     np.testing.assert_array_equal(bufs[1], ref5)
     v.dispose()
+
+
+def _one_frame(threshold):
+    v = _viewport({"maxBounces": 8})
+    v.ctx.check(v.ctx.lib.dspbr_set_drain_threshold(v.ctx.h, int(threshold)))
+    v.start(1)
+    tl = v.timeline(1024)
+    img = v.readAccumulation()
+    v.dispose()
+    return img, tl
+
+
+def test_tail_after_an_iteration_of_either_parity():
+    """The render loop graph stops after whichever iteration first leaves
+    fewer live paths than the drain threshold, and runs the tail of that
+    iteration's parity; one sample per pixel, so the image is the same bits
+    whichever iteration the tail starts after."""
+    ref, tl = _one_frame(1)  # below 1 live path: no drain before the end
+    live = [int(x) for x in tl[:, 2]]
+    k = next(i for i in range(1, len(live) - 1) if live[i] > 0 and live[i + 1] > 0)
+    counts = []
+    for thr in (live[k] + 1, live[k + 1] + 1):  # the tail after iteration k, then k + 1
+        img, t = _one_frame(thr)
+        counts.append(len(t))
+        np.testing.assert_array_equal(img, ref)
+    assert counts[1] == counts[0] + 1  # consecutive iterations: both parities
