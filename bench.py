@@ -257,11 +257,19 @@ def _pct(v, q):
 
 def scene_build_section(local, sc, args):
     """Scene creation (BVH build, 4-wide collapse, upload) of the workload with
-    the host binned-SAH builder and the device LBVH builder, and the render
-    throughput over each tree."""
-    from dspbr.viewport import PathtracingCamera, PathtracingViewport
+    the host binned-SAH builder, the device binned-SAH builder and the device
+    LBVH builder, and the render throughput over each tree."""
+    from dspbr import synth
+    from dspbr.viewport import Context, DeviceScene, PathtracingCamera, PathtracingViewport
     out = {}
-    for builder in ("host", "device"):
+    # process warm-up, untimed: each builder's first use loads its kernels
+    small = synth.make_small(0)
+    for builder in ("device", "device_lbvh"):
+        wc = Context(local)
+        wc.set_bvh_builder(builder)
+        DeviceScene(wc, small.vertices, small.indices, small.materials).close()
+        wc.close()
+    for builder in ("host", "device", "device_lbvh"):
         v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
                                 settings={"maxBounces": sc.max_bounces, "bvhBuilder": builder})
         scene = type(sc)(sc.name, sc.vertices, sc.indices, sc.materials, sc.camera, sc.width, sc.height,

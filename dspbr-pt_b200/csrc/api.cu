@@ -171,7 +171,10 @@ static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t
       (rc = s.cuda(cudaMemcpyAsync(sc->materials.p, materials, size_t(num_materials) * 272, cudaMemcpyHostToDevice, c->stream), "upload materials")))
     return rc;
   DeviceBvh bin;
-  if ((rc = build_bvh_device(sc->verts.p, sc->indices.p, sc->num_tris, c->stream, &bin, s))) return rc;
+  rc = c->bvh_builder == DSPBR_BVH_BUILD_DEVICE_LBVH
+           ? build_bvh_device(sc->verts.p, sc->indices.p, sc->num_tris, c->stream, &bin, s)
+           : build_bvh_device_sah(sc->verts.p, sc->indices.p, sc->num_tris, c->stream, &bin, s);
+  if (rc) return rc;
   DeviceWideBvh wide;
   if ((rc = collapse_bvh4_device(bin, c->stream, &wide, s))) return rc;
   sc->bvh_build_ms = now_ms() - t0;
@@ -308,7 +311,8 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
       return s.fail(DSPBR_ERR_INVALID, "scene: vertex %u references material %g of %u", v, m, num_materials);
   }
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
-  if ((!bvh_nodes || !bvh_indices) && c->bvh_builder == DSPBR_BVH_BUILD_DEVICE)
+  if ((!bvh_nodes || !bvh_indices) &&
+      (c->bvh_builder == DSPBR_BVH_BUILD_DEVICE || c->bvh_builder == DSPBR_BVH_BUILD_DEVICE_LBVH))
     return scene_create_device_bvh(c, vertices, num_vertices, indices, num_indices, materials, num_materials, out);
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   auto* sc = new dspbr_scene();
@@ -400,7 +404,9 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
 }
 
 int dspbr_set_bvh_builder(dspbr_ctx* c, int builder) {
-  if (!c || (builder != DSPBR_BVH_BUILD_HOST && builder != DSPBR_BVH_BUILD_DEVICE)) return DSPBR_ERR_INVALID;
+  if (!c || (builder != DSPBR_BVH_BUILD_HOST && builder != DSPBR_BVH_BUILD_DEVICE &&
+             builder != DSPBR_BVH_BUILD_DEVICE_LBVH))
+    return DSPBR_ERR_INVALID;
   c->bvh_builder = builder;
   return DSPBR_OK;
 }

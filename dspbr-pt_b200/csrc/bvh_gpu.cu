@@ -1,12 +1,14 @@
-// BVH construction on the device (linear BVH), emitting the reference's
-// binary node layout (bvh.glsl:1-6) so that every later stage -- the leaf
-// triangle gather, the 4-wide collapse, both traversals -- is unchanged.
+// BVH construction on the device, emitting the reference's binary node layout
+// (bvh.glsl:1-6) so that every later stage -- the leaf triangle gather, the
+// 4-wide collapse, both traversals -- is unchanged.  Two builders: the binned
+// SAH with the host builder's rules (build_bvh_device_sah, below) and a
+// linear BVH (build_bvh_device).
 //
 // The reference builds its BVH on the host with TinyBVH (tinybvh_builder.ts);
 // the host binned-SAH builder here (bvh_build.cpp) plays that role and is the
 // default.  For large scenes admitted while others render, a host build of
-// seconds dominates the time to the first frame, so this builder trades some
-// tree quality for speed:
+// seconds dominates the time to the first frame.  The linear BVH trades some
+// tree quality for the fastest build:
 //   1. per triangle: bounds and centroid; centroid bounds of the scene;
 //   2. 63-bit Morton codes of the centroids (21 bits per axis), sorted with
 //      the triangle index (CUB radix sort);
@@ -26,6 +28,7 @@
 #include <algorithm>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "bvh_gpu.h"
 #include "kernels.h"
@@ -582,6 +585,420 @@ int build_bvh_device(const float4* verts, const uint32_t* indices, uint32_t ntri
   TRY_CUDA(s, cudaStreamSynchronize(st), "device BVH");
   out->num_nodes = uint32_t(total);
   out->num_slots = uint32_t(n);
+  return DSPBR_OK;
+}
+
+// ---- binned SAH on the device, level by level ----------------------------------------------
+// The host builder's rules (bvh_build.cpp: 16 bins per centroid axis, SAH
+// with unit costs relative to the parent's area, a leaf when the SAH prefers
+// it at <= 8 triangles, a median split when the centroids coincide, depth
+// <= 56), evaluated for every open node of a level at once:
+//   1. binning: each triangle of an open node adds itself to its node's bins
+//      (count, box, centroid box per axis and bin) with integer atomics on
+//      order-preserving encodings of the floats (min / max are exact and
+//      independent of the order);
+//   2. one thread per open node evaluates the 3 x 15 candidate planes and
+//      decides leaf / split / median split;
+//   3. child ids: an exclusive scan over the level (2 per split node), so
+//      the ids and the tree do not depend on scheduling; the children of the
+//      k-th split node are consecutive and ordered like the parent ranges;
+//   4. a stable partition of every split node's range (an exclusive scan of
+//      goes-left flags over all slots) into the left and right child ranges.
+// Node records are written in the reference layout as nodes are decided.
+constexpr int kSahBins = 16;
+constexpr int kSahMaxLeaf = 8;
+constexpr int kSahMaxDepth = 56;
+constexpr int kBinWords = 13;  // count, box lo / hi, centroid lo / hi (encoded)
+
+__device__ __forceinline__ int f2o(float f) {  // order-preserving float -> int
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+struct SahNode {
+  float4 lo, hi;    // box
+  float4 clo, chi;  // centroid box
+  int begin, end;   // slot range
+  int depth, pad;
+};
+
+// the bin of centroid c along one axis of the centroid box [lo, lo + ext]
+__device__ __forceinline__ int sah_bin(float c, float lo, float ext) {
+  const int b = int((c - lo) * (float(kSahBins) / ext));
+  return min(kSahBins - 1, max(0, b));
+}
+
+__device__ __forceinline__ float comp(const float4& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ float sah_area(float lx, float ly, float lz, float hx, float hy, float hz) {
+  const float dx = fmaxf(0.f, hx - lx), dy = fmaxf(0.f, hy - ly), dz = fmaxf(0.f, hz - lz);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void k_sah_init(uint32_t n, int* __restrict__ bins, uint32_t nbins_words) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nbins_words; i += gridDim.x * blockDim.x) {
+    const uint32_t w = i % kBinWords;
+    bins[i] = w == 0 ? 0 : ((w - 1) % 6 < 3 ? 0x7fffffff : int(0x80000000));
+  }
+}
+
+// 1. binning of the triangles whose node is in the chunk [c_begin, c_end) of this level
+__global__ void k_sah_bin(uint32_t n, const uint32_t* __restrict__ order, const int* __restrict__ pnode,
+                          const float4* __restrict__ tlo, const float4* __restrict__ thi,
+                          const SahNode* __restrict__ nodes, int c_begin, int c_end, int* __restrict__ bins) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int v = pnode[s];
+    if (v < c_begin || v >= c_end) continue;
+    const SahNode nd = nodes[v];
+    const uint32_t t = order[s];
+    const float4 l = tlo[t], h = thi[t];
+    const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    int* nb = bins + size_t(v - c_begin) * (3 * kSahBins * kBinWords);
+    for (int a = 0; a < 3; ++a) {
+      const float lo = comp(nd.clo, a), ext = comp(nd.chi, a) - lo;
+      if (!(ext > 0.f)) continue;
+      int* w = nb + (a * kSahBins + sah_bin(c[a], lo, ext)) * kBinWords;
+      atomicAdd(w, 1);
+      atomicMin(w + 1, f2o(l.x)); atomicMin(w + 2, f2o(l.y)); atomicMin(w + 3, f2o(l.z));
+      atomicMax(w + 4, f2o(h.x)); atomicMax(w + 5, f2o(h.y)); atomicMax(w + 6, f2o(h.z));
+      atomicMin(w + 7, f2o(c[0])); atomicMin(w + 8, f2o(c[1])); atomicMin(w + 9, f2o(c[2]));
+      atomicMax(w + 10, f2o(c[0])); atomicMax(w + 11, f2o(c[1])); atomicMax(w + 12, f2o(c[2]));
+    }
+  }
+}
+
+// 2. decision per open node of one chunk [c_begin, c_end) of the level:
+// split[v - lvl_begin] = {axis (-1: leaf, 3: median), bin, left count}, and
+// for a split the two children's boxes (from the bins on each side of the
+// plane; a median split keeps the parent's boxes) in kids[2 (v - lvl_begin)].
+__global__ void k_sah_split(const SahNode* __restrict__ nodes, int lvl_begin, int c_begin, int c_end,
+                            const int* __restrict__ bins, int4* __restrict__ split, SahNode* __restrict__ kids,
+                            int* __restrict__ nkids) {
+  const int v = c_begin + int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (v >= c_end) return;
+  const SahNode nd = nodes[v];
+  const int n = nd.end - nd.begin;
+  const int* nb = bins + size_t(v - c_begin) * (3 * kSahBins * kBinWords);
+  int best_axis = -1, best_split = -1, best_left = 0;
+  float best_cost = 3.402823466e38f;
+  if (n > 1 && nd.depth < kSahMaxDepth) {
+    for (int a = 0; a < 3; ++a) {
+      if (!(comp(nd.chi, a) - comp(nd.clo, a) > 0.f)) continue;
+      const int* ab = nb + a * kSahBins * kBinWords;
+      float right_area[kSahBins];
+      int right_cnt[kSahBins];
+      float lx = 3.402823466e38f, ly = lx, lz = lx, hx = -lx, hy = -lx, hz = -lx;
+      int cnt = 0;
+      for (int b = kSahBins - 1; b > 0; --b) {
+        const int* w = ab + b * kBinWords;
+        if (w[0]) {
+          lx = fminf(lx, o2f(w[1])); ly = fminf(ly, o2f(w[2])); lz = fminf(lz, o2f(w[3]));
+          hx = fmaxf(hx, o2f(w[4])); hy = fmaxf(hy, o2f(w[5])); hz = fmaxf(hz, o2f(w[6]));
+        }
+        cnt += w[0];
+        right_area[b] = sah_area(lx, ly, lz, hx, hy, hz);
+        right_cnt[b] = cnt;
+      }
+      lx = 3.402823466e38f; ly = lx; lz = lx; hx = -lx; hy = -lx; hz = -lx;
+      cnt = 0;
+      for (int b = 0; b < kSahBins - 1; ++b) {
+        const int* w = ab + b * kBinWords;
+        if (w[0]) {
+          lx = fminf(lx, o2f(w[1])); ly = fminf(ly, o2f(w[2])); lz = fminf(lz, o2f(w[3]));
+          hx = fmaxf(hx, o2f(w[4])); hy = fmaxf(hy, o2f(w[5])); hz = fmaxf(hz, o2f(w[6]));
+        }
+        cnt += w[0];
+        if (cnt == 0 || right_cnt[b + 1] == 0) continue;
+        const float cost = sah_area(lx, ly, lz, hx, hy, hz) * float(cnt) + right_area[b + 1] * float(right_cnt[b + 1]);
+        if (cost < best_cost) {
+          best_cost = cost;
+          best_axis = a;
+          best_split = b;
+          best_left = cnt;
+        }
+      }
+    }
+    const float area = sah_area(nd.lo.x, nd.lo.y, nd.lo.z, nd.hi.x, nd.hi.y, nd.hi.z);
+    if (best_axis < 0) {
+      if (n > kSahMaxLeaf) {  // coincident centroids: halve the range
+        best_axis = 3;
+        best_left = n / 2;
+      }
+    } else if (n <= kSahMaxLeaf && area * float(n) <= area + best_cost) {
+      best_axis = -1;
+    }
+  }
+  const int k = v - lvl_begin;
+  split[k] = make_int4(best_axis, best_split, best_left, 0);
+  nkids[k] = best_axis >= 0 ? 2 : 0;
+  if (best_axis < 0) return;
+  SahNode L = nd, R = nd;
+  L.depth = R.depth = nd.depth + 1;
+  L.end = nd.begin + best_left;
+  R.begin = L.end;
+  if (best_axis < 3) {
+    const int* ab = nb + best_axis * kSahBins * kBinWords;
+    float b[2][12];
+    for (int side = 0; side < 2; ++side)
+      for (int j = 0; j < 12; ++j) b[side][j] = (j % 6) < 3 ? 3.402823466e38f : -3.402823466e38f;
+    for (int bin = 0; bin < kSahBins; ++bin) {
+      const int* w = ab + bin * kBinWords;
+      if (!w[0]) continue;
+      float* d = b[bin <= best_split ? 0 : 1];
+      for (int j = 0; j < 12; ++j) d[j] = (j % 6) < 3 ? fminf(d[j], o2f(w[1 + j])) : fmaxf(d[j], o2f(w[1 + j]));
+    }
+    SahNode* c[2] = {&L, &R};
+    for (int side = 0; side < 2; ++side) {
+      const float* d = b[side];
+      c[side]->lo = make_float4(d[0], d[1], d[2], 0.f);
+      c[side]->hi = make_float4(d[3], d[4], d[5], 0.f);
+      c[side]->clo = make_float4(d[6], d[7], d[8], 0.f);
+      c[side]->chi = make_float4(d[9], d[10], d[11], 0.f);
+    }
+  }
+  kids[2 * k] = L;
+  kids[2 * k + 1] = R;
+}
+
+// 3. child records and this level's node records (reference layout)
+__global__ void k_sah_children(SahNode* __restrict__ nodes, int lvl_begin, int lvl_end, const int4* __restrict__ split,
+                               const SahNode* __restrict__ kids, const int* __restrict__ kid_base, int next_begin,
+                               float4* __restrict__ out) {
+  const int v = lvl_begin + int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (v >= lvl_end) return;
+  const int k = v - lvl_begin;
+  const SahNode nd = nodes[v];
+  float4* o = out + 4 * size_t(v);
+  if (split[k].x < 0) {
+    o[0] = make_float4(0.f, 0.f, 0.f, ibits(0));
+    o[1] = make_float4(0.f, 0.f, 0.f, ibits(0));
+    o[2] = make_float4(0.f, 0.f, 0.f, ibits(nd.end - nd.begin));
+    o[3] = make_float4(0.f, 0.f, 0.f, ibits(nd.begin));
+    return;
+  }
+  const int left = next_begin + kid_base[k], right = left + 1;
+  const SahNode L = kids[2 * k], R = kids[2 * k + 1];
+  nodes[left] = L;
+  nodes[right] = R;
+  o[0] = make_float4(L.lo.x, L.lo.y, L.lo.z, ibits(left));
+  o[1] = make_float4(L.hi.x, L.hi.y, L.hi.z, ibits(right));
+  o[2] = make_float4(R.lo.x, R.lo.y, R.lo.z, ibits(0));
+  o[3] = make_float4(R.hi.x, R.hi.y, R.hi.z, ibits(0));
+}
+
+// 4a. goes-left flags of the slots of split nodes (0 elsewhere)
+__global__ void k_sah_flags(uint32_t n, const uint32_t* __restrict__ order, const int* __restrict__ pnode,
+                            const float4* __restrict__ tlo, const float4* __restrict__ thi,
+                            const SahNode* __restrict__ nodes, int lvl_begin, int lvl_end,
+                            const int4* __restrict__ split, int* __restrict__ flag) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int v = pnode[s];
+    int f = 0;
+    if (v >= lvl_begin && v < lvl_end) {
+      const int4 sp = split[v - lvl_begin];
+      if (sp.x == 3) {
+        f = int(s) < nodes[v].begin + sp.z ? 1 : 0;
+      } else if (sp.x >= 0) {
+        const SahNode nd = nodes[v];
+        const uint32_t t = order[s];
+        const float4 l = tlo[t], h = thi[t];
+        const float c = sp.x == 0 ? 0.5f * (l.x + h.x) : (sp.x == 1 ? 0.5f * (l.y + h.y) : 0.5f * (l.z + h.z));
+        const float lo = comp(nd.clo, sp.x), ext = comp(nd.chi, sp.x) - lo;
+        f = sah_bin(c, lo, ext) <= sp.y ? 1 : 0;
+      }
+    }
+    flag[s] = f;
+  }
+}
+
+// 4b. stable partition: left slots keep their order at the front of the
+// range, right slots after them; slots of leaves stay
+__global__ void k_sah_scatter(uint32_t n, const uint32_t* __restrict__ order, const int* __restrict__ pnode,
+                              const SahNode* __restrict__ nodes, int lvl_begin, int lvl_end,
+                              const int4* __restrict__ split, const int* __restrict__ kid_base, int next_begin,
+                              const int* __restrict__ flag, const int* __restrict__ scan,
+                              uint32_t* __restrict__ order2, int* __restrict__ pnode2, int* __restrict__ err) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int v = pnode[s];
+    uint32_t dst = s;
+    int nv = v;
+    if (v >= lvl_begin && v < lvl_end) {
+      const int4 sp = split[v - lvl_begin];
+      if (sp.x >= 0) {
+        const int b = nodes[v].begin;
+        const int left_before = scan[s] - scan[b];  // goes-left slots in [b, s)
+        const int left = next_begin + kid_base[v - lvl_begin];
+        if (flag[s]) {
+          dst = uint32_t(b + left_before);
+          nv = left;
+        } else {
+          dst = uint32_t(b + sp.z + (int(s) - b - left_before));
+          nv = left + 1;
+        }
+      }
+    }
+    if (dst >= n) {  // a left count that disagrees with the flags: reported, never written
+      atomicExch(err, 1);
+      continue;
+    }
+    order2[dst] = order[s];
+    pnode2[dst] = nv;
+  }
+}
+
+__global__ void k_sah_root(uint32_t n, const float* __restrict__ block_bounds, int nblocks, SahNode* __restrict__ root,
+                           uint32_t* __restrict__ order, int* __restrict__ pnode) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    float cb[6] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f, -3.402823466e38f, -3.402823466e38f,
+                   -3.402823466e38f};
+    for (int b = 0; b < nblocks; ++b)
+      for (int k = 0; k < 6; ++k)
+        cb[k] = k < 3 ? fminf(cb[k], block_bounds[6 * b + k]) : fmaxf(cb[k], block_bounds[6 * b + k]);
+    SahNode r{};
+    r.clo = make_float4(cb[0], cb[1], cb[2], 0.f);
+    r.chi = make_float4(cb[3], cb[4], cb[5], 0.f);
+    r.begin = 0;
+    r.end = int(n);
+    r.depth = 0;
+    *root = r;
+  }
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    order[t] = t;
+    pnode[t] = 0;
+  }
+}
+
+// the root's box: a reduction over the triangle boxes
+__global__ void k_sah_root_box(uint32_t n, const float4* __restrict__ tlo, const float4* __restrict__ thi,
+                               int* __restrict__ box) {
+  int l[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, h[3] = {int(0x80000000), int(0x80000000), int(0x80000000)};
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const float4 a = tlo[t], b = thi[t];
+    l[0] = min(l[0], f2o(a.x)); l[1] = min(l[1], f2o(a.y)); l[2] = min(l[2], f2o(a.z));
+    h[0] = max(h[0], f2o(b.x)); h[1] = max(h[1], f2o(b.y)); h[2] = max(h[2], f2o(b.z));
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      l[k] = min(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
+      h[k] = max(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(box + k, l[k]);
+      atomicMax(box + 3 + k, h[k]);
+    }
+}
+
+__global__ void k_sah_root_set(SahNode* root, const int* __restrict__ box) {
+  if (threadIdx.x == 0) {
+    root->lo = make_float4(o2f(box[0]), o2f(box[1]), o2f(box[2]), 0.f);
+    root->hi = make_float4(o2f(box[3]), o2f(box[4]), o2f(box[5]), 0.f);
+  }
+}
+
+__global__ void k_sah_remap(uint32_t n, const uint32_t* __restrict__ order, int32_t* __restrict__ remap) {
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+    remap[s] = int32_t(order[s]);
+}
+
+int build_bvh_device_sah(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st,
+                         DeviceBvh* out, Status& s) {
+  if (ntris == 0) return s.fail(DSPBR_ERR_INVALID, "device BVH: no triangles");
+  if (ntris > (1u << 28)) return s.fail(DSPBR_ERR_INVALID, "device BVH: too many triangles");
+  const uint32_t n = ntris;
+  const size_t cap = 2 * size_t(n) - 1;  // every split leaves both sides non-empty
+  constexpr int kChunk = 1 << 16;        // nodes binned per pass (bins: 2.5 KB per node)
+  DevBuf<float4> tlo, thi;
+  DevBuf<float> bb;
+  DevBuf<uint32_t> order, order2;
+  DevBuf<int> pnode, pnode2, flag, scan, bins, nkids, kid_base, box, err;
+  DevBuf<SahNode> nodes, kids;
+  DevBuf<int4> split;
+  DevBuf<unsigned char> tmp;
+  const int nb = grid(n, 256, 148 * 4);
+  TRY_CUDA(s, tlo.alloc(n), "device BVH");
+  TRY_CUDA(s, thi.alloc(n), "device BVH");
+  TRY_CUDA(s, bb.alloc(6 * size_t(nb)), "device BVH");
+  TRY_CUDA(s, order.alloc(n), "device BVH");
+  TRY_CUDA(s, order2.alloc(n), "device BVH");
+  TRY_CUDA(s, pnode.alloc(n), "device BVH");
+  TRY_CUDA(s, pnode2.alloc(n), "device BVH");
+  TRY_CUDA(s, flag.alloc(n), "device BVH");
+  TRY_CUDA(s, scan.alloc(n), "device BVH");
+  TRY_CUDA(s, nodes.alloc(cap), "device BVH");
+  TRY_CUDA(s, box.alloc(6), "device BVH");
+  TRY_CUDA(s, err.alloc(1), "device BVH");
+  TRY_CUDA(s, cudaMemsetAsync(err.p, 0, sizeof(int), st), "device BVH");
+  TRY_CUDA(s, bins.alloc(size_t(std::min<size_t>(cap, kChunk)) * 3 * kSahBins * kBinWords), "device BVH");
+  TRY_CUDA(s, out->nodes.alloc(cap * 4), "device BVH");
+  TRY_CUDA(s, out->remap.alloc(n), "device BVH");
+  size_t scan_temp = 0, t2 = 0;
+  TRY_CUDA(s, cub::DeviceScan::ExclusiveSum(nullptr, scan_temp, flag.p, scan.p, int(n), st), "device BVH scan");
+  TRY_CUDA(s, cub::DeviceScan::ExclusiveSum(nullptr, t2, nkids.p, kid_base.p, int(n) + 1, st), "device BVH scan");
+  scan_temp = std::max(scan_temp, t2);
+  TRY_CUDA(s, tmp.alloc(std::max<size_t>(scan_temp, 1)), "device BVH");
+  k_tri_bounds<<<nb, 256, 0, st>>>(verts, indices, n, tlo.p, thi.p, bb.p);
+  k_sah_root<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, bb.p, nb, nodes.p, order.p, pnode.p);
+  const int box_init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, int(0x80000000), int(0x80000000), int(0x80000000)};
+  TRY_CUDA(s, cudaMemcpyAsync(box.p, box_init, sizeof box_init, cudaMemcpyHostToDevice, st), "device BVH");
+  k_sah_root_box<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, tlo.p, thi.p, box.p);
+  k_sah_root_set<<<1, 32, 0, st>>>(nodes.p, box.p);
+  TRY_CUDA(s, cudaGetLastError(), "device BVH");
+  int lvl_begin = 0, lvl_end = 1;
+  size_t level_cap = 0;
+  while (lvl_end > lvl_begin) {
+    const int width = lvl_end - lvl_begin;
+    if (size_t(width) > level_cap) {
+      level_cap = std::max<size_t>(size_t(width), 2 * level_cap);
+      TRY_CUDA(s, split.alloc(level_cap), "device BVH");
+      TRY_CUDA(s, kids.alloc(2 * level_cap), "device BVH");
+      TRY_CUDA(s, nkids.alloc(level_cap + 1), "device BVH");
+      TRY_CUDA(s, kid_base.alloc(level_cap + 1), "device BVH");
+    }
+    for (int c_begin = lvl_begin; c_begin < lvl_end; c_begin += kChunk) {
+      const int c_end = std::min(lvl_end, c_begin + kChunk);
+      const uint32_t words = uint32_t(c_end - c_begin) * 3u * kSahBins * kBinWords;
+      k_sah_init<<<grid(words, 256, 148 * 8), 256, 0, st>>>(n, bins.p, words);
+      k_sah_bin<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, pnode.p, tlo.p, thi.p, nodes.p, c_begin, c_end,
+                                                       bins.p);
+      k_sah_split<<<(c_end - c_begin + 127) / 128, 128, 0, st>>>(nodes.p, lvl_begin, c_begin, c_end, bins.p,
+                                                                 split.p, kids.p, nkids.p);
+    }
+    TRY_CUDA(s, cudaMemsetAsync(nkids.p + width, 0, sizeof(int), st), "device BVH");
+    TRY_CUDA(s, cub::DeviceScan::ExclusiveSum(tmp.p, scan_temp, nkids.p, kid_base.p, width + 1, st),
+             "device BVH scan");
+    int total_kids = 0;
+    TRY_CUDA(s, cudaMemcpyAsync(&total_kids, kid_base.p + width, sizeof(int), cudaMemcpyDeviceToHost, st),
+             "device BVH");
+    TRY_CUDA(s, cudaStreamSynchronize(st), "device BVH");
+    if (size_t(lvl_end) + size_t(total_kids) > cap) return s.fail(DSPBR_ERR_DEVICE_FAULT, "device BVH: node overflow");
+    k_sah_children<<<(width + 127) / 128, 128, 0, st>>>(nodes.p, lvl_begin, lvl_end, split.p, kids.p, kid_base.p,
+                                                        lvl_end, out->nodes.p);
+    if (total_kids > 0) {
+      k_sah_flags<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, pnode.p, tlo.p, thi.p, nodes.p, lvl_begin,
+                                                         lvl_end, split.p, flag.p);
+      TRY_CUDA(s, cub::DeviceScan::ExclusiveSum(tmp.p, scan_temp, flag.p, scan.p, int(n), st), "device BVH scan");
+      k_sah_scatter<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, pnode.p, nodes.p, lvl_begin, lvl_end, split.p,
+                                                           kid_base.p, lvl_end, flag.p, scan.p, order2.p, pnode2.p,
+                                                           err.p);
+      order.swap(order2);
+      pnode.swap(pnode2);
+    }
+    TRY_CUDA(s, cudaGetLastError(), "device BVH");
+    lvl_begin = lvl_end;
+    lvl_end += total_kids;
+  }
+  k_sah_remap<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, out->remap.p);
+  TRY_CUDA(s, cudaGetLastError(), "device BVH");
+  int bad = 0;
+  TRY_CUDA(s, cudaMemcpyAsync(&bad, err.p, sizeof(int), cudaMemcpyDeviceToHost, st), "device BVH");
+  // the temporaries are freed at return: wait for the kernels that use them
+  TRY_CUDA(s, cudaStreamSynchronize(st), "device BVH");
+  if (bad) return s.fail(DSPBR_ERR_DEVICE_FAULT, "device BVH: partition counts disagree");
+  out->num_nodes = uint32_t(lvl_end);
+  out->num_slots = n;
   return DSPBR_OK;
 }
 

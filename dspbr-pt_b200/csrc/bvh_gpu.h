@@ -20,6 +20,12 @@ struct DeviceBvh {
 int build_bvh_device(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st, DeviceBvh* out,
                      Status& s);
 
+// Binned-SAH BVH over the triangles with the host builder's rules
+// (bvh_build.cpp), built level by level on the device; same inputs and output
+// layout as build_bvh_device.  Synchronises `st` before returning.
+int build_bvh_device_sah(const float4* verts, const uint32_t* indices, uint32_t ntris, cudaStream_t st,
+                         DeviceBvh* out, Status& s);
+
 // 4-wide collapse of a well-formed binary BVH already on the device (the same
 // rule as collapse_bvh4, level by level).  wnodes: 8 float4 per wide node.
 struct DeviceWideBvh {

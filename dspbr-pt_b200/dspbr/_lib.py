@@ -20,7 +20,7 @@ PROFILE_FULL, PROFILE_LEAN = 0, 1
 RNG_MWC, RNG_PCG = 0, 1
 ENV_ALIAS, ENV_CDF = 0, 1
 TRAVERSAL_WIDE, TRAVERSAL_REFERENCE = 0, 1
-BVH_BUILD_HOST, BVH_BUILD_DEVICE = 0, 1
+BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_DEVICE_LBVH = 0, 1, 2
 
 
 class DspbrError(RuntimeError):

@@ -80,9 +80,14 @@ class Context:
         check(rc, self.h)
 
     def set_bvh_builder(self, builder: str) -> None:
-        """BVH builder of scenes created without one: "host" (binned SAH) or "device" (linear BVH)."""
-        self.check(self.lib.dspbr_set_bvh_builder(self.h, _lib.BVH_BUILD_DEVICE if builder == "device"
-                                                  else _lib.BVH_BUILD_HOST))
+        """BVH builder of scenes created without one: "host" (binned SAH on the
+        host), "device" (binned SAH on the device) or "device_lbvh" (linear
+        BVH on the device: the fastest build)."""
+        codes = {"host": _lib.BVH_BUILD_HOST, "device": _lib.BVH_BUILD_DEVICE,
+                 "device_lbvh": _lib.BVH_BUILD_DEVICE_LBVH}
+        if builder not in codes:
+            raise ValueError(f"set_bvh_builder: {builder!r} is not one of {sorted(codes)}")
+        self.check(self.lib.dspbr_set_bvh_builder(self.h, codes[builder]))
 
     def host_array(self, shape, dtype=np.float32) -> np.ndarray:
         """numpy array over page-locked host memory (dspbr_host_alloc)."""

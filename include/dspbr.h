@@ -39,7 +39,7 @@ enum {
 enum { DSPBR_PROFILE_FULL = 0, DSPBR_PROFILE_LEAN = 1 };
 enum { DSPBR_RNG_MWC = 0, DSPBR_RNG_PCG = 1 };
 enum { DSPBR_TRAVERSAL_WIDE = 0, DSPBR_TRAVERSAL_REFERENCE = 1 };
-enum { DSPBR_BVH_BUILD_HOST = 0, DSPBR_BVH_BUILD_DEVICE = 1 };
+enum { DSPBR_BVH_BUILD_HOST = 0, DSPBR_BVH_BUILD_DEVICE = 1, DSPBR_BVH_BUILD_DEVICE_LBVH = 2 };
 enum { DSPBR_ENV_ALIAS = 0, DSPBR_ENV_CDF = 1 };
 
 typedef struct dspbr_ctx dspbr_ctx;
@@ -123,10 +123,13 @@ void dspbr_bvh_free(dspbr_bvh* bvh);
  *      (scene_data_webgl2.ts:74-100, renderer.ts:872-912) ----------------- */
 /* bvh_nodes/bvh_indices may be NULL: the BVH is then built here, by the
  * builder dspbr_set_bvh_builder selects:
- *   DSPBR_BVH_BUILD_HOST    binned SAH on the host (default; TinyBVH's role);
- *   DSPBR_BVH_BUILD_DEVICE  linear BVH on the device (Morton order, radix
- *                           tree, leaves of <= 4 triangles) and 4-wide collapse
- *                           on the device: much faster, somewhat slower to trace. */
+ *   DSPBR_BVH_BUILD_HOST         binned SAH on the host (default; TinyBVH's role);
+ *   DSPBR_BVH_BUILD_DEVICE       binned SAH on the device with the host
+ *                                builder's rules, level by level, and the
+ *                                4-wide collapse on the device;
+ *   DSPBR_BVH_BUILD_DEVICE_LBVH  linear BVH on the device (Morton order, radix
+ *                                tree, leaves of <= 4 triangles): the fastest
+ *                                build, somewhat slower to trace. */
 int dspbr_scene_create(dspbr_ctx* ctx, const float* vertices, uint32_t num_vertices, const uint32_t* indices,
                        uint32_t num_indices, const float* materials, uint32_t num_materials,
                        const float* bvh_nodes, uint32_t num_bvh_nodes, const int32_t* bvh_indices,

@@ -1,6 +1,6 @@
-"""BVH built on the device (DSPBR_BVH_BUILD_DEVICE): a valid tree in the
-reference layout, the same closest hits as the host-built tree, and the same
-images."""
+"""BVH built on the device (DSPBR_BVH_BUILD_DEVICE: binned SAH;
+DSPBR_BVH_BUILD_DEVICE_LBVH: linear BVH): a valid tree in the reference
+layout, the same closest hits as the host-built tree, and the same images."""
 import time
 
 import numpy as np
@@ -28,20 +28,25 @@ def _leaves(bvh: Bvh):
     return out
 
 
+# the largest leaf each builder makes (SAH: the host builder's leaf cap)
+MAX_LEAF = {"device": 8, "device_lbvh": 4}
+
+
+@pytest.mark.parametrize("builder", ["device", "device_lbvh"])
 @pytest.mark.parametrize("ntris", [1, 7, 3000, 200_000])
-def test_device_bvh_is_a_valid_reference_layout_tree(ntris):
+def test_device_bvh_is_a_valid_reference_layout_tree(ntris, builder):
     sc = synth.make_sized(41, max(ntris, 20), env_size=(16, 8)) if ntris > 7 else synth.make_small(0)
     if ntris <= 7:  # a tiny mesh: the first `ntris` triangles of the small scene
         sc.indices = np.ascontiguousarray(sc.indices[: 3 * ntris])
     ctx = Context(0)
-    ctx.set_bvh_builder("device")
+    ctx.set_bvh_builder(builder)
     ds = DeviceScene(ctx, sc.vertices, sc.indices, sc.materials)
     bvh = ds.bvh()
     n = sc.indices.size // 3
-    # every triangle in exactly one reachable leaf, leaves of <= 4 triangles
+    # every triangle in exactly one reachable leaf, leaves of at most the builder's size
     seen = np.zeros(n, np.int32)
     for first, cnt in _leaves(bvh):
-        assert 1 <= cnt <= 4
+        assert 1 <= cnt <= MAX_LEAF[builder]
         seen[bvh.indices[first:first + cnt]] += 1
     assert (seen == 1).all()
     # closest hits of the reference traversal over it = brute force (ties aside)
@@ -57,16 +62,17 @@ def test_device_bvh_is_a_valid_reference_layout_tree(ntris):
     ctx.close()
 
 
-def test_device_bvh_same_hits_and_image_as_host_bvh():
+@pytest.mark.parametrize("builder", ["device", "device_lbvh"])
+def test_device_bvh_same_hits_and_image_as_host_bvh(builder):
     sc = synth.make_sized(43, 400_000, env_size=(64, 32))
     hc, dc = Context(0), Context(0)
-    dc.set_bvh_builder("device")
+    dc.set_bvh_builder(builder)
     t0 = time.perf_counter()
     hs = DeviceScene(hc, sc.vertices, sc.indices, sc.materials)
     t1 = time.perf_counter()
     ds = DeviceScene(dc, sc.vertices, sc.indices, sc.materials)
     t2 = time.perf_counter()
-    print(f"scene creation: host SAH {t1 - t0:.3f} s, device LBVH {t2 - t1:.3f} s")
+    print(f"scene creation: host SAH {t1 - t0:.3f} s, {builder} {t2 - t1:.3f} s")
     from tests.test_gpu_parity import trace_gpu
     rays = helpers.random_rays(sc.vertices, 100_000, seed=44)
     htri, ht, _ = trace_gpu(hc, hs, rays)
@@ -80,8 +86,8 @@ def test_device_bvh_same_hits_and_image_as_host_bvh():
     hc.close()
     dc.close()
     imgs = []
-    for builder in ("host", "device"):
-        v = PathtracingViewport(width=96, height=64, settings={"maxBounces": 6, "bvhBuilder": builder})
+    for b in ("host", builder):
+        v = PathtracingViewport(width=96, height=64, settings={"maxBounces": 6, "bvhBuilder": b})
         v.setScene(sc)
         v.setIBL(sc.env)
         v.setCamera(helpers.camera_of(sc))

@@ -28,7 +28,7 @@ def _deform(v, k=0.6, seed=0):
     return out
 
 
-@pytest.mark.parametrize("builder", ["host", "device"])
+@pytest.mark.parametrize("builder", ["host", "device", "device_lbvh"])
 def test_refit_hits_match_reference_traversal_and_a_fresh_build(builder):
     sc = synth.make_sized(7, 30000, env_size=(16, 8))
     ctx = Context(0)
