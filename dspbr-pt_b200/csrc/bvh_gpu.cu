@@ -631,9 +631,11 @@ __device__ __forceinline__ int sah_bin(float c, float lo, float ext) {
 
 __device__ __forceinline__ float comp(const float4& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 
+// Area and costs with every product and sum rounded on its own (no FMA
+// contraction), as the host builder computes them: equal costs, equal planes.
 __device__ __forceinline__ float sah_area(float lx, float ly, float lz, float hx, float hy, float hz) {
   const float dx = fmaxf(0.f, hx - lx), dy = fmaxf(0.f, hy - ly), dz = fmaxf(0.f, hz - lz);
-  return dx * dy + dy * dz + dz * dx;
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
 }
 
 __global__ void k_sah_init(uint32_t n, int* __restrict__ bins, uint32_t nbins_words) {
@@ -710,7 +712,8 @@ __global__ void k_sah_split(const SahNode* __restrict__ nodes, int lvl_begin, in
         }
         cnt += w[0];
         if (cnt == 0 || right_cnt[b + 1] == 0) continue;
-        const float cost = sah_area(lx, ly, lz, hx, hy, hz) * float(cnt) + right_area[b + 1] * float(right_cnt[b + 1]);
+        const float cost = __fadd_rn(__fmul_rn(sah_area(lx, ly, lz, hx, hy, hz), float(cnt)),
+                                     __fmul_rn(right_area[b + 1], float(right_cnt[b + 1])));
         if (cost < best_cost) {
           best_cost = cost;
           best_axis = a;
@@ -725,7 +728,7 @@ __global__ void k_sah_split(const SahNode* __restrict__ nodes, int lvl_begin, in
         best_axis = 3;
         best_left = n / 2;
       }
-    } else if (n <= kSahMaxLeaf && area * float(n) <= area + best_cost) {
+    } else if (n <= kSahMaxLeaf && __fmul_rn(area, float(n)) <= __fadd_rn(area, best_cost)) {
       best_axis = -1;
     }
   }

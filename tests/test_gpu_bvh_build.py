@@ -96,3 +96,42 @@ def test_device_bvh_same_hits_and_image_as_host_bvh(builder):
         v.dispose()
     close = helpers.close_mask(imgs[0][..., :3], imgs[1][..., :3], 1e-4, 1e-5).all(-1)
     assert close.mean() > 0.99
+
+
+def _canonical(bvh: Bvh):
+    """The tree from the root as nested tuples: inner nodes by their two
+    child boxes (float bits), leaves by their sorted triangle ids, so that
+    trees numbered in different orders compare equal."""
+    nodes = bvh.nodes.reshape(-1, 16)
+    bits = nodes.view(np.uint32)
+
+    def walk(n):
+        cnt, first = int(nodes[n, 11]), int(nodes[n, 15])
+        if cnt > 0:
+            return ("leaf", tuple(sorted(int(t) for t in bvh.indices[first:first + cnt])))
+        boxes = tuple(int(x) for k in (0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14) for x in [bits[n, k]])
+        return ("inner", boxes, walk(int(nodes[n, 3])), walk(int(nodes[n, 7])))
+
+    import sys
+    limit = sys.getrecursionlimit()
+    sys.setrecursionlimit(max(limit, 10_000))
+    try:
+        return walk(0)
+    finally:
+        sys.setrecursionlimit(limit)
+
+
+@pytest.mark.parametrize("ntris", [3000, 60_000])
+def test_device_sah_builds_the_host_tree(ntris):
+    """The device binned SAH applies the host builder's rules: the same tree
+    (structure, child boxes bit for bit, leaf triangle sets)."""
+    sc = synth.make_sized(47, ntris, env_size=(16, 8))
+    host = Bvh.build(sc.vertices, sc.indices)
+    ctx = Context(0)
+    ctx.set_bvh_builder("device")
+    ds = DeviceScene(ctx, sc.vertices, sc.indices, sc.materials)
+    dev = ds.bvh()
+    assert dev.nodes.size == host.nodes.size
+    assert _canonical(dev) == _canonical(host)
+    ds.close()
+    ctx.close()
