@@ -55,7 +55,9 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region:
+    every 20 ms; the region starts after the first sample has arrived, and the
+    samples taken before it are not counted."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -71,10 +73,20 @@ class ClockSampler:
             os.close(fd)
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        self.skip = 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 10.0 and self.proc.poll() is None:
+            with open(self.path) as f:
+                n = sum(1 for _ in f)
+            if n:
+                self.skip = n
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -91,9 +103,9 @@ class ClockSampler:
             return None
         rows = []
         with open(self.path) as f:
-            for line in f:
+            for k, line in enumerate(f):
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if k >= getattr(self, "skip", 0) and len(parts) >= 9:
                     rows.append(parts)
         os.unlink(self.path)
         if not rows:
@@ -702,7 +714,7 @@ def run_gpu_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
