@@ -224,18 +224,31 @@ def _submit(srv, dev, r, out=None):
     return srv.submit(ds, di, cam, r["width"], r["height"], r["spp"], {"maxBounces": r["maxBounces"]}, out=out)
 
 
+def _images(mix):
+    """One output image per request, allocated and touched before any timing:
+    both arms then time the library, not the host's page faults."""
+    outs = []
+    for r in mix:
+        a = np.empty((r["height"], r["width"], 4), np.float32)
+        a.fill(0.0)
+        outs.append(a)
+    return outs
+
+
 def _one_at_a_time(ctx, dev, mix):
     """The same requests through the single-viewport API (dspbr_set_scene /
     set_camera / resize / render / read_accum), one after the other, scenes
-    resident.  Returns per-request service times (s) and the images.  The
-    request with the most samples runs once untimed first, as the batched arm
-    runs a warm-up request: the context's path pool reaches its size and its
-    render graph is captured before the timed requests."""
+    resident, each read into its own preallocated image.  Returns per-request
+    service times (s) and the images.  The request with the most samples runs
+    once untimed first, as the batched arm runs a warm-up request: the
+    context's path pool reaches its size and its render graph is captured
+    before the timed requests."""
     import ctypes as C
     from dspbr import _lib
     lib, h = ctx.lib, ctx.h
     times, imgs = [], []
     big = max(mix, key=lambda r: r["width"] * r["height"] * r["spp"])
+    outs = _images([big] + list(mix))
     for k, r in enumerate([big] + list(mix)):
         t0 = time.perf_counter()
         ds, di, _ = dev[r["scene"]]
@@ -248,7 +261,7 @@ def _one_at_a_time(ctx, dev, mix):
         ctx.check(lib.dspbr_set_camera(h, _lib.fptr(m), float(r["camera"].fov), float(r["camera"].near)))
         ctx.check(lib.dspbr_resize(h, r["width"], r["height"]))
         ctx.check(lib.dspbr_render(h, r["spp"]))
-        out = np.empty((r["height"], r["width"], 4), np.float32)
+        out = outs[k]
         ctx.check(lib.dspbr_read_accum(h, _lib.fptr(out), out.size))
         if k == 0:
             continue
@@ -446,8 +459,9 @@ def serving_section(local, quick=False):
     # warm-up request (graph capture, memory pool)
     srv.wait(_submit(srv, bdev, dict(mix[0], spp=1)))
     r0 = _rays(srv)
+    outs_b = _images(mix)
     t0 = time.perf_counter()
-    ids = [_submit(srv, bdev, r) for r in mix]
+    ids = [_submit(srv, bdev, r, out=outs_b[k]) for k, r in enumerate(mix)]
     done = [srv.wait(i) for i in ids]
     t_batch = time.perf_counter() - t0
     rays_b = _rays(srv) - r0
@@ -481,7 +495,7 @@ def serving_section(local, quick=False):
     rates = []
     for rate in ((10.0, 50.0, 200.0, 500.0) if not quick else (50.0,)):
         arr = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))
-        outs = [np.empty((r["height"], r["width"], 4), np.float32) for r in smix]
+        outs = _images(smix)
         ids = [None] * n
         r0 = _rays(srv)
         start = time.perf_counter()
