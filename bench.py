@@ -432,8 +432,17 @@ def configs_section(local, args):
 def gltf_section(local, args):
     """glTF asset to first frame: a ~1.9M-triangle .glb (256 instancing nodes,
     four materials, four 1024x1024 PNG textures) packed by dspbr.gltf
-    (scene_loader.ts), then setScene (host binned-SAH BVH, 4-wide collapse,
-    upload, textures) and setIBL, then frames at 1280x720."""
+    (scene_loader.ts), then setScene (binned-SAH BVH, 4-wide collapse,
+    upload, textures) and setIBL, then frames at 1280x720.  The BVH is built
+    on the host (the default); `device_bvh` repeats the load with the
+    device builder, which builds the same tree."""
+    res = _gltf_first_frame(local, args, "host")
+    res["device_bvh"] = {k: x for k, x in _gltf_first_frame(local, args, "device").items()
+                         if k in ("load_gltf_ms", "set_scene_ms", "to_first_frame_ms", "mrays_per_s")}
+    return res
+
+
+def _gltf_first_frame(local, args, builder):
     from dspbr import gltf, synth
     from dspbr.viewport import PathtracingCamera, PathtracingViewport
     from tests.gltf_writer import large_asset
@@ -441,7 +450,7 @@ def gltf_section(local, args):
     t0 = time.perf_counter()
     sc = gltf.load_gltf(glb)
     t1 = time.perf_counter()
-    v = PathtracingViewport(device=local, width=1280, height=720, settings={"maxBounces": 8})
+    v = PathtracingViewport(device=local, width=1280, height=720, settings={"maxBounces": 8, "bvhBuilder": builder})
     v.setScene(sc)
     t2 = time.perf_counter()
     env = synth.make_small(0).env
