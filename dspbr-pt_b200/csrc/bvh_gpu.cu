@@ -670,6 +670,53 @@ __global__ void k_sah_bin(uint32_t n, const uint32_t* __restrict__ order, const 
   }
 }
 
+// 1'. the same for the first levels (few nodes, every triangle of the
+// level in their bins): each block bins into shared memory, then adds its
+// non-empty bins to the global ones, so that the global atomics per bin are
+// one per block instead of one per triangle.
+constexpr int kSharedBinNodes = 32;  // 32 nodes x 2.5 KB of bins
+__global__ void k_sah_bin_shared(uint32_t n, const uint32_t* __restrict__ order, const int* __restrict__ pnode,
+                                 const float4* __restrict__ tlo, const float4* __restrict__ thi,
+                                 const SahNode* __restrict__ nodes, int c_begin, int c_end, int* __restrict__ bins) {
+  extern __shared__ int sb[];
+  const int nbins = (c_end - c_begin) * 3 * kSahBins;
+  for (int i = threadIdx.x; i < nbins * kBinWords; i += blockDim.x) {
+    const int w = i % kBinWords;
+    sb[i] = w == 0 ? 0 : ((w - 1) % 6 < 3 ? 0x7fffffff : int(0x80000000));
+  }
+  __syncthreads();
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int v = pnode[s];
+    if (v < c_begin || v >= c_end) continue;
+    const SahNode nd = nodes[v];
+    const uint32_t t = order[s];
+    const float4 l = tlo[t], h = thi[t];
+    const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    int* nb = sb + (v - c_begin) * (3 * kSahBins * kBinWords);
+    for (int a = 0; a < 3; ++a) {
+      const float lo = comp(nd.clo, a), ext = comp(nd.chi, a) - lo;
+      if (!(ext > 0.f)) continue;
+      int* w = nb + (a * kSahBins + sah_bin(c[a], lo, ext)) * kBinWords;
+      atomicAdd(w, 1);
+      atomicMin(w + 1, f2o(l.x)); atomicMin(w + 2, f2o(l.y)); atomicMin(w + 3, f2o(l.z));
+      atomicMax(w + 4, f2o(h.x)); atomicMax(w + 5, f2o(h.y)); atomicMax(w + 6, f2o(h.z));
+      atomicMin(w + 7, f2o(c[0])); atomicMin(w + 8, f2o(c[1])); atomicMin(w + 9, f2o(c[2]));
+      atomicMax(w + 10, f2o(c[0])); atomicMax(w + 11, f2o(c[1])); atomicMax(w + 12, f2o(c[2]));
+    }
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+    const int* w = sb + b * kBinWords;
+    if (!w[0]) continue;
+    int* g = bins + size_t(b) * kBinWords;
+    atomicAdd(g, w[0]);
+    for (int k = 1; k < kBinWords; ++k) {
+      if ((k - 1) % 6 < 3) atomicMin(g + k, w[k]);
+      else atomicMax(g + k, w[k]);
+    }
+  }
+}
+
 // 2. decision per open node of one chunk [c_begin, c_end) of the level:
 // split[v - lvl_begin] = {axis (-1: leaf, 3: median), bin, left count}, and
 // for a split the two children's boxes (from the bins on each side of the
@@ -942,6 +989,9 @@ int build_bvh_device_sah(const float4* verts, const uint32_t* indices, uint32_t 
   TRY_CUDA(s, cub::DeviceScan::ExclusiveSum(nullptr, t2, nkids.p, kid_base.p, int(n) + 1, st), "device BVH scan");
   scan_temp = std::max(scan_temp, t2);
   TRY_CUDA(s, tmp.alloc(std::max<size_t>(scan_temp, 1)), "device BVH");
+  TRY_CUDA(s, cudaFuncSetAttribute(k_sah_bin_shared, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   kSharedBinNodes * 3 * kSahBins * kBinWords * int(sizeof(int))),
+           "device BVH");
   k_tri_bounds<<<nb, 256, 0, st>>>(verts, indices, n, tlo.p, thi.p, bb.p);
   k_sah_root<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, bb.p, nb, nodes.p, order.p, pnode.p);
   const int box_init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, int(0x80000000), int(0x80000000), int(0x80000000)};
@@ -964,8 +1014,14 @@ int build_bvh_device_sah(const float4* verts, const uint32_t* indices, uint32_t 
       const int c_end = std::min(lvl_end, c_begin + kChunk);
       const uint32_t words = uint32_t(c_end - c_begin) * 3u * kSahBins * kBinWords;
       k_sah_init<<<grid(words, 256, 148 * 8), 256, 0, st>>>(n, bins.p, words);
-      k_sah_bin<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, pnode.p, tlo.p, thi.p, nodes.p, c_begin, c_end,
-                                                       bins.p);
+      if (c_end - c_begin <= kSharedBinNodes) {
+        const size_t smem = size_t(words) * sizeof(int);
+        k_sah_bin_shared<<<grid(n, 256, 148 * 2), 256, smem, st>>>(n, order.p, pnode.p, tlo.p, thi.p, nodes.p,
+                                                                   c_begin, c_end, bins.p);
+      } else {
+        k_sah_bin<<<grid(n, 256, 148 * 8), 256, 0, st>>>(n, order.p, pnode.p, tlo.p, thi.p, nodes.p, c_begin, c_end,
+                                                         bins.p);
+      }
       k_sah_split<<<(c_end - c_begin + 127) / 128, 128, 0, st>>>(nodes.p, lvl_begin, c_begin, c_end, bins.p,
                                                                  split.p, kids.p, nkids.p);
     }
