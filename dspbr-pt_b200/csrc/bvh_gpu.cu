@@ -5,10 +5,11 @@
 // linear BVH (build_bvh_device).
 //
 // The reference builds its BVH on the host with TinyBVH (tinybvh_builder.ts);
-// the host binned-SAH builder here (bvh_build.cpp) plays that role and is the
-// default.  For large scenes admitted while others render, a host build of
-// seconds dominates the time to the first frame.  The linear BVH trades some
-// tree quality for the fastest build:
+// the host binned-SAH builder here (bvh_build.cpp) plays that role.  The
+// device binned SAH builds the same tree and is the default for scenes
+// created without a BVH: for large scenes admitted while others render, a
+// host build of seconds dominates the time to the first frame.  The linear
+// BVH trades some tree quality for the fastest build:
 //   1. per triangle: bounds and centroid; centroid bounds of the scene;
 //   2. 63-bit Morton codes of the centroids (21 bits per axis), sorted with
 //      the triangle index (CUB radix sort);

@@ -97,7 +97,10 @@ struct dspbr_ctx {
   // paths per wave: of 2^20..2^24 the large workload's frames per second
   // rise up to 2^23 and flatten after (2^21: -9%)
   uint32_t wave_paths = 1u << 23;
-  int bvh_builder = DSPBR_BVH_BUILD_HOST;  // for scenes created without a BVH
+  // for scenes created without a BVH: the binned SAH on the device, which
+  // builds the host builder's tree (47-132 ms against ~430 ms on the host for
+  // 1.15M triangles)
+  int bvh_builder = DSPBR_BVH_BUILD_DEVICE;
   std::unique_ptr<dspbr::Engine> eng;  // path pool + job table; this context's render is job slot 0
   // render_async: the iteration loop runs on a worker thread
   std::thread worker;

@@ -336,7 +336,7 @@ class PathtracingViewport:
     def setScene(self, scene) -> None:
         """scene: a synth.Scene or any object with vertices / indices / materials arrays."""
         try:
-            self.ctx.set_bvh_builder(self._display.get("bvhBuilder", "host"))
+            self.ctx.set_bvh_builder(self._display.get("bvhBuilder", "device"))
             ds = DeviceScene(self.ctx, scene.vertices, scene.indices, scene.materials, getattr(scene, "bvh", None))
             if getattr(scene, "tex_infos", None) is not None:
                 ds.set_textures(scene.tex_infos, scene.tex_arrays)

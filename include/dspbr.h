@@ -123,10 +123,11 @@ void dspbr_bvh_free(dspbr_bvh* bvh);
  *      (scene_data_webgl2.ts:74-100, renderer.ts:872-912) ----------------- */
 /* bvh_nodes/bvh_indices may be NULL: the BVH is then built here, by the
  * builder dspbr_set_bvh_builder selects:
- *   DSPBR_BVH_BUILD_HOST         binned SAH on the host (default; TinyBVH's role);
+ *   DSPBR_BVH_BUILD_HOST         binned SAH on the host (TinyBVH's role);
  *   DSPBR_BVH_BUILD_DEVICE       binned SAH on the device with the host
  *                                builder's rules, level by level, and the
- *                                4-wide collapse on the device;
+ *                                4-wide collapse on the device (default: the
+ *                                host builder's tree, built faster);
  *   DSPBR_BVH_BUILD_DEVICE_LBVH  linear BVH on the device (Morton order, radix
  *                                tree, leaves of <= 4 triangles): the fastest
  *                                build, somewhat slower to trace. */
