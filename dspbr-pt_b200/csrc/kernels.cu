@@ -7,9 +7,10 @@
 //               to one queue, hits to the queue of their material class,
 //   connect     any-hit test of the NEE shadow rays emitted by the previous
 //               shade; visible contributions are added to the path radiance,
-//   shade_miss  background / MIS-weighted environment (misptdl.glsl:41-46, 84-88),
-//   shade       RR, absorption, emission, BSDF sampling, NEE sample generation
-//               (misptdl.glsl:54-90, renderer.frag:94-123),
+//   shade       surface hits by material class: RR, absorption, emission, BSDF
+//               sampling, NEE sample generation (misptdl.glsl:54-90,
+//               renderer.frag:94-123); then, in the same launch, the misses:
+//               background / MIS-weighted environment (misptdl.glsl:41-46, 84-88),
 //   regen       new samples (rng_init + calcuateViewRay) of the active jobs,
 //               in priority order, into the slots freed by terminated paths,
 //   commit      job progress, free-list head, queue counter resets and the
