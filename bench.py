@@ -170,9 +170,12 @@ def config_of(sc):
             "seed": sc.seed}
 
 
-def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0):
+def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0, target_s=20.0):
     """Times oracle/_ref (the reference shader compiled for the host) on pixel
-    samples of the workload; returns (Mrays/s, cores, sample description, per-step values)."""
+    samples of the workload; returns (Mrays/s, cores, sample description, per-step values).
+    With `steps`, the warm-up steps (4096 pixels each, at least one) measure
+    the rate and each timed step then takes enough pixels for the timed steps
+    to last about `target_s` seconds together."""
     from oracle import ref_lib
     kind = "reference"
     if not ref_lib.available("f32"):
@@ -199,11 +202,16 @@ def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0):
             tot_rays += rays
             tot_t += dt
         step += 1
+        if steps is not None and step == max(warmup, 1) and step <= warmup + 1:
+            # size the timed steps from the rate of the steps so far (pixels per second)
+            px_rate = npx * step / max(time.perf_counter() - t_start, 1e-6)
+            npx = int(min(max(4096, px_rate * target_s / max(steps, 1)), 1 << 20))
         if steps is not None and step >= steps + warmup:
             break
         if steps is None and time.perf_counter() - t_start > seconds:
             break
-    sample = f"{npx} random pixels x 1 sample per step, {len(vals)} steps ({tot_t:.1f} s of CPU time), same scene/BVH/env"
+    sample = (f"{npx} random pixels x 1 sample per step, {len(vals)} steps ({tot_t:.2f} s of CPU time), "
+              f"same scene/BVH/env")
     return tot_rays / tot_t / 1e6, cores, sample, vals, kind
 
 
