@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
     if (i < count) {
       slot = q[i];
       const float4 o = b.st[slot].org, d = b.st[slot].dir;
-      const DevScene s = sc.jobs[__float_as_uint(d.w)].s;
+      const DevScene& s = sc.jobs[__float_as_uint(d.w)].s;
       Hit h;
       trace_path_ray<false, kCount, kTrav>(s, mk(o), mk(d), kTfarMax, h, aborted, &nodes, &tris);
       b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
     if (i < count) {
       slot = q[i];
       const float4 o = b.st[slot].org, d = b.st[slot].dir;
-      const DevScene s = sc.jobs[__float_as_uint(d.w)].s;
+      const DevScene& s = sc.jobs[__float_as_uint(d.w)].s;
       Hit h;
       bool aborted = false;
       traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
@@ -475,7 +475,7 @@ template <bool kCount, int kTrav>
 DEV void connect_slot(const Sched& sc, const PathBuf& b, uint32_t slot, bool& aborted, int& nrays, uint32_t* nodes,
                       uint32_t* tris) {
   const float4 o4 = b.st[slot].org, d4 = b.st[slot].dir;
-  const DevScene s = sc.jobs[__float_as_uint(d4.w)].s;
+  const DevScene& s = sc.jobs[__float_as_uint(d4.w)].s;
   const float4 w4 = b.st[slot].weight, L = b.st[slot].rad;
   const int flags = __float_as_int(L.w);
   v3 org = mk(o4);
@@ -779,7 +779,7 @@ __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
       job = __float_as_uint(b.st[slot].dir.w);
       bool pending = false;  // shadow rays of the last vertex not yet traced (pair-uniform)
       for (int guard = 0; guard < 4 * kMaxSteps; ++guard) {
-        const DevScene s = sc.jobs[job].s;
+        const DevScene& s = sc.jobs[job].s;
         Hit h;
         h.tri = -1;
         h.t = h.u = h.v = 0.f;
