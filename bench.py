@@ -300,7 +300,8 @@ def server_stream(v, sc, steps, dist):
     settings = {"maxBounces": sc.max_bounces}
     srv = Server(v.ctx)
     outs = [v.ctx.host_array((sc.height, sc.width, 4)) for _ in range(steps)]
-    warm = [srv.submit(v._scene, v._ibl, cam, sc.width, sc.height, 1, settings, out=outs[k]) for k in range(3)]
+    warm = [srv.submit(v._scene, v._ibl, cam, sc.width, sc.height, 1, settings, out=outs[k % steps])
+            for k in range(min(3, steps))]
     for i in warm:
         srv.wait(i)
         srv.release(i)
