@@ -135,3 +135,19 @@ def test_device_sah_builds_the_host_tree(ntris):
     assert _canonical(dev) == _canonical(host)
     ds.close()
     ctx.close()
+
+
+def test_builder_selection_checks_its_argument():
+    """dspbr_set_bvh_builder takes the three builder codes only; the Python
+    mirror takes their names."""
+    from dspbr import _lib
+    ctx = Context(0)
+    for code in (_lib.BVH_BUILD_HOST, _lib.BVH_BUILD_DEVICE, _lib.BVH_BUILD_DEVICE_LBVH):
+        assert ctx.lib.dspbr_set_bvh_builder(ctx.h, code) == 0
+    assert ctx.lib.dspbr_set_bvh_builder(ctx.h, 3) != 0
+    assert ctx.lib.dspbr_set_bvh_builder(ctx.h, -1) != 0
+    with pytest.raises(ValueError):
+        ctx.set_bvh_builder("gpu")
+    for name in ("host", "device", "device_lbvh"):
+        ctx.set_bvh_builder(name)
+    ctx.close()
