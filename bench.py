@@ -36,8 +36,9 @@ METRIC = "Mrays/s"
 
 
 def extend_traffic():
-    """DRAM bytes per frame of the k_extend launches, from the committed ncu
-    summary (profiles/k_extend_dyn_large_1080p.md), or None."""
+    """DRAM bytes per frame of the k_extend launches (ncu dram__bytes_read.sum
+    + dram__bytes_write.sum of one capture, committed beside the ncu
+    summaries under profiles/), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "k_extend_traffic.json")) as f:
             return int(json.load(f)["dram_bytes_per_frame"])
@@ -161,6 +162,33 @@ def make_workload():
     return sc
 
 
+def write_workload_bvh(path):
+    """Child-process entry (--write-bvh PATH): the workload's BVH, built by the
+    library's host binned-SAH builder, saved as an .npz."""
+    sc = make_workload()
+    np.savez(path, nodes=sc.bvh.nodes, indices=sc.bvh.indices)
+    return 0
+
+
+def reference_workload():
+    """The workload for the reference arm.  Its BVH (the reference's node
+    layout) is built by a child process, so the process that times the
+    reference's shader loads no library of this repository, only oracle/_ref."""
+    from dspbr import synth
+    from dspbr.viewport import Bvh  # a plain container: its constructor loads nothing
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    try:
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--write-bvh", path], check=True)
+        with np.load(path) as z:
+            nodes, indices = z["nodes"], z["indices"]
+    finally:
+        os.unlink(path)
+    sc = synth.make_large(0)
+    sc.bvh = Bvh(nodes, indices, 0, sc.num_triangles)
+    return sc
+
+
 def config_of(sc):
     return {"workload": "large: 256 seeded instances (displaced grids + icospheres), DSPBR feature-set materials, "
                         "2048x1024 log-normal HDR env + 1e4 sun", "triangles": int(sc.num_triangles),
@@ -213,6 +241,45 @@ def cpu_reference_sample(sc, seconds=12.0, steps=None, warmup=0, target_s=20.0):
     sample = (f"{npx} random pixels x 1 sample per step, {len(vals)} steps ({tot_t:.2f} s of CPU time), "
               f"same scene/BVH/env")
     return tot_rays / tot_t / 1e6, cores, sample, vals, kind
+
+
+def cpu_config_baseline(sc, bvh, full_image, seconds=10.0):
+    """The reference shader compiled for the host (oracle/_ref, FP32, all host
+    threads) on another scene configuration.  full_image: every pixel at the
+    configuration's samples per pixel (its whole render); otherwise a fixed
+    seeded subset of 16384 pixels, one sample per pixel and frame, frames
+    until about `seconds` have passed, extrapolated to the full render.  The
+    reference shader applies its own Russian roulette (after bounce 2,
+    renderer.frag:119-123) whatever the configuration asks."""
+    from oracle import ref_lib
+    if not ref_lib.available("f32"):
+        return None
+    ref = ref_lib.GlslReference("f32")
+    ref.set_scene(sc.vertices, sc.indices, sc.materials, bvh.nodes, bvh.indices)
+    ref.set_ibl(sc.env)
+    cores = os.cpu_count() or 1
+    if full_image:
+        ys, xs = np.mgrid[0:sc.height, 0:sc.width]
+        xy = np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)
+    else:
+        rng = np.random.default_rng(17)
+        xy = np.stack([rng.integers(0, sc.width, 16384), rng.integers(0, sc.height, 16384)], 1).astype(np.int32)
+    rays, frames, t = 0, 0, 0.0
+    while (full_image and frames < sc.spp) or (not full_image and t < seconds):
+        frames += 1
+        ref.set_uniforms(ref_lib.uniform_block(sc.camera.matrix_world, sc.camera.fov, sc.camera.near, sc.width,
+                                               sc.height, frames, sc.max_bounces))
+        t0 = time.perf_counter()
+        _, r = ref.render_pixels(xy, sc.width, sc.height, cores)
+        t += time.perf_counter() - t0
+        rays += r
+    samples = xy.shape[0] * frames
+    full_s = t * (sc.width * sc.height * sc.spp) / samples
+    sample = (f"all {sc.width}x{sc.height} pixels x {frames} spp (the whole render)" if full_image else
+              f"{xy.shape[0]} seeded pixels x {frames} spp; full render ({sc.width}x{sc.height} x {sc.spp} spp) "
+              f"extrapolated by pixel samples")
+    return {"value": rays / t / 1e6, "unit": "Mrays/s", "samples_per_s": samples / t, "cores": cores,
+            "kind": "reference", "sample": sample, "cpu_s": t, "full_render_s": full_s}
 
 
 # ---- batching / serving ---------------------------------------------------------------------
@@ -372,28 +439,66 @@ def scene_build_section(local, sc, args):
     return out
 
 
+def primary_hit_fraction(v):
+    """Fraction of the viewport's camera rays (one per pixel, through the
+    pixel's jitter centre) that hit geometry: dspbr_camera_rays, then
+    dspbr_trace_closest over the viewport's scene."""
+    from dspbr import _lib
+    lib, h = v.ctx.lib, v.ctx.h
+    ys, xs = np.mgrid[0:v.height, 0:v.width]
+    xy = np.ascontiguousarray(np.stack([xs.ravel(), ys.ravel()], 1), np.int32)
+    n = xy.shape[0]
+    r2 = np.full((n, 2), 0.5, np.float32)
+    rays6 = np.zeros((n, 6), np.float32)
+    v.ctx.check(lib.dspbr_camera_rays(h, n, _lib.iptr(xy), _lib.fptr(r2), _lib.fptr(rays6)))
+    rays8 = np.zeros((n, 8), np.float32)
+    rays8[:, :6] = rays6
+    rays8[:, 6] = 1e30
+    tri, t, uv = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros((n, 2), np.float32)
+    v.ctx.check(lib.dspbr_trace_closest(h, v._scene.h, _lib.fptr(rays8), n, _lib.iptr(tri), _lib.fptr(t),
+                                        _lib.fptr(uv)))
+    return float((tri >= 0).mean())
+
+
+def path_statistics(v, d0, d1):
+    """What the frames between diagnostics d0 and d1 traced per path (one path
+    per pixel sample): closest-hit segments (camera + extension rays) and
+    shadow rays; and the camera rays' hit fraction."""
+    prim = max(1, d1["rays_primary"] - d0["rays_primary"])
+    return {"primary_hit_fraction": primary_hit_fraction(v),
+            "closest_segments_per_path": (prim + d1["rays_extension"] - d0["rays_extension"]) / prim,
+            "shadow_rays_per_path": (d1["rays_shadow"] - d0["rays_shadow"]) / prim}
+
+
+CONFIG_CPU_BASELINE = {"small": True, "large_framed": False, "divergence": False}  # True: the whole render
+
+
 def configs_section(local, args):
-    """The other two scene configurations at one progressive frame (1 spp) per
+    """The other scene configurations at one progressive frame (1 spp) per
     step: "small" (1,324 triangles, 512x512, 8 bounces: BVH and triangles sit
-    in L2) and "divergence" (4M triangles, 60% transmissive / volume /
-    dispersive and 20% iridescent materials, 4096x2048 env, 1280x720, 32
-    bounces, Russian roulette after bounce 4).  PCG32 per pixel sample and the
-    alias-table environment sampling; the BVH is built by the library (host
-    binned SAH).  Device time of K frames in one render call, the k_extend
-    time of the same frames, and the reference traversal's node / triangle
-    counts of one more frame for the traversal roofline."""
+    in L2), "large_framed" (the headline scene and settings seen by a camera
+    that frames the instance cloud: 72% of camera rays hit) and "divergence"
+    (4M triangles, 60% transmissive / volume / dispersive and 20% iridescent
+    materials, 4096x2048 env, 1280x720, 32 bounces, Russian roulette after
+    bounce 4).  small and divergence use PCG32 per pixel sample, large_framed
+    the headline's MWC; all use the alias-table environment sampling; the BVH
+    is built by the library.  Device time of K frames in one render call, the
+    k_extend time of the same frames, the reference traversal's node /
+    triangle counts of one more frame for the traversal roofline, and the
+    reference shader on the host cores (cpu_baseline)."""
     from dspbr import synth
     from dspbr.viewport import PathtracingCamera, PathtracingViewport
     out = {}
     peak, peak_kind = peaks()
-    for name in ("small", "divergence"):
+    for name in ("small", "large_framed", "divergence"):
         t0 = time.perf_counter()
         sc = synth.WORKLOADS[name](0)
         t1 = time.perf_counter()
         v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
                                 settings={"maxBounces": sc.max_bounces,
                                           "russianRouletteStartDepth": sc.rr_start_depth,
-                                          "rng": "pcg", "envSampling": "alias"})
+                                          "rng": "mwc" if name == "large_framed" else "pcg",
+                                          "envSampling": "alias"})
         v.setScene(sc)
         v.setIBL(sc.env)
         v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
@@ -425,6 +530,7 @@ def configs_section(local, args):
             "mrays_per_s": rays / (ms * 1e-3) / 1e6, "ms_per_frame": ms / k,
             "samples_per_s": sc.width * sc.height * k / (ms * 1e-3),
             "rays_per_frame": rays / k, "traversal_aborted": d1["traversal_aborted"] - d0["traversal_aborted"],
+            "paths": path_statistics(v, d0, d1),
             "extend_roofline": {"achieved": achieved, "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
                                 "frac": achieved / peak if achieved else None, "bytes_per_frame": alg,
                                 "nodes_per_ray": dc1["nodes_closest"] / max(1, closest),
@@ -434,7 +540,15 @@ def configs_section(local, args):
             "scene_gen_s": t1 - t0, "scene_load_s": t2 - t1,
             "full_config_estimate_s": ms / k * sc.spp / 1e3,
         }
+        if name == "large_framed":
+            out[name]["camera"] = "look_at((-48, 28, -33), (0, 5, -14)), fov 46"
+        bvh = v._scene.bvh() if not args.no_cpu_baseline else None
         v.dispose()
+        if bvh is not None:
+            cpu = cpu_config_baseline(sc, bvh, CONFIG_CPU_BASELINE[name])
+            if cpu is not None:
+                cpu["gpu_ratio"] = out[name]["mrays_per_s"] / cpu["value"]
+            out[name]["cpu_baseline"] = cpu
     return out
 
 
@@ -454,7 +568,7 @@ def gltf_section(local, args):
 def _gltf_first_frame(local, args, builder):
     from dspbr import gltf, synth
     from dspbr.viewport import PathtracingCamera, PathtracingViewport
-    from tests.gltf_writer import large_asset
+    from dspbr.gltf_writer import large_asset
     glb = large_asset().glb_bytes()
     t0 = time.perf_counter()
     sc = gltf.load_gltf(glb)
@@ -598,7 +712,7 @@ def run_reference_arm(args):
     rank, ws, local, dist = dist_setup()
     if rank != 0:
         return 0
-    sc = make_workload()
+    sc = reference_workload()
     res = cpu_reference_sample(sc, steps=args.steps, warmup=args.warmup)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference shaders compiled for the host) "
@@ -721,6 +835,7 @@ def run_gpu_arm(args):
         e2e_parts["one_frame_iterations"] = [[round(float(r[1] - tl[0, 1]), 4), int(r[2])] for r in tl]
     e2e_parts["server_stream"] = server_stream(v, sc, e2e_steps, dist)
     cs = clocks.summary()
+    paths = path_statistics(v, d0, d1)
     v.dispose()
     build = scene_build_section(local, sc, args) if ws == 1 and not args.no_serving else None
     other = configs_section(local, args) if ws == 1 and not args.no_serving else None
@@ -732,7 +847,9 @@ def run_gpu_arm(args):
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            r = cpu_reference_sample(sc, seconds=12.0)
+            # steps sized like the reference arm's (about a second of CPU work
+            # each), so that thread start-up is amortised the same way
+            r = cpu_reference_sample(sc, steps=4, warmup=1, target_s=12.0)
             if r is not None:
                 cpu = {"value": r[0], "unit": "Mrays/s", "cores": r[1], "kind": r[4], "sample": r[2]}
         line = {
@@ -749,7 +866,7 @@ def run_gpu_arm(args):
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
                          "traffic": extend_traffic(),
                          "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_extend "
-                                          "launches per frame (profiles/k_extend_dyn_large_1080p.md); achieved "
+                                          "launches per frame (one capture, profiles/); achieved "
                                           "and bytes_per_frame use the reference traversal's node/triangle counts",
                          "bytes_per_frame": alg_bytes_frame, "closest_rays_per_frame": rays_closest_frame,
                          "nodes_per_ray": d2["nodes_closest"] / max(1, rays_closest_frame),
@@ -761,6 +878,7 @@ def run_gpu_arm(args):
             "cpu_baseline": cpu,
             "clocks": cs,
             "rays_per_step": rays / max(1, args.steps),
+            "paths": paths,
             "traversal_aborted": d1["traversal_aborted"],
         }
         if build is not None:
@@ -786,7 +904,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the batching / serving sections")
     ap.add_argument("--quick-serving", action="store_true", help="small batching / serving mixes (smoke runs)")
+    ap.add_argument("--write-bvh", metavar="PATH", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.write_bvh:
+        return write_workload_bvh(args.write_bvh)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

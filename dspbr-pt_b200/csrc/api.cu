@@ -964,11 +964,29 @@ int dspbr_read_wait(dspbr_ctx* c) {
 }
 
 // tonemap (+ FXAA) of the running mean into `out` (float4 or uchar4 per pixel)
+// The canvas the display pass draws: true (and its size) when it differs from
+// the render resolution.
+static bool canvas_size(const dspbr_ctx* c, const dspbr_display* d, int* w, int* h) {
+  if (d->canvas_width <= 0 || d->canvas_height <= 0) return false;
+  if (d->canvas_width == c->width && d->canvas_height == c->height) return false;
+  *w = d->canvas_width;
+  *h = d->canvas_height;
+  return true;
+}
+
+static size_t display_pixels(const dspbr_ctx* c, const dspbr_display* d) {
+  int w = 0, h = 0;
+  return canvas_size(c, d, &w, &h) ? size_t(w) * h : size_t(c->width) * c->height;
+}
+
 static int display_pass(dspbr_ctx* c, const dspbr_display* d, bool bytes8, void** out) {
   Status s = c->st();
   size_t npix = size_t(c->width) * c->height;
   if (!c->accum.p) return s.fail(DSPBR_ERR_STATE, "read_display: no image");
   if (!(d->exposure == d->exposure)) return s.fail(DSPBR_ERR_INVALID, "read_display: exposure is NaN");
+  if (d->canvas_width < 0 || d->canvas_height < 0 || (d->canvas_width == 0) != (d->canvas_height == 0) ||
+      int64_t(d->canvas_width) * d->canvas_height > (int64_t(1) << 28))
+    return s.fail(DSPBR_ERR_INVALID, "read_display: canvas %d x %d", d->canvas_width, d->canvas_height);
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   if (c->display.n < npix) TRY_CUDA(s, c->display.alloc(npix), "alloc display buffer");
   TRY_CUDA(s, after_pending_copy(c), "read display");  // the mean buffer is the epilogue's scratch
@@ -991,13 +1009,24 @@ static int display_pass(dspbr_ctx* c, const dspbr_display* d, bool bytes8, void*
     launch_tonemap(c->accum.p, inv, p, f, int(npix), c->stream);
     *out = f;
   }
+  int dw = 0, dh = 0;
+  if (canvas_size(c, d, &dw, &dh)) {
+    const size_t n = size_t(dw) * dh;
+    if (c->present.n < n) TRY_CUDA(s, c->present.alloc(n), "alloc canvas buffer");
+    if (bytes8)
+      launch_present8(static_cast<const uchar4*>(*out), c->width, c->height,
+                      reinterpret_cast<uchar4*>(c->present.p), dw, dh, c->stream);
+    else
+      launch_present(static_cast<const float4*>(*out), c->width, c->height, c->present.p, dw, dh, c->stream);
+    *out = c->present.p;
+  }
   return s.cuda(cudaGetLastError(), "display pass");
 }
 
 int dspbr_read_display(dspbr_ctx* c, const dspbr_display* d, float* rgba, size_t num_floats) {
   if (!c || !d || !rgba) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
-  size_t npix = size_t(c->width) * c->height;
+  size_t npix = display_pixels(c, d);
   if (num_floats < npix * 4)
     return c->st().fail(DSPBR_ERR_INVALID, "read_display: buffer holds %zu floats, need %zu", num_floats, npix * 4);
   void* src = nullptr;
@@ -1009,7 +1038,7 @@ int dspbr_read_display(dspbr_ctx* c, const dspbr_display* d, float* rgba, size_t
 int dspbr_read_display_rgba8(dspbr_ctx* c, const dspbr_display* d, uint8_t* rgba8, size_t num_bytes) {
   if (!c || !d || !rgba8) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
-  size_t npix = size_t(c->width) * c->height;
+  size_t npix = display_pixels(c, d);
   if (num_bytes < npix * 4)
     return c->st().fail(DSPBR_ERR_INVALID, "read_display_rgba8: buffer holds %zu bytes, need %zu", num_bytes, npix * 4);
   void* src = nullptr;

@@ -150,6 +150,23 @@ __global__ void k_fxaa(const float4* __restrict__ img, int w, int h, float inv_w
   }
 }
 
+// display.frag: the canvas (dw x dh) draws the postprocess buffer (w x h, the
+// render resolution) as a full-screen quad; each canvas pixel samples it at
+// uv = (x + 0.5) / dw with NEAREST filtering and CLAMP_TO_EDGE
+// (gl_utils.ts:22-33, renderer.ts:689-697)
+template <class T>
+__global__ void k_present(const T* __restrict__ src, int w, int h, T* __restrict__ dst, int dw, int dh) {
+  const int n = dw * dh;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int x = p % dw, y = p / dw;
+    const float u = (float(x) + 0.5f) / float(dw), v = (float(y) + 0.5f) / float(dh);
+    int i = int(floorf(u * float(w))), j = int(floorf(v * float(h)));
+    i = i < 0 ? 0 : (i >= w ? w - 1 : i);
+    j = j < 0 ? 0 : (j >= h ? h - 1 : j);
+    dst[p] = src[size_t(j) * w + i];
+  }
+}
+
 int grid(int n) {
   int b = (n + 255) / 256;
   return b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b);
@@ -170,6 +187,13 @@ void launch_fxaa(const float4* img, int w, int h, float4* out, cudaStream_t st) 
 }
 void launch_fxaa8(const float4* img, int w, int h, uchar4* out, cudaStream_t st) {
   k_fxaa<uchar4><<<grid(w * h), 256, 0, st>>>(img, w, h, 1.0f / float(w), 1.0f / float(h), out);
+}
+
+void launch_present(const float4* src, int w, int h, float4* dst, int dw, int dh, cudaStream_t st) {
+  k_present<float4><<<grid(dw * dh), 256, 0, st>>>(src, w, h, dst, dw, dh);
+}
+void launch_present8(const uchar4* src, int w, int h, uchar4* dst, int dw, int dh, cudaStream_t st) {
+  k_present<uchar4><<<grid(dw * dh), 256, 0, st>>>(src, w, h, dst, dw, dh);
 }
 
 }  // namespace dspbr

@@ -13,8 +13,17 @@
 // keeps the contents of the last call; every row sum is rewritten before it is
 // read, so nothing needs clearing between calls, but two calls whose kernels
 // overlap on the GPU (different streams without ordering) race on it.
+//
+// The array's device address is looked up once per device and kept.  A host
+// that tears the device's context down (cudaDeviceReset) and goes on using the
+// device in the same process must not call this entry point afterwards: the
+// kept address belongs to the destroyed context.
+//
+// There is no context object here, so errors are reported on stderr, not
+// through dspbr_last_error.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -103,6 +112,14 @@ extern "C" int dspbr_ibl_tables_noalloc(const float* rgba32f, int width, int hei
   using namespace dspbr;
   if (!rgba32f || !pdf || !cdf || !ypdf || !ycdf || !total_sum || width <= 0 || height <= 0)
     return DSPBR_ERR_INVALID;
+  // the kernels read the image as float4 and write the total as a double
+  if (reinterpret_cast<uintptr_t>(rgba32f) % 16 != 0 || reinterpret_cast<uintptr_t>(total_sum) % 8 != 0 ||
+      reinterpret_cast<uintptr_t>(pdf) % 4 != 0 || reinterpret_cast<uintptr_t>(cdf) % 4 != 0 ||
+      reinterpret_cast<uintptr_t>(ypdf) % 4 != 0 || reinterpret_cast<uintptr_t>(ycdf) % 4 != 0) {
+    std::fprintf(stderr, "dspbr_ibl_tables_noalloc: rgba32f must be 16-byte aligned, total_sum 8-byte aligned and "
+                         "the tables 4-byte aligned\n");
+    return DSPBR_ERR_INVALID;
+  }
   if (height > kNoallocMaxRows) {
     std::fprintf(stderr, "dspbr_ibl_tables_noalloc: environment map has %d rows, this entry point handles at most %d\n",
                  height, kNoallocMaxRows);

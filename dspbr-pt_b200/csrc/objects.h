@@ -109,6 +109,7 @@ struct dspbr_ctx {
   dspbr::DevBuf<double4> accum;
   dspbr::DevBuf<float4> mean;
   dspbr::DevBuf<float4> display;  // display epilogue output (allocated on first use)
+  dspbr::DevBuf<float4> present;  // canvas-size output of the display pass (allocated on first use)
   float* stage = nullptr;  // page-locked staging for readback into pageable memory
   size_t stage_bytes = 0;
   // read_accum_async: the mean is computed on `stream`, copied on `copy_stream`

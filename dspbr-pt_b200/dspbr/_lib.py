@@ -63,20 +63,24 @@ class TextureArray(C.Structure):
 
 class Display(C.Structure):
     _fields_ = [("exposure", C.c_float), ("tonemapping", C.c_int32), ("gamma", C.c_int32), ("fxaa", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("canvas_width", C.c_int32), ("canvas_height", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 TONEMAPPING_MODES = ["None", "Reinhard", "Cineon", "AcesFilm"]  # renderer.ts:192
 
 
-def display_params(exposure=1.0, toneMapping="None", enableGamma=True, enableFxaa=False, **_) -> Display:
+def display_params(exposure=1.0, toneMapping="None", enableGamma=True, enableFxaa=False, canvas=None,
+                   **_) -> Display:
     """Display settings of the viewport -> dspbr_display.  A mode name outside
-    tonemappingModes selects no operator, as the reference's indexOf() = -1 does."""
+    tonemappingModes selects no operator, as the reference's indexOf() = -1 does.
+    canvas: (width, height) of the presented canvas, or None for the render size."""
     d = Display()
     d.exposure = float(exposure)
     d.tonemapping = TONEMAPPING_MODES.index(toneMapping) if toneMapping in TONEMAPPING_MODES else -1
     d.gamma = int(bool(enableGamma))
     d.fxaa = int(bool(enableFxaa))
+    if canvas is not None:
+        d.canvas_width, d.canvas_height = int(canvas[0]), int(canvas[1])
     return d
 
 

@@ -1,6 +1,8 @@
-"""A small glTF 2.0 writer for the loader tests (glTF 2.0 specification:
-buffers, buffer views, accessors, meshes, nodes, materials, images, textures;
-.gltf with an external .bin or data: URIs, and .glb)."""
+"""A small glTF 2.0 writer (glTF 2.0 specification: buffers, buffer views,
+accessors, meshes, nodes, materials, images, textures; .gltf with an external
+.bin or data: URIs, and .glb).  It makes the seeded synthetic assets that the
+loader's tests and the glTF-to-first-frame benchmark read back through
+dspbr.gltf.load_gltf."""
 from __future__ import annotations
 
 import base64

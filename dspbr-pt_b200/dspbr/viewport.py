@@ -238,7 +238,19 @@ DISPLAY_SETTINGS = ("bvhBuilder", "exposure", "toneMapping", "pixelRatio", "inte
                     "tileResolution", "debugMode")
 
 
-RESETTING_DISPLAY_SETTINGS = ("exposure", "enableGamma", "debugMode", "pixelRatio")
+RESETTING_DISPLAY_SETTINGS = ("exposure", "enableGamma", "debugMode")
+
+
+def render_resolution(display_w: int, display_h: int, pixel_ratio: float) -> tuple[int, int]:
+    """renderRes = ceil(displayRes * pixelRatio) (renderer.ts:365-369), at least 1 x 1."""
+    return max(1, math.ceil(display_w * pixel_ratio)), max(1, math.ceil(display_h * pixel_ratio))
+
+
+def check_pixel_ratio(name: str, v) -> float:
+    r = float(v)
+    if not (r > 0.0 and math.isfinite(r)):
+        raise ValueError(f"{name} must be a positive finite number, got {v!r}")
+    return r
 
 
 def apply_settings(p, settings: dict, display: dict | None = None) -> None:
@@ -300,6 +312,10 @@ class PathtracingViewport:
         self._ibl: DeviceIbl | None = None
         self.camera = PathtracingCamera(look_at_matrix((0, 0, 6), (0, 0, 0)), 45.0, 0.01)
         self.running = False
+        self.interactionActive = False
+        # displayWidth x displayHeight: the canvas (resize); width x height: the
+        # render resolution the accumulation holds, scaled by the pixel ratio
+        self.displayWidth, self.displayHeight = 0, 0
         self.width, self.height = 0, 0
         self._apply_params()
         self.resize(width, height)
@@ -321,13 +337,42 @@ class PathtracingViewport:
 
     # ---- settings (pathtracing_viewport.ts:147-170) ----
     def setSettings(self, settings: dict) -> None:
+        for k in ("pixelRatio", "interactionPixelRatio"):
+            if k in settings:
+                check_pixel_ratio(k, settings[k])
         apply_settings(self.params, settings, self._display)
         # the renderer setters of exposure, enableGamma, debugMode and every
         # render setting reset the accumulation; toneMapping, enableFxaa,
-        # interactionPixelRatio and tileResolution do not (renderer.ts:172-306)
+        # and tileResolution do not (renderer.ts:172-306)
         if any(k not in DISPLAY_SETTINGS or k in RESETTING_DISPLAY_SETTINGS for k in settings):
             self._apply_params()
+        # pixelRatio applies unless interaction mode is on, interactionPixelRatio
+        # only while it is; the renderer's pixelRatio setter resizes, which
+        # resets the accumulation (pathtracing_viewport.ts:150-157, renderer.ts:260-263)
+        if ("pixelRatio" in settings and not self.interactionActive) or \
+                ("interactionPixelRatio" in settings and self.interactionActive):
+            self._apply_size()
         self._emit_diag()
+
+    def setInteractionMode(self, active: bool) -> None:
+        """pathtracing_viewport.ts:293-298: while the user interacts, render at
+        interactionPixelRatio (0.5 by default) of the canvas resolution, else at
+        pixelRatio; either way the accumulation restarts (renderer.ts:354-363)."""
+        self.interactionActive = bool(active)
+        self._apply_size()
+        self._emit_diag()
+
+    def _pixel_ratio(self) -> float:
+        return float(self._display["interactionPixelRatio" if self.interactionActive else "pixelRatio"])
+
+    def _apply_size(self):
+        """renderer.resize(displayRes): render resolution from the active pixel
+        ratio; always resets the accumulation (renderer.ts:365-372)."""
+        self.width, self.height = render_resolution(self.displayWidth, self.displayHeight, self._pixel_ratio())
+        self._resize_device(self.width, self.height)
+
+    def _resize_device(self, w: int, h: int):
+        self.ctx.check(self.ctx.lib.dspbr_resize(self.ctx.h, w, h))
 
     def _apply_params(self):
         self.ctx.check(self.ctx.lib.dspbr_set_params(self.ctx.h, C.byref(self.params)))
@@ -391,8 +436,9 @@ class PathtracingViewport:
 
     # ---- size / progressive rendering ----
     def resize(self, width: int, height: int) -> None:
-        self.width, self.height = max(1, int(width)), max(1, int(height))
-        self.ctx.check(self.ctx.lib.dspbr_resize(self.ctx.h, self.width, self.height))
+        """The canvas size (pathtracing_viewport.ts:255-260): max(1, floor(.))."""
+        self.displayWidth, self.displayHeight = max(1, math.floor(width)), max(1, math.floor(height))
+        self._apply_size()
         self._emit_diag()
 
     def start(self, sampleLimit: int = -1, frames_per_call: int | None = None) -> None:
@@ -420,7 +466,7 @@ class PathtracingViewport:
         self._emit_diag()
 
     def readAccumulation(self, out: np.ndarray | None = None) -> np.ndarray:
-        """Running mean, (height, width, 4) float32, row 0 = bottom row.
+        """Running mean, (height, width, 4) float32 at the render resolution, row 0 = bottom row.
 
         With `out` (a C-contiguous float32 array of that shape, e.g. from
         allocReadbackBuffer()) the image is written there and `out` returned;
@@ -452,14 +498,17 @@ class PathtracingViewport:
         """The presented frame: the running mean through the reference's
         tone-mapping / gamma / FXAA passes with the viewport's display
         settings (exposure, toneMapping, enableGamma, enableFxaa;
-        renderer.ts:666-700).  rgba8: the 8-bit canvas bytes, else RGBA32F."""
-        d = _lib.display_params(**self._display)
+        renderer.ts:666-700), drawn on the canvas (displayHeight, displayWidth,
+        4): nearest-neighbour from the render resolution when the pixel ratio
+        is not 1 (display.frag).  rgba8: the 8-bit canvas bytes, else RGBA32F."""
+        d = _lib.display_params(canvas=(self.displayWidth, self.displayHeight), **self._display)
+        shape = (self.displayHeight, self.displayWidth, 4)
         if rgba8:
-            out = np.empty((self.height, self.width, 4), np.uint8)
+            out = np.empty(shape, np.uint8)
             self.ctx.check(self.ctx.lib.dspbr_read_display_rgba8(self.ctx.h, C.byref(d),
                                                                  out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size))
         else:
-            out = np.empty((self.height, self.width, 4), np.float32)
+            out = np.empty(shape, np.float32)
             self.ctx.check(self.ctx.lib.dspbr_read_display(self.ctx.h, C.byref(d), fptr(out), out.size))
         return out
 
@@ -475,7 +524,14 @@ class PathtracingViewport:
         self.ctx.check(self.ctx.lib.dspbr_get_diagnostics(self.ctx.h, C.byref(d)))
         out = d.as_dict()
         out["display"] = dict(self._display)
+        out.update(self._resolution_diag())
         return out
+
+    def _resolution_diag(self) -> dict:
+        """renderResolution / displayResolution / mode as renderer.ts:971-976 reports them."""
+        mode = "interactive" if self.interactionActive else ("accumulating" if self.running else "stopped")
+        return {"renderResolution": f"{self.width}x{self.height}",
+                "displayResolution": f"{self.displayWidth}x{self.displayHeight}", "mode": mode}
 
     def timeline(self, max_entries: int = 1024) -> np.ndarray:
         """(n, 3) float64: iteration, device clock (ms), paths queued after it;

@@ -188,9 +188,14 @@ int dspbr_ibl_destroy(dspbr_ibl* ibl);
  * double), and the work is enqueued on `stream` (a cudaStream_t, NULL for the
  * default stream) without synchronising.  Scratch is a fixed 64 KiB device
  * array inside the library, so height is limited to 16384 rows; larger maps
- * are refused with DSPBR_ERR_INVALID.  The first call on a device looks up that
- * array's address, so make it before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race on it. */
+ * are refused with DSPBR_ERR_INVALID.  rgba32f must be 16-byte aligned,
+ * total_sum 8-byte aligned and the four tables 4-byte aligned (else
+ * DSPBR_ERR_INVALID).  The first call on a device looks up that array's
+ * address and keeps it, so make it before any stream capture, and do not call
+ * this entry point after a cudaDeviceReset of that device in the same process.
+ * All calls share the array: calls that overlap on the GPU race on it.  With
+ * no context to hold a message, errors are reported on stderr, not through
+ * dspbr_last_error. */
 int dspbr_ibl_tables_noalloc(const float* rgba32f, int width, int height, float* pdf, float* cdf, float* ypdf,
                              float* ycdf, double* total_sum, void* stream);
 
@@ -224,14 +229,21 @@ int dspbr_read_accum_async(dspbr_ctx* ctx, float* rgba, size_t num_floats);
 int dspbr_read_wait(dspbr_ctx* ctx);
 /* Display epilogue (renderer.ts:666-700): the accumulation mean through
  * tonemap.frag (exposure, operator, gamma) and optionally fxaa.frag -- the
- * reference's "postprocess" buffer -- as RGBA32F, or converted to the 8-bit
- * canvas bytes. */
+ * reference's "postprocess" buffer, at the render resolution -- as RGBA32F,
+ * or converted to the 8-bit canvas bytes.  With a canvas size set, the output
+ * is the canvas instead: display.frag's nearest-neighbour draw of the
+ * postprocess buffer at that size (renderer.ts:689-697), which is how the
+ * reference presents a render resolution scaled by pixelRatio
+ * (renderer.ts:365-372); the output buffer then holds canvas_width *
+ * canvas_height pixels. */
 typedef struct dspbr_display {
   float exposure;             /* renderer.ts `exposure` (1.0) */
   int tonemapping;            /* DSPBR_TONEMAP_*: renderer.ts tonemappingModes index */
   int gamma;                  /* enableGamma: pow(c, 1/2.2) */
   int fxaa;                   /* enableFxaa */
-  int reserved[4];
+  int canvas_width;           /* displayRes; 0 (or both equal to the render size): no resampling */
+  int canvas_height;
+  int reserved[2];
 } dspbr_display;
 enum {
   DSPBR_TONEMAP_OFF = -1,     /* a mode name not in tonemappingModes: no operator, no exposure */

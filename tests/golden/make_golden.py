@@ -153,7 +153,7 @@ def main():
     g["pl_image_whf"] = np.array([W, H, F], np.int32)
     # a glTF asset packed by dspbr.gltf (scene_loader.ts), rendered by the
     # reference shaders with its textures
-    from tests.gltf_writer import sample_camera, sample_scene
+    from dspbr.gltf_writer import sample_camera, sample_scene
     from dspbr import gltf
     gs = gltf.load_gltf(sample_scene().glb_bytes())
     cam = sample_camera()

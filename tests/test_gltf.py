@@ -9,7 +9,7 @@ import pytest
 
 from dspbr import gltf, synth
 from dspbr.synth import MAT
-from tests.gltf_writer import GltfBuilder, png_bytes, quad_grid
+from dspbr.gltf_writer import GltfBuilder, png_bytes, quad_grid
 
 
 def quat_y(deg):
@@ -292,7 +292,7 @@ def packed_sha(sc) -> bytes:
 def test_sample_asset_packs_to_the_golden_buffers():
     """The asset the golden glTF image was rendered from still packs to the same bytes."""
     from tests import helpers
-    from tests.gltf_writer import sample_scene
+    from dspbr.gltf_writer import sample_scene
     g = helpers.load_golden()
     sc = gltf.load_gltf(sample_scene().glb_bytes())
     assert packed_sha(sc) == bytes(g["gltf_vertices_sha"])

@@ -100,3 +100,57 @@ def test_viewport_read_display(g):
     np.testing.assert_array_equal(shown8, ref8)
     np.testing.assert_array_equal(raw, ref_raw)
     assert shown8.dtype == np.uint8 and shown8[..., 3].min() == 255
+
+
+def nearest_canvas(img, dw, dh):
+    """display.frag's draw of a w x h buffer on a dw x dh canvas: NEAREST at
+    uv = (x + 0.5) / dw, CLAMP_TO_EDGE (gl_utils.ts:22-33), in float32."""
+    h, w = img.shape[:2]
+    u = (np.arange(dw, dtype=np.float32) + np.float32(0.5)) / np.float32(dw)
+    v = (np.arange(dh, dtype=np.float32) + np.float32(0.5)) / np.float32(dh)
+    i = np.clip(np.floor(u * np.float32(w)).astype(np.int64), 0, w - 1)
+    j = np.clip(np.floor(v * np.float32(h)).astype(np.int64), 0, h - 1)
+    return img[j[:, None], i[None, :]]
+
+
+def test_interaction_mode_renders_at_the_interaction_pixel_ratio(g):
+    """setInteractionMode(true) renders at interactionPixelRatio of the canvas
+    and restarts the accumulation; the displayed canvas is the render-size
+    postprocess buffer drawn at the canvas size (display.frag)."""
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    v = PathtracingViewport(width=67, height=45, settings={"maxBounces": 4, "toneMapping": "AcesFilm"})
+    v.setScene(sc)
+    v.setIBL(sc.env)
+    v.setCamera(helpers.camera_of(sc))
+    v.start(2)
+    full = v.readAccumulation()
+    assert full.shape == (45, 67, 4)
+    v.setInteractionMode(True)
+    d = v.diagnostics
+    assert d["sample_count"] == 0 and d["renderResolution"] == "34x23" and d["displayResolution"] == "67x45"
+    v.start(3)
+    low = v.readAccumulation()
+    assert low.shape == (23, 34, 4) and v.diagnostics["rays_primary"] == 67 * 45 * 2 + 34 * 23 * 3
+    shown = v.readDisplay(rgba8=False)
+    shown8 = v.readDisplay()
+    assert shown.shape == (45, 67, 4) and shown8.shape == (45, 67, 4)
+    c = Context(0)
+    ref, ref8 = display(c, low, 3, gamma=True)
+    c.close()
+    np.testing.assert_array_equal(shown, nearest_canvas(ref, 67, 45))
+    np.testing.assert_array_equal(shown8, nearest_canvas(ref8, 67, 45))
+    # the same camera at half resolution: the low image is the half-resolution render
+    h = PathtracingViewport(width=34, height=23, settings={"maxBounces": 4})
+    h.setScene(sc)
+    h.setIBL(sc.env)
+    h.setCamera(helpers.camera_of(sc))
+    h.start(3)
+    np.testing.assert_allclose(low, h.readAccumulation(), rtol=1e-6, atol=1e-7)
+    h.dispose()
+    # back to pixelRatio 1: full resolution, accumulation restarted
+    v.setInteractionMode(False)
+    assert v.diagnostics["sample_count"] == 0 and v.diagnostics["renderResolution"] == "67x45"
+    v.start(2)
+    np.testing.assert_allclose(v.readAccumulation(), full, rtol=1e-6, atol=1e-7)
+    v.dispose()

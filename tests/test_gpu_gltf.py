@@ -6,7 +6,7 @@ import pytest
 from dspbr import gltf, synth
 from dspbr.viewport import Bvh, PathtracingCamera, PathtracingViewport
 from tests import helpers
-from tests.gltf_writer import sample_camera, sample_scene
+from dspbr.gltf_writer import sample_camera, sample_scene
 from tests.test_gltf import packed_sha
 
 pytestmark = pytest.mark.gpu

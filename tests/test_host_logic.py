@@ -19,12 +19,24 @@ class _Recorder(viewport.PathtracingViewport):
 
     def __init__(self):
         self.params = _lib.default_params()
-        self._display = {"exposure": 1.0, "toneMapping": "None", "enableGamma": True, "enableFxaa": False}
+        self._display = {"exposure": 1.0, "toneMapping": "None", "enableGamma": True, "enableFxaa": False,
+                         "pixelRatio": 1.0, "interactionPixelRatio": 0.5}
         self._listeners = {e: set() for e in self.EVENTS}
         self.applied = 0
+        self.resizes = []  # render sizes given to dspbr_resize (each resets the accumulation)
+        self.running = False
+        self.interactionActive = False
+        self.displayWidth = self.displayHeight = self.width = self.height = 0
 
     def _apply_params(self):
         self.applied += 1
+
+    def _resize_device(self, w, h):
+        self.resizes.append((w, h))
+
+    @property
+    def diagnostics(self):
+        return self._resolution_diag()
 
 
 def test_settings_reset_accumulation_like_the_reference_setters():
@@ -42,6 +54,47 @@ def test_settings_reset_accumulation_like_the_reference_setters():
     assert v.params.max_bounces == 3 and abs(v.params.ray_eps - 1e-3) < 1e-9
     with pytest.raises(KeyError):
         v.setSettings({"noSuchSetting": 1})
+
+
+def test_pixel_ratio_and_interaction_mode_set_the_render_resolution():
+    # pathtracing_viewport.ts:147-160, 255-260, 293-298; renderer.ts:256-263, 354-372
+    v = _Recorder()
+    v.resize(801.7, 451)
+    assert (v.displayWidth, v.displayHeight) == (801, 451) and v.resizes == [(801, 451)]
+    assert v.diagnostics["renderResolution"] == "801x451" and v.diagnostics["mode"] == "stopped"
+    # interaction mode: interactionPixelRatio (0.5) -> ceil(801 * 0.5) = 401, ceil(225.5) = 226
+    v.setInteractionMode(True)
+    assert v.resizes[-1] == (401, 226) and (v.width, v.height) == (401, 226)
+    assert v.diagnostics == {"renderResolution": "401x226", "displayResolution": "801x451", "mode": "interactive"}
+    # pixelRatio changes are stored but not applied while interacting ...
+    n = len(v.resizes)
+    v.setSettings({"pixelRatio": 2.0})
+    assert len(v.resizes) == n
+    # ... interactionPixelRatio applies at once (and resets)
+    v.setSettings({"interactionPixelRatio": 0.25})
+    assert v.resizes[-1] == (201, 113)
+    # leaving interaction mode restores pixelRatio and resets even if the size is unchanged
+    v.setInteractionMode(False)
+    assert v.resizes[-1] == (1602, 902)
+    v.setInteractionMode(False)
+    assert v.resizes[-2:] == [(1602, 902), (1602, 902)]
+    # outside interaction mode: pixelRatio applies, interactionPixelRatio is stored
+    v.setSettings({"pixelRatio": 0.75})
+    assert v.resizes[-1] == (601, 339)
+    n = len(v.resizes)
+    v.setSettings({"interactionPixelRatio": 0.5})
+    assert len(v.resizes) == n and v._display["interactionPixelRatio"] == 0.5
+    # a canvas resize keeps the ratio
+    v.resize(100, 10)
+    assert v.resizes[-1] == (75, 8)
+    assert viewport.render_resolution(3, 3, 1e-9) == (1, 1)
+    for bad in (0.0, -1.0, float("nan"), float("inf")):
+        with pytest.raises(ValueError):
+            v.setSettings({"pixelRatio": bad})
+    # the canvas size reaches dspbr_display
+    d = _lib.display_params(canvas=(801, 451))
+    assert (d.canvas_width, d.canvas_height) == (801, 451)
+    assert _lib.display_params().canvas_width == 0
 
 
 def test_display_mode_mapping():
