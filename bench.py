@@ -322,6 +322,13 @@ def _one_at_a_time(ctx, dev, mix):
     from dspbr import _lib
     lib, h = ctx.lib, ctx.h
     times, imgs = [], []
+    busy = {"device_ms": 0.0, "rays": 0}
+
+    def diag():
+        d = _lib.Diag()
+        ctx.check(lib.dspbr_get_diagnostics(h, C.byref(d)))
+        return d
+
     big = max(mix, key=lambda r: r["width"] * r["height"] * r["spp"])
     outs = _images([big] + list(mix))
     for k, r in enumerate([big] + list(mix)):
@@ -335,6 +342,7 @@ def _one_at_a_time(ctx, dev, mix):
         ctx.check(lib.dspbr_set_params(h, C.byref(p)))
         ctx.check(lib.dspbr_set_camera(h, _lib.fptr(m), float(r["camera"].fov), float(r["camera"].near)))
         ctx.check(lib.dspbr_resize(h, r["width"], r["height"]))
+        d0 = diag()
         ctx.check(lib.dspbr_render(h, r["spp"]))
         out = outs[k]
         ctx.check(lib.dspbr_read_accum(h, _lib.fptr(out), out.size))
@@ -342,6 +350,16 @@ def _one_at_a_time(ctx, dev, mix):
             continue
         times.append(time.perf_counter() - t0)
         imgs.append(out)
+        d1 = diag()
+        # device time of the render call (CUDA events around it on the context's stream)
+        busy["device_ms"] += d1.last_render_ms
+        busy["rays"] += sum(getattr(d1, f) - getattr(d0, f) for f in ("rays_primary", "rays_extension",
+                                                                      "rays_shadow"))
+    wall = sum(times)
+    busy.update({"wall_ms": 1e3 * wall, "device_busy_fraction": busy["device_ms"] / (1e3 * wall),
+                 "mrays_per_s_wall": busy["rays"] / wall / 1e6,
+                 "mrays_per_s_device": busy["rays"] / (busy["device_ms"] * 1e-3) / 1e6})
+    _one_at_a_time.busy = busy
     return times, imgs
 
 
@@ -642,8 +660,14 @@ def serving_section(local, quick=False):
         "sample_frames_per_s": spp_total / t_batch, "mrays_per_s": rays_b / t_batch / 1e6,
         "p50_ms": _pct(lat, 0.5), "p99_ms": _pct(lat, 0.99),
         "max_abs_diff_vs_one_at_a_time": diff, "scene_gen_s": gen_s,
-        "autotuned": {k: tuned[k] for k in ("path_pool", "trace_threads", "trace_blocks", "shade_threads",
-                                            "shade_blocks")}}
+        "autotuned": {k: tuned[k] for k in ("path_pool", "trace_threads", "trace_blocks", "connect_blocks",
+                                            "shade_threads", "shade_blocks", "autotune_source")},
+        "one_at_a_time_busy": dict(_one_at_a_time.busy),
+        # speedup = (1 / busy fraction of the one-at-a-time arm) x (batched ray
+        # rate / the one-at-a-time arm's ray rate while its GPU is busy)
+        "speedup_decomposition": {
+            "idle_removed": 1.0 / _one_at_a_time.busy["device_busy_fraction"],
+            "ray_rate_gain": (rays_b / t_batch / 1e6) / _one_at_a_time.busy["mrays_per_s_device"]}}
     for i in ids:
         srv.release(i)
     for d in bdev:
@@ -657,6 +681,7 @@ def serving_section(local, quick=False):
     smix = synth.request_mix(22, n, ns, 256 * 256, 1920 * 1080, 16, 256, 30.0, 90.0, 12, aspect_hi=16 / 9)
     gen_s = time.perf_counter() - t0
     t_single, imgs1 = _one_at_a_time(ctx, sdev, smix)
+    busy_serving = dict(_one_at_a_time.busy)
     rates = []
     for rate in ((10.0, 50.0, 200.0, 500.0) if not quick else (50.0,)):
         arr = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))
@@ -699,6 +724,7 @@ def serving_section(local, quick=False):
     res["serving"] = {"scenes": ns, "scene_triangles": [int(d[2].num_triangles) for d in sdev],
                       "hbm_budget_gb": 120, "bytes_peak": st["bytes_peak"], "scene_gen_s": gen_s,
                       "one_at_a_time_service_s": {"p50": _pct(t_single, 0.5), "max": max(t_single)},
+                      "one_at_a_time_busy": busy_serving,
                       "rates": rates}
     srv.close()
     for d in sdev:

@@ -1133,6 +1133,20 @@ int dspbr_get_timeline(dspbr_ctx* c, uint32_t max_entries, uint64_t* iteration, 
   return DSPBR_OK;
 }
 
+int dspbr_get_device_info(dspbr_ctx* c, dspbr_device_info* info) {
+  if (!c || !info) return DSPBR_ERR_INVALID;
+  Status s = c->st();
+  cudaDeviceProp prop{};
+  TRY_CUDA(s, cudaGetDeviceProperties(&prop, c->device), "device properties");
+  std::memset(info, 0, sizeof *info);
+  std::snprintf(info->name, sizeof info->name, "%s", prop.name);
+  info->sm_count = prop.multiProcessorCount;
+  info->cc_major = prop.major;
+  info->cc_minor = prop.minor;
+  info->total_bytes = uint64_t(prop.totalGlobalMem);
+  return DSPBR_OK;
+}
+
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   if (!c || !d) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }

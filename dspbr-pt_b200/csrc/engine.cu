@@ -126,7 +126,10 @@ int Engine::reset_pool() {
 
 void Engine::set_launch(const LaunchCfg& lc) {
   if (lc.trace_blocks == lc_.trace_blocks && lc.trace_threads == lc_.trace_threads &&
-      lc.shade_blocks == lc_.shade_blocks && lc.shade_threads == lc_.shade_threads)
+      lc.shade_blocks == lc_.shade_blocks && lc.shade_threads == lc_.shade_threads &&
+      lc.dyn_blocks == lc_.dyn_blocks && lc.connect_dyn_blocks == lc_.connect_dyn_blocks &&
+      lc.shade_dyn_blocks[0] == lc_.shade_dyn_blocks[0] &&
+      lc.shade_dyn_blocks[1] == lc_.shade_dyn_blocks[1])
     return;
   cudaStreamSynchronize(stream_);
   drop_graph();

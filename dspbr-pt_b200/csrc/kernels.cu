@@ -973,20 +973,31 @@ static int grid_for(uint64_t n, int threads, int cap) {
   return int(b < uint64_t(cap) ? b : uint64_t(cap));
 }
 
-void init_launch_sizes(LaunchCfg& lc) {
-  int dev = 0, sms = 148, n = 0;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+LaunchLimits launch_limits() {
+  LaunchLimits l{148, 8, 8, {5, 5}};
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev);
   auto resident = [&](const void* fn, int threads, int fallback) {
-    n = 0;
+    int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0) != cudaSuccess || n <= 0) {
       cudaGetLastError();
       n = fallback;
     }
-    return n * sms;
+    return n;
   };
-  lc.dyn_blocks = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
-  lc.shade_dyn_blocks[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 5);
-  lc.shade_dyn_blocks[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 5);
+  l.trace_per_sm = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
+  l.connect_per_sm = resident(reinterpret_cast<const void*>(k_connect_dyn), 128, 8);
+  l.shade_per_sm[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 5);
+  l.shade_per_sm[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 5);
+  return l;
+}
+
+void init_launch_sizes(LaunchCfg& lc) {
+  const LaunchLimits l = launch_limits();
+  lc.dyn_blocks = l.trace_per_sm * l.sms;
+  lc.connect_dyn_blocks = l.connect_per_sm * l.sms;
+  lc.shade_dyn_blocks[0] = l.shade_per_sm[0] * l.sms;
+  lc.shade_dyn_blocks[1] = l.shade_per_sm[1] * l.sms;
 }
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
@@ -1015,7 +1026,7 @@ void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
   if (count) k_connect<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
-  else if (lc.traversal == kTravWide) k_connect_dyn<<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_connect_dyn<<<lc.connect_dyn_blocks, 128, 0, st>>>(sc, b, cur);
   else if (lc.traversal == kTravReference) k_connect<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
   else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }

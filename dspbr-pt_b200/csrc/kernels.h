@@ -162,7 +162,8 @@ struct LaunchCfg {
   int shade_blocks = 148 * 8, shade_threads = 128;
   int traversal = kTravPerPath;
   bool textured = false;  // some active job samples material textures
-  int dyn_blocks = 148 * 8;  // k_extend / k_connect: resident blocks of 128 threads (64 registers)
+  int dyn_blocks = 148 * 8;          // k_extend_dyn: resident blocks of 128 threads (64 registers)
+  int connect_dyn_blocks = 148 * 8;  // k_connect_dyn: the same
   // resident blocks of the persistent shading kernels (set by init_launch_sizes)
   int shade_dyn_blocks[2] = {148 * 5, 148 * 5};  // k_shade<false>, k_shade<true>, 128 threads
 };
@@ -170,6 +171,11 @@ struct LaunchCfg {
 void launch_init_pool(const PathBuf& b, cudaStream_t st);
 // resident-block counts of the persistent kernels on this device (occupancy API)
 void init_launch_sizes(LaunchCfg& lc);
+// the most blocks per SM each persistent kernel can keep resident, and the SM count
+struct LaunchLimits {
+  int sms, trace_per_sm, connect_per_sm, shade_per_sm[2];
+};
+LaunchLimits launch_limits();
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);

@@ -534,10 +534,11 @@ int dspbr_server_get_stats(dspbr_server* s, dspbr_server_stats* out) {
   }
   out->path_pool = s->eng->capacity();
   const LaunchCfg& lc = s->eng->launch();
-  out->trace_threads = lc.trace_threads;
-  out->trace_blocks = lc.trace_blocks;
-  out->shade_threads = lc.shade_threads;
-  out->shade_blocks = lc.shade_blocks;
+  out->trace_threads = 128;
+  out->trace_blocks = lc.dyn_blocks;
+  out->shade_threads = 128;
+  out->shade_blocks = lc.shade_dyn_blocks[0];
+  out->connect_blocks = lc.connect_dyn_blocks;
   return DSPBR_OK;
 }
 
@@ -570,6 +571,48 @@ int dspbr_server_destroy(dspbr_server* s) {
 // steady state (full pool) on the sample requests with CUDA events over a
 // fixed number of graph-launched iterations; the score is traced rays per
 // second from the device counters.
+int dspbr_server_get_launch(dspbr_server* s, dspbr_launch* out) {
+  if (!s || !out) return DSPBR_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = dspbr_launch{};
+  out->path_pool = s->eng->capacity();
+  const LaunchCfg& lc = s->eng->launch();
+  out->extend_blocks = lc.dyn_blocks;
+  out->connect_blocks = lc.connect_dyn_blocks;
+  out->shade_blocks = lc.shade_dyn_blocks[0];
+  return DSPBR_OK;
+}
+
+int dspbr_server_set_launch(dspbr_server* s, const dspbr_launch* l) {
+  if (!s || !l) return DSPBR_ERR_INVALID;
+  Status st = s->st();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->running) return st.fail(DSPBR_ERR_STATE, "set_launch: call while the server is idle");
+  }
+  TRY_CUDA(st, cudaSetDevice(s->device), "cudaSetDevice");
+  const LaunchLimits L = launch_limits();
+  auto ok = [&](int blocks, int per_sm) { return blocks >= L.sms && blocks % L.sms == 0 && blocks <= per_sm * L.sms; };
+  if (!ok(l->extend_blocks, L.trace_per_sm) || !ok(l->connect_blocks, L.connect_per_sm) ||
+      !ok(l->shade_blocks, L.shade_per_sm[0]))
+    return st.fail(DSPBR_ERR_INVALID, "set_launch: grids must be 1..%d / %d / %d x %d SMs", L.trace_per_sm,
+                   L.connect_per_sm, L.shade_per_sm[0], L.sms);
+  if (l->path_pool < 1024 || l->path_pool > (1u << 26))
+    return st.fail(DSPBR_ERR_INVALID, "set_launch: path pool %u outside 1024..2^26", l->path_pool);
+  Engine& E = *s->eng;
+  int rc = E.set_active({});
+  if (!rc) rc = l->path_pool != E.capacity() ? E.ensure_pool(l->path_pool) : E.reset_pool();
+  if (rc) return rc;
+  LaunchCfg lc = E.launch();
+  lc.dyn_blocks = l->extend_blocks;
+  lc.connect_dyn_blocks = l->connect_blocks;
+  lc.shade_dyn_blocks[0] = l->shade_blocks;
+  lc.shade_dyn_blocks[1] = std::min(l->shade_blocks / L.sms, L.shade_per_sm[1]) * L.sms;
+  E.set_launch(lc);
+  s->cfg.path_pool = l->path_pool;
+  return st.cuda(cudaStreamSynchronize(s->stream), "set_launch");
+}
+
 int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, double seconds) {
   if (!s || !samples || n <= 0 || n > kMaxJobs) return DSPBR_ERR_INVALID;
   Status st = s->st();
@@ -646,10 +689,28 @@ int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, 
     }
     return DSPBR_OK;
   };
-  // the path kernels size their grids from the occupancy API: the pool size is
-  // what is left to choose
   for (uint32_t pool : {1u << 20, 1u << 21, 1u << 22, 1u << 23})
     if (!rc && pool != best_pool) rc = consider(pool, best);
+  // then the grids of the persistent kernels: resident blocks per SM from the
+  // occupancy limit down (fewer blocks: more L1 per block, less contention on
+  // the queue cursors; the limit: more warps to hide memory latency)
+  const LaunchLimits L = launch_limits();
+  for (int k = L.trace_per_sm - 1; k >= std::max(2, L.trace_per_sm - 4) && !rc; --k) {
+    LaunchCfg lc = best;
+    lc.dyn_blocks = k * L.sms;
+    rc = consider(best_pool, lc);
+  }
+  for (int k = L.connect_per_sm - 1; k >= std::max(2, L.connect_per_sm - 4) && !rc; --k) {
+    LaunchCfg lc = best;
+    lc.connect_dyn_blocks = k * L.sms;
+    rc = consider(best_pool, lc);
+  }
+  for (int k = L.shade_per_sm[0] - 1; k >= std::max(2, L.shade_per_sm[0] - 3) && !rc; --k) {
+    LaunchCfg lc = best;
+    lc.shade_dyn_blocks[0] = k * L.sms;
+    lc.shade_dyn_blocks[1] = std::min(k, L.shade_per_sm[1]) * L.sms;
+    rc = consider(best_pool, lc);
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   // leave an empty pool of the chosen size with the chosen launch sizes

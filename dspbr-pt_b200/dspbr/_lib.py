@@ -109,10 +109,24 @@ class ServerStats(C.Structure):
                 ("iterations", C.c_uint64), ("rays_closest", C.c_uint64), ("rays_shadow", C.c_uint64),
                 ("bytes_in_use", C.c_uint64), ("bytes_peak", C.c_uint64), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("path_pool", C.c_uint32), ("trace_threads", C.c_int32),
-                ("trace_blocks", C.c_int32), ("shade_threads", C.c_int32), ("shade_blocks", C.c_int32)]
+                ("trace_blocks", C.c_int32), ("shade_threads", C.c_int32), ("shade_blocks", C.c_int32),
+                ("connect_blocks", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Launch(C.Structure):
+    _fields_ = [("path_pool", C.c_uint32), ("extend_blocks", C.c_int32), ("connect_blocks", C.c_int32),
+                ("shade_blocks", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("sm_count", C.c_int32), ("cc_major", C.c_int32),
+                ("cc_minor", C.c_int32), ("total_bytes", C.c_uint64)]
 
 
 REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = 0, 1, 2, 3, 4
@@ -190,6 +204,9 @@ SIGNATURES = {
     "dspbr_server_release": (C.c_int, [_V, C.c_uint64]),
     "dspbr_server_get_stats": (C.c_int, [_V, C.POINTER(ServerStats)]),
     "dspbr_server_autotune": (C.c_int, [_V, C.POINTER(Request), C.c_int, C.c_double]),
+    "dspbr_server_get_launch": (C.c_int, [_V, C.POINTER(Launch)]),
+    "dspbr_server_set_launch": (C.c_int, [_V, C.POINTER(Launch)]),
+    "dspbr_get_device_info": (C.c_int, [_V, C.POINTER(DeviceInfo)]),
     "dspbr_server_destroy": (C.c_int, [_V]),
 }
 

@@ -9,6 +9,8 @@ mean image into the request's output array.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
 
 import numpy as np
 
@@ -18,6 +20,30 @@ from .viewport import Context, DeviceIbl, DeviceScene, PathtracingCamera, apply_
 
 STATES = {_lib.REQ_QUEUED: "queued", _lib.REQ_RUNNING: "running", _lib.REQ_DONE: "done",
           _lib.REQ_CANCELLED: "cancelled", _lib.REQ_FAILED: "failed"}
+
+
+def autotune_cache_path() -> str:
+    """The autotuner's cache beside the shared library."""
+    return os.path.join(os.path.dirname(os.path.abspath(_lib.LIB_PATH)), "autotune.json")
+
+
+def load_tuning(path: str) -> dict:
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d if isinstance(d, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def store_tuning(path: str, key: str, launch: dict) -> None:
+    """Adds (or replaces) one GPU's entry; written to a temporary file and renamed."""
+    d = load_tuning(path)
+    d[key] = {k: int(v) for k, v in launch.items()}
+    tmp = f"{path}.{os.getpid()}.tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
 
 
 class Server:
@@ -101,9 +127,43 @@ class Server:
         self._check(self.lib.dspbr_server_get_stats(self.h, C.byref(st)))
         return st.as_dict()
 
-    def autotune(self, samples: list, seconds: float = 10.0) -> dict:
+    def autotune(self, samples: list, seconds: float = 10.0, cache: str | None = None) -> dict:
         """samples: requests from request(); renders them under candidate pool
-        and block sizes and keeps the fastest.  Before the first submit."""
+        and block sizes and keeps the fastest.  Before the first submit.
+
+        cache: a JSON file of earlier choices keyed by GPU (name, SM count,
+        compute capability) and library build (size and modification time of
+        the shared object), e.g. autotune_cache_path(): an entry for this GPU
+        and build is applied without tuning; otherwise the tuner runs and its
+        choice is added to the file.  Returns the stats with the launch sizes
+        in use and "autotune_source" ("cache" or "tuned")."""
+        key = self.tuning_key()
+        if cache is not None:
+            entry = load_tuning(cache).get(key)
+            if entry is not None:
+                self.set_launch(entry)
+                return dict(self.stats(), autotune_source="cache")
         arr = (_lib.Request * len(samples))(*[s[0] if isinstance(s, tuple) else s for s in samples])
         self._check(self.lib.dspbr_server_autotune(self.h, arr, len(samples), float(seconds)))
-        return self.stats()
+        if cache is not None:
+            store_tuning(cache, key, self.launch())
+        return dict(self.stats(), autotune_source="tuned")
+
+    def launch(self) -> dict:
+        """Path pool and the grids of the persistent extend / connect / shade kernels in use."""
+        lc = _lib.Launch()
+        self._check(self.lib.dspbr_server_get_launch(self.h, C.byref(lc)))
+        return lc.as_dict()
+
+    def set_launch(self, launch: dict) -> None:
+        lc = _lib.Launch()
+        for k in ("path_pool", "extend_blocks", "connect_blocks", "shade_blocks"):
+            setattr(lc, k, int(launch[k]))
+        self._check(self.lib.dspbr_server_set_launch(self.h, C.byref(lc)))
+
+    def tuning_key(self) -> str:
+        info = _lib.DeviceInfo()
+        self.ctx.check(self.lib.dspbr_get_device_info(self.ctx.h, C.byref(info)))
+        st = os.stat(_lib.LIB_PATH)
+        return (f"{info.name.decode()}|sm{info.sm_count}|cc{info.cc_major}{info.cc_minor}|"
+                f"lib{st.st_size}-{int(st.st_mtime)}")

@@ -266,6 +266,15 @@ int dspbr_display_image(dspbr_ctx* ctx, const float* rgba, int width, int height
 int dspbr_host_alloc(dspbr_ctx* ctx, size_t bytes, void** out);
 int dspbr_host_free(dspbr_ctx* ctx, void* ptr);
 int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
+/* The context's GPU (diagnostics.backend's counterpart, renderer.ts:79-110):
+ * name, SM count, compute capability, device memory; keys per-GPU caches
+ * such as the autotuner's. */
+typedef struct dspbr_device_info {
+  char name[256];
+  int sm_count, cc_major, cc_minor;
+  uint64_t total_bytes;
+} dspbr_device_info;
+int dspbr_get_device_info(dspbr_ctx* ctx, dspbr_device_info* info);
 /* The last iterations of the path engine (at most max_entries, at most 1024),
  * oldest first: iteration number, device clock (ns) at its end and the paths
  * queued for the next one.  New: the reference renders one full-screen pass
@@ -356,8 +365,21 @@ typedef struct dspbr_server_stats {
   uint64_t bytes_in_use, bytes_peak;
   double p50_ms, p99_ms;      /* submit -> done latency of completed requests */
   uint32_t path_pool;
-  int trace_threads, trace_blocks, shade_threads, shade_blocks;  /* launch sizes in use */
+  /* launch sizes in use: threads per block and grid (resident blocks) of the
+   * persistent extend (trace_*), shade and connect kernels */
+  int trace_threads, trace_blocks, shade_threads, shade_blocks;
+  int connect_blocks;
 } dspbr_server_stats;
+
+/* Launch sizes of the path kernels, as the autotuner chooses them: the path
+ * pool and the grids (resident blocks of 128 threads) of the persistent
+ * extend, connect and shade kernels.  A grid is a multiple of the SM count, at
+ * least one and at most the kernel's occupancy limit per SM. */
+typedef struct dspbr_launch {
+  uint32_t path_pool;
+  int extend_blocks, connect_blocks, shade_blocks;
+  int reserved[4];
+} dspbr_launch;
 
 int dspbr_server_create(dspbr_ctx* ctx, const dspbr_server_config* cfg, dspbr_server** out);
 /* queue a request; DSPBR_ERR_ADMISSION if it can never fit the budget */
@@ -372,10 +394,18 @@ int dspbr_server_cancel(dspbr_server* srv, uint64_t id);
 /* forgets a finished request (its info is no longer available) */
 int dspbr_server_release(dspbr_server* srv, uint64_t id);
 int dspbr_server_get_stats(dspbr_server* srv, dspbr_server_stats* stats);
-/* Autotuner: renders the sample requests (results discarded) under candidate
- * path-pool sizes (2^20..2^23, within half the HBM budget), keeps the fastest
- * in rays per second.  Call while the server is idle.  seconds bounds the time. */
+/* Autotuner: renders the sample requests (results discarded) in steady state
+ * under candidate launch sizes and keeps the fastest in rays per second, one
+ * coordinate at a time: the path pool (2^20..2^23, within half the HBM
+ * budget), then the resident blocks per SM of the extend, connect and shade
+ * kernels (from the occupancy limit down).  Call while the server is idle.
+ * seconds bounds the time.  New: the reference has one fixed fragment-shader
+ * pass (renderer.ts:512-565) and nothing to tune. */
 int dspbr_server_autotune(dspbr_server* srv, const dspbr_request* samples, int n, double seconds);
+/* The launch sizes in use, and setting them (an idle server only; e.g. the
+ * autotuner's choice cached from an earlier run on the same GPU). */
+int dspbr_server_get_launch(dspbr_server* srv, dspbr_launch* launch);
+int dspbr_server_set_launch(dspbr_server* srv, const dspbr_launch* launch);
 int dspbr_server_destroy(dspbr_server* srv);
 
 #ifdef __cplusplus

@@ -1,11 +1,12 @@
 #!/bin/sh
 # ORACLE TEST INFRASTRUCTURE: compiles the reference's own shader sources
-# (read from the reference checkout, default /root/reference) as C++ into
+# (read from the reference checkout: $DSPBR_REFERENCE, else the directory
+# "reference" beside this repository) as C++ into
 # oracle/_ref/ (git-ignored).  FP32 and FP64 variants.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 ORACLE=$(dirname "$HERE")
-REF=${DSPBR_REFERENCE:-/root/reference}
+REF=${DSPBR_REFERENCE:-$(dirname "$ORACLE")/../reference}
 OUT="$ORACLE/_ref"
 CXX=${CXX:-g++}
 if [ ! -f "$REF/packages/lib/shader/renderer.frag" ]; then

@@ -132,16 +132,29 @@ def test_hbm_budget_admission(world):
     srv.close()
 
 
-def test_autotune_then_serve(world):
+def test_autotune_then_serve(world, tmp_path):
     ctx, hosts, scenes, ibls = world
     srv = Server(ctx)
     samples = [srv.request(scenes[i], ibls[i], _cam(hosts[i]), 256, 256, 4)[0] for i in (0, 1)]
-    st = srv.autotune(samples, seconds=5.0)
+    cache = str(tmp_path / "autotune.json")
+    st = srv.autotune(samples, seconds=8.0, cache=cache)
+    assert st["autotune_source"] == "tuned"
     assert st["path_pool"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
-    assert st["trace_threads"] in (64, 128, 256) and st["shade_threads"] in (64, 128, 256)
+    assert st["trace_threads"] == 128 and st["shade_threads"] == 128
+    sms = 148
+    for k in ("trace_blocks", "connect_blocks", "shade_blocks"):
+        assert st[k] % sms == 0 and sms <= st[k] <= 8 * sms, (k, st[k])
+    chosen = srv.launch()
     r = _requests(world)[0]
     img, info = srv.wait(_submit(srv, world, r))
     srv.close()
+    # a second server on the same GPU takes the cached choice without tuning
+    again = Server(ctx)
+    st2 = again.autotune(samples, seconds=8.0, cache=cache)
+    assert st2["autotune_source"] == "cache" and again.launch() == chosen
+    with pytest.raises(_lib.DspbrError):
+        again.set_launch(dict(chosen, extend_blocks=chosen["extend_blocks"] + 1))  # not a multiple of the SMs
+    again.close()
     ref_srv = Server(ctx, path_pool=1 << 16)
     ref, _ = ref_srv.wait(_submit(ref_srv, world, r))
     ref_srv.close()

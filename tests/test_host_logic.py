@@ -161,3 +161,18 @@ def test_first_scene_light_sets_the_point_light():
     assert not viewport.apply_scene_lights(p, [{"position": (1, 2, 3), "type": 0, "emission": (4, 5, 6)}])
     assert viewport.apply_scene_lights(p, [])
     assert tuple(p.point_light_position) == (0, 0, 0, 0)
+
+
+def test_autotune_cache_round_trip(tmp_path):
+    from dspbr import server
+    path = str(tmp_path / "autotune.json")
+    assert server.load_tuning(path) == {}
+    a = {"path_pool": 1 << 22, "extend_blocks": 1184, "connect_blocks": 1036, "shade_blocks": 740}
+    server.store_tuning(path, "NVIDIA B200|sm148|cc100|lib1-2", a)
+    server.store_tuning(path, "other|sm1|cc00|lib3-4", dict(a, path_pool=1 << 20))
+    d = server.load_tuning(path)
+    assert d["NVIDIA B200|sm148|cc100|lib1-2"] == a and d["other|sm1|cc00|lib3-4"]["path_pool"] == 1 << 20
+    with open(path, "w") as f:
+        f.write("not json")
+    assert server.load_tuning(path) == {}
+    assert server.autotune_cache_path().endswith(os.path.join("dspbr", "autotune.json"))
