@@ -843,11 +843,22 @@ def run_gpu_arm(args):
 
     e2e_run(True)  # untimed: the second buffer's first use
     e2e_serial, parts_serial = e2e_run(False)
+    e2e_copy, parts_copy = e2e_run(True)
+    # pipelined frames: step k+1's samples start while step k's last paths
+    # finish; step k's image is copied as soon as they have
+    v.setSettings({"pipelinedFrames": True})
+    e2e_run(True)  # untimed: the second sum buffer's first use
     e2e_value, parts = e2e_run(True)
+    v.setSettings({"pipelinedFrames": False})
     e2e_parts = {"set_camera_ms": 1e3 * parts[0], "render_1_frame_ms": 1e3 * parts[1],
                  "read_wait_and_enqueue_ms": 1e3 * parts[2],
-                 "readback": "pipelined: step k's device-to-host copy runs during step k+1's render; "
-                             "the last step's copy is waited for inside the timed region",
+                 "frames": "pipelined (viewport setting pipelinedFrames): a step's render returns once its "
+                           "samples have started; its last paths finish during the next step's render",
+                 "readback": "step k's device-to-host copy starts when its paths have finished and runs during "
+                             "step k+1's render; the last step's paths and copy are waited for inside the "
+                             "timed region",
+                 "frames_not_pipelined": {"value": e2e_copy, "render_1_frame_ms": 1e3 * parts_copy[1],
+                                          "read_wait_and_enqueue_ms": 1e3 * parts_copy[2]},
                  "serial": {"value": e2e_serial, "render_1_frame_ms": 1e3 * parts_serial[1],
                             "read_accumulation_ms": 1e3 * parts_serial[2]}}
     # the iterations of one more single-frame call (untimed): device clock at

@@ -69,11 +69,77 @@ WaveParams make_job_params(const dspbr_params& q, const float matrix[16], float 
 // Joins the worker of a render_async call, so that the caller's next stream
 // operation is ordered after all of that render's launches.  Returns the
 // worker's status.
-static int settle(dspbr_ctx* c) {
+// A copy of read_accum_async may still be reading the mean buffer: the
+// stream's next writes to it wait for that copy.
+static cudaError_t after_pending_copy(dspbr_ctx* c) {
+  return c->copy_pending ? cudaStreamWaitEvent(c->stream, c->ev_copied, 0) : cudaSuccess;
+}
+
+// Joins the render_async worker; returns its status.
+static int settle_worker(dspbr_ctx* c) {
   if (c->worker.joinable()) c->worker.join();
   int rc = c->worker_rc;
   c->worker_rc = 0;
   return rc;
+}
+
+// Mean and device-to-host copy of an epoch's sums on the copy stream, after
+// `after` (recorded on the context's stream) when given.
+static int issue_read(dspbr_ctx* c, const double4* accum, uint64_t count, float* dst, cudaEvent_t after) {
+  Status s = c->st();
+  const size_t npix = size_t(c->width) * c->height;
+  const double inv = count ? 1.0 / double(count) : 0.0;
+  if (!after) {
+    TRY_CUDA(s, cudaEventRecord(c->ev_mean, c->stream), "event");
+    after = c->ev_mean;
+  }
+  TRY_CUDA(s, cudaStreamWaitEvent(c->copy_stream, after, 0), "read accumulation");
+  launch_mean(accum, inv, c->mean.p, int(npix), c->copy_stream);
+  TRY_CUDA(s, cudaGetLastError(), "read accumulation");
+  TRY_CUDA(s, cudaMemcpyAsync(dst, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->copy_stream), "read accumulation");
+  TRY_CUDA(s, cudaEventRecord(c->ev_copied, c->copy_stream), "event");
+  c->copy_pending = true;
+  return DSPBR_OK;
+}
+
+// Pipelined frames: finishes every path of the context's epochs in the pool
+// (the render loop with its tail drain) and enqueues a deferred read.
+static int flush_pipeline(dspbr_ctx* c) {
+  if (!c->tail_live && !c->prev_live && !c->deferred) return DSPBR_OK;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  Engine& E = *c->eng;
+  if (c->tail_live || c->prev_live) {
+    std::vector<int> act;
+    if (c->prev_live) act.push_back(c->slot ^ 1);
+    if (c->tail_live) act.push_back(c->slot);
+    int rc = E.set_active(act);
+    // every work item has started: iterations until fewer than the drain
+    // threshold of paths are alive, then the tail drain (the bound only
+    // guards the loop: a path lives at most max_bounces + 1 iterations)
+    if (!rc) rc = E.run_loop(act.back(), 4096 + 8);
+    if (rc) return rc;
+    if (c->prev_live && !E.job_done(c->slot ^ 1))
+      return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: previous frame not finished by the drain");
+    c->tail_live = c->prev_live = false;
+  }
+  if (c->deferred) {
+    float* dst = c->deferred;
+    const bool prev = c->deferred_prev;
+    c->deferred = nullptr;
+    c->deferred_prev = false;
+    return issue_read(c, prev ? c->accum_prev.p : c->accum.p, prev ? c->prev_sample_count : c->sample_count, dst,
+                      nullptr);
+  }
+  return DSPBR_OK;
+}
+
+// Joins the render_async worker and finishes pipelined frames: the state every
+// call that is not pipeline-aware starts from.
+static int settle(dspbr_ctx* c) {
+  int rc = settle_worker(c);
+  if (rc) return rc;
+  return c->pipelined ? flush_pipeline(c) : DSPBR_OK;
 }
 
 // Texture slots of the material record (material.ts layout): 39, 44-59, 63.
@@ -276,6 +342,7 @@ int dspbr_destroy(dspbr_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_mean) cudaEventDestroy(c->ev_mean);
   if (c->ev_copied) cudaEventDestroy(c->ev_copied);
+  if (c->ev_between) cudaEventDestroy(c->ev_between);
   c->eng.reset();
   if (c->stage) cudaFreeHost(c->stage);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -721,8 +788,28 @@ int dspbr_resize(dspbr_ctx* c, int w, int h) {
 
 int dspbr_reset(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
-  { int rc_ = settle(c); if (rc_) return rc_; }
+  { int rc_ = settle_worker(c); if (rc_) return rc_; }
   Status s = c->st();
+  if (c->pipelined && c->tail_live) {
+    if (c->prev_live || (c->deferred && c->deferred_prev)) {
+      int rc = flush_pipeline(c);
+      if (rc) return rc;
+    } else {
+      // a new epoch in the other slot and sum buffer; the old one finishes
+      // during the next render call
+      TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+      const size_t npix = size_t(c->width) * c->height;
+      if (c->accum_prev.n < npix) TRY_CUDA(s, c->accum_prev.alloc(npix), "alloc accumulation");
+      c->accum.swap(c->accum_prev);
+      c->prev_sample_count = c->sample_count;
+      c->prev_live = true;
+      c->tail_live = false;
+      c->slot ^= 1;
+      if (c->deferred) c->deferred_prev = true;
+      // the buffer taken over may still be read by the copy of an earlier epoch
+      TRY_CUDA(s, after_pending_copy(c), "reset");
+    }
+  }
   c->sample_count = 0;
   if (c->accum.p) {
     TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
@@ -794,6 +881,88 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
   return DSPBR_OK;
 }
 
+// Pipelined frames: the render loop until the previous epoch (if it still
+// has paths in the pool) has finished, its deferred read enqueued on the copy
+// stream right then, and on until every sample of these frames has started.
+// The call returns with this epoch's last paths possibly still in the pool.
+static int render_pipelined(dspbr_ctx* c, int frames) {
+  Status s = c->st();
+  int rc = settle_worker(c);
+  if (rc) return rc;
+  if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
+  if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
+  if (int64_t(c->scene->max_tex_id) >= int64_t(c->scene->num_texinfo))
+    return s.fail(DSPBR_ERR_STATE, "render: the scene's materials use textures; call dspbr_scene_set_textures");
+  if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
+  if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
+  // a read of this epoch waits for the samples rendered so far, not these
+  if (c->deferred && !c->deferred_prev && (rc = flush_pipeline(c))) return rc;
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  Engine& E = *c->eng;
+  const unsigned long long npix = uint64_t(c->width) * uint64_t(c->height);
+  const unsigned long long items = npix * uint64_t(frames);
+  // room for this epoch's samples and the previous epoch's last paths; the
+  // pool changes size only when empty
+  const uint32_t want = uint32_t(std::min<uint64_t>(c->wave_paths, 2 * items));
+  if (E.capacity() < want || E.capacity() > c->wave_paths) {
+    if ((rc = flush_pipeline(c)) || (rc = E.ensure_pool(want))) return rc;
+  }
+  if (c->tail_live) {
+    // the epoch goes on: its job takes more work items (frame numbers continue)
+    if ((rc = E.add_items(c->slot, items))) return rc;
+  } else {
+    Job job{};
+    job.p = make_wave(c, uint32_t(c->sample_count + 1));
+    job.s = c->scene->view();
+    job.s.wide = c->params.traversal == DSPBR_TRAVERSAL_WIDE;
+    if (c->ibl) job.e = c->ibl->view();
+    job.accum = reinterpret_cast<double*>(c->accum.p);
+    if ((rc = E.set_job(c->slot, job, items))) return rc;
+  }
+  const int prev = c->prev_live ? (c->slot ^ 1) : -1;
+  if ((rc = E.set_active(prev >= 0 ? std::vector<int>{prev, c->slot} : std::vector<int>{c->slot}))) return rc;
+  c->sample_count += uint64_t(frames);
+  c->rays_primary += items;
+  const uint64_t pool = E.capacity();
+  const uint64_t per_path = uint64_t(std::max(c->params.max_bounces, 0)) + 1;
+  const unsigned long long max_iter = (items * per_path + pool - 1) / pool + 2 * per_path + 8;
+  TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
+  const bool read_prev = c->deferred && c->deferred_prev;
+  unsigned long long it0 = 0, eager = 0;
+  rc = E.launch_pipelined(prev, max_iter, read_prev ? c->ev_between : nullptr, &it0, &eager);
+  if (!rc && read_prev) {
+    // the previous epoch is complete at ev_between: its image is copied
+    // while this epoch's iterations run
+    float* dst = c->deferred;
+    c->deferred = nullptr;
+    c->deferred_prev = false;
+    rc = issue_read(c, c->accum_prev.p, c->prev_sample_count, dst, c->ev_between);
+  }
+  if (!rc) rc = s.cuda(cudaEventRecord(c->ev1, c->stream), "event");
+  if (!rc) rc = s.cuda(cudaStreamSynchronize(c->stream), "render");
+  if (rc) return rc;
+  E.finish_pipelined(it0, eager);
+  if (prev >= 0 && !E.job_done(prev))
+    return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: previous frame not finished after %llu iterations", max_iter);
+  c->prev_live = false;
+  c->tail_live = !E.job_done(c->slot);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_render_ms = ms;
+  return DSPBR_OK;
+}
+
+int dspbr_set_pipelining(dspbr_ctx* c, int enable) {
+  if (!c) return DSPBR_ERR_INVALID;
+  int rc = settle(c);
+  if (rc) return rc;
+  Status s = c->st();
+  if (enable && !c->ev_between)
+    TRY_CUDA(s, cudaEventCreateWithFlags(&c->ev_between, cudaEventDisableTiming), "event");
+  c->pipelined = enable != 0;
+  return DSPBR_OK;
+}
+
 int dspbr_wait(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
   Status s = c->st();
@@ -838,6 +1007,7 @@ int dspbr_set_profiling(dspbr_ctx* c, int enable) {
 
 int dspbr_render(dspbr_ctx* c, int frames) {
   if (!c) return DSPBR_ERR_INVALID;
+  if (c->pipelined && !c->counting && !c->eng->profiling) return render_pipelined(c, frames);
   int rc = enqueue_frames(c, frames, false);
   if (rc) {
     dspbr_wait(c);
@@ -885,12 +1055,6 @@ static void parallel_copy(void* dst, const void* src, size_t bytes) {
 
 // Device-to-host copy of a result: one DMA into page-locked memory, else
 // through the context's page-locked staging buffer and a parallel host copy.
-// A copy of read_accum_async still reading the mean buffer: the stream's
-// next writes to it wait for that copy.
-static cudaError_t after_pending_copy(dspbr_ctx* c) {
-  return c->copy_pending ? cudaStreamWaitEvent(c->stream, c->ev_copied, 0) : cudaSuccess;
-}
-
 static int copy_out(dspbr_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
   Status s = c->st();
   cudaPointerAttributes attr{};
@@ -930,7 +1094,11 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
 
 int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c || !rgba) return DSPBR_ERR_INVALID;
-  { int rc_ = settle(c); if (rc_) return rc_; }
+  { int rc_ = settle_worker(c); if (rc_) return rc_; }
+  if (c->pipelined && c->deferred) {  // one deferred read at a time
+    int rc = flush_pipeline(c);
+    if (rc) return rc;
+  }
   Status s = c->st();
   size_t npix = size_t(c->width) * c->height;
   if (num_floats < npix * 4)
@@ -941,6 +1109,18 @@ int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
   const bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
   cudaGetLastError();
   if (!pinned) return s.fail(DSPBR_ERR_INVALID, "read_accum_async: the buffer is not page-locked (dspbr_host_alloc)");
+  if (c->pipelined && (c->tail_live || c->prev_live)) {
+    if (!c->tail_live) {  // only the previous epoch is in flight: this one's sums are complete
+      int rc = flush_pipeline(c);
+      if (rc) return rc;
+    } else {
+      // this epoch's last paths are in the pool: the mean and copy follow
+      // when they finish (in the next render call, or dspbr_read_wait)
+      c->deferred = rgba;
+      c->deferred_prev = false;
+      return DSPBR_OK;
+    }
+  }
   double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
   TRY_CUDA(s, after_pending_copy(c), "read accumulation");
   launch_mean(c->accum.p, inv, c->mean.p, int(npix), c->stream);
@@ -955,6 +1135,10 @@ int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
 
 int dspbr_read_wait(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
+  if (c->deferred) {
+    int rc = settle(c);  // finishes the epoch and enqueues the read
+    if (rc) return rc;
+  }
   if (!c->copy_pending) return DSPBR_OK;
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
@@ -1149,7 +1333,8 @@ int dspbr_get_device_info(dspbr_ctx* c, dspbr_device_info* info) {
 
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   if (!c || !d) return DSPBR_ERR_INVALID;
-  { int rc_ = settle(c); if (rc_) return rc_; }
+  // pipelined frames stay in flight: the ray counters cover the iterations run so far
+  { int rc_ = settle_worker(c); if (rc_) return rc_; }
   Status s = c->st();
   std::memset(d, 0, sizeof *d);
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1169,7 +1354,7 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->bvh_build_ms = c->scene->bvh_build_ms;
     d->upload_ms = c->scene->upload_ms;
   }
-  d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->mean.bytes();
+  d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->accum_prev.bytes() + c->mean.bytes();
   d->last_render_ms = c->last_render_ms;
   d->nodes_closest = st[3];
   d->tris_closest = st[4];

@@ -265,9 +265,17 @@ DEV void wide_begin(WideTrav& w, int root) {
 // reached, no accepted triangle for an any-hit ray).  `any` is a run-time
 // flag so that closest-hit and any-hit rays can share one instruction stream;
 // the callers with a constant get the specialised code.
+//
+// Stack entries carry the entry distance of the child's box.  A closest-hit
+// ray pops an inner node only while that distance is below the closest hit
+// found so far: every box below the node lies inside its box, so their slab
+// entries are at least as far (the rounded slab arithmetic is monotone in the
+// planes) and the reference's test `tmin >= tfar` would reject them all.  The
+// result is the same; the node's load is saved.  Leaves are always visited
+// (a triangle on a box face may round to a t just below the box's entry).
 template <bool kExactNaN>
 DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
-                      const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack,
+                      const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int2* stack,
                       bool any) {
   const int e = w.cur;
   bool next_in_register = false;
@@ -314,7 +322,7 @@ DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict_
     cswap(d1, c1, d2, c2);
     auto push = [&](float d, int c) {
       if (d < kBvhFar) {
-        if (w.top < kWideStack) stack[w.top++] = c;
+        if (w.top < kWideStack) stack[w.top++] = make_int2(c, __float_as_int(d));
         else w.overflow = true;
       }
     };
@@ -327,8 +335,14 @@ DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict_
     }
   }
   if (!next_in_register) {
-    if (w.top > 0) w.cur = stack[--w.top];
-    else w.have = false;
+    w.have = false;
+    while (w.top > 0) {
+      const int2 en = stack[--w.top];
+      if (!kExactNaN && !any && en.x >= 0 && __int_as_float(en.y) >= hit.t) continue;
+      w.cur = en.x;
+      w.have = true;
+      break;
+    }
   }
   ++w.step;
   return w.have && w.step < kMaxSteps;
@@ -336,7 +350,7 @@ DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict_
 
 template <bool kAny, bool kExactNaN>
 DEV bool wide_step(const float4* __restrict__ wnodes, const int2* __restrict__ wleaves,
-                   const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int* stack) {
+                   const float4* __restrict__ tris, v3 org, v3 inv, v3 dir, Hit& hit, WideTrav& w, int2* stack) {
   return wide_step_rt<kExactNaN>(wnodes, wleaves, tris, org, inv, dir, hit, w, stack, kAny);
 }
 
@@ -349,7 +363,7 @@ DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfa
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
-  int stack[kWideStack];
+  int2 stack[kWideStack];
   WideTrav w;
   wide_begin(w, s.wroot);
   while (wide_step<kAny, kExactNaN>(s.wnodes, s.wleaves, s.tris, org, inv, dir, hit, w, stack)) {
@@ -365,7 +379,7 @@ DEV bool traverse_wide_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool an
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
-  int stack[kWideStack];
+  int2 stack[kWideStack];
   WideTrav w;
   wide_begin(w, s.wroot);
   if (exact) {

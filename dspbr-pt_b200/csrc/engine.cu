@@ -39,6 +39,14 @@ __global__ void k_read_stats(const unsigned long long* stats, HostStatus* out) {
   if (threadIdx.x < 8) out->stats[threadIdx.x] = stats[threadIdx.x];
 }
 
+__global__ void k_add_items(int slot, unsigned long long items, JobState* js, HostStatus* hs) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  js[slot].items_total += items;
+  volatile JobStatus* st = &hs->job[slot];
+  st->items_total = js[slot].items_total;
+  st->done = 0;
+}
+
 __global__ void k_cancel_job(int slot, JobState* js) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   if (js[slot].items_total > js[slot].items_next) js[slot].items_total = js[slot].items_next;
@@ -170,6 +178,14 @@ int Engine::set_job(int slot, const Job& job, unsigned long long items_total) {
   slot_textured_[slot] = job.s.num_texinfo > 0;
   ++kind_launches[3];
   return s.cuda(cudaGetLastError(), "set job");
+}
+
+int Engine::add_items(int slot, unsigned long long items) {
+  Status s{err_};
+  if (slot < 0 || slot >= kMaxJobs) return s.fail(DSPBR_ERR_INVALID, "job slot %d out of range", slot);
+  k_add_items<<<1, 32, 0, stream_>>>(slot, items, js_.p, d_status_);
+  ++kind_launches[3];
+  return s.cuda(cudaGetLastError(), "add work items");
 }
 
 int Engine::cancel_job(int slot) {
@@ -412,7 +428,7 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
     int rc = capture_loop_graph();
     if (rc) return rc;
   }
-  launch_set_loop(loop_ctl_.p, max_iter, drain_below_, stream_);
+  launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopDrain, -1, stream_);
   TRY_CUDA(s, cudaGetLastError(), "loop control");
   TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
   TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");
@@ -425,6 +441,45 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
   cur_ = 0;  // the tail drained every path: both queues are empty
   if (job_done(slot)) return DSPBR_OK;
   return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: job not finished after %llu iterations", max_iter);
+}
+
+int Engine::launch_pipelined(int wait_slot, unsigned long long max_iter, cudaEvent_t between,
+                             unsigned long long* it0, unsigned long long* eager) {
+  Status s{err_};
+  TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");  // the iteration counter below is current
+  *it0 = h_status_->iteration;
+  *eager = 0;
+  if (cur_ == 1) {  // the loop body starts at parity 0
+    int rc = one_iteration(false);
+    if (rc) return rc;
+    *eager = 1;
+  }
+  if (!loop_graph_) {
+    int rc = capture_loop_graph();
+    if (rc) return rc;
+  }
+  if (wait_slot >= 0) {
+    // the previous epoch's paths were all started: each ends within
+    // max_bounces + 1 more iterations; the bound only guards the loop
+    launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopUntilDone, wait_slot, stream_);
+    TRY_CUDA(s, cudaGetLastError(), "loop control");
+    TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+  }
+  if (between) TRY_CUDA(s, cudaEventRecord(between, stream_), "event");
+  launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopUntilStarted, -1, stream_);
+  TRY_CUDA(s, cudaGetLastError(), "loop control");
+  TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+  return DSPBR_OK;
+}
+
+void Engine::finish_pipelined(unsigned long long it0, unsigned long long eager) {
+  // whole pairs only: the queues of parity 0 hold the paths still alive
+  const unsigned long long body = h_status_->iteration - it0 - eager;
+  kind_launches[0] += body;
+  kind_launches[1] += body;
+  kind_launches[2] += 3 * body;
+  kind_launches[3] += 2;
+  cur_ = 0;
 }
 
 // Two iterations (parity 0, then 1) captured from the stream.  Every argument

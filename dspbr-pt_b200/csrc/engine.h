@@ -53,6 +53,21 @@ class Engine {
   // iterations (the commit kernel decides whether another pair runs), then
   // the tail drain; the host waits once.  Not while profiling or counting.
   int run_loop(int slot, unsigned long long max_iter);
+  // Pipelined frames (the renders of consecutive accumulation epochs overlap):
+  // enqueues the loop graph until job `wait_slot` has finished (skipped when
+  // wait_slot < 0), records `between` (if not null), then the loop graph until
+  // every work item of the active jobs has started; no tail, no host wait.
+  // The paths still alive stay in the pool.  Returns the eager iteration count
+  // in *eager and the iteration counter before the launches in *it0, for
+  // finish_pipelined() once the stream has passed them.
+  int launch_pipelined(int wait_slot, unsigned long long max_iter, cudaEvent_t between, unsigned long long* it0,
+                       unsigned long long* eager);
+  void finish_pipelined(unsigned long long it0, unsigned long long eager);
+  // More work items for a job already in the table (a progressive render that
+  // continues the same accumulation while its earlier paths are in flight).
+  int add_items(int slot, unsigned long long items);
+  // Any path of any job in the pool (from the last completed iteration).
+  bool pool_live() const { return h_status_ && h_status_->live_paths != 0u; }
   void set_drain_below(uint32_t paths) { drain_below_ = paths ? paths : kDrainBelow; }
   unsigned drain_below() const { return drain_below_; }
   // The last (up to max_entries, at most kTimeline) iterations' records, oldest first.

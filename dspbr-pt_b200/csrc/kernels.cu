@@ -346,23 +346,41 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
     if (ctl) {  // the render loop's next iteration, or the tail
       const bool started = total <= avail;  // the regen that just ran placed every remaining work item
       const unsigned long long left = ctl->iters_left;
-      const bool go = left > 1 && !(started && live < ctl->drain_below);
-      ctl->iters_left = left ? left - 1 : 0;
-      if (lh.first) {
-        cudaGraphSetConditional(lh.second, go ? 1u : 0u);
-        if (!go) cudaGraphSetConditional(lh.loop, 0u);
+      const int mode = ctl->mode;
+      bool stop;
+      if (mode == kLoopDrain) {
+        stop = started && live < ctl->drain_below;
+      } else if (mode == kLoopUntilDone) {
+        const int w = ctl->wait_job;
+        stop = w < 0 || w >= kMaxJobs || (sc.js[w].items_next >= sc.js[w].items_total && sc.js[w].live == 0u);
       } else {
-        cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
+        stop = started;
       }
-      if (!go) cudaGraphSetConditional(lh.tail, 1u);
+      const bool go = left > 1 && !stop;
+      ctl->iters_left = left ? left - 1 : 0;
+      if (mode != kLoopDrain) {  // whole pairs, no tail
+        if (lh.first) cudaGraphSetConditional(lh.second, 1u);
+        else cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
+      } else {
+        if (lh.first) {
+          cudaGraphSetConditional(lh.second, go ? 1u : 0u);
+          if (!go) cudaGraphSetConditional(lh.loop, 0u);
+        } else {
+          cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
+        }
+        if (!go) cudaGraphSetConditional(lh.tail, 1u);
+      }
     }
   }
 }
 
-__global__ void k_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below) {
+__global__ void k_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, int mode,
+                           int wait_job) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->iters_left = iterations;
     ctl->drain_below = drain_below;
+    ctl->mode = mode;
+    ctl->wait_job = wait_job;
   }
 }
 
@@ -1013,8 +1031,9 @@ void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, const LoopHa
                         cudaStream_t st) {
   k_commit<<<1, kMaxJobs, 0, st>>>(sc, b, cur, 1, h, ctl);
 }
-void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, cudaStream_t st) {
-  k_set_loop<<<1, 32, 0, st>>>(ctl, iterations, drain_below);
+void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, int mode,
+                     int wait_job, cudaStream_t st) {
+  k_set_loop<<<1, 32, 0, st>>>(ctl, iterations, drain_below, mode, wait_job);
 }
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);

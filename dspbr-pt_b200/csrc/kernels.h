@@ -183,13 +183,22 @@ void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& 
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
 
 // Device-side loop control of a render call run as one graph.  The loop body
-// is iteration A (parity 0), then iteration B (parity 1) under an IF node;
-// after each iteration k_commit keeps going while iterations remain and either
-// a work item has not started or at least drain_below paths are alive.  The
-// commit that stops selects the tail of its parity (an IF node each).
+// is iteration A (parity 0), then iteration B (parity 1) under an IF node.
+// kLoopDrain: after each iteration k_commit keeps going while iterations
+// remain and either a work item has not started or at least drain_below paths
+// are alive; the commit that stops selects the tail of its parity (an IF node
+// each), which runs every remaining path to its end.
+// kLoopUntilDone / kLoopUntilStarted (pipelined frames): no tail; the loop
+// runs whole pairs (A always continues to B, so the next launch starts at
+// parity 0) until job wait_job has finished (every item started, no live
+// path), or until every work item of the active jobs has started; the paths
+// still alive stay in the pool for the next launch.
+enum { kLoopDrain = 0, kLoopUntilDone = 1, kLoopUntilStarted = 2 };
 struct LoopCtl {
   unsigned long long iters_left;
   unsigned long long drain_below;
+  int mode;      // kLoop*
+  int wait_job;  // kLoopUntilDone: the job slot to finish
 };
 struct LoopHandles {
   cudaGraphConditionalHandle loop;    // the while node
@@ -199,7 +208,8 @@ struct LoopHandles {
 };
 void launch_commit_loop(const Sched& sc, const PathBuf& b, int cur, const LoopHandles& h, LoopCtl* ctl,
                         cudaStream_t st);
-void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, cudaStream_t st);
+void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long long drain_below, int mode,
+                     int wait_job, cudaStream_t st);
 // runs every path queued in q[cur] to its end (call after connect(cur), when no work item is left)
 void launch_drain(const Sched& sc, const PathBuf& b, int cur, const LaunchCfg& lc, cudaStream_t st);
 void launch_mean(const double4* accum, double inv_count, float4* out, int npix, cudaStream_t st);

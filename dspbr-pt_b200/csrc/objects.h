@@ -121,6 +121,22 @@ struct dspbr_ctx {
   double last_render_ms = 0;
   bool pending = false;
   bool counting = false;
+  // Pipelined frames (dspbr_set_pipelining).  The frames since the last reset
+  // (an accumulation epoch) render as job `slot`; a render call returns once
+  // every sample has started, so the epoch's last paths may still be in the
+  // pool (tail_live).  A reset then starts a new epoch in the other job slot
+  // and sum buffer while the old one (prev_live, sums in accum_prev) finishes
+  // during the next render call, which waits for it before it returns.
+  bool pipelined = false;
+  int slot = 0;
+  bool tail_live = false, prev_live = false;
+  dspbr::DevBuf<double4> accum_prev;
+  uint64_t prev_sample_count = 0;
+  // a read_accum_async of an epoch with paths in the pool: its mean and copy
+  // are enqueued once that epoch has finished
+  float* deferred = nullptr;
+  bool deferred_prev = false;  // the read is of the previous epoch
+  cudaEvent_t ev_between = nullptr;
   dspbr::Status st() { return dspbr::Status{&err}; }
 };
 

@@ -340,6 +340,13 @@ class PathtracingViewport:
         for k in ("pixelRatio", "interactionPixelRatio"):
             if k in settings:
                 check_pixel_ratio(k, settings[k])
+        settings = dict(settings)
+        if "pipelinedFrames" in settings:
+            # not a reference setting: frames of consecutive accumulations
+            # overlap on the device (dspbr_set_pipelining); start() then
+            # returns once every sample has started, and readAccumulationAsync
+            # of frames still in flight completes in readWait() or the next start()
+            self._set_pipelining(bool(settings.pop("pipelinedFrames")))
         apply_settings(self.params, settings, self._display)
         # the renderer setters of exposure, enableGamma, debugMode and every
         # render setting reset the accumulation; toneMapping, enableFxaa,
@@ -361,6 +368,10 @@ class PathtracingViewport:
         self.interactionActive = bool(active)
         self._apply_size()
         self._emit_diag()
+
+    def _set_pipelining(self, on: bool):
+        self.ctx.check(self.ctx.lib.dspbr_set_pipelining(self.ctx.h, int(on)))
+        self._display["pipelinedFrames"] = on
 
     def _pixel_ratio(self) -> float:
         return float(self._display["interactionPixelRatio" if self.interactionActive else "pixelRatio"])

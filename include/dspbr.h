@@ -227,6 +227,18 @@ int dspbr_read_accum(dspbr_ctx* ctx, float* rgba, size_t num_floats);
  * read, a display read, a resize) are ordered after the pending copy. */
 int dspbr_read_accum_async(dspbr_ctx* ctx, float* rgba, size_t num_floats);
 int dspbr_read_wait(dspbr_ctx* ctx);
+/* Pipelined frames (off by default).  The reference renders one frame per
+ * requestAnimationFrame and presents it (renderer.ts:512-565, 595-714); here
+ * the frames of consecutive accumulations overlap on the device.  With it on,
+ * dspbr_render returns once every sample of its frames has started: the last
+ * paths stay in the path pool and finish during the next dspbr_render, which
+ * first completes the previous accumulation.  A reset (setCamera, setSettings,
+ * resetAccumulation) starts the new accumulation in a second sum buffer while
+ * the old one finishes.  dspbr_read_accum_async of an accumulation still in
+ * flight is enqueued when its paths finish (during the next render, or in
+ * dspbr_read_wait); dspbr_read_accum, the display reads and every other call
+ * finish all paths first.  Images are the same as with it off. */
+int dspbr_set_pipelining(dspbr_ctx* ctx, int enable);
 /* Display epilogue (renderer.ts:666-700): the accumulation mean through
  * tonemap.frag (exposure, operator, gamma) and optionally fxaa.frag -- the
  * reference's "postprocess" buffer, at the render resolution -- as RGBA32F,

@@ -1,0 +1,112 @@
+"""Pipelined frames (dspbr_set_pipelining): the render of one accumulation
+overlaps the tail of the previous one on the device.  Every image must equal
+the image of the same calls without pipelining (FP64 pixel sums in another
+order: allclose 1e-6), whatever mix of camera changes, progressive renders,
+asynchronous and synchronous reads, display reads and resizes comes."""
+import numpy as np
+import pytest
+
+from dspbr import synth
+from dspbr.viewport import Bvh, PathtracingCamera, PathtracingViewport, look_at_matrix
+
+pytestmark = pytest.mark.gpu
+
+TOL = dict(rtol=1e-6, atol=1e-7)
+
+
+@pytest.fixture(scope="module")
+def scene():
+    sc = synth.make_small(0)
+    sc.bvh = Bvh.build(sc.vertices, sc.indices, 20)
+    return sc
+
+
+def _viewport(sc, pipelined, w=96, h=64, pool=0):
+    v = PathtracingViewport(width=w, height=h, settings={"maxBounces": 8, "pipelinedFrames": pipelined})
+    if pool:
+        v.ctx.check(v.ctx.lib.dspbr_set_wave_paths(v.ctx.h, pool))
+    v.setScene(sc)
+    v.setIBL(sc.env)
+    return v
+
+
+def _cam(k):
+    return PathtracingCamera(look_at_matrix((0.25 * k - 0.5, 1.0, 3.4 - 0.1 * k), (0, 0.9, 0)), 45.0, 0.1)
+
+
+@pytest.mark.parametrize("pool", [0, 4000])
+def test_camera_per_frame_with_async_reads(scene, pool):
+    """The interactive loop: per frame setCamera, start(1), then the previous
+    frame's readWait and this frame's readAccumulationAsync."""
+    out = {}
+    for pipelined in (False, True):
+        v = _viewport(scene, pipelined, pool=pool)
+        bufs = [v.allocReadbackBuffer() for _ in range(6)]
+        for k in range(6):
+            v.setCamera(_cam(k))
+            v.start(1)
+            assert v.diagnostics["sample_count"] == 1
+            v.readWait()
+            v.readAccumulationAsync(bufs[k])
+        v.readWait()
+        out[pipelined] = [b.copy() for b in bufs]
+        d = v.diagnostics
+        assert d["rays_primary"] == 6 * 96 * 64 and d["traversal_aborted"] == 0
+        v.dispose()
+    for a, b in zip(out[False], out[True]):
+        assert np.isfinite(b).all() and b[..., 3].min() == 1.0
+        np.testing.assert_allclose(b, a, **TOL)
+    # the frames differ (different cameras): the reads did not repeat one image
+    assert not np.allclose(out[True][0], out[True][1])
+
+
+def test_progressive_and_mixed_calls(scene):
+    """Progressive renders that continue an accumulation in flight, a read of
+    an accumulation in flight followed by more frames of it, a synchronous
+    read, a display read, a resize and a reset with nothing rendered."""
+    res = {}
+    for pipelined in (False, True):
+        v = _viewport(scene, pipelined)
+        got = []
+        v.setCamera(_cam(0))
+        v.start(1)
+        v.start(2)  # the same accumulation: 2 samples
+        buf = v.allocReadbackBuffer()
+        v.readAccumulationAsync(buf)
+        v.start(4)  # two more samples after the read was requested
+        v.readWait()
+        got.append(buf.copy())  # the 2-sample mean
+        got.append(v.readAccumulation())  # 4 samples
+        v.setCamera(_cam(1))
+        v.start(1)
+        v.setCamera(_cam(2))  # a new accumulation while the last one is in flight ...
+        v.resetAccumulation()  # ... and another reset with nothing rendered
+        v.start(2)
+        got.append(v.readDisplay(rgba8=False))
+        v.resize(80, 48)
+        v.setCamera(_cam(3))
+        v.start(1)
+        got.append(v.readAccumulation())
+        assert v.diagnostics["sample_count"] == 1
+        res[pipelined] = got
+        v.dispose()
+    for a, b in zip(res[False], res[True]):
+        np.testing.assert_allclose(b, a, **TOL)
+
+
+def test_pipelined_frames_equal_single_frames_of_a_fresh_viewport(scene):
+    """Each frame of a pipelined sequence is the one-frame render of its camera."""
+    v = _viewport(scene, True)
+    bufs = [v.allocReadbackBuffer() for _ in range(3)]
+    for k in range(3):
+        v.setCamera(_cam(k))
+        v.start(1)
+        v.readAccumulationAsync(bufs[k])
+    v.readWait()
+    v.dispose()
+    for k in range(3):
+        f = _viewport(scene, False)
+        f.setCamera(_cam(k))
+        f.start(1)
+        np.testing.assert_allclose(bufs[k], f.readAccumulation(), **TOL)
+        f.dispose()
