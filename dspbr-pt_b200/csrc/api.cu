@@ -196,14 +196,6 @@ static uint32_t material_signature(const float* m) {
   return sig;
 }
 
-// material << 4 | class into the leaf records (after every gather of them and
-// every change of the classes)
-static void tag_triangles(dspbr_scene* sc, cudaStream_t st) {
-  if (sc->tris.p && sc->mat_class.p && sc->num_slots)
-    launch_tag_tris(sc->tris.p, sc->num_slots, sc->verts.p, sc->indices.p, sc->num_tris, sc->mat_class.p,
-                    int(sc->num_materials), st);
-}
-
 static int classify_triangles(Status& s, dspbr_scene* sc, cudaStream_t st) {
   std::vector<uint32_t> sigs;
   std::vector<uint8_t> mat_class(sc->num_materials);
@@ -222,14 +214,6 @@ static int classify_triangles(Status& s, dspbr_scene* sc, cudaStream_t st) {
   }
   int rc = s.cuda(cudaMemcpyAsync(sc->tri_class.p, cls.data(), cls.size(), cudaMemcpyHostToDevice, st), "upload classes");
   if (rc) return rc;
-  if (!sc->mat_class.p && (rc = s.cuda(sc->mat_class.alloc(std::max<size_t>(mat_class.size(), 1)), "alloc classes")))
-    return rc;
-  if (!mat_class.empty() &&
-      (rc = s.cuda(cudaMemcpyAsync(sc->mat_class.p, mat_class.data(), mat_class.size(), cudaMemcpyHostToDevice, st),
-                   "upload classes")))
-    return rc;
-  tag_triangles(sc, st);
-  if ((rc = s.cuda(cudaGetLastError(), "tag triangles"))) return rc;
   return s.cuda(cudaStreamSynchronize(st), "upload classes");
 }
 
@@ -280,7 +264,6 @@ static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t
   if ((rc = classify_triangles(s, sc.get(), c->stream))) return rc;
   if ((rc = s.cuda(sc->tris.alloc(size_t(sc->num_slots) * 3), "alloc tris"))) return rc;
   launch_gather_tris(sc->verts.p, sc->indices.p, bin.remap.p, sc->num_slots, sc->num_tris, sc->tris.p, c->stream);
-  tag_triangles(sc.get(), c->stream);
   if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) ||
       (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload")))
     return rc;
@@ -476,10 +459,8 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
     delete sc;
     return rc;
   }
-  if (num_bvh_indices) {
+  if (num_bvh_indices)
     launch_gather_tris(sc->verts.p, sc->indices.p, remap.p, num_bvh_indices, sc->num_tris, sc->tris.p, c->stream);
-    tag_triangles(sc, c->stream);
-  }
   if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) || (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload"))) {
     delete sc;
     return rc;
@@ -604,9 +585,6 @@ int dspbr_scene_update_vertices(dspbr_scene* sc, const float* vertices, uint32_t
   int rc = refit_scene_device(sc->nodes.p, sc->num_nodes, sc->num_slots, sc->wnodes.p, sc->num_wnodes, sc->wleaves.p,
                               sc->tris.p, sc->device_remap.p, sc->verts.p, sc->indices.p, sc->num_tris, st, s);
   if (rc) return rc;
-  // the records were gathered again (and a vertex may name another material)
-  tag_triangles(sc, st);
-  TRY_CUDA(s, cudaGetLastError(), "tag triangles");
   sc->refit_ms = now_ms() - t0;
   for (uint32_t v = 0; v < count && sc->boxes_finite; ++v)
     for (int k = 0; k < 3; ++k)

@@ -119,9 +119,6 @@ struct Rng {
 struct Hit {
   int tri;
   float t, u, v;
-  // the 4-wide traversal's closest triangle's tag from its leaf record:
-  // material index << 4 | shading class; -1 when untagged (the other traversals)
-  int aux;
 };
 
 // bvh_intersect_bounds (bvh.glsl:31-41).  kExactNaN keeps GLSL's min/max
@@ -179,7 +176,6 @@ DEV bool traverse_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfar, Hi
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
-  hit.aux = -1;
   int stack[kStackSize];
   int top = 1;
   stack[0] = 0;
@@ -291,10 +287,8 @@ DEV bool wide_step_rt(const float4* __restrict__ wnodes, const int2* __restrict_
       int id = __float_as_int(a.w);
       if (id < 0) continue;
       float t, u, v;
-      const float4 e2 = __ldg(tp + 2);
-      if (intersect_tri(org, dir, a, __ldg(tp + 1), e2, hit.t, t, u, v)) {
+      if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
         hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
-        hit.aux = __float_as_int(e2.w);
         if (any) {
           w.any_hit = true;
           return false;
@@ -369,7 +363,6 @@ DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfa
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
-  hit.aux = -1;
   int2 stack[kWideStack];
   WideTrav w;
   wide_begin(w, s.wroot);
@@ -386,7 +379,6 @@ DEV bool traverse_wide_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool an
   hit.t = tfar;
   hit.tri = -1;
   hit.u = hit.v = 0.f;
-  hit.aux = -1;
   int2 stack[kWideStack];
   WideTrav w;
   wide_begin(w, s.wroot);

@@ -23,8 +23,6 @@
 // per-path arithmetic and RNG consumption order follow the reference exactly.
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
 #include "kernels.h"
 
 namespace dspbr {
@@ -414,8 +412,7 @@ __global__ void __launch_bounds__(256, 4) k_extend(Sched sc, PathBuf b, int cur)
       const DevScene& s = sc.jobs[__float_as_uint(d.w)].s;
       Hit h;
       trace_path_ray<false, kCount, kTrav>(s, mk(o), mk(d), kTfarMax, h, aborted, &nodes, &tris);
-      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)),
-                             make_float4(__int_as_float(h.aux), 0.f, 0.f, 0.f)};
+      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
       if (is_hit) cls = __ldg(s.tri_class + h.tri);
@@ -475,12 +472,10 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
       Hit h;
       bool aborted = false;
       traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
-      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)),
-                             make_float4(__int_as_float(h.aux), 0.f, 0.f, 0.f)};
+      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
-      // the class comes with the triangle's leaf record (no lookup per hit)
-      if (is_hit) cls = h.aux >= 0 ? (h.aux & (kNumClasses - 1)) : __ldg(s.tri_class + h.tri);
+      if (is_hit) cls = __ldg(s.tri_class + h.tri);
       ++rays;
       aborted_n += aborted ? 1u : 0u;
     }
@@ -621,21 +616,8 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
   // read in place (the job table does not change during an iteration): fewer
   // registers held across the outlined material calls than a local copy
   const WaveParams& p = J.p;
-  const PathHit ph = b.hits[slot];
-  const float4 hit = ph.h;
+  float4 hit = b.hits[slot].h;
   int tri = __float_as_int(hit.w);
-  {
-    // the material record (272 B) into L1 now: its loads come after the
-    // index and vertex loads, which the material index no longer waits for
-    const int tag = __float_as_int(ph.pad.x);
-    if (tag >= 0) {
-      const char* m = reinterpret_cast<const char*>(J.s.materials + 17 * size_t(tag >> 4));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(m));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(m + 128));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(m + 256));
-      asm volatile("prefetch.global.L1 [%0];" ::"l"(m + 271));
-    }
-  }
   v3 dir = mk(d4);
   v3 w = mk(w4);
   v3 L = mk(l4);
@@ -880,8 +862,7 @@ __global__ void __launch_bounds__(128) k_drain(Sched sc, PathBuf b, int cur) {
         bool cont = false, shadow = false;
         if (!helper) {
           ++closest;
-          b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)),
-                                 make_float4(__int_as_float(h.aux), 0.f, 0.f, 0.f)};
+          b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
           if (h.tri < 0) shade_miss_path(sc, b, slot);
           else cont = shade_path<kTextured>(sc, b, slot, shadow);
         }
@@ -925,29 +906,7 @@ __global__ void k_gather_tris(const float4* verts, const uint32_t* indices, cons
     float4 c = verts[5 * size_t(indices[3 * size_t(t) + 2])];
     tris[3 * size_t(i)] = make_float4(a.x, a.y, a.z, __int_as_float(t));
     tris[3 * size_t(i) + 1] = make_float4(__fsub_rn(b.x, a.x), __fsub_rn(b.y, a.y), __fsub_rn(b.z, a.z), 0.f);
-    // the tag (k_tag_tris) is written once the shading classes are known
-    tris[3 * size_t(i) + 2] = make_float4(__fsub_rn(c.x, a.x), __fsub_rn(c.y, a.y), __fsub_rn(c.z, a.z),
-                                          __int_as_float(-1));
-  }
-}
-
-// Tags every leaf record with its triangle's material index (the shader's
-// int() of vertex 0's material slot, bvh.glsl:91-93) and shading class:
-// material << 4 | class in the w lane of the third float4, which the traversal
-// loads with the edges anyway.  The closest-hit kernel then queues a hit by
-// class without a lookup, and the hit record carries the material index, so
-// the shading kernel can fetch the material while the vertices load.
-__global__ void k_tag_tris(float4* tris, uint32_t nslots, const float4* verts, const uint32_t* indices,
-                           uint32_t ntris, const uint8_t* mat_class, int num_materials) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nslots; i += gridDim.x * blockDim.x) {
-    const int t = __float_as_int(tris[3 * size_t(i)].w);
-    int tag = -1;
-    if (t >= 0 && uint32_t(t) < ntris) {
-      int m = int(verts[5 * size_t(indices[3 * size_t(t)])].w);
-      m = min(max(m, 0), num_materials - 1);
-      if (m < (1 << 26)) tag = (m << 4) | (mat_class[m] & (kNumClasses - 1));
-    }
-    tris[3 * size_t(i) + 2].w = __int_as_float(tag);
+    tris[3 * size_t(i) + 2] = make_float4(__fsub_rn(c.x, a.x), __fsub_rn(c.y, a.y), __fsub_rn(c.z, a.z), 0.f);
   }
 }
 
@@ -1053,37 +1012,6 @@ LaunchLimits launch_limits() {
 
 void init_launch_sizes(LaunchCfg& lc) {
   const LaunchLimits l = launch_limits();
-  // The persistent path kernels keep their per-thread stack frames (the
-  // traversal stack, the outlined material calls' saved registers and
-  // closures) in local memory, which is cached in L1: ask for the smallest
-  // shared-memory carveout that still holds their resident blocks, leaving
-  // the rest of the SM's 256 KB to L1.
-  int dev = 0, smem_sm = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
-      smem_sm <= 0) {
-    cudaGetLastError();
-    smem_sm = 0;
-  }
-  struct K {
-    const void* fn;
-    int blocks;
-  } ks[] = {{reinterpret_cast<const void*>(k_extend_dyn), l.trace_per_sm},
-            {reinterpret_cast<const void*>(k_connect_dyn), l.connect_per_sm},
-            {reinterpret_cast<const void*>(k_shade<false>), l.shade_per_sm[0]},
-            {reinterpret_cast<const void*>(k_shade<true>), l.shade_per_sm[1]}};
-  for (const K& k : ks) {
-    cudaFuncAttributes fa{};
-    if (!smem_sm || cudaFuncGetAttributes(&fa, k.fn) != cudaSuccess) {
-      cudaGetLastError();
-      continue;
-    }
-    // static shared memory plus the 1 KB the system reserves per block
-    const size_t need = size_t(k.blocks) * (fa.sharedSizeBytes + 1024);
-    const int pct = int(std::min<size_t>(100, (need * 100 + size_t(smem_sm) - 1) / size_t(smem_sm)));
-    if (cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct) != cudaSuccess)
-      cudaGetLastError();
-  }
   lc.dyn_blocks = l.trace_per_sm * l.sms;
   lc.connect_dyn_blocks = l.connect_per_sm * l.sms;
   lc.shade_dyn_blocks[0] = l.shade_per_sm[0] * l.sms;
@@ -1135,12 +1063,6 @@ void launch_mean(const double4* accum, double inv_count, float4* out, int npix, 
 void launch_gather_tris(const float4* verts, const uint32_t* indices, const int32_t* remap, uint32_t nslots,
                         uint32_t ntris, float4* tris, cudaStream_t st) {
   k_gather_tris<<<grid_for(nslots, 256, 148 * 16), 256, 0, st>>>(verts, indices, remap, nslots, ntris, tris);
-}
-void launch_tag_tris(float4* tris, uint32_t nslots, const float4* verts, const uint32_t* indices, uint32_t ntris,
-                     const uint8_t* mat_class, int num_materials, cudaStream_t st) {
-  if (nslots && num_materials > 0)
-    k_tag_tris<<<grid_for(nslots, 256, 148 * 16), 256, 0, st>>>(tris, nslots, verts, indices, ntris, mat_class,
-                                                                num_materials);
 }
 void launch_trace_rays(const DevScene& s, const float4* rays, uint32_t n, int any, int32_t* tri, float* t, float2* uv,
                        int32_t* occ, cudaStream_t st) {

@@ -99,11 +99,10 @@ struct __align__(32) PathState {
   uint32_t pad[4];
 };
 static_assert(sizeof(PathState) == 96, "PathState is three sectors");
-// closest hit of the slot's extension ray: t, u, v, triangle id bits; the
-// triangle's tag (material << 4 | class, -1: none) and pad to a sector
+// closest hit of the slot's extension ray: t, u, v, triangle id bits (+ pad to a sector)
 struct __align__(32) PathHit {
   float4 h;
-  float4 pad;  // x: tag bits
+  float4 pad;
 };
 // NEE shadow rays of the slot's last vertex, 64 B
 struct __align__(32) PathShadow {
@@ -232,8 +231,5 @@ void launch_ibl_tables(const float4* rgba, int w, int h, float* lum, float* pdf,
 // scene preparation (kernels.cu)
 void launch_gather_tris(const float4* verts, const uint32_t* indices, const int32_t* remap, uint32_t nslots,
                         uint32_t ntris, float4* tris, cudaStream_t st);
-// material index << 4 | shading class into each leaf record (k_tag_tris)
-void launch_tag_tris(float4* tris, uint32_t nslots, const float4* verts, const uint32_t* indices, uint32_t ntris,
-                     const uint8_t* mat_class, int num_materials, cudaStream_t st);
 
 }  // namespace dspbr

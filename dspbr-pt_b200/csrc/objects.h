@@ -19,7 +19,6 @@ struct dspbr_scene {
   dspbr::DevBuf<float4> nodes, tris, verts, materials;
   dspbr::DevBuf<uint32_t> indices;
   dspbr::DevBuf<uint8_t> tri_class;
-  dspbr::DevBuf<uint8_t> mat_class;  // shading class per material (the leaf records' tags)
   dspbr::DevBuf<float4> wnodes;  // 4-wide BVH (8 float4 per node)
   dspbr::DevBuf<int2> wleaves;
   int wroot = 0;
