@@ -454,7 +454,14 @@ DEV bool next_warp_batch(uint32_t* cursor, uint32_t count, uint32_t& i, bool& fi
   return true;
 }
 
-// closest hits of q[cur], 4-wide traversal
+DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot);
+
+// closest hits of q[cur], 4-wide traversal.  A camera ray that leaves the
+// scene ends its path here: its sample is the background (misptdl.glsl:41-46),
+// added to the job's sums before the slot is freed, instead of a trip through
+// the miss queue and the shading kernel.  Only camera rays: a later vertex's
+// path may still receive its shadow rays' contribution from k_connect, which
+// runs beside this kernel; its misses are shaded after both.
 __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
@@ -462,25 +469,30 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
   uint32_t i;
   bool first = true;
   while (next_warp_batch(b.counts + kCntFetchExt, count, i, first)) {
-    bool is_hit = false, is_miss = false;
-    uint32_t slot = 0;
+    bool is_hit = false, is_miss = false, sky = false;
+    uint32_t slot = 0, job = 0;
     int cls = 0;
     if (i < count) {
       slot = q[i];
       const float4 o = b.st[slot].org, d = b.st[slot].dir;
-      const DevScene& s = sc.jobs[__float_as_uint(d.w)].s;
+      job = __float_as_uint(d.w);
+      const DevScene& s = sc.jobs[job].s;
       Hit h;
       bool aborted = false;
       traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
-      b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
+      sky = is_miss && __float_as_int(o.w) == 0;
+      if (!sky)
+        b.hits[slot] = PathHit{make_float4(h.t, h.u, h.v, __int_as_float(h.tri)), make_float4(0.f, 0.f, 0.f, 0.f)};
       if (is_hit) cls = __ldg(s.tri_class + h.tri);
       ++rays;
       aborted_n += aborted ? 1u : 0u;
     }
+    if (sky) shade_miss_path(sc, b, slot);
+    free_slots(sc, b, sky, slot, job);
     enqueue_keyed(b.qh, b.counts + kCntHit0, b.capacity, is_hit, cls, slot);
-    enqueue(b.qm, b.counts + kCntMiss, is_miss, slot);
+    enqueue(b.qm, b.counts + kCntMiss, is_miss && !sky, slot);
   }
   add_warp(b.stats + 0, rays);
   add_warp(b.stats + 2, aborted_n);
