@@ -35,13 +35,14 @@ sys.path.insert(0, ROOT)
 METRIC = "Mrays/s"
 
 
-def extend_traffic():
-    """DRAM bytes per frame of the k_extend launches (ncu dram__bytes_read.sum
-    + dram__bytes_write.sum of one capture, committed beside the ncu
-    summaries under profiles/), or None."""
+def extend_traffic_rate():
+    """DRAM bytes per millisecond of k_extend_dyn launches (ncu
+    dram__bytes_read.sum + dram__bytes_write.sum over gpu__time_duration.sum
+    of three launches of one capture, committed beside the ncu summaries
+    under profiles/), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "k_extend_traffic.json")) as f:
-            return int(json.load(f)["dram_bytes_per_frame"])
+            return float(json.load(f)["dram_bytes_per_ms"])
     except Exception:
         return None
 
@@ -901,10 +902,11 @@ def run_gpu_arm(args):
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                         "traffic": extend_traffic(),
-                         "traffic_basis": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_extend "
-                                          "launches per frame (one capture, profiles/); achieved "
-                                          "and bytes_per_frame use the reference traversal's node/triangle counts",
+                         "traffic": (extend_traffic_rate() * ext_ms_frame) if extend_traffic_rate() else None,
+                         "traffic_basis": "DRAM bytes per frame of k_extend_dyn: the DRAM bytes per ms of three "
+                                          "launches of one ncu capture (profiles/) times this run's k_extend "
+                                          "ms per frame; achieved and bytes_per_frame use the reference "
+                                          "traversal's node/triangle counts",
                          "bytes_per_frame": alg_bytes_frame, "closest_rays_per_frame": rays_closest_frame,
                          "nodes_per_ray": d2["nodes_closest"] / max(1, rays_closest_frame),
                          "tris_per_ray": d2["tris_closest"] / max(1, rays_closest_frame),
