@@ -334,7 +334,7 @@ def test_image_matches_golden_path_for_path(g, traversal):
     v.dispose()
     close = helpers.close_mask(img[..., :3], g["image"][..., :3], 1e-3, 1e-4).all(-1)
     print("pixels equal to the reference path for path:", close.mean())
-    assert close.mean() > 0.95
+    assert close.mean() >= 0.999  # measured 1.0 with either traversal
     assert np.abs(img - g["image"]).mean() < 0.01 * g["image"][..., :3].mean()
 
 
@@ -356,7 +356,7 @@ def test_image_mwc_matches_oracle_per_pixel(traversal):
     ref = o.render_image(p, F)
     close = helpers.close_mask(img[..., :3], ref[..., :3], 1e-3, 1e-4).all(-1)
     print("pixels equal path for path:", close.mean())
-    assert close.mean() > 0.95
+    assert close.mean() >= 0.999  # measured 0.99921 with either traversal
 
 
 def test_converged_image_statistics_pcg_alias_vs_oracle():
@@ -498,5 +498,5 @@ def test_divergence_materials_image_matches_golden_path_for_path(g, traversal):
     ref = g["div_image"]
     close = helpers.close_mask(img[..., :3], ref[..., :3], 1e-3, 1e-4).all(-1)
     print("divergence materials: pixels equal to the reference path for path:", close.mean())
-    assert close.mean() > 0.95
+    assert close.mean() >= 0.99  # measured 0.99248 with either traversal
     assert np.abs(img - ref).mean() < 0.01 * ref[..., :3].mean()

@@ -64,7 +64,7 @@ def test_textured_image_matches_golden_path_for_path(g, traversal):
     ref = g["tex_image"]
     close = helpers.close_mask(img[..., :3], ref[..., :3], 1e-3, 1e-4).all(-1)
     print("textured pixels equal to the reference path for path:", close.mean())
-    assert close.mean() > 0.95
+    assert close.mean() >= 0.99  # measured 0.9941 (reference traversal), 0.9922 (wide)
     assert np.abs(img - ref).mean() < 0.01 * ref[..., :3].mean()
 
 
