@@ -689,8 +689,8 @@ DEV bool shade_path(const Sched& sc, const PathBuf& b, uint32_t slot, bool& shad
     v3 ld = ibl_sample(J.e, p.ibl_rot, p.env_mode, r0, r1, ipdf);
     float cosnl = sat(dot(ld, n_nee));
     if (cosnl > kEpsCos && ipdf > kEpsPdf) {
-      v3 f = bsdf_eval(S.c, S.n, wi, ld) / fmaxf(fabsf(dot(S.n, ld)), kEps);
-      float bpdf = bsdf_pdf(S.c, S.n, wi, ld);
+      float bpdf;
+      v3 f = bsdf_eval_pdf(S.c, S.n, wi, ld, bpdf) / fmaxf(fabsf(dot(S.n, ld)), kEps);
       v3 c = ibl_eval(J.e, p.ibl_rot, ld) * f * cosnl / ipdf;
       if (bpdf > kEpsPdf) c = c * mis_balance(ipdf, bpdf);
       b.sh[slot].sh_dir = f4(ld, kTfarMax);  // one whole sector

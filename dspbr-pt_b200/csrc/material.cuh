@@ -671,6 +671,19 @@ DEV float bsdf_pdf(const Closure& c, v3 n, v3 v, v3 d) {
   return bsdf_pdf_f(c, f, n, v, d);
 }
 
+// bsdf_eval and bsdf_pdf of one direction in one call: the anisotropy frame is
+// built once and the caller saves its registers around one call, not two;
+// the values are those of the two separate calls.
+NOINL v3 bsdf_eval_pdf(const Closure& c, v3 n, v3 v, v3 l, float& pdf) {
+  Frame f = aniso_frame(n, c.aniso_tangent);
+  pdf = bsdf_pdf_f(c, f, n, v, l);
+  if (!(dot(n, v) * dot(n, l) > 0.f))
+    return eval_diffuse_transmission(c, n, l) + eval_dielectric_transmission(c, f, n, v, l);
+  v3 base = eval_reflected_base(c, f, n, v, l);
+  if (c.thin < 0.5f && c.transparency > 0.f) base = base + eval_dielectric_transmission(c, f, n, v, l);
+  return eval_clearcoat(c, n, v, l) + base * clearcoat_base_weight(c, n, v, l);
+}
+
 // ---- sampling (kernel:2625-3567) ----------------------------------------------
 DEV void orthonormal_basis(v3 n, v3& t, v3& b) {
   float sign = n.z >= 0.f ? 1.f : -1.f;
