@@ -176,3 +176,18 @@ def test_autotune_cache_round_trip(tmp_path):
         f.write("not json")
     assert server.load_tuning(path) == {}
     assert server.autotune_cache_path().endswith(os.path.join("dspbr", "autotune.json"))
+
+
+def test_reference_arm_loads_no_library_of_this_repository():
+    """bench.py --impl reference times the reference's shader compiled for the
+    host (oracle/_ref); the workload's BVH is built by a child process, so the
+    timing process maps no shared object of the product."""
+    import subprocess
+    code = ("import sys; sys.path.insert(0, %r); import bench; sc = bench.reference_workload(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_LIB' if 'libdspbr_cuda' in maps else 'CLEAN', sc.bvh.nodes.size // 16, sc.num_triangles)"
+            % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    word, nodes, tris = out.stdout.split()[-3:]
+    assert word == "CLEAN" and int(nodes) > 0 and int(tris) > 1_000_000
