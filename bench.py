@@ -489,7 +489,7 @@ def path_statistics(v, d0, d1):
             "shadow_rays_per_path": (d1["rays_shadow"] - d0["rays_shadow"]) / prim}
 
 
-CONFIG_CPU_BASELINE = {"small": True, "large_framed": False, "divergence": False}  # True: the whole render
+CONFIG_CPU_WHOLE_RENDER = {"small": True, "large_framed": False, "divergence": False}  # True: the whole render
 
 
 def configs_section(local, args):
@@ -564,7 +564,7 @@ def configs_section(local, args):
         bvh = v._scene.bvh() if not args.no_cpu_baseline else None
         v.dispose()
         if bvh is not None:
-            cpu = cpu_config_baseline(sc, bvh, CONFIG_CPU_BASELINE[name])
+            cpu = cpu_config_baseline(sc, bvh, CONFIG_CPU_WHOLE_RENDER[name])
             if cpu is not None:
                 cpu["gpu_ratio"] = out[name]["mrays_per_s"] / cpu["value"]
             out[name]["cpu_baseline"] = cpu
