@@ -155,6 +155,10 @@ def barrier(dist):
         dist.barrier()
 
 
+# wide BVH of the path kernels in every GPU render of this run (--wide-bvh)
+WIDE_BVH = 4
+
+
 def make_workload():
     from dspbr import synth
     from dspbr.viewport import Bvh
@@ -517,7 +521,7 @@ def configs_section(local, args):
                                 settings={"maxBounces": sc.max_bounces,
                                           "russianRouletteStartDepth": sc.rr_start_depth,
                                           "rng": "mwc" if name == "large_framed" else "pcg",
-                                          "envSampling": "alias"})
+                                          "envSampling": "alias", "wideBvh": WIDE_BVH})
         v.setScene(sc)
         v.setIBL(sc.env)
         v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
@@ -762,8 +766,9 @@ def run_gpu_arm(args):
 
     sc = make_workload()
     v = PathtracingViewport(device=local, width=sc.width, height=sc.height,
-                            settings={"maxBounces": sc.max_bounces})
+                            settings={"maxBounces": sc.max_bounces, "wideBvh": WIDE_BVH})
     v.setScene(sc)
+    wide_info = v._scene.wide_bvh()
     v.setIBL(sc.env)
     v.setCamera(PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near))
     lib, h = v.ctx.lib, v.ctx.h
@@ -899,10 +904,12 @@ def run_gpu_arm(args):
                     "d2h_bytes_per_step": int(img.nbytes), "steps": e2e_steps,
                     "per_step": e2e_parts},
             "gpu_launches": gpu_launches,
+            "wide_bvh": wide_info,
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                         "traffic": (extend_traffic_rate() * ext_ms_frame) if extend_traffic_rate() else None,
+                         "traffic": (extend_traffic_rate() * ext_ms_frame)
+                         if extend_traffic_rate() and WIDE_BVH == 4 else None,
                          "traffic_basis": "DRAM bytes per frame of k_extend_dyn: the DRAM bytes per ms of three "
                                           "launches of one ncu capture (profiles/) times this run's k_extend "
                                           "ms per frame; achieved and bytes_per_frame use the reference "
@@ -944,7 +951,11 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the batching / serving sections")
     ap.add_argument("--quick-serving", action="store_true", help="small batching / serving mixes (smoke runs)")
     ap.add_argument("--write-bvh", metavar="PATH", help=argparse.SUPPRESS)
+    ap.add_argument("--wide-bvh", type=int, default=4, choices=[4, 8],
+                    help="wide BVH of the path kernels: 4 (float boxes, default) or 8 (compressed)")
     args = ap.parse_args()
+    global WIDE_BVH
+    WIDE_BVH = args.wide_bvh
     if args.write_bvh:
         return write_workload_bvh(args.write_bvh)
     if args.impl == "reference":

@@ -217,6 +217,23 @@ static int classify_triangles(Status& s, dspbr_scene* sc, cudaStream_t st) {
   return s.cuda(cudaStreamSynchronize(st), "upload classes");
 }
 
+// The compressed 8-wide BVH of a scene whose binary tree and leaf-ordered
+// triangle records are on the device (context option dspbr_set_wide_bvh).
+// Rays of scenes with non-finite boxes take the binary traversal anyway.
+static int attach_cw8(dspbr_ctx* c, dspbr_scene* sc, Status& s) {
+  DeviceCw8 cw;
+  if (c->wide_bvh == 8 && sc->boxes_finite && sc->num_nodes) {
+    int rc = build_cw8_device(sc->nodes.p, sc->num_nodes, sc->num_slots, sc->tris.p, c->stream, &cw, s);
+    if (rc) return rc;
+  }
+  sc->cnodes.swap(cw.nodes);
+  sc->ctris.swap(cw.recs);
+  sc->num_cnodes = cw.num_nodes;
+  sc->num_crecs = cw.num_recs;
+  sc->cw8_levels = cw.levels;
+  return DSPBR_OK;
+}
+
 // Scene creation with the BVH built and collapsed on the device.
 static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t num_vertices,
                                    const uint32_t* indices, uint32_t num_indices, const float* materials,
@@ -268,6 +285,7 @@ static int scene_create_device_bvh(dspbr_ctx* c, const float* vertices, uint32_t
       (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload")))
     return rc;
   sc->device_remap.swap(bin.remap);
+  if ((rc = attach_cw8(c, sc.get(), s))) return rc;
   sc->upload_ms = now_ms() - t0;
   *out = sc.release();
   return DSPBR_OK;
@@ -461,12 +479,27 @@ int dspbr_scene_create(dspbr_ctx* c, const float* vertices, uint32_t num_vertice
   }
   if (num_bvh_indices)
     launch_gather_tris(sc->verts.p, sc->indices.p, remap.p, num_bvh_indices, sc->num_tris, sc->tris.p, c->stream);
-  if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) || (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload"))) {
+  if ((rc = s.cuda(cudaGetLastError(), "gather triangles")) || (rc = s.cuda(cudaStreamSynchronize(c->stream), "scene upload")) ||
+      (rc = attach_cw8(c, sc, s))) {
     delete sc;
     return rc;
   }
   sc->upload_ms = now_ms() - t0;
   *out = sc;
+  return DSPBR_OK;
+}
+
+int dspbr_set_wide_bvh(dspbr_ctx* c, int width) {
+  if (!c || (width != 4 && width != 8)) return DSPBR_ERR_INVALID;
+  c->wide_bvh = width;
+  return DSPBR_OK;
+}
+
+int dspbr_scene_wide_bvh(const dspbr_scene* sc, int* width, uint32_t* nodes, uint32_t* levels) {
+  if (!sc) return DSPBR_ERR_INVALID;
+  if (width) *width = sc->num_cnodes ? 8 : 4;
+  if (nodes) *nodes = sc->num_cnodes ? sc->num_cnodes : sc->num_wnodes;
+  if (levels) *levels = sc->cw8_levels;
   return DSPBR_OK;
 }
 
@@ -585,10 +618,12 @@ int dspbr_scene_update_vertices(dspbr_scene* sc, const float* vertices, uint32_t
   int rc = refit_scene_device(sc->nodes.p, sc->num_nodes, sc->num_slots, sc->wnodes.p, sc->num_wnodes, sc->wleaves.p,
                               sc->tris.p, sc->device_remap.p, sc->verts.p, sc->indices.p, sc->num_tris, st, s);
   if (rc) return rc;
-  sc->refit_ms = now_ms() - t0;
   for (uint32_t v = 0; v < count && sc->boxes_finite; ++v)
     for (int k = 0; k < 3; ++k)
       if (!std::isfinite(vertices[size_t(v) * 20 + k])) sc->boxes_finite = false;
+  // the 8-wide tree is rebuilt from the refitted binary tree (its grouping follows the new boxes)
+  if ((rc = attach_cw8(sc->ctx, sc, s))) return rc;
+  sc->refit_ms = now_ms() - t0;
   dspbr_reset(sc->ctx);
   return DSPBR_OK;
 }

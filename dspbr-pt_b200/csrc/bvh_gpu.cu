@@ -311,6 +311,236 @@ __global__ void k_collapse_level(const float4* __restrict__ bin, uint32_t num_no
   }
 }
 
+// ---- compressed 8-wide BVH, one frontier level per launch ----------------------------------
+constexpr int kLeafSlotsMax = 64;  // MAX_TRIANGLES_PER_LEAF (bvh.glsl:10)
+
+struct Cw8Counters {
+  int nodes, next, recs, error;  // nodes and leaf records allocated, next frontier entries, overflow
+};
+
+// the plane of byte q in a frame (P, 2^e): bit-identical to device.cuh cw8_plane
+__device__ __forceinline__ float cw8_plane_q(uint32_t q, float scale, float p) {
+  return fmaf(__uint_as_float(0x4B000000u | q), scale, p);
+}
+
+// The frame of one axis of a node box [lo, hi]: the smallest power-of-two
+// step (up to 2^100) whose 256 planes reach from at most lo to at least hi.
+__device__ bool cw8_frame(float lo, float hi, uint32_t& ebyte, float& p_out) {
+  int e0;
+  if (hi > lo) {
+    e0 = int(floor(log2(double(hi) - double(lo)) - log2(255.0))) - 1;
+  } else {
+    int ex;
+    frexpf(fabsf(lo) > 0.f ? lo : 1.f, &ex);
+    e0 = ex - 40;
+  }
+  if (e0 < -100) e0 = -100;
+  for (int e = e0; e <= 100; ++e) {
+    const float scale = ldexpf(1.f, e);
+    float p = __fsub_rn(lo, ldexpf(1.f, e + 23));
+    for (int g = 0; g < 64 && cw8_plane_q(0u, scale, p) > lo; ++g) p = nextafterf(p, -INFINITY);
+    if (cw8_plane_q(0u, scale, p) <= lo && cw8_plane_q(255u, scale, p) >= hi) {
+      ebyte = uint32_t(e + 127);
+      p_out = p;
+      return true;
+    }
+  }
+  return false;
+}
+// the largest byte whose plane is <= c, and the smallest whose plane is >= c
+__device__ uint32_t cw8_qlo(float c, float scale, float p, float lo) {
+  const double d = floor((double(c) - double(lo)) / double(scale));
+  int q = int(fmin(255.0, fmax(0.0, d)));
+  for (int g = 0; g < 256 && q > 0 && cw8_plane_q(q, scale, p) > c; ++g) --q;
+  for (int g = 0; g < 256 && q < 255 && cw8_plane_q(q + 1, scale, p) <= c; ++g) ++q;
+  return uint32_t(q);
+}
+__device__ uint32_t cw8_qhi(float c, float scale, float p, float lo) {
+  const double d = ceil((double(c) - double(lo)) / double(scale));
+  int q = int(fmin(255.0, fmax(0.0, d)));
+  for (int g = 0; g < 256 && q < 255 && cw8_plane_q(q, scale, p) < c; ++g) ++q;
+  for (int g = 0; g < 256 && q > 0 && cw8_plane_q(q - 1, scale, p) >= c; ++g) --q;
+  return uint32_t(q);
+}
+__device__ __forceinline__ void cw8_setb(uint32_t* w, int k, uint32_t v) {
+  w[k >> 2] = (w[k >> 2] & ~(0xFFu << (8 * (k & 3)))) | (v << (8 * (k & 3)));
+}
+// the leaf-slot range a binary leaf tests (the reference's leaf loop)
+__device__ __forceinline__ void leaf_range(const float4* bin, uint32_t num_slots, int c, long long& b0, long long& b1) {
+  const int cnt = bin_int(bin, c, 11), first = bin_int(bin, c, 15);
+  b0 = first > 0 ? first : 0;
+  b1 = (long long)first + (cnt < kLeafSlotsMax ? cnt : kLeafSlotsMax);
+  if (b1 > (long long)num_slots) b1 = num_slots;
+  if (b1 < b0) b1 = b0;
+}
+
+// records a binary leaf needs: a header and its slots
+__global__ void k_cw8_count(const float4* __restrict__ bin, uint32_t num_nodes, uint32_t num_slots,
+                            unsigned long long* total) {
+  unsigned long long mine = 0;
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nodes; n += gridDim.x * blockDim.x) {
+    if (bin_int(bin, int(n), 11) <= 0) continue;
+    long long b0, b1;
+    leaf_range(bin, num_slots, int(n), b0, b1);
+    mine += (unsigned long long)(b1 - b0) + 1ull;
+  }
+  if (mine) atomicAdd(total, mine);
+}
+
+// One level: each frontier entry (binary inner node, compressed node index)
+// takes up to 8 children by opening its largest inner child while there is
+// room (the 4-wide collapse's rule), places them in slots by the alignment of
+// their centre with the slot's corner, quantises their boxes and allocates
+// its inner children (contiguous node indices) and its leaf records.
+__global__ void k_cw8_level(const float4* __restrict__ bin, uint32_t num_nodes, uint32_t num_slots,
+                            const int2* __restrict__ frontier, int count, int2* __restrict__ next, int next_cap,
+                            uint4* __restrict__ cnodes, int node_cap, float4* __restrict__ recs,
+                            int32_t* __restrict__ rec_src, int rec_cap, Cw8Counters* ctr) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < count; f += gridDim.x * blockDim.x) {
+    const int2 fe = frontier[f];
+    WChild kids[8];
+    int nk = bin_children(bin, num_nodes, fe.x, kids);
+    for (int guard = 0; guard < 8; ++guard) {
+      int best = -1;
+      float best_area = -1.f;
+      WChild grand[2];
+      for (int k = 0; k < nk; ++k) {
+        if (bin_int(bin, kids[k].node, 11) > 0) continue;
+        if (nk - 1 + bin_children(bin, num_nodes, kids[k].node, grand) > 8) continue;
+        const float a = box_area(kids[k].lo[0], kids[k].lo[1], kids[k].lo[2], kids[k].hi[0], kids[k].hi[1], kids[k].hi[2]);
+        if (a > best_area) {
+          best_area = a;
+          best = k;
+        }
+      }
+      if (best < 0) break;
+      const int ng = bin_children(bin, num_nodes, kids[best].node, grand);
+      for (int k = best; k + 1 < nk; ++k) kids[k] = kids[k + 1];
+      --nk;
+      for (int k = 0; k < ng; ++k) kids[nk++] = grand[k];
+    }
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int k = 0; k < nk; ++k)
+      for (int a = 0; a < 3; ++a) {
+        const float l = fminf(kids[k].lo[a], kids[k].hi[a]), h = fmaxf(kids[k].lo[a], kids[k].hi[a]);
+        kids[k].lo[a] = l;
+        kids[k].hi[a] = h;
+        lo[a] = fminf(lo[a], l);
+        hi[a] = fmaxf(hi[a], h);
+      }
+    int kid_in[8];
+    bool used[8];
+    for (int s = 0; s < 8; ++s) {
+      kid_in[s] = -1;
+      used[s] = false;
+    }
+    float pc[3];
+    for (int a = 0; a < 3; ++a) pc[a] = 0.5f * lo[a] + 0.5f * hi[a];
+    for (int r = 0; r < nk; ++r) {
+      float bs = -INFINITY;
+      int bk = -1, bsl = -1;
+      for (int k = 0; k < nk; ++k) {
+        if (used[k]) continue;
+        for (int s = 0; s < 8; ++s) {
+          if (kid_in[s] >= 0) continue;
+          float sc = 0.f;
+          for (int a = 0; a < 3; ++a) {
+            const float c = 0.5f * kids[k].lo[a] + 0.5f * kids[k].hi[a] - pc[a];
+            sc += ((s >> a) & 1) ? c : -c;
+          }
+          if (bk < 0 || sc > bs) {
+            bs = sc;
+            bk = k;
+            bsl = s;
+          }
+        }
+      }
+      used[bk] = true;
+      kid_in[bsl] = bk;
+    }
+    uint32_t eb[3];
+    float P[3], S[3];
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      if (!cw8_frame(lo[a], hi[a], eb[a], P[a])) ok = false;
+      S[a] = ok ? ldexpf(1.f, int(eb[a]) - 127) : 1.f;
+    }
+    if (!ok) {
+      atomicOr(&ctr->error, 1);
+      continue;
+    }
+    uint32_t imask = 0, meta[2] = {0u, 0u}, ql[3][2], qh[3][2];
+    for (int a = 0; a < 3; ++a) {
+      ql[a][0] = ql[a][1] = 0xFFFFFFFFu;  // empty slot: an inverted box on every axis
+      qh[a][0] = qh[a][1] = 0u;
+    }
+    int ninner = 0, nrec = 0;
+    for (int s = 0; s < 8; ++s) {
+      const int k = kid_in[s];
+      if (k < 0) continue;
+      for (int a = 0; a < 3; ++a) {
+        cw8_setb(ql[a], s, cw8_qlo(kids[k].lo[a], S[a], P[a], lo[a]));
+        cw8_setb(qh[a], s, cw8_qhi(kids[k].hi[a], S[a], P[a], lo[a]));
+      }
+      if (bin_int(bin, kids[k].node, 11) > 0) {
+        long long b0, b1;
+        leaf_range(bin, num_slots, kids[k].node, b0, b1);
+        cw8_setb(meta, s, uint32_t(b1 - b0) + 1u);
+        nrec += int(b1 - b0) + 1;
+      } else {
+        imask |= 1u << s;
+        ++ninner;
+      }
+    }
+    const int cbase = ninner ? atomicAdd(&ctr->nodes, ninner) : 0;
+    const int rbase = nrec ? atomicAdd(&ctr->recs, nrec) : 0;
+    if (cbase + ninner > node_cap || rbase + nrec > rec_cap) {
+      atomicOr(&ctr->error, 2);
+      continue;
+    }
+    for (int s = 0, r = 0, at = rbase; s < 8; ++s) {
+      const int k = kid_in[s];
+      if (k < 0) continue;
+      const int c = kids[k].node;
+      if (bin_int(bin, c, 11) > 0) {
+        long long b0, b1;
+        leaf_range(bin, num_slots, c, b0, b1);
+        const int n = int(b1 - b0);
+        recs[3 * size_t(at)] = make_float4(kids[k].lo[0], kids[k].lo[1], kids[k].lo[2], __int_as_float(-1));
+        recs[3 * size_t(at) + 1] = make_float4(kids[k].hi[0], kids[k].hi[1], kids[k].hi[2], __int_as_float(n));
+        recs[3 * size_t(at) + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        rec_src[at] = -1;
+        for (int j = 0; j < n; ++j) rec_src[at + 1 + j] = int(b0) + j;
+        at += n + 1;
+      } else {
+        const int slot = atomicAdd(&ctr->next, 1);
+        if (slot < next_cap) next[slot] = make_int2(c, cbase + r);
+        else atomicOr(&ctr->error, 4);
+        ++r;
+      }
+    }
+    uint4* o = cnodes + 5 * size_t(fe.y);
+    o[0] = make_uint4(__float_as_uint(P[0]), __float_as_uint(P[1]), __float_as_uint(P[2]),
+                      eb[0] | eb[1] << 8 | eb[2] << 16 | imask << 24);
+    o[1] = make_uint4(uint32_t(cbase), uint32_t(rbase), meta[0], meta[1]);
+    o[2] = make_uint4(ql[0][0], ql[0][1], ql[1][0], ql[1][1]);
+    o[3] = make_uint4(ql[2][0], ql[2][1], qh[0][0], qh[0][1]);
+    o[4] = make_uint4(qh[1][0], qh[1][1], qh[2][0], qh[2][1]);
+  }
+}
+
+// the triangle records of the leaves, in the compressed tree's order
+__global__ void k_cw8_gather(const int32_t* __restrict__ rec_src, int n, const float4* __restrict__ tris,
+                             float4* __restrict__ recs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int src = rec_src[i];
+    if (src < 0) continue;
+    recs[3 * size_t(i)] = tris[3 * size_t(src)];
+    recs[3 * size_t(i) + 1] = tris[3 * size_t(src) + 1];
+    recs[3 * size_t(i) + 2] = tris[3 * size_t(src) + 2];
+  }
+}
+
 // ---- refit: the same trees over moved vertices --------------------------------------------
 constexpr int kMaxLeaf = 64;  // MAX_TRIANGLES_PER_LEAF (bvh.glsl:10): the slots a leaf test visits
 
@@ -1115,6 +1345,69 @@ int collapse_bvh4_device(const DeviceBvh& bin, cudaStream_t st, DeviceWideBvh* o
   out->root = 0;
   out->num_nodes = uint32_t(h.nodes);
   out->num_leaves = uint32_t(h.leaves);
+  return DSPBR_OK;
+}
+
+int build_cw8_device(const float4* bin, uint32_t nn, uint32_t num_slots, const float4* tris, cudaStream_t st,
+                     DeviceCw8* out, Status& s) {
+  out->nodes.reset();
+  out->recs.reset();
+  out->num_nodes = out->num_recs = out->levels = 0;
+  if (nn == 0) return DSPBR_OK;
+  int32_t root_cnt = 0;
+  TRY_CUDA(s, cudaMemcpyAsync(&root_cnt, reinterpret_cast<const char*>(bin) + 44, 4, cudaMemcpyDeviceToHost, st),
+           "8-wide BVH");
+  DevBuf<unsigned long long> total;
+  TRY_CUDA(s, total.alloc(1), "8-wide BVH");
+  TRY_CUDA(s, cudaMemsetAsync(total.p, 0, sizeof(unsigned long long), st), "8-wide BVH");
+  k_cw8_count<<<grid(nn, 256, 148 * 8), 256, 0, st>>>(bin, nn, num_slots, total.p);
+  TRY_CUDA(s, cudaGetLastError(), "8-wide BVH");
+  unsigned long long nrec = 0;
+  TRY_CUDA(s, cudaMemcpyAsync(&nrec, total.p, sizeof nrec, cudaMemcpyDeviceToHost, st), "8-wide BVH");
+  TRY_CUDA(s, cudaStreamSynchronize(st), "8-wide BVH");
+  // a leaf root has no box to quantise, and record indices are int: the 4-wide tree serves those
+  if (root_cnt > 0 || nrec == 0 || nrec > 0x7fffffffull / 3) return DSPBR_OK;
+  DevBuf<uint4> nodes;
+  DevBuf<float4> recs;
+  DevBuf<int32_t> src;
+  DevBuf<int2> fa, fb;
+  DevBuf<Cw8Counters> ctr;
+  TRY_CUDA(s, nodes.alloc(size_t(nn) * 5), "8-wide BVH");
+  TRY_CUDA(s, recs.alloc(size_t(nrec) * 3), "8-wide BVH");
+  TRY_CUDA(s, src.alloc(nrec), "8-wide BVH");
+  TRY_CUDA(s, fa.alloc(nn), "8-wide BVH");
+  TRY_CUDA(s, fb.alloc(nn), "8-wide BVH");
+  TRY_CUDA(s, ctr.alloc(1), "8-wide BVH");
+  Cw8Counters h{1, 0, 0, 0};  // node 0 is the root
+  int2 first = make_int2(0, 0);
+  TRY_CUDA(s, cudaMemcpyAsync(ctr.p, &h, sizeof h, cudaMemcpyHostToDevice, st), "8-wide BVH");
+  TRY_CUDA(s, cudaMemcpyAsync(fa.p, &first, sizeof first, cudaMemcpyHostToDevice, st), "8-wide BVH");
+  int count = 1;
+  uint32_t levels = 0;
+  int2* cur = fa.p;
+  int2* nxt = fb.p;
+  for (; count > 0 && levels <= nn; ++levels) {
+    TRY_CUDA(s, cudaMemsetAsync(&ctr.p->next, 0, sizeof(int), st), "8-wide BVH");
+    k_cw8_level<<<grid(count, 64, 148 * 16), 64, 0, st>>>(bin, nn, num_slots, cur, count, nxt, int(nn), nodes.p,
+                                                          int(nn), recs.p, src.p, int(nrec), ctr.p);
+    TRY_CUDA(s, cudaGetLastError(), "8-wide BVH");
+    TRY_CUDA(s, cudaMemcpyAsync(&h, ctr.p, sizeof h, cudaMemcpyDeviceToHost, st), "8-wide BVH");
+    TRY_CUDA(s, cudaStreamSynchronize(st), "8-wide BVH");
+    if (h.error) return DSPBR_OK;  // an axis no frame fits, or a malformed tree: the 4-wide tree serves
+    count = std::min(h.next, int(nn));
+    std::swap(cur, nxt);
+  }
+  if (count != 0) return DSPBR_OK;
+  k_cw8_gather<<<grid(size_t(h.recs), 256, 148 * 8), 256, 0, st>>>(src.p, h.recs, tris, recs.p);
+  TRY_CUDA(s, cudaGetLastError(), "8-wide BVH");
+  TRY_CUDA(s, out->nodes.alloc(size_t(h.nodes) * 5), "8-wide BVH");
+  TRY_CUDA(s, cudaMemcpyAsync(out->nodes.p, nodes.p, size_t(h.nodes) * 5 * sizeof(uint4), cudaMemcpyDeviceToDevice, st),
+           "8-wide BVH");
+  TRY_CUDA(s, cudaStreamSynchronize(st), "8-wide BVH");
+  out->recs.swap(recs);
+  out->num_nodes = uint32_t(h.nodes);
+  out->num_recs = uint32_t(h.recs);
+  out->levels = levels;
   return DSPBR_OK;
 }
 

@@ -36,6 +36,23 @@ struct DeviceWideBvh {
 };
 int collapse_bvh4_device(const DeviceBvh& bin, cudaStream_t st, DeviceWideBvh* out, Status& s);
 
+// Compressed 8-wide BVH (traversal: device.cuh cw8_step) built on the device
+// from a binary BVH in the reference layout and its leaf-ordered triangle
+// records.  Node: 5 x 16 B (per axis a frame P and power-of-two step, per
+// child six plane bytes, the inner-child mask, the first inner child's index
+// and the first leaf record's index, and per child its record count).  Leaf
+// records: a header (the leaf's exact box and its slot count) and then the
+// triangle records of the leaf's slots.  Leaves nothing in `out` (and returns
+// DSPBR_OK) when the tree cannot be compressed: a leaf root, an axis no frame
+// fits, a malformed tree.  Synchronises `st`.
+struct DeviceCw8 {
+  DevBuf<uint4> nodes;  // 5 per node
+  DevBuf<float4> recs;  // 3 per record
+  uint32_t num_nodes = 0, num_recs = 0, levels = 0;
+};
+int build_cw8_device(const float4* bin_nodes, uint32_t num_nodes, uint32_t num_slots, const float4* tris,
+                     cudaStream_t st, DeviceCw8* out, Status& s);
+
 // Refit after the vertices moved (indices unchanged): the boxes of the binary
 // tree (reference layout) and of the 4-wide tree are recomputed bottom-up from
 // their leaves' triangles, keeping both topologies, and the leaf-ordered

@@ -40,6 +40,8 @@ struct DevScene {
   const float4* __restrict__ wnodes;      // 4-wide BVH: 8 float4 per node (bvh_wide.h WideNode4)
   const int2* __restrict__ wleaves;       // leaf-slot range [x, y) per wide leaf
   int wroot;                              // >= 0: wide node; < 0: ~leaf (the binary root is a leaf)
+  const uint4* __restrict__ cnodes;       // compressed 8-wide BVH (5 uint4 per node), or null
+  const float4* __restrict__ ctris;       // its leaf records: header (exact box, count) + triangle records
   int num_nodes, num_slots, num_tris, num_materials;
   int boxes_finite;  // every node bound is finite (checked at upload)
   int wide;          // closest-hit / any-hit queries of paths use the wide BVH
@@ -372,8 +374,164 @@ DEV bool traverse_wide_impl(const DevScene& s, v3 org, v3 inv, v3 dir, float tfa
   return kAny ? (w.any_hit || hit.tri >= 0) : hit.tri >= 0;
 }
 
+// ---- compressed 8-wide traversal --------------------------------------------------------
+// Node (5 x 16 B, bvh_gpu.h Cw8Node): per axis a frame (P_a, exponent e_a) and
+// per child one byte for each of its six planes; the plane of byte q is
+// fmaf(2^23 + q, 2^e_a, P_a), the float 2^23 + q made by a byte permute.  The
+// builder picks every byte so that this plane lies on or outside the child's
+// exact box, evaluated with the same fmaf, and the slab below applies the
+// reference's arithmetic, (plane - o) * (1/d) with each operation rounded, to
+// that plane.  Rounding is monotone, so a quantised slab is never tighter
+// than the exact one: every box the reference's test accepts passes here too.
+// Leaves keep their exact box in a header record ahead of their triangles;
+// it is tested, like the 4-wide traversal's child boxes, against the closest
+// hit of the moment the parent node was visited, so the leaves whose
+// triangles are tested are those the exact boxes admit.
+//
+// Order: the nearest child (quantised entry) is visited next from a register,
+// the others are pushed with their entry distance (inner nodes; popped only
+// while it lies below the closest hit) or with the closest hit at the push
+// (leaves).  Rays whose slab arithmetic can produce NaN (a zero direction
+// component, a non-finite origin or box) take the reference's binary
+// traversal instead.
+struct Cw8Trav {
+  int cur;         // node index, or ~header index of a leaf
+  float cur_tfar;  // a leaf: the closest hit when its parent was visited
+  int top, step;
+  bool have, overflow, any_hit;
+};
+
+DEV float cw8_plane(uint32_t word, uint32_t sel, float scale, float p) {
+  return fmaf(__uint_as_float(__byte_perm(word, 0x4B000000u, sel)), scale, p);
+}
+DEV float cw8_t(uint32_t word, uint32_t sel, float scale, float p, float o, float inv) {
+  return __fmul_rn(__fsub_rn(cw8_plane(word, sel, scale, p), o), inv);
+}
+
+DEV bool cw8_step(const uint4* __restrict__ cnodes, const float4* __restrict__ ctris, v3 org, v3 inv, v3 dir,
+                  Hit& hit, Cw8Trav& w, int2* stack, bool any) {
+  bool next_in_register = false;
+  if (w.cur < 0) {
+    const float4* hp = ctris + 3 * size_t(~w.cur);
+    const float4 h0 = __ldg(hp), h1 = __ldg(hp + 1);
+    if (slab<false>(h0, h1, org, inv, w.cur_tfar) < kBvhFar) {
+      const int n = __float_as_int(h1.w);
+      for (int i = 1; i <= n; ++i) {
+        const float4* tp = hp + 3 * size_t(i);
+        float4 a = __ldg(tp);
+        int id = __float_as_int(a.w);
+        if (id < 0) continue;
+        float t, u, v;
+        if (intersect_tri(org, dir, a, __ldg(tp + 1), __ldg(tp + 2), hit.t, t, u, v)) {
+          hit.t = t; hit.tri = id; hit.u = u; hit.v = v;
+          if (any) {
+            w.any_hit = true;
+            return false;
+          }
+        }
+      }
+    }
+  } else {
+    const uint4* nd = cnodes + 5 * size_t(w.cur);
+    const uint4 q0 = __ldg(nd), q1 = __ldg(nd + 1), q2 = __ldg(nd + 2), q3 = __ldg(nd + 3), q4 = __ldg(nd + 4);
+    const float px = __uint_as_float(q0.x), py = __uint_as_float(q0.y), pz = __uint_as_float(q0.z);
+    const float sx = __uint_as_float((q0.w & 0xFFu) << 23), sy = __uint_as_float(((q0.w >> 8) & 0xFFu) << 23),
+                sz = __uint_as_float(((q0.w >> 16) & 0xFFu) << 23);
+    const uint32_t imask = q0.w >> 24;
+    // the near and far planes of each axis (low and high bytes by the sign of the direction)
+    const bool nx = inv.x < 0.f, ny = inv.y < 0.f, nz = inv.z < 0.f;
+    const uint32_t nx0 = nx ? q3.z : q2.x, nx1 = nx ? q3.w : q2.y, fx0 = nx ? q2.x : q3.z, fx1 = nx ? q2.y : q3.w;
+    const uint32_t ny0 = ny ? q4.x : q2.z, ny1 = ny ? q4.y : q2.w, fy0 = ny ? q2.z : q4.x, fy1 = ny ? q2.w : q4.y;
+    const uint32_t nz0 = nz ? q4.z : q3.x, nz1 = nz ? q4.w : q3.y, fz0 = nz ? q3.x : q4.z, fz1 = nz ? q3.y : q4.w;
+    bool have_best = false;
+    int2 best = make_int2(0, 0);
+    float best_d = 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t sel = 0x7540u | uint32_t(c & 3);
+      const bool hi = c >= 4;
+      const float tnx = cw8_t(hi ? nx1 : nx0, sel, sx, px, org.x, inv.x);
+      const float tny = cw8_t(hi ? ny1 : ny0, sel, sy, py, org.y, inv.y);
+      const float tnz = cw8_t(hi ? nz1 : nz0, sel, sz, pz, org.z, inv.z);
+      const float tfx = cw8_t(hi ? fx1 : fx0, sel, sx, px, org.x, inv.x);
+      const float tfy = cw8_t(hi ? fy1 : fy0, sel, sy, py, org.y, inv.y);
+      const float tfz = cw8_t(hi ? fz1 : fz0, sel, sz, pz, org.z, inv.z);
+      const float tmin = fmaxf(fmaxf(tnx, tny), tnz), tmax = fminf(fminf(tfx, tfy), tfz);
+      const bool inner = (imask >> c) & 1u;
+      const uint32_t meta = (hi ? q1.w : q1.z) >> (8 * (c & 3)) & 0xFFu;
+      if (!(tmin > tmax || tmax < 0.f || tmin >= hit.t) && (inner || meta != 0u)) {
+        int2 e;
+        if (inner) {
+          e = make_int2(int(q1.x + __popc(imask & ((1u << c) - 1u))), __float_as_int(tmin));
+        } else {
+          // records of the leaf children in lower slots come first
+          uint32_t before = c == 0 ? 0u : __dp4a(c < 4 ? q1.z & ((1u << (8 * (c & 3))) - 1u) : q1.z, 0x01010101u, 0u);
+          if (c > 4) before = __dp4a(q1.w & ((1u << (8 * (c & 3))) - 1u), 0x01010101u, before);
+          e = make_int2(~int(q1.y + before), __float_as_int(hit.t));
+        }
+        int2 push_e = e;
+        bool do_push = have_best;
+        if (have_best && tmin < best_d) {
+          push_e = best;
+          best = e;
+          best_d = tmin;
+        } else if (!have_best) {
+          best = e;
+          best_d = tmin;
+          have_best = true;
+        }
+        if (do_push) {
+          if (w.top < kWideStack) stack[w.top++] = push_e;
+          else w.overflow = true;
+        }
+      }
+    }
+    if (have_best) {
+      w.cur = best.x;
+      w.cur_tfar = __int_as_float(best.y);
+      next_in_register = true;
+    }
+  }
+  if (!next_in_register) {
+    w.have = false;
+    while (w.top > 0) {
+      const int2 en = stack[--w.top];
+      if (!any && en.x >= 0 && __int_as_float(en.y) >= hit.t) continue;
+      w.cur = en.x;
+      w.cur_tfar = __int_as_float(en.y);
+      w.have = true;
+      break;
+    }
+  }
+  ++w.step;
+  return w.have && w.step < kMaxSteps;
+}
+
+// The compressed 8-wide traversal of one ray (any: stop at the first accepted
+// triangle).  Same closest t as the binary traversal except for ties within
+// rounding between coplanar faces (two triangles whose t differ by an ulp:
+// which is found depends on the visiting order, as in the reference itself).
+DEV bool traverse_cw8_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool any, Hit& hit, bool& aborted) {
+  v3 inv = inv_dir(dir);
+  if (!(s.boxes_finite && finite3(org) && finite3(inv))) {
+    bool r = any ? traverse_impl<true, true>(s, org, inv, dir, tfar, hit, aborted, nullptr, nullptr)
+                 : traverse_impl<false, true>(s, org, inv, dir, tfar, hit, aborted, nullptr, nullptr);
+    return r;
+  }
+  hit.t = tfar;
+  hit.tri = -1;
+  hit.u = hit.v = 0.f;
+  int2 stack[kWideStack];
+  Cw8Trav w{0, tfar, 0, 0, true, false, false};
+  while (cw8_step(s.cnodes, s.ctris, org, inv, dir, hit, w, stack, any)) {
+  }
+  aborted = !w.any_hit && (w.overflow || (w.have && w.step >= kMaxSteps));
+  return w.any_hit || hit.tri >= 0;
+}
+
 // closest hit (any = false) or any hit (any = true) chosen at run time
 DEV bool traverse_wide_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool any, Hit& hit, bool& aborted) {
+  if (s.cnodes) return traverse_cw8_rt(s, org, dir, tfar, any, hit, aborted);
   v3 inv = inv_dir(dir);
   const bool exact = !(s.boxes_finite && finite3(org) && finite3(inv));
   hit.t = tfar;
@@ -393,12 +551,20 @@ DEV bool traverse_wide_rt(const DevScene& s, v3 org, v3 dir, float tfar, bool an
   return w.any_hit || hit.tri >= 0;
 }
 
+// the 4-wide tree only (kernels specialised for scenes without an 8-wide tree)
 template <bool kAny>
-DEV bool traverse_wide(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted) {
+DEV bool traverse_wide4(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted) {
   v3 inv = inv_dir(dir);
   if (s.boxes_finite && finite3(org) && finite3(inv))
     return traverse_wide_impl<kAny, false>(s, org, inv, dir, tfar, hit, aborted);
   return traverse_wide_impl<kAny, true>(s, org, inv, dir, tfar, hit, aborted);
+}
+
+// the scene's wide tree: the compressed 8-wide one where it has one
+template <bool kAny>
+DEV bool traverse_wide(const DevScene& s, v3 org, v3 dir, float tfar, Hit& hit, bool& aborted) {
+  if (s.cnodes) return traverse_cw8_rt(s, org, dir, tfar, kAny, hit, aborted);
+  return traverse_wide4<kAny>(s, org, dir, tfar, hit, aborted);
 }
 
 template <bool kAny>

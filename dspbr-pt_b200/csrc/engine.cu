@@ -174,7 +174,7 @@ int Engine::set_job(int slot, const Job& job, unsigned long long items_total) {
   Status s{err_};
   if (slot < 0 || slot >= kMaxJobs) return s.fail(DSPBR_ERR_INVALID, "job slot %d out of range", slot);
   k_set_job<<<1, 32, 0, stream_>>>(job, items_total, slot, jobs_.p, js_.p, d_status_);
-  slot_traversal_[slot] = job.s.wide ? kTravWide : kTravReference;
+  slot_traversal_[slot] = job.s.wide ? (job.s.cnodes ? kTravWide8 : kTravWide) : kTravReference;
   slot_textured_[slot] = job.s.num_texinfo > 0;
   ++kind_launches[3];
   return s.cuda(cudaGetLastError(), "set job");
@@ -206,8 +206,13 @@ int Engine::set_active(const std::vector<int>& order) {
   ++kind_launches[3];
   // one traversal kind for all active jobs: launch the kernels specialised for it
   int trav = order.empty() ? lc_.traversal : slot_traversal_[order[0]];
-  for (int k : order)
-    if (slot_traversal_[k] != trav) trav = kTravPerPath;
+  for (int k : order) {
+    const int t = slot_traversal_[k];
+    if (t == trav) continue;
+    // 4-wide and 8-wide jobs together: the 4-wide tree, which every scene keeps
+    const bool wide_mix = (t == kTravWide || t == kTravWide8) && (trav == kTravWide || trav == kTravWide8);
+    trav = wide_mix ? kTravWide : kTravPerPath;
+  }
   // the shade kernels without the texture code when no active job samples textures
   bool tex = false;
   for (int k : order) tex = tex || slot_textured_[k];

@@ -391,8 +391,9 @@ __global__ void k_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned
 template <bool kAny, bool kCount, int kTrav>
 DEV bool trace_path_ray(const DevScene& s, v3 org, v3 dir, float tfar, Hit& h, bool& aborted, uint32_t* nodes,
                         uint32_t* tris) {
+  if (!kCount && kTrav == kTravWide8) return traverse_cw8_rt(s, org, dir, tfar, kAny, h, aborted);
   if (!kCount && (kTrav == kTravWide || (kTrav == kTravPerPath && s.wide)))
-    return traverse_wide<kAny>(s, org, dir, tfar, h, aborted);
+    return traverse_wide4<kAny>(s, org, dir, tfar, h, aborted);
   return traverse<kAny>(s, org, dir, tfar, h, aborted, kCount ? nodes : nullptr, kCount ? tris : nullptr);
 }
 
@@ -456,12 +457,13 @@ DEV bool next_warp_batch(uint32_t* cursor, uint32_t count, uint32_t& i, bool& fi
 
 DEV void shade_miss_path(const Sched& sc, const PathBuf& b, uint32_t slot);
 
-// closest hits of q[cur], 4-wide traversal.  A camera ray that leaves the
+// closest hits of q[cur], 4-wide traversal (kTrav kTravWide) or compressed 8-wide (kTravWide8).  A camera ray that leaves the
 // scene ends its path here: its sample is the background (misptdl.glsl:41-46),
 // added to the job's sums before the slot is freed, instead of a trip through
 // the miss queue and the shading kernel.  Only camera rays: a later vertex's
 // path may still receive its shadow rays' contribution from k_connect, which
 // runs beside this kernel; its misses are shaded after both.
+template <int kTrav>
 __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[cur];
   const uint32_t* q = b.q[cur];
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(128, 8) k_extend_dyn(Sched sc, PathBuf b, int 
       const DevScene& s = sc.jobs[job].s;
       Hit h;
       bool aborted = false;
-      traverse_wide<false>(s, mk(o), mk(d), kTfarMax, h, aborted);
+      trace_path_ray<false, false, kTrav>(s, mk(o), mk(d), kTfarMax, h, aborted, nullptr, nullptr);
       is_hit = h.tri >= 0;
       is_miss = !is_hit;
       sky = is_miss && __float_as_int(o.w) == 0;
@@ -554,7 +556,8 @@ __global__ void __launch_bounds__(256, 4) k_connect(Sched sc, PathBuf b, int cur
   }
 }
 
-// the shadow rays of qs[cur] by persistent warps (see next_warp_batch), 4-wide traversal
+// the shadow rays of qs[cur] by persistent warps (see next_warp_batch), 4-wide or 8-wide traversal
+template <int kTrav>
 __global__ void __launch_bounds__(128, 8) k_connect_dyn(Sched sc, PathBuf b, int cur) {
   const uint32_t count = b.counts[kCntShadow0 + cur];
   const uint32_t* qs = b.qs[cur];
@@ -565,7 +568,7 @@ __global__ void __launch_bounds__(128, 8) k_connect_dyn(Sched sc, PathBuf b, int
     if (i < count) {
       bool aborted = false;
       int nrays = 0;
-      connect_slot<false, kTravWide>(sc, b, qs[i], aborted, nrays, nullptr, nullptr);
+      connect_slot<false, kTrav>(sc, b, qs[i], aborted, nrays, nullptr, nullptr);
       rays += uint32_t(nrays);
       aborted_n += aborted ? 1u : 0u;
     }
@@ -1015,8 +1018,8 @@ LaunchLimits launch_limits() {
     }
     return n;
   };
-  l.trace_per_sm = resident(reinterpret_cast<const void*>(k_extend_dyn), 128, 8);
-  l.connect_per_sm = resident(reinterpret_cast<const void*>(k_connect_dyn), 128, 8);
+  l.trace_per_sm = resident(reinterpret_cast<const void*>(k_extend_dyn<kTravWide>), 128, 8);
+  l.connect_per_sm = resident(reinterpret_cast<const void*>(k_connect_dyn<kTravWide>), 128, 8);
   l.shade_per_sm[0] = resident(reinterpret_cast<const void*>(k_shade<false>), 128, 5);
   l.shade_per_sm[1] = resident(reinterpret_cast<const void*>(k_shade<true>), 128, 5);
   return l;
@@ -1050,14 +1053,17 @@ void launch_set_loop(LoopCtl* ctl, unsigned long long iterations, unsigned long 
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
   if (count) k_extend<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
-  else if (lc.traversal == kTravWide) k_extend_dyn<<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_extend_dyn<kTravWide><<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide8) k_extend_dyn<kTravWide8><<<lc.dyn_blocks, 128, 0, st>>>(sc, b, cur);
   else if (lc.traversal == kTravReference) k_extend<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
   else k_extend<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st) {
   const dim3 g(lc.trace_blocks), t(lc.trace_threads);
   if (count) k_connect<true, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
-  else if (lc.traversal == kTravWide) k_connect_dyn<<<lc.connect_dyn_blocks, 128, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide) k_connect_dyn<kTravWide><<<lc.connect_dyn_blocks, 128, 0, st>>>(sc, b, cur);
+  else if (lc.traversal == kTravWide8)
+    k_connect_dyn<kTravWide8><<<lc.connect_dyn_blocks, 128, 0, st>>>(sc, b, cur);
   else if (lc.traversal == kTravReference) k_connect<false, kTravReference><<<g, t, 0, st>>>(sc, b, cur);
   else k_connect<false, kTravPerPath><<<g, t, 0, st>>>(sc, b, cur);
 }

@@ -155,7 +155,10 @@ struct Sched {
 
 // Traversal of the path kernels: per path (the job's DevScene::wide), or one
 // kind for every path when all active jobs use the same (smaller kernels).
-enum : int { kTravPerPath = 0, kTravWide = 1, kTravReference = 2 };
+// kTravWide: the 4-wide tree; kTravWide8: the compressed 8-wide tree (every
+// active job's scene has one); kTravPerPath: each job's own choice (wide
+// jobs take the 4-wide tree, which every scene keeps)
+enum : int { kTravPerPath = 0, kTravWide = 1, kTravReference = 2, kTravWide8 = 3 };
 
 struct LaunchCfg {
   int trace_blocks = 148 * 16, trace_threads = 128;

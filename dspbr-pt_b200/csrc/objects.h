@@ -23,6 +23,10 @@ struct dspbr_scene {
   dspbr::DevBuf<int2> wleaves;
   int wroot = 0;
   uint32_t num_wnodes = 0;  // wide nodes in use
+  // compressed 8-wide BVH (bvh_gpu.h DeviceCw8), empty when the 4-wide one serves
+  dspbr::DevBuf<uint4> cnodes;
+  dspbr::DevBuf<float4> ctris;
+  uint32_t num_cnodes = 0, num_crecs = 0, cw8_levels = 0;
   double refit_ms = 0.0;    // the last dspbr_scene_update_vertices
   dspbr::DevBuf<int32_t> device_remap;  // leaf-slot remap of a device-built BVH
   // material textures
@@ -46,6 +50,8 @@ struct dspbr_scene {
     s.wnodes = wnodes.p;
     s.wleaves = wleaves.p;
     s.wroot = wroot;
+    s.cnodes = num_cnodes ? cnodes.p : nullptr;
+    s.ctris = num_cnodes ? ctris.p : nullptr;
     s.wide = 1;
     s.texinfo = texinfo.p;
     s.tex_arrays = tex_arrays.p;
@@ -56,7 +62,7 @@ struct dspbr_scene {
   }
   uint64_t bytes() const {
     return nodes.bytes() + tris.bytes() + verts.bytes() + materials.bytes() + indices.bytes() + tri_class.bytes() +
-           wnodes.bytes() + wleaves.bytes() + device_remap.bytes() + texinfo.bytes() + tex_arrays.bytes() +
+           wnodes.bytes() + wleaves.bytes() + cnodes.bytes() + ctris.bytes() + device_remap.bytes() + texinfo.bytes() + tex_arrays.bytes() +
            tex_bytes();
   }
   uint64_t tex_bytes() const {
@@ -101,6 +107,8 @@ struct dspbr_ctx {
   // builds the host builder's tree (47-132 ms against ~430 ms on the host for
   // 1.15M triangles)
   int bvh_builder = DSPBR_BVH_BUILD_DEVICE;
+  // width of the wide BVH the path kernels trace: 4 (float boxes) or 8 (quantised boxes)
+  int wide_bvh = 4;
   std::unique_ptr<dspbr::Engine> eng;  // path pool + job table; this context's render is job slot 0
   // render_async: the iteration loop runs on a worker thread
   std::thread worker;

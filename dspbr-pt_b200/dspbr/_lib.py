@@ -153,6 +153,8 @@ SIGNATURES = {
     "dspbr_scene_create": (C.c_int, [_V, _F, C.c_uint32, _U, C.c_uint32, _F, C.c_uint32, _F, C.c_uint32, _I,
                                       C.c_uint32, _PV]),
     "dspbr_set_bvh_builder": (C.c_int, [_V, C.c_int]),
+    "dspbr_set_wide_bvh": (C.c_int, [_V, C.c_int]),
+    "dspbr_scene_wide_bvh": (C.c_int, [_V, C.POINTER(C.c_int), _U, _U]),
     "dspbr_scene_set_textures": (C.c_int, [_V, _F, C.c_uint32, C.POINTER(TextureArray), C.c_uint32]),
     "dspbr_scene_bvh": (C.c_int, [_V, _F, _I, _U, _U]),
     "dspbr_scene_update_materials": (C.c_int, [_V, _F, C.c_uint32, C.c_uint32]),

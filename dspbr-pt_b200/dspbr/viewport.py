@@ -89,6 +89,13 @@ class Context:
             raise ValueError(f"set_bvh_builder: {builder!r} is not one of {sorted(codes)}")
         self.check(self.lib.dspbr_set_bvh_builder(self.h, codes[builder]))
 
+    def set_wide_bvh(self, width: int) -> None:
+        """Width of the wide BVH the path kernels trace in scenes created
+        afterwards: 4 (float boxes) or 8 (compressed: quantised child boxes)."""
+        if width not in (4, 8):
+            raise ValueError(f"set_wide_bvh: {width!r} is not 4 or 8")
+        self.check(self.lib.dspbr_set_wide_bvh(self.h, int(width)))
+
     def host_array(self, shape, dtype=np.float32) -> np.ndarray:
         """numpy array over page-locked host memory (dspbr_host_alloc)."""
         import weakref
@@ -167,6 +174,13 @@ class DeviceScene:
         self.ctx.check(self.ctx.lib.dspbr_scene_bvh(self.h, fptr(nodes), iptr(remap), None, None))
         return Bvh(nodes, remap, 0, self.num_triangles)
 
+    def wide_bvh(self) -> dict:
+        """The wide BVH the path kernels use: width (4 or 8), nodes and, for
+        the 8-wide tree, its depth in levels."""
+        w, nodes, levels = C.c_int(), C.c_uint32(), C.c_uint32()
+        self.ctx.check(self.ctx.lib.dspbr_scene_wide_bvh(self.h, C.byref(w), C.byref(nodes), C.byref(levels)))
+        return {"width": w.value, "nodes": nodes.value, "levels": levels.value}
+
     def device_bytes(self) -> int:
         b = C.c_uint64()
         self.ctx.check(self.ctx.lib.dspbr_scene_device_bytes(self.h, C.byref(b)))
@@ -234,7 +248,7 @@ def look_at_matrix(position, target, up=(0.0, 1.0, 0.0)) -> np.ndarray:
     return e
 
 
-DISPLAY_SETTINGS = ("bvhBuilder", "exposure", "toneMapping", "pixelRatio", "interactionPixelRatio", "enableGamma", "enableFxaa",
+DISPLAY_SETTINGS = ("bvhBuilder", "wideBvh", "exposure", "toneMapping", "pixelRatio", "interactionPixelRatio", "enableGamma", "enableFxaa",
                     "tileResolution", "debugMode")
 
 
@@ -272,6 +286,11 @@ def apply_settings(p, settings: dict, display: dict | None = None) -> None:
             p.ray_eps = float(v)
         elif k == "clampThreshold":
             p.clamp_threshold = float(v)
+        elif k == "wideBvh":
+            if v not in (4, 8):
+                raise ValueError(f"wideBvh: {v!r} is not 4 or 8")
+            if display is not None:
+                display[k] = int(v)
         elif k in DISPLAY_SETTINGS:
             if display is not None:
                 display[k] = v
@@ -288,6 +307,7 @@ def apply_settings(p, settings: dict, display: dict | None = None) -> None:
         elif k == "bvhBuilder":
             if display is not None:
                 display[k] = v
+
         elif k == "materialProfile":
             p.profile = _lib.PROFILE_LEAN if v == "webgl-lean" else _lib.PROFILE_FULL
         else:
@@ -393,6 +413,8 @@ class PathtracingViewport:
         """scene: a synth.Scene or any object with vertices / indices / materials arrays."""
         try:
             self.ctx.set_bvh_builder(self._display.get("bvhBuilder", "device"))
+            if "wideBvh" in self._display:
+                self.ctx.set_wide_bvh(self._display["wideBvh"])
             ds = DeviceScene(self.ctx, scene.vertices, scene.indices, scene.materials, getattr(scene, "bvh", None))
             if getattr(scene, "tex_infos", None) is not None:
                 ds.set_textures(scene.tex_infos, scene.tex_arrays)

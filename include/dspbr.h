@@ -137,6 +137,22 @@ int dspbr_scene_create(dspbr_ctx* ctx, const float* vertices, uint32_t num_verti
                        uint32_t num_bvh_indices, dspbr_scene** out);
 /* material edits (dirty materials re-uploaded, renderer.ts:440-448) */
 int dspbr_set_bvh_builder(dspbr_ctx* ctx, int builder);
+/* The wide BVH that the path kernels (and dspbr_trace_* with the wide
+ * traversal) use for scenes created after the call; 4 or 8:
+ *   4  4-wide nodes of 128 B with the binary tree's float boxes (default);
+ *   8  compressed 8-wide nodes of 80 B: per axis a float origin and a
+ *      power-of-two step, per child six 8-bit planes chosen on or outside its
+ *      exact box, and each leaf's exact box in a record ahead of its
+ *      triangles (published as compressed wide BVHs, Ylitie, Karras and Laine,
+ *      HPG 2017; the reference's TinyBVH offers such a layout as BVH8_CWBVH).
+ * The closest t equals the binary traversal's except for ties within
+ * rounding between coplanar faces (t differing by an ulp), where the face
+ * found first is kept.  Scenes whose tree cannot be compressed (a leaf root,
+ * non-finite boxes) keep the 4-wide tree. */
+int dspbr_set_wide_bvh(dspbr_ctx* ctx, int width);
+/* The wide BVH a scene's path kernels use: width 4 or 8, its node count and,
+ * for the 8-wide tree, its depth in levels (0 otherwise). */
+int dspbr_scene_wide_bvh(const dspbr_scene* scene, int* width, uint32_t* nodes, uint32_t* levels);
 /* Material textures (scene_data.ts:71-100, scene_data_webgl2.ts:233-363):
  * textures of one resolution form an RGBA8 texture array sampled LINEAR +
  * REPEAT; tex_infos holds 8 floats per texture reference (TexInfo,
@@ -159,7 +175,8 @@ int dspbr_scene_update_materials(dspbr_scene* scene, const float* materials, uin
  * triangles): the BVH keeps its topology and its boxes are refitted on the
  * device, bottom-up from the leaves' triangles (the binary tree of
  * dspbr_scene_bvh and the 4-wide tree of the path kernels), then the
- * leaf-ordered triangle records are gathered again.  New: the reference
+ * leaf-ordered triangle records are gathered again; a compressed 8-wide tree
+ * (dspbr_set_wide_bvh) is built again from the refitted binary tree.  New: the reference
  * rebuilds its BVH on every setScene (tinybvh_builder.ts:43-256); a refit is
  * the animated-geometry step of a device BVH.  Resets the accumulation of the
  * scene's context; not while a server request renders the scene.  Shading
