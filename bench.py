@@ -816,11 +816,11 @@ def run_gpu_arm(args):
     cam = PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near)
     # the caller's frame buffers, page-locked, reused: two, so that step k's
     # copy runs while step k+1 renders
-    bufs = [v.allocReadbackBuffer(), v.allocReadbackBuffer()]
+    bufs = [v.allocReadbackBuffer() for _ in range(3)]
     img = bufs[0]
     e2e_steps = max(1, min(args.steps, 10))
 
-    def e2e_run(pipelined):
+    def e2e_run(pipelined, ahead=False):
         v.resetAccumulation()
         d3 = v.diagnostics
         parts = np.zeros(3)
@@ -832,14 +832,17 @@ def run_gpu_arm(args):
             tb = time.perf_counter()
             v.start(1)
             tc = time.perf_counter()
-            if pipelined:
+            if ahead:
+                v.readWaitReady()  # step k-2's image is on the host
+                v.readAccumulationAsync(out=bufs[k % 3])
+            elif pipelined:
                 v.readWait()  # step k-1's image is on the host
                 v.readAccumulationAsync(out=bufs[k % 2])
             else:
                 v.readAccumulation(out=img)
             td = time.perf_counter()
             parts += (tb - ta, tc - tb, td - tc)
-        v.readWait()  # the last step's image
+        v.readWait()  # the last steps' images
         t1 = time.perf_counter()
         d4 = v.diagnostics
         rays = (d4["rays_primary"] + d4["rays_extension"] + d4["rays_shadow"]) - \
@@ -854,15 +857,25 @@ def run_gpu_arm(args):
     # finish; step k's image is copied as soon as they have
     v.setSettings({"pipelinedFrames": True})
     e2e_run(True)  # untimed: the second sum buffer's first use
-    e2e_value, parts = e2e_run(True)
+    e2e_two, parts_two = e2e_run(True)
+    # three accumulations in flight: step k takes step k-2's image (a
+    # render-ahead queue of two frames), so that a frame's last paths share
+    # the pool with the next two frames' first ones
+    v.setSettings({"pipelinedFrames": 3})
+    e2e_run(True, ahead=True)  # untimed: the third sum buffer's first use
+    e2e_value, parts = e2e_run(True, ahead=True)
     v.setSettings({"pipelinedFrames": False})
     e2e_parts = {"set_camera_ms": 1e3 * parts[0], "render_1_frame_ms": 1e3 * parts[1],
                  "read_wait_and_enqueue_ms": 1e3 * parts[2],
-                 "frames": "pipelined (viewport setting pipelinedFrames): a step's render returns once its "
-                           "samples have started; its last paths finish during the next step's render",
+                 "frames": "pipelined, three accumulations in flight (viewport setting pipelinedFrames: 3): a "
+                           "step's render returns once its samples have started and the frame two steps "
+                           "earlier has finished; a frame's last paths finish during the next two renders",
                  "readback": "step k's device-to-host copy starts when its paths have finished and runs during "
-                             "step k+1's render; the last step's paths and copy are waited for inside the "
-                             "timed region",
+                             "a later step's render; step k waits (readWaitReady) for step k-2's image; the last "
+                             "steps' paths and copies are waited for inside the timed region",
+                 "frames_two_in_flight": {"value": e2e_two, "render_1_frame_ms": 1e3 * parts_two[1],
+                                          "read_wait_and_enqueue_ms": 1e3 * parts_two[2],
+                                          "readback": "step k waits for step k-1's image"},
                  "frames_not_pipelined": {"value": e2e_copy, "render_1_frame_ms": 1e3 * parts_copy[1],
                                           "read_wait_and_enqueue_ms": 1e3 * parts_copy[2]},
                  "serial": {"value": e2e_serial, "render_1_frame_ms": 1e3 * parts_serial[1],

@@ -102,16 +102,60 @@ static int issue_read(dspbr_ctx* c, const double4* accum, uint64_t count, float*
   return DSPBR_OK;
 }
 
+// A sum buffer of at least npix pixels for a new epoch: a finished epoch's,
+// or a new allocation.  The caller orders its first write after the pending
+// copy (after_pending_copy): a read of the epoch that left it may still run.
+static cudaError_t take_spare(dspbr_ctx* c, size_t npix, std::unique_ptr<DevBuf<double4>>& out) {
+  if (!c->spare.empty()) {
+    out = std::move(c->spare.back());
+    c->spare.pop_back();
+  } else {
+    out.reset(new DevBuf<double4>());
+  }
+  return out->n < npix ? out->alloc(npix) : cudaSuccess;
+}
+
+// a job slot no epoch in flight uses
+static int free_slot(const dspbr_ctx* c) {
+  for (int k = 0;; ++k) {
+    bool used = k == c->slot;
+    for (const auto& o : c->older) used = used || o.slot == k;
+    if (!used) return k;
+  }
+}
+
+// The older epochs that have finished leave the flight list, oldest first:
+// their deferred reads are enqueued (after `after` when given) and their sum
+// buffers become spares.
+static int retire_finished(dspbr_ctx* c, cudaEvent_t after) {
+  Engine& E = *c->eng;
+  for (size_t i = 0; i < c->older.size();) {
+    auto& o = c->older[i];
+    if (!E.job_done(o.slot)) {
+      ++i;
+      continue;
+    }
+    if (o.deferred) {
+      int rc = issue_read(c, o.sums->p, o.samples, o.deferred, after);
+      if (rc) return rc;
+    }
+    c->spare.push_back(std::move(o.sums));
+    c->older.erase(c->older.begin() + long(i));
+  }
+  return DSPBR_OK;
+}
+
 // Pipelined frames: finishes every path of the context's epochs in the pool
-// (the render loop with its tail drain) and enqueues a deferred read.
+// (the render loop with its tail drain) and enqueues the deferred reads, oldest
+// epoch first.
 static int flush_pipeline(dspbr_ctx* c) {
-  if (!c->tail_live && !c->prev_live && !c->deferred) return DSPBR_OK;
+  if (!c->tail_live && c->older.empty() && !c->deferred) return DSPBR_OK;
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   Engine& E = *c->eng;
-  if (c->tail_live || c->prev_live) {
+  if (c->tail_live || !c->older.empty()) {
     std::vector<int> act;
-    if (c->prev_live) act.push_back(c->slot ^ 1);
+    for (const auto& o : c->older) act.push_back(o.slot);
     if (c->tail_live) act.push_back(c->slot);
     int rc = E.set_active(act);
     // every work item has started: iterations until fewer than the drain
@@ -119,17 +163,19 @@ static int flush_pipeline(dspbr_ctx* c) {
     // guards the loop: a path lives at most max_bounces + 1 iterations)
     if (!rc) rc = E.run_loop(act.back(), 4096 + 8);
     if (rc) return rc;
-    if (c->prev_live && !E.job_done(c->slot ^ 1))
-      return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: previous frame not finished by the drain");
-    c->tail_live = c->prev_live = false;
+    for (const auto& o : c->older)
+      if (!E.job_done(o.slot)) return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: earlier frame not finished by the drain");
+    c->tail_live = false;
+    if ((rc = retire_finished(c, nullptr))) return rc;
   }
   if (c->deferred) {
     float* dst = c->deferred;
-    const bool prev = c->deferred_prev;
     c->deferred = nullptr;
-    c->deferred_prev = false;
-    return issue_read(c, prev ? c->accum_prev.p : c->accum.p, prev ? c->prev_sample_count : c->sample_count, dst,
-                      nullptr);
+    int rc = issue_read(c, c->accum.p, c->sample_count, dst, nullptr);
+    if (rc) return rc;
+    // the copy stream's mean reads these sums: later renders and resets,
+    // which write them on the context's stream, wait for it
+    TRY_CUDA(s, after_pending_copy(c), "read accumulation");
   }
   return DSPBR_OK;
 }
@@ -826,21 +872,24 @@ int dspbr_reset(dspbr_ctx* c) {
   { int rc_ = settle_worker(c); if (rc_) return rc_; }
   Status s = c->st();
   if (c->pipelined && c->tail_live) {
-    if (c->prev_live || (c->deferred && c->deferred_prev)) {
+    if (int(c->older.size()) + 1 >= c->depth) {
       int rc = flush_pipeline(c);
       if (rc) return rc;
     } else {
-      // a new epoch in the other slot and sum buffer; the old one finishes
-      // during the next render call
+      // a new epoch in a free slot and sum buffer; the old one finishes
+      // during the next render calls
       TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
       const size_t npix = size_t(c->width) * c->height;
-      if (c->accum_prev.n < npix) TRY_CUDA(s, c->accum_prev.alloc(npix), "alloc accumulation");
-      c->accum.swap(c->accum_prev);
-      c->prev_sample_count = c->sample_count;
-      c->prev_live = true;
+      dspbr_ctx::Older o;
+      TRY_CUDA(s, take_spare(c, npix, o.sums), "alloc accumulation");
+      o.sums->swap(c->accum);
+      o.samples = c->sample_count;
+      o.slot = c->slot;
+      o.deferred = c->deferred;
+      c->deferred = nullptr;
+      c->older.push_back(std::move(o));
+      c->slot = free_slot(c);
       c->tail_live = false;
-      c->slot ^= 1;
-      if (c->deferred) c->deferred_prev = true;
       // the buffer taken over may still be read by the copy of an earlier epoch
       TRY_CUDA(s, after_pending_copy(c), "reset");
     }
@@ -931,14 +980,14 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
   if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
   if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
   // a read of this epoch waits for the samples rendered so far, not these
-  if (c->deferred && !c->deferred_prev && (rc = flush_pipeline(c))) return rc;
+  if (c->deferred && (rc = flush_pipeline(c))) return rc;
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
   Engine& E = *c->eng;
   const unsigned long long npix = uint64_t(c->width) * uint64_t(c->height);
   const unsigned long long items = npix * uint64_t(frames);
-  // room for this epoch's samples and the previous epoch's last paths; the
-  // pool changes size only when empty
-  const uint32_t want = uint32_t(std::min<uint64_t>(c->wave_paths, 2 * items));
+  // room for this epoch's samples and the last paths of the epochs in flight;
+  // the pool changes size only when empty
+  const uint32_t want = uint32_t(std::min<uint64_t>(c->wave_paths, uint64_t(c->depth) * items));
   if (E.capacity() < want || E.capacity() > c->wave_paths) {
     if ((rc = flush_pipeline(c)) || (rc = E.ensure_pool(want))) return rc;
   }
@@ -954,32 +1003,36 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
     job.accum = reinterpret_cast<double*>(c->accum.p);
     if ((rc = E.set_job(c->slot, job, items))) return rc;
   }
-  const int prev = c->prev_live ? (c->slot ^ 1) : -1;
-  if ((rc = E.set_active(prev >= 0 ? std::vector<int>{prev, c->slot} : std::vector<int>{c->slot}))) return rc;
+  std::vector<int> act;
+  for (const auto& o : c->older) act.push_back(o.slot);
+  act.push_back(c->slot);
+  // with depth - 1 older epochs in flight the oldest is waited for
+  const int wait = int(c->older.size()) + 1 >= c->depth ? c->older.front().slot : -1;
+  if ((rc = E.set_active(act))) return rc;
   c->sample_count += uint64_t(frames);
   c->rays_primary += items;
   const uint64_t pool = E.capacity();
   const uint64_t per_path = uint64_t(std::max(c->params.max_bounces, 0)) + 1;
-  const unsigned long long max_iter = (items * per_path + pool - 1) / pool + 2 * per_path + 8;
+  const unsigned long long max_iter = (items * per_path + pool - 1) / pool + uint64_t(c->depth) * per_path + 8;
   TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
-  const bool read_prev = c->deferred && c->deferred_prev;
+  const bool read_oldest = wait >= 0 && c->older.front().deferred;
   unsigned long long it0 = 0, eager = 0;
-  rc = E.launch_pipelined(prev, max_iter, read_prev ? c->ev_between : nullptr, &it0, &eager);
-  if (!rc && read_prev) {
-    // the previous epoch is complete at ev_between: its image is copied
-    // while this epoch's iterations run
-    float* dst = c->deferred;
-    c->deferred = nullptr;
-    c->deferred_prev = false;
-    rc = issue_read(c, c->accum_prev.p, c->prev_sample_count, dst, c->ev_between);
+  rc = E.launch_pipelined(wait, max_iter, read_oldest ? c->ev_between : nullptr, &it0, &eager);
+  if (!rc && read_oldest) {
+    // the oldest epoch is complete at ev_between: its image is copied while
+    // this epoch's iterations run
+    auto& o = c->older.front();
+    float* dst = o.deferred;
+    o.deferred = nullptr;
+    rc = issue_read(c, o.sums->p, o.samples, dst, c->ev_between);
   }
   if (!rc) rc = s.cuda(cudaEventRecord(c->ev1, c->stream), "event");
   if (!rc) rc = s.cuda(cudaStreamSynchronize(c->stream), "render");
   if (rc) return rc;
   E.finish_pipelined(it0, eager);
-  if (prev >= 0 && !E.job_done(prev))
-    return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: previous frame not finished after %llu iterations", max_iter);
-  c->prev_live = false;
+  if (wait >= 0 && !E.job_done(wait))
+    return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: earlier frame not finished after %llu iterations", max_iter);
+  if ((rc = retire_finished(c, nullptr))) return rc;
   c->tail_live = !E.job_done(c->slot);
   float ms = 0;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -995,6 +1048,28 @@ int dspbr_set_pipelining(dspbr_ctx* c, int enable) {
   if (enable && !c->ev_between)
     TRY_CUDA(s, cudaEventCreateWithFlags(&c->ev_between, cudaEventDisableTiming), "event");
   c->pipelined = enable != 0;
+  return DSPBR_OK;
+}
+
+int dspbr_set_pipeline_depth(dspbr_ctx* c, int depth) {
+  if (!c || depth < 2 || depth > 3) return DSPBR_ERR_INVALID;
+  int rc = settle(c);
+  if (rc) return rc;
+  c->depth = depth;
+  return DSPBR_OK;
+}
+
+int dspbr_read_wait_ready(dspbr_ctx* c, int* in_flight) {
+  if (!c) return DSPBR_ERR_INVALID;
+  { int rc_ = settle_worker(c); if (rc_) return rc_; }
+  int n = c->deferred ? 1 : 0;
+  for (const auto& o : c->older) n += o.deferred ? 1 : 0;
+  if (in_flight) *in_flight = n;
+  if (!c->copy_pending) return DSPBR_OK;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  c->copy_pending = false;
+  TRY_CUDA(s, cudaEventSynchronize(c->ev_copied), "read accumulation");
   return DSPBR_OK;
 }
 
@@ -1130,7 +1205,7 @@ int dspbr_read_accum(dspbr_ctx* c, float* rgba, size_t num_floats) {
 int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
   if (!c || !rgba) return DSPBR_ERR_INVALID;
   { int rc_ = settle_worker(c); if (rc_) return rc_; }
-  if (c->pipelined && c->deferred) {  // one deferred read at a time
+  if (c->pipelined && c->deferred) {  // one deferred read per epoch
     int rc = flush_pipeline(c);
     if (rc) return rc;
   }
@@ -1144,15 +1219,14 @@ int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
   const bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
   cudaGetLastError();
   if (!pinned) return s.fail(DSPBR_ERR_INVALID, "read_accum_async: the buffer is not page-locked (dspbr_host_alloc)");
-  if (c->pipelined && (c->tail_live || c->prev_live)) {
-    if (!c->tail_live) {  // only the previous epoch is in flight: this one's sums are complete
+  if (c->pipelined && (c->tail_live || !c->older.empty())) {
+    if (!c->tail_live) {  // only earlier epochs are in flight: this one's sums are complete
       int rc = flush_pipeline(c);
       if (rc) return rc;
     } else {
       // this epoch's last paths are in the pool: the mean and copy follow
       // when they finish (in the next render call, or dspbr_read_wait)
       c->deferred = rgba;
-      c->deferred_prev = false;
       return DSPBR_OK;
     }
   }
@@ -1170,7 +1244,9 @@ int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
 
 int dspbr_read_wait(dspbr_ctx* c) {
   if (!c) return DSPBR_ERR_INVALID;
-  if (c->deferred) {
+  bool deferred = c->deferred != nullptr;
+  for (const auto& o : c->older) deferred = deferred || o.deferred;
+  if (deferred) {
     int rc = settle(c);  // finishes the epoch and enqueues the read
     if (rc) return rc;
   }
@@ -1389,7 +1465,9 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->bvh_build_ms = c->scene->bvh_build_ms;
     d->upload_ms = c->scene->upload_ms;
   }
-  d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->accum_prev.bytes() + c->mean.bytes();
+  d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->mean.bytes();
+  for (const auto& o : c->older) d->device_bytes += o.sums->bytes();
+  for (const auto& b : c->spare) d->device_bytes += b->bytes();
   d->last_render_ms = c->last_render_ms;
   d->nodes_closest = st[3];
   d->tris_closest = st[4];

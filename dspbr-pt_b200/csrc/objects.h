@@ -130,20 +130,27 @@ struct dspbr_ctx {
   bool pending = false;
   bool counting = false;
   // Pipelined frames (dspbr_set_pipelining).  The frames since the last reset
-  // (an accumulation epoch) render as job `slot`; a render call returns once
-  // every sample has started, so the epoch's last paths may still be in the
-  // pool (tail_live).  A reset then starts a new epoch in the other job slot
-  // and sum buffer while the old one (prev_live, sums in accum_prev) finishes
-  // during the next render call, which waits for it before it returns.
+  // (an accumulation epoch) render as job `slot` into `accum`; a render call
+  // returns once every sample has started, so the epoch's last paths may still
+  // be in the pool (tail_live).  A reset then moves the epoch to `older` (its
+  // sums, job slot and any deferred read) and starts a new one in a free job
+  // slot and sum buffer.  At most `depth` epochs are in flight: a render call
+  // that finds depth - 1 older epochs waits for the oldest before it returns.
   bool pipelined = false;
+  int depth = 2;
   int slot = 0;
-  bool tail_live = false, prev_live = false;
-  dspbr::DevBuf<double4> accum_prev;
-  uint64_t prev_sample_count = 0;
-  // a read_accum_async of an epoch with paths in the pool: its mean and copy
-  // are enqueued once that epoch has finished
+  bool tail_live = false;
+  struct Older {
+    std::unique_ptr<dspbr::DevBuf<double4>> sums;
+    uint64_t samples = 0;
+    int slot = 0;
+    float* deferred = nullptr;  // a read_accum_async requested while it was in flight
+  };
+  std::vector<Older> older;                                    // oldest first, each with paths in the pool
+  std::vector<std::unique_ptr<dspbr::DevBuf<double4>>> spare;  // sum buffers of finished epochs
+  // a read_accum_async of the current epoch while it has paths in the pool:
+  // its mean and copy are enqueued once the epoch has finished
   float* deferred = nullptr;
-  bool deferred_prev = false;  // the read is of the previous epoch
   cudaEvent_t ev_between = nullptr;
   dspbr::Status st() { return dspbr::Status{&err}; }
 };

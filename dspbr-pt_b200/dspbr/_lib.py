@@ -182,6 +182,8 @@ SIGNATURES = {
     "dspbr_read_accum_async": (C.c_int, [_V, _F, C.c_size_t]),
     "dspbr_read_wait": (C.c_int, [_V]),
     "dspbr_set_pipelining": (C.c_int, [_V, C.c_int]),
+    "dspbr_set_pipeline_depth": (C.c_int, [_V, C.c_int]),
+    "dspbr_read_wait_ready": (C.c_int, [_V, C.POINTER(C.c_int)]),
     "dspbr_host_alloc": (C.c_int, [_V, C.c_size_t, C.POINTER(C.c_void_p)]),
     "dspbr_read_display": (C.c_int, [_V, C.POINTER(Display), _F, C.c_size_t]),
     "dspbr_read_display_rgba8": (C.c_int, [_V, C.POINTER(Display), C.POINTER(C.c_uint8), C.c_size_t]),

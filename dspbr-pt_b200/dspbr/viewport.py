@@ -365,8 +365,10 @@ class PathtracingViewport:
             # not a reference setting: frames of consecutive accumulations
             # overlap on the device (dspbr_set_pipelining); start() then
             # returns once every sample has started, and readAccumulationAsync
-            # of frames still in flight completes in readWait() or the next start()
-            self._set_pipelining(bool(settings.pop("pipelinedFrames")))
+            # of frames still in flight completes in readWait() or the next start().
+            # True (or 2): two accumulations in flight; 3: three, for a caller
+            # that takes each image two steps later (readWaitReady)
+            self._set_pipelining(settings.pop("pipelinedFrames"))
         apply_settings(self.params, settings, self._display)
         # the renderer setters of exposure, enableGamma, debugMode and every
         # render setting reset the accumulation; toneMapping, enableFxaa,
@@ -389,9 +391,15 @@ class PathtracingViewport:
         self._apply_size()
         self._emit_diag()
 
-    def _set_pipelining(self, on: bool):
+    def _set_pipelining(self, v):
+        depth = 2 if v is True else int(v)
+        if v is not False and depth not in (0, 1, 2, 3):
+            raise ValueError(f"pipelinedFrames: {v!r} is not a bool, 2 or 3")
+        on = v is not False and depth >= 2
+        if on:
+            self.ctx.check(self.ctx.lib.dspbr_set_pipeline_depth(self.ctx.h, depth))
         self.ctx.check(self.ctx.lib.dspbr_set_pipelining(self.ctx.h, int(on)))
-        self._display["pipelinedFrames"] = on
+        self._display["pipelinedFrames"] = depth if on else False
 
     def _pixel_ratio(self) -> float:
         return float(self._display["interactionPixelRatio" if self.interactionActive else "pixelRatio"])
@@ -526,6 +534,14 @@ class PathtracingViewport:
     def readWait(self) -> None:
         """Waits for the copies of readAccumulationAsync."""
         self.ctx.check(self.ctx.lib.dspbr_read_wait(self.ctx.h))
+
+    def readWaitReady(self) -> int:
+        """Waits for the copies of readAccumulationAsync whose frames have
+        finished and returns how many reads still wait for their frames
+        (pipelined frames); renders nothing, unlike readWait()."""
+        n = C.c_int()
+        self.ctx.check(self.ctx.lib.dspbr_read_wait_ready(self.ctx.h, C.byref(n)))
+        return n.value
 
     def readDisplay(self, rgba8: bool = True) -> np.ndarray:
         """The presented frame: the running mean through the reference's

@@ -256,6 +256,17 @@ int dspbr_read_wait(dspbr_ctx* ctx);
  * dspbr_read_wait); dspbr_read_accum, the display reads and every other call
  * finish all paths first.  Images are the same as with it off. */
 int dspbr_set_pipelining(dspbr_ctx* ctx, int enable);
+/* Accumulations in flight with pipelined frames: 2 (default) or 3.  With 3 a
+ * render call that finds two earlier accumulations with paths in the pool
+ * waits only for the oldest: a caller that takes frame k's image while frame
+ * k+2 renders (a render-ahead queue of two frames, dspbr_read_wait_ready)
+ * keeps the pool fuller.  Images are the same. */
+int dspbr_set_pipeline_depth(dspbr_ctx* ctx, int depth);
+/* Waits for the device-to-host copies enqueued so far (reads of
+ * accumulations that have finished) and returns in *in_flight the number of
+ * reads still deferred because their accumulation has paths in the pool; it
+ * renders nothing, unlike dspbr_read_wait, which finishes them all. */
+int dspbr_read_wait_ready(dspbr_ctx* ctx, int* in_flight);
 /* Display epilogue (renderer.ts:666-700): the accumulation mean through
  * tonemap.frag (exposure, operator, gamma) and optionally fxaa.frag -- the
  * reference's "postprocess" buffer, at the render resolution -- as RGBA32F,

@@ -1,5 +1,6 @@
-"""Pipelined frames (dspbr_set_pipelining): the render of one accumulation
-overlaps the tail of the previous one on the device.  Every image must equal
+"""Pipelined frames (dspbr_set_pipelining, dspbr_set_pipeline_depth): the
+render of one accumulation overlaps the tail of the previous one (or two) on
+the device.  Every image must equal
 the image of the same calls without pipelining (FP64 pixel sums in another
 order: allclose 1e-6), whatever mix of camera changes, progressive renders,
 asynchronous and synchronous reads, display reads and resizes comes."""
@@ -35,11 +36,12 @@ def _cam(k):
 
 
 @pytest.mark.parametrize("pool", [0, 4000])
-def test_camera_per_frame_with_async_reads(scene, pool):
+@pytest.mark.parametrize("mode", [True, 3])
+def test_camera_per_frame_with_async_reads(scene, pool, mode):
     """The interactive loop: per frame setCamera, start(1), then the previous
     frame's readWait and this frame's readAccumulationAsync."""
     out = {}
-    for pipelined in (False, True):
+    for pipelined in (False, mode):
         v = _viewport(scene, pipelined, pool=pool)
         bufs = [v.allocReadbackBuffer() for _ in range(6)]
         for k in range(6):
@@ -53,11 +55,11 @@ def test_camera_per_frame_with_async_reads(scene, pool):
         d = v.diagnostics
         assert d["rays_primary"] == 6 * 96 * 64 and d["traversal_aborted"] == 0
         v.dispose()
-    for a, b in zip(out[False], out[True]):
+    for a, b in zip(out[False], out[mode]):
         assert np.isfinite(b).all() and b[..., 3].min() == 1.0
         np.testing.assert_allclose(b, a, **TOL)
     # the frames differ (different cameras): the reads did not repeat one image
-    assert not np.allclose(out[True][0], out[True][1])
+    assert not np.allclose(out[mode][0], out[mode][1])
 
 
 def test_progressive_and_mixed_calls(scene):
@@ -65,7 +67,7 @@ def test_progressive_and_mixed_calls(scene):
     an accumulation in flight followed by more frames of it, a synchronous
     read, a display read, a resize and a reset with nothing rendered."""
     res = {}
-    for pipelined in (False, True):
+    for pipelined in (False, True, 3):
         v = _viewport(scene, pipelined)
         got = []
         v.setCamera(_cam(0))
@@ -90,8 +92,9 @@ def test_progressive_and_mixed_calls(scene):
         assert v.diagnostics["sample_count"] == 1
         res[pipelined] = got
         v.dispose()
-    for a, b in zip(res[False], res[True]):
-        np.testing.assert_allclose(b, a, **TOL)
+    for mode in (True, 3):
+        for a, b in zip(res[False], res[mode]):
+            np.testing.assert_allclose(b, a, **TOL)
 
 
 def test_pipelined_frames_equal_single_frames_of_a_fresh_viewport(scene):
@@ -110,3 +113,33 @@ def test_pipelined_frames_equal_single_frames_of_a_fresh_viewport(scene):
         f.start(1)
         np.testing.assert_allclose(bufs[k], f.readAccumulation(), **TOL)
         f.dispose()
+
+
+@pytest.mark.parametrize("pool", [0, 4000])
+def test_render_ahead_queue_of_two_frames(scene, pool):
+    """Three accumulations in flight: per frame setCamera, start(1),
+    readWaitReady() (frame k-2's copy is complete) and this frame's
+    readAccumulationAsync; each image equals the frame rendered alone."""
+    ref = []
+    f = _viewport(scene, False, pool=pool)
+    for k in range(7):
+        f.setCamera(_cam(k))
+        f.start(1)
+        ref.append(f.readAccumulation())
+    f.dispose()
+    v = _viewport(scene, 3, pool=pool)
+    bufs = [v.allocReadbackBuffer() for _ in range(7)]
+    for k in range(7):
+        v.setCamera(_cam(k))
+        v.start(1)
+        in_flight = v.readWaitReady()
+        assert 0 <= in_flight <= 2
+        if k >= 2:  # frame k-2 has finished and its copy is on the host
+            np.testing.assert_allclose(bufs[k - 2], ref[k - 2], **TOL)
+        v.readAccumulationAsync(bufs[k])
+    v.readWait()
+    d = v.diagnostics
+    assert d["rays_primary"] == 7 * 96 * 64 and d["traversal_aborted"] == 0
+    v.dispose()
+    for k in range(7):
+        np.testing.assert_allclose(bufs[k], ref[k], **TOL)
