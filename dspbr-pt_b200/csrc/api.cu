@@ -75,6 +75,14 @@ static cudaError_t after_pending_copy(dspbr_ctx* c) {
   return c->copy_pending ? cudaStreamWaitEvent(c->stream, c->ev_copied, 0) : cudaSuccess;
 }
 
+// the context's stream waits for the copy stream's pending mean (the sums it
+// reads may be written next), not for the device-to-host copy behind it
+static cudaError_t after_pending_mean(dspbr_ctx* c) {
+  if (!c->mean_pending) return cudaSuccess;
+  c->mean_pending = false;
+  return cudaStreamWaitEvent(c->stream, c->ev_meaned, 0);
+}
+
 // Joins the render_async worker; returns its status.
 static int settle_worker(dspbr_ctx* c) {
   if (c->worker.joinable()) c->worker.join();
@@ -96,6 +104,8 @@ static int issue_read(dspbr_ctx* c, const double4* accum, uint64_t count, float*
   TRY_CUDA(s, cudaStreamWaitEvent(c->copy_stream, after, 0), "read accumulation");
   launch_mean(accum, inv, c->mean.p, int(npix), c->copy_stream);
   TRY_CUDA(s, cudaGetLastError(), "read accumulation");
+  TRY_CUDA(s, cudaEventRecord(c->ev_meaned, c->copy_stream), "event");
+  c->mean_pending = true;
   TRY_CUDA(s, cudaMemcpyAsync(dst, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->copy_stream), "read accumulation");
   TRY_CUDA(s, cudaEventRecord(c->ev_copied, c->copy_stream), "event");
   c->copy_pending = true;
@@ -175,7 +185,7 @@ static int flush_pipeline(dspbr_ctx* c) {
     if (rc) return rc;
     // the copy stream's mean reads these sums: later renders and resets,
     // which write them on the context's stream, wait for it
-    TRY_CUDA(s, after_pending_copy(c), "read accumulation");
+    TRY_CUDA(s, after_pending_mean(c), "read accumulation");
   }
   return DSPBR_OK;
 }
@@ -383,6 +393,7 @@ int dspbr_create(int device, dspbr_ctx** out) {
       s.cuda(cudaEventCreate(&c->ev0), "event") || s.cuda(cudaEventCreate(&c->ev1), "event") ||
       s.cuda(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "stream") ||
       s.cuda(cudaEventCreateWithFlags(&c->ev_mean, cudaEventDisableTiming), "event") ||
+      s.cuda(cudaEventCreateWithFlags(&c->ev_meaned, cudaEventDisableTiming), "event") ||
       s.cuda(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming), "event")) {
     dspbr_destroy(c);
     return DSPBR_ERR_CUDA;
@@ -405,6 +416,7 @@ int dspbr_destroy(dspbr_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_mean) cudaEventDestroy(c->ev_mean);
+  if (c->ev_meaned) cudaEventDestroy(c->ev_meaned);
   if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   if (c->ev_between) cudaEventDestroy(c->ev_between);
   c->eng.reset();
@@ -890,8 +902,9 @@ int dspbr_reset(dspbr_ctx* c) {
       c->older.push_back(std::move(o));
       c->slot = free_slot(c);
       c->tail_live = false;
-      // the buffer taken over may still be read by the copy of an earlier epoch
-      TRY_CUDA(s, after_pending_copy(c), "reset");
+      // the buffer taken over may still be read by the mean of an earlier
+      // epoch's read (the device-to-host copy behind it reads the mean buffer)
+      TRY_CUDA(s, after_pending_mean(c), "reset");
     }
   }
   c->sample_count = 0;

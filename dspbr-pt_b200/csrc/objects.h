@@ -124,6 +124,10 @@ struct dspbr_ctx {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_mean = nullptr, ev_copied = nullptr;
   bool copy_pending = false;
+  // a read's mean on the copy stream (issue_read) is done at ev_meaned: what
+  // next writes the sums it read waits for that, not for the whole copy
+  cudaEvent_t ev_meaned = nullptr;
+  bool mean_pending = false;
   uint64_t sample_count = 0;
   uint64_t rays_primary = 0;
   double last_render_ms = 0;
