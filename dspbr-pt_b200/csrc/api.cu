@@ -91,22 +91,35 @@ static int settle_worker(dspbr_ctx* c) {
   return rc;
 }
 
-// Mean and device-to-host copy of an epoch's sums on the copy stream, after
-// `after` (recorded on the context's stream) when given.
+// Mean and device-to-host copy of an epoch's sums, after `after` (recorded
+// on the context's stream) when given: the mean on the mean stream into the
+// next read buffer, the copy on the copy stream.
 static int issue_read(dspbr_ctx* c, const double4* accum, uint64_t count, float* dst, cudaEvent_t after) {
   Status s = c->st();
   const size_t npix = size_t(c->width) * c->height;
   const double inv = count ? 1.0 / double(count) : 0.0;
+  const int r = c->read_next;
+  c->read_next = (r + 1) % dspbr_ctx::kReadRing;
+  if (c->read_mean[r].n < npix) {
+    // the buffer is replaced: its last copy has to be done first
+    if (c->read_used[r]) TRY_CUDA(s, cudaEventSynchronize(c->ev_read_copied[r]), "read accumulation");
+    TRY_CUDA(s, c->read_mean[r].alloc(npix), "alloc readback");
+  }
   if (!after) {
     TRY_CUDA(s, cudaEventRecord(c->ev_mean, c->stream), "event");
     after = c->ev_mean;
   }
-  TRY_CUDA(s, cudaStreamWaitEvent(c->copy_stream, after, 0), "read accumulation");
-  launch_mean(accum, inv, c->mean.p, int(npix), c->copy_stream);
+  TRY_CUDA(s, cudaStreamWaitEvent(c->mean_stream, after, 0), "read accumulation");
+  if (c->read_used[r]) TRY_CUDA(s, cudaStreamWaitEvent(c->mean_stream, c->ev_read_copied[r], 0), "read accumulation");
+  launch_mean(accum, inv, c->read_mean[r].p, int(npix), c->mean_stream);
   TRY_CUDA(s, cudaGetLastError(), "read accumulation");
-  TRY_CUDA(s, cudaEventRecord(c->ev_meaned, c->copy_stream), "event");
+  TRY_CUDA(s, cudaEventRecord(c->ev_meaned, c->mean_stream), "event");
   c->mean_pending = true;
-  TRY_CUDA(s, cudaMemcpyAsync(dst, c->mean.p, npix * 16, cudaMemcpyDeviceToHost, c->copy_stream), "read accumulation");
+  TRY_CUDA(s, cudaStreamWaitEvent(c->copy_stream, c->ev_meaned, 0), "read accumulation");
+  TRY_CUDA(s, cudaMemcpyAsync(dst, c->read_mean[r].p, npix * 16, cudaMemcpyDeviceToHost, c->copy_stream),
+           "read accumulation");
+  TRY_CUDA(s, cudaEventRecord(c->ev_read_copied[r], c->copy_stream), "event");
+  c->read_used[r] = true;
   TRY_CUDA(s, cudaEventRecord(c->ev_copied, c->copy_stream), "event");
   c->copy_pending = true;
   return DSPBR_OK;
@@ -394,10 +407,16 @@ int dspbr_create(int device, dspbr_ctx** out) {
       s.cuda(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "stream") ||
       s.cuda(cudaEventCreateWithFlags(&c->ev_mean, cudaEventDisableTiming), "event") ||
       s.cuda(cudaEventCreateWithFlags(&c->ev_meaned, cudaEventDisableTiming), "event") ||
+      s.cuda(cudaStreamCreateWithFlags(&c->mean_stream, cudaStreamNonBlocking), "stream") ||
       s.cuda(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming), "event")) {
     dspbr_destroy(c);
     return DSPBR_ERR_CUDA;
   }
+  for (int r = 0; r < dspbr_ctx::kReadRing; ++r)
+    if (s.cuda(cudaEventCreateWithFlags(&c->ev_read_copied[r], cudaEventDisableTiming), "event")) {
+      dspbr_destroy(c);
+      return DSPBR_ERR_CUDA;
+    }
   c->eng.reset(new Engine(device, c->stream, &c->err));
   if (int rc = c->eng->init()) {
     dspbr_destroy(c);
@@ -417,6 +436,10 @@ int dspbr_destroy(dspbr_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->ev_mean) cudaEventDestroy(c->ev_mean);
   if (c->ev_meaned) cudaEventDestroy(c->ev_meaned);
+  if (c->mean_stream) cudaStreamSynchronize(c->mean_stream);
+  for (int r = 0; r < dspbr_ctx::kReadRing; ++r)
+    if (c->ev_read_copied[r]) cudaEventDestroy(c->ev_read_copied[r]);
+  if (c->mean_stream) cudaStreamDestroy(c->mean_stream);
   if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   if (c->ev_between) cudaEventDestroy(c->ev_between);
   c->eng.reset();
@@ -910,6 +933,7 @@ int dspbr_reset(dspbr_ctx* c) {
   c->sample_count = 0;
   if (c->accum.p) {
     TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+    TRY_CUDA(s, after_pending_mean(c), "reset");  // a read's mean may still read these sums
     TRY_CUDA(s, cudaMemsetAsync(c->accum.p, 0, size_t(c->width) * c->height * sizeof(double4), c->stream),
              "clear accumulation");
   }
@@ -1232,16 +1256,16 @@ int dspbr_read_accum_async(dspbr_ctx* c, float* rgba, size_t num_floats) {
   const bool pinned = cudaPointerGetAttributes(&attr, rgba) == cudaSuccess && attr.type == cudaMemoryTypeHost;
   cudaGetLastError();
   if (!pinned) return s.fail(DSPBR_ERR_INVALID, "read_accum_async: the buffer is not page-locked (dspbr_host_alloc)");
-  if (c->pipelined && (c->tail_live || !c->older.empty())) {
-    if (!c->tail_live) {  // only earlier epochs are in flight: this one's sums are complete
-      int rc = flush_pipeline(c);
-      if (rc) return rc;
-    } else {
-      // this epoch's last paths are in the pool: the mean and copy follow
-      // when they finish (in the next render call, or dspbr_read_wait)
+  if (c->pipelined) {
+    // this epoch's last paths are in the pool: the mean and copy follow when
+    // they finish (in a later render call, or dspbr_read_wait)
+    if (c->tail_live) {
       c->deferred = rgba;
       return DSPBR_OK;
     }
+    // its sums are complete: mean and copy on the copy stream, so that the
+    // context's stream (the next renders) never waits for a copy
+    return issue_read(c, c->accum.p, c->sample_count, rgba, nullptr);
   }
   double inv = c->sample_count ? 1.0 / double(c->sample_count) : 0.0;
   TRY_CUDA(s, after_pending_copy(c), "read accumulation");
@@ -1479,6 +1503,7 @@ int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
     d->upload_ms = c->scene->upload_ms;
   }
   d->device_bytes = c->eng->pool_bytes() + c->accum.bytes() + c->mean.bytes();
+  for (const auto& m : c->read_mean) d->device_bytes += m.bytes();
   for (const auto& o : c->older) d->device_bytes += o.sums->bytes();
   for (const auto& b : c->spare) d->device_bytes += b->bytes();
   d->last_render_ms = c->last_render_ms;

@@ -347,18 +347,22 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
       const bool started = total <= avail;  // the regen that just ran placed every remaining work item
       const unsigned long long left = ctl->iters_left;
       const int mode = ctl->mode;
-      bool stop;
+      bool stop, tail = false;
       if (mode == kLoopDrain) {
         stop = started && live < ctl->drain_below;
       } else if (mode == kLoopUntilDone) {
         const int w = ctl->wait_job;
         stop = w < 0 || w >= kMaxJobs || (sc.js[w].items_next >= sc.js[w].items_total && sc.js[w].live == 0u);
+        // every work item of every active job has started and few paths are
+        // left: the tail drain finishes them all (the iterations it replaces
+        // would each cost a path's latency, whatever they hold)
+        if (!stop && started && live < ctl->drain_below) stop = tail = true;
       } else {
         stop = started;
       }
       const bool go = left > 1 && !stop;
       ctl->iters_left = left ? left - 1 : 0;
-      if (mode != kLoopDrain) {  // whole pairs, no tail
+      if (mode != kLoopDrain && !tail) {  // whole pairs, no tail
         if (lh.first) cudaGraphSetConditional(lh.second, 1u);
         else cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
       } else {

@@ -191,11 +191,13 @@ void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, 
 // remain and either a work item has not started or at least drain_below paths
 // are alive; the commit that stops selects the tail of its parity (an IF node
 // each), which runs every remaining path to its end.
-// kLoopUntilDone / kLoopUntilStarted (pipelined frames): no tail; the loop
-// runs whole pairs (A always continues to B, so the next launch starts at
-// parity 0) until job wait_job has finished (every item started, no live
-// path), or until every work item of the active jobs has started; the paths
-// still alive stay in the pool for the next launch.
+// kLoopUntilDone / kLoopUntilStarted (pipelined frames): the loop runs whole
+// pairs (A always continues to B, so the next launch starts at parity 0) until
+// job wait_job has finished (every item started, no live path), or until every
+// work item of the active jobs has started; the paths still alive stay in the
+// pool for the next launch.  kLoopUntilDone ends in the tail instead, like
+// kLoopDrain, once every work item has started and fewer than drain_below
+// paths are alive: the pool is then empty.
 enum { kLoopDrain = 0, kLoopUntilDone = 1, kLoopUntilStarted = 2 };
 struct LoopCtl {
   unsigned long long iters_left;

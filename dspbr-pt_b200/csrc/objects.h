@@ -124,8 +124,17 @@ struct dspbr_ctx {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_mean = nullptr, ev_copied = nullptr;
   bool copy_pending = false;
-  // a read's mean on the copy stream (issue_read) is done at ev_meaned: what
-  // next writes the sums it read waits for that, not for the whole copy
+  // issue_read: the mean of an accumulation runs on mean_stream into one of
+  // kReadRing buffers in turn, its device-to-host copy on copy_stream; a mean
+  // waits only for its own inputs and for the copy that last used its buffer,
+  // never behind other copies.  ev_meaned: the latest such mean (what next
+  // writes the sums it read waits for that, not for the copy).
+  static constexpr int kReadRing = 3;
+  cudaStream_t mean_stream = nullptr;
+  dspbr::DevBuf<float4> read_mean[kReadRing];
+  cudaEvent_t ev_read_copied[kReadRing] = {};
+  bool read_used[kReadRing] = {};
+  int read_next = 0;
   cudaEvent_t ev_meaned = nullptr;
   bool mean_pending = false;
   uint64_t sample_count = 0;
