@@ -99,7 +99,7 @@ int Engine::init() {
 }
 
 size_t Engine::pool_bytes() const {
-  return st_.bytes() + hits_.bytes() + sh_.bytes() + q0_.bytes() * 6 + qh_.bytes();
+  return st_.bytes() + hits_.bytes() + sh_.bytes() + q0_.bytes() * 6 + qh_.bytes() + fmap_.bytes() + fblock_.bytes();
 }
 
 int Engine::ensure_pool(uint32_t cap) {
@@ -115,7 +115,9 @@ int Engine::ensure_pool(uint32_t cap) {
       (rc = s.cuda(sh_.alloc(cap), "paths")) || (rc = s.cuda(q0_.alloc(cap), "queues")) ||
       (rc = s.cuda(q1_.alloc(cap), "queues")) || (rc = s.cuda(qs0_.alloc(cap), "queues")) ||
       (rc = s.cuda(qs1_.alloc(cap), "queues")) || (rc = s.cuda(qh_.alloc(size_t(cap) * kNumClasses), "queues")) ||
-      (rc = s.cuda(qm_.alloc(cap), "queues")) || (rc = s.cuda(qfree_.alloc(cap), "queues")))
+      (rc = s.cuda(qm_.alloc(cap), "queues")) || (rc = s.cuda(qfree_.alloc(cap), "queues")) ||
+      (rc = s.cuda(fmap_.alloc((size_t(cap) + 31) / 32), "free map")) ||
+      (rc = s.cuda(fblock_.alloc(((size_t(cap) + 31) / 32 + kFreeMapBlock - 1) / kFreeMapBlock), "free map")))
     return rc;
   capacity_ = cap;
   cur_ = 0;
@@ -164,7 +166,8 @@ PathBuf Engine::paths() const {
   PathBuf b{};
   b.st = st_.p; b.hits = hits_.p; b.sh = sh_.p;
   b.q[0] = q0_.p; b.q[1] = q1_.p; b.qs[0] = qs0_.p; b.qs[1] = qs1_.p; b.qh = qh_.p; b.qm = qm_.p;
-  b.qfree = qfree_.p; b.free_head = cursors_.p; b.free_tail = cursors_.p + 1;
+  b.qfree = qfree_.p; b.fmap = fmap_.p; b.fblock = fblock_.p;
+  b.free_head = cursors_.p; b.free_tail = cursors_.p + 1;
   b.counts = counts_.p; b.stats = stats_.p;
   b.capacity = capacity_;
   return b;
@@ -267,12 +270,13 @@ int Engine::one_iteration(bool counting) {
   mark_end();
   mark_begin(2);
   launch_shade(sc, b, cur ^ 1, lc_, stream_);
+  launch_free_list(b, stream_);
   launch_regen(sc, b, cur ^ 1, stream_);
   launch_commit(sc, b, cur, stream_);
   mark_end();
   kind_launches[0] += 1;
   kind_launches[1] += 1;
-  kind_launches[2] += 3;
+  kind_launches[2] += 5;  // shade, free list (2), regen, commit
   cur_ ^= 1;
   return Status{err_}.cuda(cudaGetLastError(), "render launch");
 }
@@ -353,6 +357,7 @@ int Engine::capture_loop_graph() {
   auto iteration = [&](int cur, const LoopHandles& lh) {
     extend_and_connect(sc, b, cur);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
+    launch_free_list(b, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     launch_commit_loop(sc, b, cur, lh, loop_ctl_.p, stream_);
   };
@@ -441,7 +446,7 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
   const unsigned long long body = hs->iteration - it0 - 1 - eager;
   kind_launches[0] += body;
   kind_launches[1] += body + 1;
-  kind_launches[2] += 3 * body;
+  kind_launches[2] += 5 * body;
   kind_launches[3] += 3;
   cur_ = 0;  // the tail drained every path: both queues are empty
   if (job_done(slot)) return DSPBR_OK;
@@ -482,7 +487,7 @@ void Engine::finish_pipelined(unsigned long long it0, unsigned long long eager) 
   const unsigned long long body = h_status_->iteration - it0 - eager;
   kind_launches[0] += body;
   kind_launches[1] += body;
-  kind_launches[2] += 3 * body;
+  kind_launches[2] += 5 * body;
   kind_launches[3] += 2;
   cur_ = 0;
 }
@@ -499,6 +504,7 @@ int Engine::capture_graph() {
   for (int cur = 0; cur < 2; ++cur) {
     extend_and_connect(sc, b, cur);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
+    launch_free_list(b, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     launch_commit(sc, b, cur, stream_);
   }
@@ -529,7 +535,7 @@ int Engine::iterate(int n, bool counting, int* done) {
       TRY_CUDA(s, cudaGraphLaunch(graph_, stream_), "graph launch");
       kind_launches[0] += 2;
       kind_launches[1] += 2;
-      kind_launches[2] += 6;
+      kind_launches[2] += 10;
       k += 2;
     } else {
       int rc = one_iteration(counting);

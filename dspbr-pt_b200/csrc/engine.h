@@ -117,7 +117,7 @@ class Engine {
   DevBuf<PathState> st_;
   DevBuf<PathHit> hits_;
   DevBuf<PathShadow> sh_;
-  DevBuf<uint32_t> q0_, q1_, qs0_, qs1_, qh_, qm_, qfree_;
+  DevBuf<uint32_t> q0_, q1_, qs0_, qs1_, qh_, qm_, qfree_, fmap_, fblock_;
   // job table and counters
   DevBuf<Job> jobs_;
   DevBuf<JobState> js_;

@@ -76,20 +76,15 @@ DEV void finish_path(const Job& J, uint32_t pixel, float4 c) {
   atomicAdd(a + 3, double(c.w));
 }
 
-// Frees the slots of terminated paths: free-list append (ring buffer, 64-bit
-// cursors) and the live-path count of each job, one atomic per job per warp.
+// Frees the slots of terminated paths: their bits in the free map, the count
+// of freed slots and the live-path count of each job (one atomic per job per warp).
 DEV void free_slots(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot, uint32_t job) {
   unsigned m = __ballot_sync(0xffffffffu, pred);
   if (!m) return;
   int lane = threadIdx.x & 31;
   int leader = __ffs(m) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(b.free_tail, (unsigned long long)__popc(m));
-  uint32_t pos = 0;
-  if (lane == leader) pos = uint32_t(base % b.capacity);
-  pos = __shfl_sync(0xffffffffu, pos, leader) + __popc(m & ((1u << lane) - 1u));
-  while (pos >= b.capacity) pos -= b.capacity;
-  if (pred) b.qfree[pos] = slot;
+  if (lane == leader) atomicAdd(b.free_tail, (unsigned long long)__popc(m));
+  if (pred) atomicOr(b.fmap + (slot >> 5), 1u << (slot & 31u));
   unsigned peers = __match_any_sync(0xffffffffu, pred ? int(job) : -1);
   if (pred && lane == __ffs(peers) - 1) atomicSub(&sc.js[job].live, uint32_t(__popc(peers)));
 }
@@ -97,9 +92,9 @@ DEV void free_slots(const Sched& sc, const PathBuf& b, bool pred, uint32_t slot,
 // The same for persistent warps, batched: freed slots collect in a per-warp
 // shared-memory buffer and go to the free list with one atomic on its tail
 // per kFreeBuf slots; live-path decrements collect per job in a register.
-// Per batch of 32 paths, free_slots costs two atomics on two addresses that
-// every warp of the kernel updates; here a warp flushes a few times per
-// launch.  flush() must run before the warp exits.
+// Per batch of 32 paths, free_slots costs an atomic on a counter that every
+// warp of the kernel updates; here a warp flushes a few times per launch.
+// flush() must run before the warp exits.
 constexpr int kFreeBuf = 256;
 struct WarpFree {
   uint32_t* buf;  // this warp's kFreeBuf entries (shared memory)
@@ -115,15 +110,11 @@ struct WarpFree {
   DEV void flush_slots(const PathBuf& b) {
     if (!n) return;
     const int lane = threadIdx.x & 31;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(b.free_tail, (unsigned long long)n);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const uint32_t pos0 = uint32_t(base % b.capacity);
+    if (lane == 0) atomicAdd(b.free_tail, (unsigned long long)n);
     __syncwarp();
     for (uint32_t k = uint32_t(lane); k < n; k += 32u) {
-      uint32_t pos = pos0 + k;
-      if (pos >= b.capacity) pos -= b.capacity;
-      b.qfree[pos] = buf[k];
+      const uint32_t slot = buf[k];
+      atomicOr(b.fmap + (slot >> 5), 1u << (slot & 31u));
     }
     __syncwarp();
     n = 0;
@@ -201,12 +192,79 @@ DEV unsigned long long remaining(const Sched& sc, int a, int n, int& j) {
 __global__ void k_init_pool(PathBuf b) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < b.capacity; i += gridDim.x * blockDim.x)
     b.qfree[i] = i;
+  const uint32_t words = (b.capacity + 31u) / 32u;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+    const uint32_t left = b.capacity - w * 32u;  // every slot starts free
+    b.fmap[w] = left >= 32u ? 0xffffffffu : (1u << left) - 1u;
+  }
   if (blockIdx.x == 0 && threadIdx.x < kCntNum) {
     b.counts[threadIdx.x] = 0u;
     if (threadIdx.x == 0) {
       *b.free_head = 0ull;
       *b.free_tail = b.capacity;
     }
+  }
+}
+
+// ---- the free list: fmap -> qfree in ascending order ------------------------------------------
+DEV uint32_t block_sum_1024(uint32_t v, uint32_t* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) warp_sums[warp] = v;
+  __syncthreads();
+  uint32_t t = threadIdx.x < (blockDim.x >> 5) ? warp_sums[threadIdx.x] : 0u;
+  if (warp == 0)
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  __syncthreads();
+  return t;  // the total in thread 0
+}
+
+// free slots per block of kFreeMapBlock map words
+__global__ void __launch_bounds__(kFreeMapBlock) k_free_count(PathBuf b) {
+  __shared__ uint32_t warp_sums[32];
+  const uint32_t words = (b.capacity + 31u) / 32u;
+  const uint32_t w = blockIdx.x * kFreeMapBlock + threadIdx.x;
+  const uint32_t total = block_sum_1024(w < words ? uint32_t(__popc(b.fmap[w])) : 0u, warp_sums);
+  if (threadIdx.x == 0) b.fblock[blockIdx.x] = total;
+}
+
+// each block writes its words' free slots at its offset (the counts of the
+// blocks before it), in ascending slot order
+__global__ void __launch_bounds__(kFreeMapBlock) k_free_emit(PathBuf b) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t block_base;
+  const uint32_t words = (b.capacity + 31u) / 32u;
+  uint32_t before = 0;
+  for (uint32_t k = threadIdx.x; k < blockIdx.x; k += blockDim.x) before += b.fblock[k];
+  before = block_sum_1024(before, warp_sums);
+  if (threadIdx.x == 0) block_base = before;
+  __syncthreads();
+  const uint32_t w = blockIdx.x * kFreeMapBlock + threadIdx.x;
+  uint32_t bits = w < words ? b.fmap[w] : 0u;
+  // exclusive scan of the per-word counts over the block
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t c = uint32_t(__popc(bits));
+  uint32_t incl = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += n;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = lane < int(blockDim.x >> 5) ? warp_sums[lane] : 0u, ti = t;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t n = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += n;
+    }
+    warp_sums[lane] = ti - t;  // exclusive prefix of the warps
+  }
+  __syncthreads();
+  uint32_t pos = block_base + warp_sums[warp] + incl - c;
+  while (bits) {
+    const int k = __ffs(bits) - 1;
+    bits &= bits - 1u;
+    b.qfree[pos++] = w * 32u + uint32_t(k);
   }
 }
 
@@ -228,10 +286,18 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
   const unsigned long long head = *b.free_head;
   const unsigned long long nfree = *b.free_tail - head;
   const uint32_t avail = uint32_t(min(nfree, total));
-  const uint32_t head_pos = uint32_t(head % b.capacity);
   uint32_t* q = b.q[next] + b.counts[next];
   for (uint32_t base = blockIdx.x * blockDim.x; base < avail; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
+    {
+      // the slots taken leave the free map: one atomic per map word and warp
+      // (consecutive entries of the ascending list share words)
+      const bool take = i < avail;
+      const uint32_t s = take ? b.qfree[i] : 0u;
+      const unsigned peers = __match_any_sync(0xffffffffu, take ? int(s >> 5) : -1);
+      const uint32_t bits = __reduce_or_sync(peers, take ? 1u << (s & 31u) : 0u);
+      if (take && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAnd(b.fmap + (s >> 5), ~bits);
+    }
     if (i < avail) {
       uint32_t slot = 0;
       int lo = 0, hi = n - 1;  // last active job whose range starts at or before i
@@ -243,9 +309,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
       const int jj = act[lo];
       const WaveParams& p = sc.jobs[jj].p;
       unsigned long long item = sc.js[jj].items_next + (i - pre[lo]);
-      uint32_t pos = head_pos + i;  // i < capacity
-      if (pos >= b.capacity) pos -= b.capacity;
-      slot = b.qfree[pos];
+      slot = b.qfree[i];
       uint32_t pixel, frame;
       if (item <= 0xffffffffull) {
         pixel = uint32_t(item) % uint32_t(p.npix);
@@ -1039,6 +1103,12 @@ void init_launch_sizes(LaunchCfg& lc) {
 
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
   k_init_pool<<<grid_for(b.capacity, 256, 148 * 8), 256, 0, st>>>(b);
+}
+void launch_free_list(const PathBuf& b, cudaStream_t st) {
+  const uint32_t words = (b.capacity + 31u) / 32u;
+  const int blocks = int((words + kFreeMapBlock - 1) / kFreeMapBlock);
+  k_free_count<<<blocks, kFreeMapBlock, 0, st>>>(b);
+  k_free_emit<<<blocks, kFreeMapBlock, 0, st>>>(b);
 }
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st) {
   k_regen<<<grid_for(b.capacity, kMaxJobs, 148 * 8), kMaxJobs, 0, st>>>(sc, b, next);

@@ -124,9 +124,15 @@ struct PathBuf {
   uint32_t* qs[2];  // shadow queues
   uint32_t* qh;     // hit queues: class k at qh + k * capacity
   uint32_t* qm;     // miss queue
-  uint32_t* qfree;  // free slots: ring buffer [free_head, free_tail) mod capacity
-  unsigned long long* free_head;
-  unsigned long long* free_tail;
+  // Free slots.  fmap holds one bit per slot, set while it is free; before
+  // each regen k_free_count / k_free_emit write the free slots into qfree in
+  // ascending order, and the regen takes the lowest ones, so that new paths
+  // sit close together in the path arrays however the old ones ended.
+  uint32_t* qfree;
+  uint32_t* fmap;    // (capacity + 31) / 32 words
+  uint32_t* fblock;  // free slots per kFreeMapBlock words of fmap
+  unsigned long long* free_head;  // slots taken by regens so far
+  unsigned long long* free_tail;  // slots freed so far (free_tail - free_head = bits set in fmap)
   uint32_t* counts; // kCnt*
   // [0] closest-hit rays, [1] shadow rays, [2] aborted traversals,
   // [3]/[4] nodes visited / triangles tested by closest-hit rays, [5]/[6] by shadow rays
@@ -179,6 +185,9 @@ struct LaunchLimits {
   int sms, trace_per_sm, connect_per_sm, shade_per_sm[2];
 };
 LaunchLimits launch_limits();
+constexpr int kFreeMapBlock = 1024;  // fmap words per block of the free-list kernels
+// the free slots in ascending order (qfree), from fmap: call right before launch_regen
+void launch_free_list(const PathBuf& b, cudaStream_t st);
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
