@@ -873,7 +873,7 @@ int dspbr_get_params(const dspbr_ctx* c, dspbr_params* p) {
 int dspbr_set_wave_paths(dspbr_ctx* c, uint32_t paths) {
   if (!c) return DSPBR_ERR_INVALID;
   { int rc_ = settle(c); if (rc_) return rc_; }
-  c->wave_paths = paths ? paths : (1u << 23);
+  c->wave_paths = paths ? paths : (1u << 24);
   return DSPBR_OK;
 }
 

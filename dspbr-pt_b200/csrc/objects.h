@@ -100,9 +100,9 @@ struct dspbr_ctx {
   int width = 0, height = 0;
   dspbr_scene* scene = nullptr;
   dspbr_ibl* ibl = nullptr;
-  // paths per wave: of 2^20..2^24 the large workload's frames per second
-  // rise up to 2^23 and flatten after (2^21: -9%)
-  uint32_t wave_paths = 1u << 23;
+  // paths per wave: of 2^22..2^24 the large workload's frames per second over
+  // long calls rise with the pool (2^22: -5%, 2^23: -2% against 2^24; ~4.4 GB)
+  uint32_t wave_paths = 1u << 24;
   // for scenes created without a BVH: the binned SAH on the device, which
   // builds the host builder's tree (47-132 ms against ~430 ms on the host for
   // 1.15M triangles)

@@ -689,7 +689,7 @@ int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, 
     }
     return DSPBR_OK;
   };
-  for (uint32_t pool : {1u << 20, 1u << 21, 1u << 22, 1u << 23})
+  for (uint32_t pool : {1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24})
     if (!rc && pool != best_pool) rc = consider(pool, best);
   // then the grids of the persistent kernels: resident blocks per SM from the
   // occupancy limit down (fewer blocks: more L1 per block, less contention on

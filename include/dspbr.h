@@ -321,7 +321,7 @@ int dspbr_get_device_info(dspbr_ctx* ctx, dspbr_device_info* info);
  * per frame and has no iterations to report (renderer.ts:512-565). */
 int dspbr_get_timeline(dspbr_ctx* ctx, uint32_t max_entries, uint64_t* iteration, uint64_t* t_ns, uint32_t* live,
                        uint32_t* count);
-/* paths per wave (0 = default 2^23); the wave covers min(frames, paths/pixels)
+/* paths per wave (0 = default 2^24); the wave covers min(frames, paths/pixels)
  * samples of every pixel.  Set by the autotuner. */
 int dspbr_set_wave_paths(dspbr_ctx* ctx, uint32_t paths);
 /* live paths below which a render call, once every sample has started,

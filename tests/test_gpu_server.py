@@ -139,7 +139,7 @@ def test_autotune_then_serve(world, tmp_path):
     cache = str(tmp_path / "autotune.json")
     st = srv.autotune(samples, seconds=8.0, cache=cache)
     assert st["autotune_source"] == "tuned"
-    assert st["path_pool"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+    assert st["path_pool"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24)
     assert st["trace_threads"] == 128 and st["shade_threads"] == 128
     sms = 148
     for k in ("trace_blocks", "connect_blocks", "shade_blocks"):
