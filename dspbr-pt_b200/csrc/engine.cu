@@ -117,7 +117,7 @@ int Engine::ensure_pool(uint32_t cap) {
       (rc = s.cuda(qs1_.alloc(cap), "queues")) || (rc = s.cuda(qh_.alloc(size_t(cap) * kNumClasses), "queues")) ||
       (rc = s.cuda(qm_.alloc(cap), "queues")) || (rc = s.cuda(qfree_.alloc(cap), "queues")) ||
       (rc = s.cuda(fmap_.alloc((size_t(cap) + 31) / 32), "free map")) ||
-      (rc = s.cuda(fblock_.alloc(((size_t(cap) + 31) / 32 + kFreeMapBlock - 1) / kFreeMapBlock), "free map")))
+      (rc = s.cuda(fblock_.alloc(((size_t(cap) + 31) / 32 + kFreeMapBlock - 1) / kFreeMapBlock + 1), "free map")))
     return rc;
   capacity_ = cap;
   cur_ = 0;
@@ -270,7 +270,7 @@ int Engine::one_iteration(bool counting) {
   mark_end();
   mark_begin(2);
   launch_shade(sc, b, cur ^ 1, lc_, stream_);
-  launch_free_list(b, stream_);
+  launch_free_list(sc, b, stream_);
   launch_regen(sc, b, cur ^ 1, stream_);
   launch_commit(sc, b, cur, stream_);
   mark_end();
@@ -357,7 +357,7 @@ int Engine::capture_loop_graph() {
   auto iteration = [&](int cur, const LoopHandles& lh) {
     extend_and_connect(sc, b, cur);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
-    launch_free_list(b, stream_);
+    launch_free_list(sc, b, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     launch_commit_loop(sc, b, cur, lh, loop_ctl_.p, stream_);
   };
@@ -504,7 +504,7 @@ int Engine::capture_graph() {
   for (int cur = 0; cur < 2; ++cur) {
     extend_and_connect(sc, b, cur);
     launch_shade(sc, b, cur ^ 1, lc_, stream_);
-    launch_free_list(b, stream_);
+    launch_free_list(sc, b, stream_);
     launch_regen(sc, b, cur ^ 1, stream_);
     launch_commit(sc, b, cur, stream_);
   }

@@ -219,29 +219,48 @@ DEV uint32_t block_sum_1024(uint32_t v, uint32_t* warp_sums) {
   return t;  // the total in thread 0
 }
 
-// free slots per block of kFreeMapBlock map words
-__global__ void __launch_bounds__(kFreeMapBlock) k_free_count(PathBuf b) {
+// Free slots per block of kFreeMapBlock map words, and (block 0) how many
+// the regen will take: min(free slots, work items the active jobs have left),
+// in fblock[nblocks].
+__global__ void __launch_bounds__(kFreeMapBlock) k_free_count(Sched sc, PathBuf b) {
   __shared__ uint32_t warp_sums[32];
+  __shared__ unsigned long long scan[kMaxJobs];
   const uint32_t words = (b.capacity + 31u) / 32u;
   const uint32_t w = blockIdx.x * kFreeMapBlock + threadIdx.x;
   const uint32_t total = block_sum_1024(w < words ? uint32_t(__popc(b.fmap[w])) : 0u, warp_sums);
   if (threadIdx.x == 0) b.fblock[blockIdx.x] = total;
+  if (blockIdx.x == 0) {
+    const int n = min(*sc.nactive, kMaxJobs);
+    int j;
+    unsigned long long rem = threadIdx.x < kMaxJobs ? remaining(sc, threadIdx.x, n, j) : 0ull;
+    if (threadIdx.x < kMaxJobs) scan[threadIdx.x] = rem;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long sum = 0;
+      for (int k = 0; k < n; ++k) sum += scan[k];
+      const unsigned long long nfree = *b.free_tail - *b.free_head;
+      b.fblock[gridDim.x] = uint32_t(min(sum, nfree));
+    }
+  }
 }
 
-// each block writes its words' free slots at its offset (the counts of the
-// blocks before it), in ascending slot order
+// The first `need` free slots in ascending order: each block starts at the
+// count of the blocks before it; a warp writes its 32 words' slots
+// cooperatively (lane k of a round takes the warp's k-th free slot), so that
+// consecutive lanes store consecutive entries.
 __global__ void __launch_bounds__(kFreeMapBlock) k_free_emit(PathBuf b) {
   __shared__ uint32_t warp_sums[32];
   __shared__ uint32_t block_base;
   const uint32_t words = (b.capacity + 31u) / 32u;
+  const uint32_t need = b.fblock[gridDim.x];
   uint32_t before = 0;
   for (uint32_t k = threadIdx.x; k < blockIdx.x; k += blockDim.x) before += b.fblock[k];
   before = block_sum_1024(before, warp_sums);
   if (threadIdx.x == 0) block_base = before;
   __syncthreads();
+  if (block_base >= need) return;  // every slot the regen takes lies before this block
   const uint32_t w = blockIdx.x * kFreeMapBlock + threadIdx.x;
-  uint32_t bits = w < words ? b.fmap[w] : 0u;
-  // exclusive scan of the per-word counts over the block
+  const uint32_t bits = w < words ? b.fmap[w] : 0u;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t c = uint32_t(__popc(bits));
   uint32_t incl = c;
@@ -249,6 +268,7 @@ __global__ void __launch_bounds__(kFreeMapBlock) k_free_emit(PathBuf b) {
     const uint32_t n = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += n;
   }
+  const uint32_t warp_total = __shfl_sync(0xffffffffu, incl, 31);
   if (lane == 31) warp_sums[warp] = incl;
   __syncthreads();
   if (warp == 0) {
@@ -260,11 +280,24 @@ __global__ void __launch_bounds__(kFreeMapBlock) k_free_emit(PathBuf b) {
     warp_sums[lane] = ti - t;  // exclusive prefix of the warps
   }
   __syncthreads();
-  uint32_t pos = block_base + warp_sums[warp] + incl - c;
-  while (bits) {
-    const int k = __ffs(bits) - 1;
-    bits &= bits - 1u;
-    b.qfree[pos++] = w * 32u + uint32_t(k);
+  const uint32_t pos0 = block_base + warp_sums[warp];
+  const uint32_t word0 = blockIdx.x * kFreeMapBlock + uint32_t(warp) * 32u;
+  for (uint32_t k0 = 0; k0 < warp_total && pos0 + k0 < need; k0 += 32u) {
+    const uint32_t k = k0 + uint32_t(lane);
+    // the lane j whose word holds the warp's k-th free slot: the first with incl > k
+    int lo = 0, hi = 31;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      const uint32_t v = __shfl_sync(0xffffffffu, incl, mid);
+      if (v > k) hi = mid;
+      else lo = mid + 1;
+    }
+    const uint32_t jb = __shfl_sync(0xffffffffu, bits, lo);
+    const uint32_t jc = __shfl_sync(0xffffffffu, c, lo), ji = __shfl_sync(0xffffffffu, incl, lo);
+    if (k < warp_total && pos0 + k < need) {
+      const uint32_t bit = __fns(jb, 0u, int(k - (ji - jc)) + 1);
+      b.qfree[pos0 + k] = (word0 + uint32_t(lo)) * 32u + bit;
+    }
   }
 }
 
@@ -1104,10 +1137,10 @@ void init_launch_sizes(LaunchCfg& lc) {
 void launch_init_pool(const PathBuf& b, cudaStream_t st) {
   k_init_pool<<<grid_for(b.capacity, 256, 148 * 8), 256, 0, st>>>(b);
 }
-void launch_free_list(const PathBuf& b, cudaStream_t st) {
+void launch_free_list(const Sched& sc, const PathBuf& b, cudaStream_t st) {
   const uint32_t words = (b.capacity + 31u) / 32u;
   const int blocks = int((words + kFreeMapBlock - 1) / kFreeMapBlock);
-  k_free_count<<<blocks, kFreeMapBlock, 0, st>>>(b);
+  k_free_count<<<blocks, kFreeMapBlock, 0, st>>>(sc, b);
   k_free_emit<<<blocks, kFreeMapBlock, 0, st>>>(b);
 }
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st) {

@@ -130,7 +130,7 @@ struct PathBuf {
   // sit close together in the path arrays however the old ones ended.
   uint32_t* qfree;
   uint32_t* fmap;    // (capacity + 31) / 32 words
-  uint32_t* fblock;  // free slots per kFreeMapBlock words of fmap
+  uint32_t* fblock;  // free slots per kFreeMapBlock words of fmap; last entry: the slots the regen takes
   unsigned long long* free_head;  // slots taken by regens so far
   unsigned long long* free_tail;  // slots freed so far (free_tail - free_head = bits set in fmap)
   uint32_t* counts; // kCnt*
@@ -186,8 +186,9 @@ struct LaunchLimits {
 };
 LaunchLimits launch_limits();
 constexpr int kFreeMapBlock = 1024;  // fmap words per block of the free-list kernels
-// the free slots in ascending order (qfree), from fmap: call right before launch_regen
-void launch_free_list(const PathBuf& b, cudaStream_t st);
+// the free slots the next regen takes, in ascending order (qfree), from fmap:
+// call right before launch_regen
+void launch_free_list(const Sched& sc, const PathBuf& b, cudaStream_t st);
 void launch_regen(const Sched& sc, const PathBuf& b, int next, cudaStream_t st);
 void launch_extend(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
 void launch_connect(const Sched& sc, const PathBuf& b, int cur, bool count, const LaunchCfg& lc, cudaStream_t st);
