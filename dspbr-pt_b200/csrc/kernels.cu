@@ -302,6 +302,32 @@ __global__ void __launch_bounds__(kFreeMapBlock) k_free_emit(PathBuf b) {
 }
 
 // ---- regen: new samples in free slots (renderer.frag:146-150) ----------------------------
+// The k-th pixel of a frame in the order its samples start: 8 x 4 tiles (the
+// 32 consecutive work items a warp takes), tile rows top to bottom; then the
+// columns right of the last whole tile of each band of 4 rows, and the rows
+// below the last whole band, in row order.  A bijection of [0, width*height):
+// only the order changes, not a pixel's index, random stream or sums; the rays
+// of a warp start from a compact patch instead of a 32 x 1 strip.
+DEV void tile_pixel(uint32_t k, uint32_t w, uint32_t h, int& px, int& py) {
+  const uint32_t w8 = w & ~7u, h4 = h & ~3u;
+  if (k < h4 * w) {
+    const uint32_t band = k / (4u * w), r = k - band * 4u * w;
+    if (r < 4u * w8) {
+      const uint32_t t = r >> 5, j = r & 31u;
+      px = int(t * 8u + (j & 7u));
+      py = int(band * 4u + (j >> 3));
+    } else {
+      const uint32_t r2 = r - 4u * w8, wr = w - w8;
+      px = int(w8 + r2 % wr);
+      py = int(band * 4u + r2 / wr);
+    }
+  } else {
+    const uint32_t r = k - h4 * w;
+    px = int(r % w);
+    py = int(h4 + r / w);
+  }
+}
+
 // Free slot i (in free-list order) takes the i-th unstarted work item of the
 // active jobs in priority order and entry base + i of q[next], where base is
 // the queue's length after this iteration's shade (no atomic: k_commit adds
@@ -343,15 +369,17 @@ __global__ void __launch_bounds__(kMaxJobs) k_regen(Sched sc, PathBuf b, int nex
       const WaveParams& p = sc.jobs[jj].p;
       unsigned long long item = sc.js[jj].items_next + (i - pre[lo]);
       slot = b.qfree[i];
-      uint32_t pixel, frame;
+      uint32_t k, frame;
       if (item <= 0xffffffffull) {
-        pixel = uint32_t(item) % uint32_t(p.npix);
+        k = uint32_t(item) % uint32_t(p.npix);
         frame = p.frame_base + uint32_t(item) / uint32_t(p.npix);
       } else {
-        pixel = uint32_t(item % uint64_t(p.npix));
+        k = uint32_t(item % uint64_t(p.npix));
         frame = p.frame_base + uint32_t(item / uint64_t(p.npix));
       }
-      int px = int(pixel % uint32_t(p.cam.width)), py = int(pixel / uint32_t(p.cam.width));
+      int px, py;
+      tile_pixel(k, uint32_t(p.cam.width), uint32_t(p.cam.height), px, py);
+      const uint32_t pixel = uint32_t(py) * uint32_t(p.cam.width) + uint32_t(px);
       Rng r;
       if (p.rng_pcg) {
         uint64_t stream = uint64_t(frame) * uint64_t(p.npix) + pixel;
