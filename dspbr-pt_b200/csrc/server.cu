@@ -613,6 +613,9 @@ int dspbr_server_set_launch(dspbr_server* s, const dspbr_launch* l) {
   return st.cuda(cudaStreamSynchronize(s->stream), "set_launch");
 }
 
+// the gain a tuning candidate needs over the best so far
+constexpr double kTuneMargin = 1.02;
+
 int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, double seconds) {
   if (!s || !samples || n <= 0 || n > kMaxJobs) return DSPBR_ERR_INVALID;
   Status st = s->st();
@@ -682,7 +685,11 @@ int dspbr_server_autotune(dspbr_server* s, const dspbr_request* samples, int n, 
     double sc = 0;
     int r = measure(pool, lc, &sc);
     if (r) return r;
-    if (sc > best_score) {
+    // a candidate replaces the best only by a clear margin: one short
+    // measurement each, so the largest of many scores is partly noise (a
+    // sweep without the margin once settled on 2 shading blocks per SM, and
+    // the batched mix then ran 16% below the occupancy limits' rate)
+    if (sc > kTuneMargin * best_score) {
       best_score = sc;
       best_pool = pool;
       best = lc;
