@@ -814,29 +814,36 @@ def run_gpu_arm(args):
     # ---- end to end through the public API: per step camera upload (H2D),
     #      one frame, read back of the accumulation buffer (D2H) ----
     cam = PathtracingCamera(sc.camera.matrix_world, sc.camera.fov, sc.camera.near)
-    # the caller's frame buffers, page-locked, reused: two, so that step k's
-    # copy runs while step k+1 renders
-    e2e_steps = max(1, min(args.steps, 10))
-    # one page-locked buffer per step: a step's copy runs while later steps render
-    bufs = [v.allocReadbackBuffer() for _ in range(max(3, e2e_steps))]
+    # the render-ahead loop (the headline) runs every step of the bench; the
+    # other forms, measured beside it, 10 steps each
+    e2e_steps = max(1, args.steps)
+    part_steps = max(1, min(args.steps, 10))
+    AHEAD = 16  # accumulations in flight (viewport setting pipelinedFrames)
+    # the caller's page-locked frame buffers, reused in turn: step k's image
+    # is copied while later steps render, and its buffer is taken again
+    # AHEAD + 4 steps later, after readWaitReady() has seen the copy done
+    ring = AHEAD + 4
+    bufs = [v.allocReadbackBuffer() for _ in range(ring)]
     img = bufs[0]
 
-    def e2e_run(pipelined, ahead=False):
+    def e2e_run(pipelined, ahead=False, steps=part_steps):
         v.resetAccumulation()
         d3 = v.diagnostics
         parts = np.zeros(3)
         barrier(dist)
         t0 = time.perf_counter()
-        for k in range(e2e_steps):
+        for k in range(steps):
             ta = time.perf_counter()
             v.setCamera(cam)
             tb = time.perf_counter()
             v.start(1)
             tc = time.perf_counter()
             if ahead:
-                # enqueued: the copy starts when the frame's last paths have
-                # finished (two render calls later) and runs beside the renders
-                v.readAccumulationAsync(out=bufs[k])
+                # the copies of the frames that have finished are on the
+                # host; this frame's copy is enqueued and starts when its
+                # last paths have finished, during the next renders
+                v.readWaitReady()
+                v.readAccumulationAsync(out=bufs[k % ring])
             elif pipelined:
                 v.readWait()  # step k-1's image is on the host
                 v.readAccumulationAsync(out=bufs[k % 2])
@@ -850,7 +857,7 @@ def run_gpu_arm(args):
         rays = (d4["rays_primary"] + d4["rays_extension"] + d4["rays_shadow"]) - \
                (d3["rays_primary"] + d3["rays_extension"] + d3["rays_shadow"])
         value = reduce_sum(dist, float(rays)) / reduce_max(dist, t1 - t0) / 1e6
-        return value, parts / e2e_steps
+        return value, parts / steps
 
     e2e_run(True)  # untimed: the second buffer's first use
     e2e_serial, parts_serial = e2e_run(False)
@@ -860,27 +867,36 @@ def run_gpu_arm(args):
     v.setSettings({"pipelinedFrames": True})
     e2e_run(True)  # untimed: the second sum buffer's first use
     e2e_two, parts_two = e2e_run(True)
-    # three accumulations in flight: a frame's last paths share the pool with
-    # the next two frames' first ones; every image is copied to the host
-    # without a per-step wait
     v.setSettings({"pipelinedFrames": 3})
     e2e_run(True, ahead=True)  # untimed: the third sum buffer's first use
-    e2e_value, parts = e2e_run(True, ahead=True)
+    e2e_three, parts_three = e2e_run(True, ahead=True)
+    # the headline: AHEAD accumulations in flight; each render call runs one
+    # iteration over the new frame's camera rays and the earlier frames' last
+    # paths, and returns while it runs
+    v.setSettings({"pipelinedFrames": AHEAD})
+    e2e_run(True, ahead=True, steps=2 * AHEAD)  # untimed: every sum buffer's first use
+    e2e_value, parts = e2e_run(True, ahead=True, steps=e2e_steps)
     v.setSettings({"pipelinedFrames": False})
     e2e_parts = {"set_camera_ms": 1e3 * parts[0], "render_1_frame_ms": 1e3 * parts[1],
-                 "enqueue_read_ms": 1e3 * parts[2],
-                 "frames": "pipelined, three accumulations in flight (viewport setting pipelinedFrames: 3): a "
-                           "step's render returns once its samples have started and the frame two steps "
-                           "earlier has finished; a frame's last paths finish during the next two renders",
-                 "readback": "every step enqueues the device-to-host copy of its image into its own page-locked "
-                             "buffer; the copy starts when the frame's paths have finished and runs beside later "
-                             "renders; the host waits once, for every image, inside the timed region",
-                 "frames_two_in_flight": {"value": e2e_two, "render_1_frame_ms": 1e3 * parts_two[1],
+                 "read_wait_ready_and_enqueue_ms": 1e3 * parts[2],
+                 "frames": f"pipelined, {AHEAD} accumulations in flight (viewport setting pipelinedFrames: "
+                           f"{AHEAD}): a step's render enqueues one render-loop launch that runs until its "
+                           "samples have started and returns without waiting for it; the next step's render "
+                           f"waits for it, and for the frame that started {AHEAD - 1} steps earlier",
+                 "readback": f"every step enqueues the device-to-host copy of its image into one of {ring} "
+                             "page-locked buffers taken in turn; the copy starts when the frame's paths have "
+                             "finished and runs beside later renders; each step first waits for the copies "
+                             "of the frames that have finished (readWaitReady), the last step for every image",
+                 "frames_three_in_flight": {"value": e2e_three, "steps": part_steps,
+                                            "render_1_frame_ms": 1e3 * parts_three[1]},
+                 "frames_two_in_flight": {"value": e2e_two, "steps": part_steps,
+                                          "render_1_frame_ms": 1e3 * parts_two[1],
                                           "read_wait_and_enqueue_ms": 1e3 * parts_two[2],
                                           "readback": "step k waits for step k-1's image"},
-                 "frames_not_pipelined": {"value": e2e_copy, "render_1_frame_ms": 1e3 * parts_copy[1],
+                 "frames_not_pipelined": {"value": e2e_copy, "steps": part_steps,
+                                          "render_1_frame_ms": 1e3 * parts_copy[1],
                                           "read_wait_and_enqueue_ms": 1e3 * parts_copy[2]},
-                 "serial": {"value": e2e_serial, "render_1_frame_ms": 1e3 * parts_serial[1],
+                 "serial": {"value": e2e_serial, "steps": part_steps, "render_1_frame_ms": 1e3 * parts_serial[1],
                             "read_accumulation_ms": 1e3 * parts_serial[2]}}
     # the iterations of one more single-frame call (untimed): device clock at
     # the end of each iteration from the first one's end, and the paths left
@@ -891,7 +907,7 @@ def run_gpu_arm(args):
     tl = tl[tl[:, 0] > (last[-1, 0] if len(last) else -1)]
     if len(tl):
         e2e_parts["one_frame_iterations"] = [[round(float(r[1] - tl[0, 1]), 4), int(r[2])] for r in tl]
-    e2e_parts["server_stream"] = server_stream(v, sc, e2e_steps, dist)
+    e2e_parts["server_stream"] = server_stream(v, sc, part_steps, dist)
     cs = clocks.summary()
     paths = path_statistics(v, d0, d1)
     v.dispose()

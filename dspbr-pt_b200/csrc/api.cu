@@ -168,10 +168,35 @@ static int retire_finished(dspbr_ctx* c, cudaEvent_t after) {
   return DSPBR_OK;
 }
 
+// Waits for the loop launches of the last pipelined render call and takes
+// over its results: the parity the pool's queues are at, the epochs that
+// finished (their deferred reads enqueued, their sums spare), whether the
+// call's epoch still has paths in the pool, and the call's device time.
+static int complete_call(dspbr_ctx* c) {
+  if (!c->call_inflight) return DSPBR_OK;
+  c->call_inflight = false;
+  Status s = c->st();
+  TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
+  TRY_CUDA(s, cudaStreamSynchronize(c->stream), "render");
+  Engine& E = *c->eng;
+  E.finish_pipelined(c->call_it0, c->call_loops);
+  if (c->call_wait >= 0 && !E.job_done(c->call_wait))
+    return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: earlier frame not finished by the render loop");
+  int rc = retire_finished(c, nullptr);
+  if (rc) return rc;
+  // a reset since the call has moved its epoch to the older ones
+  if (c->slot == c->call_slot && c->tail_live) c->tail_live = !E.job_done(c->slot);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_render_ms = ms;
+  return DSPBR_OK;
+}
+
 // Pipelined frames: finishes every path of the context's epochs in the pool
 // (the render loop with its tail drain) and enqueues the deferred reads, oldest
 // epoch first.
 static int flush_pipeline(dspbr_ctx* c) {
+  if (int rc = complete_call(c)) return rc;
   if (!c->tail_live && c->older.empty() && !c->deferred) return DSPBR_OK;
   Status s = c->st();
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
@@ -907,7 +932,10 @@ int dspbr_reset(dspbr_ctx* c) {
   { int rc_ = settle_worker(c); if (rc_) return rc_; }
   Status s = c->st();
   if (c->pipelined && c->tail_live) {
-    if (int(c->older.size()) + 1 >= c->depth) {
+    // with a render call in flight, its epochs that finish leave the older
+    // ones when it completes (at the latest in the next render call, before
+    // its launches): until then one more epoch than depth - 1 may wait there
+    if (int(c->older.size()) + 1 >= c->depth && !c->call_inflight) {
       int rc = flush_pipeline(c);
       if (rc) return rc;
     } else {
@@ -1005,10 +1033,13 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
 // Pipelined frames: the render loop until the previous epoch (if it still
 // has paths in the pool) has finished, its deferred read enqueued on the copy
 // stream right then, and on until every sample of these frames has started.
-// The call returns with this epoch's last paths possibly still in the pool.
+// The call returns once the loop launches are enqueued, with this epoch's
+// last paths possibly still in the pool; the next call that needs the pool's
+// state waits for them (complete_call).
 static int render_pipelined(dspbr_ctx* c, int frames) {
   Status s = c->st();
   int rc = settle_worker(c);
+  if (!rc) rc = complete_call(c);
   if (rc) return rc;
   if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
   if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
@@ -1053,8 +1084,9 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
   const unsigned long long max_iter = (items * per_path + pool - 1) / pool + uint64_t(c->depth) * per_path + 8;
   TRY_CUDA(s, cudaEventRecord(c->ev0, c->stream), "event");
   const bool read_oldest = wait >= 0 && c->older.front().deferred;
-  unsigned long long it0 = 0, eager = 0;
-  rc = E.launch_pipelined(wait, max_iter, read_oldest ? c->ev_between : nullptr, &it0, &eager);
+  unsigned long long it0 = 0;
+  int loops = 0;
+  rc = E.launch_pipelined(wait, max_iter, read_oldest ? c->ev_between : nullptr, &it0, &loops);
   if (!rc && read_oldest) {
     // the oldest epoch is complete at ev_between: its image is copied while
     // this epoch's iterations run
@@ -1064,16 +1096,15 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
     rc = issue_read(c, o.sums->p, o.samples, dst, c->ev_between);
   }
   if (!rc) rc = s.cuda(cudaEventRecord(c->ev1, c->stream), "event");
-  if (!rc) rc = s.cuda(cudaStreamSynchronize(c->stream), "render");
   if (rc) return rc;
-  E.finish_pipelined(it0, eager);
-  if (wait >= 0 && !E.job_done(wait))
-    return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: earlier frame not finished after %llu iterations", max_iter);
-  if ((rc = retire_finished(c, nullptr))) return rc;
-  c->tail_live = !E.job_done(c->slot);
-  float ms = 0;
-  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-  c->last_render_ms = ms;
+  // the host goes on (the caller's next camera, reads and render call) while
+  // the loop runs; complete_call takes over its results
+  c->call_inflight = true;
+  c->call_it0 = it0;
+  c->call_loops = loops;
+  c->call_wait = wait;
+  c->call_slot = c->slot;
+  c->tail_live = true;
   return DSPBR_OK;
 }
 
@@ -1089,7 +1120,7 @@ int dspbr_set_pipelining(dspbr_ctx* c, int enable) {
 }
 
 int dspbr_set_pipeline_depth(dspbr_ctx* c, int depth) {
-  if (!c || depth < 2 || depth > 3) return DSPBR_ERR_INVALID;
+  if (!c || depth < 2 || depth > dspbr_ctx::kMaxDepth) return DSPBR_ERR_INVALID;
   int rc = settle(c);
   if (rc) return rc;
   c->depth = depth;
@@ -1479,10 +1510,17 @@ int dspbr_get_device_info(dspbr_ctx* c, dspbr_device_info* info) {
   return DSPBR_OK;
 }
 
+int dspbr_get_sample_count(dspbr_ctx* c, unsigned long long* count) {
+  if (!c || !count) return DSPBR_ERR_INVALID;
+  *count = c->sample_count;
+  return DSPBR_OK;
+}
+
 int dspbr_get_diagnostics(dspbr_ctx* c, dspbr_diag* d) {
   if (!c || !d) return DSPBR_ERR_INVALID;
   // pipelined frames stay in flight: the ray counters cover the iterations run so far
   { int rc_ = settle_worker(c); if (rc_) return rc_; }
+  { int rc_ = complete_call(c); if (rc_) return rc_; }
   Status s = c->st();
   std::memset(d, 0, sizeof *d);
   unsigned long long st[8] = {0, 0, 0, 0, 0, 0, 0, 0};

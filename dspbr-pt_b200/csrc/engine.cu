@@ -298,8 +298,10 @@ void Engine::extend_and_connect(const Sched& sc, const PathBuf& b, int cur) {
 void Engine::drop_graph() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
-  if (loop_graph_) cudaGraphExecDestroy(loop_graph_);
-  loop_graph_ = nullptr;
+  for (auto& g : loop_graph_) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
 }
 
 // Nodes of `g` that no other node depends on.
@@ -317,14 +319,14 @@ static cudaError_t graph_sinks(cudaGraph_t g, std::vector<cudaGraphNode_t>& out)
   return cudaSuccess;
 }
 
-// while (loop) { iteration(0); if (second) iteration(1) }; if (tail[1])
-// { connect(1); drain(1); commit(1) }; if (tail[0]) { connect(0); drain(0);
-// commit(0) }.  The loop condition starts at 1 on every launch; each
+// while (loop) { iteration(p0); if (second) iteration(p0 ^ 1) }; if (tail[0])
+// { connect(0); drain(0); commit(0) }; if (tail[1]) { connect(1); drain(1);
+// commit(1) }.  The loop condition starts at 1 on every launch; each
 // iteration's commit (kernels.cu, k_commit) decides whether the next one
 // runs, so the tail starts after the first iteration that leaves fewer than
 // the drain threshold of paths, at either parity.  LoopCtl::iters_left
 // bounds the number of iterations.
-int Engine::capture_loop_graph() {
+int Engine::capture_loop_graph(int p0) {
   Status s{err_};
   const Sched sc = sched();
   const PathBuf b = paths();
@@ -368,20 +370,20 @@ int Engine::capture_loop_graph() {
   if (e != cudaSuccess) return fail(e, "loop graph node");
   e = cudaGraphConditionalHandleCreate(&h_second, body, 0u, cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return fail(e, "loop graph condition");
-  // iteration A (parity 0)
+  // iteration A (parity p0); the tail after an iteration drains the other parity's queue
   e = cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return fail(e, "loop body capture");
-  iteration(0, LoopHandles{h_loop, h_second, h_tail[1], 1});
+  iteration(p0, LoopHandles{h_loop, h_second, h_tail[p0 ^ 1], 1});
   e = cudaStreamEndCapture(stream_, &captured);
   if (e != cudaSuccess) return fail(e, "loop body capture");
-  // iteration B (parity 1) after A's commit, the only node of the body without dependents
+  // iteration B (parity p0 ^ 1) after A's commit, the only node of the body without dependents
   std::vector<cudaGraphNode_t> sinks;
   if ((e = graph_sinks(body, sinks)) != cudaSuccess) return fail(e, "loop body");
   e = add_cond(body, sinks.data(), sinks.size(), h_second, cudaGraphCondTypeIf, second_node, body_b);
   if (e != cudaSuccess) return fail(e, "loop graph node");
   e = cudaStreamBeginCaptureToGraph(stream_, body_b, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return fail(e, "loop body capture");
-  iteration(1, LoopHandles{h_loop, cudaGraphConditionalHandle(0), h_tail[0], 0});
+  iteration(p0 ^ 1, LoopHandles{h_loop, cudaGraphConditionalHandle(0), h_tail[p0], 0});
   e = cudaStreamEndCapture(stream_, &captured);
   if (e != cudaSuccess) return fail(e, "loop body capture");
   // the tails: connect, drain and commit of the parity the loop stopped at
@@ -397,11 +399,11 @@ int Engine::capture_loop_graph() {
     e = cudaStreamEndCapture(stream_, &captured);
     if (e != cudaSuccess) return fail(e, "loop tail capture");
   }
-  e = cudaGraphInstantiate(&loop_graph_, g, 0);
+  e = cudaGraphInstantiate(&loop_graph_[p0], g, 0);
   cudaGraphDestroy(g);
   g = nullptr;
   if (e != cudaSuccess) {
-    loop_graph_ = nullptr;
+    loop_graph_[p0] = nullptr;
     return fail(e, "loop graph instantiate");
   }
   return DSPBR_OK;
@@ -427,23 +429,17 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
   Status s{err_};
   const volatile HostStatus* hs = h_status_;
   const unsigned long long it0 = hs->iteration;  // every earlier launch has completed
-  unsigned long long eager = 0;
-  if (cur_ == 1) {  // the loop body starts at parity 0
-    int rc = one_iteration(false);
-    if (rc) return rc;
-    eager = 1;
-    max_iter = max_iter > 1 ? max_iter - 1 : 1;
-  }
-  if (!loop_graph_) {
-    int rc = capture_loop_graph();
+  const int p0 = cur_;
+  if (!loop_graph_[p0]) {
+    int rc = capture_loop_graph(p0);
     if (rc) return rc;
   }
   launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopDrain, -1, stream_);
   TRY_CUDA(s, cudaGetLastError(), "loop control");
-  TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+  TRY_CUDA(s, cudaGraphLaunch(loop_graph_[p0], stream_), "loop graph launch");
   TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");
   // the tail's commit counts as one more iteration
-  const unsigned long long body = hs->iteration - it0 - 1 - eager;
+  const unsigned long long body = hs->iteration - it0 - 1;
   kind_launches[0] += body;
   kind_launches[1] += body + 1;
   kind_launches[2] += 5 * body;
@@ -454,42 +450,42 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
 }
 
 int Engine::launch_pipelined(int wait_slot, unsigned long long max_iter, cudaEvent_t between,
-                             unsigned long long* it0, unsigned long long* eager) {
+                             unsigned long long* it0, int* loops) {
   Status s{err_};
-  TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");  // the iteration counter below is current
+  TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");  // the status below is current
   *it0 = h_status_->iteration;
-  *eager = 0;
-  if (cur_ == 1) {  // the loop body starts at parity 0
-    int rc = one_iteration(false);
+  *loops = 0;
+  // the loop starts at the parity the last iteration left: kLoopUntilDone
+  // ends at the parity it started at (or empties the pool), so the same
+  // graph serves the kLoopUntilStarted launch after it
+  const int p0 = cur_;
+  if (!loop_graph_[p0]) {
+    int rc = capture_loop_graph(p0);
     if (rc) return rc;
-    *eager = 1;
   }
-  if (!loop_graph_) {
-    int rc = capture_loop_graph();
-    if (rc) return rc;
-  }
-  if (wait_slot >= 0) {
+  if (wait_slot >= 0 && !job_done(wait_slot)) {
     // the previous epoch's paths were all started: each ends within
     // max_bounces + 1 more iterations; the bound only guards the loop
     launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopUntilDone, wait_slot, stream_);
     TRY_CUDA(s, cudaGetLastError(), "loop control");
-    TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+    TRY_CUDA(s, cudaGraphLaunch(loop_graph_[p0], stream_), "loop graph launch");
+    ++*loops;
   }
   if (between) TRY_CUDA(s, cudaEventRecord(between, stream_), "event");
   launch_set_loop(loop_ctl_.p, max_iter, drain_below_, kLoopUntilStarted, -1, stream_);
   TRY_CUDA(s, cudaGetLastError(), "loop control");
-  TRY_CUDA(s, cudaGraphLaunch(loop_graph_, stream_), "loop graph launch");
+  TRY_CUDA(s, cudaGraphLaunch(loop_graph_[p0], stream_), "loop graph launch");
+  ++*loops;
   return DSPBR_OK;
 }
 
-void Engine::finish_pipelined(unsigned long long it0, unsigned long long eager) {
-  // whole pairs only: the queues of parity 0 hold the paths still alive
-  const unsigned long long body = h_status_->iteration - it0 - eager;
+void Engine::finish_pipelined(unsigned long long it0, int loops) {
+  const unsigned long long body = h_status_->iteration - it0;
   kind_launches[0] += body;
   kind_launches[1] += body;
   kind_launches[2] += 5 * body;
-  kind_launches[3] += 2;
-  cur_ = 0;
+  kind_launches[3] += unsigned(loops);
+  cur_ = int(h_status_->next_cur & 1u);  // the queues of this parity hold the paths still alive
 }
 
 // Two iterations (parity 0, then 1) captured from the stream.  Every argument

@@ -55,14 +55,15 @@ class Engine {
   int run_loop(int slot, unsigned long long max_iter);
   // Pipelined frames (the renders of consecutive accumulation epochs overlap):
   // enqueues the loop graph until job `wait_slot` has finished (skipped when
-  // wait_slot < 0), records `between` (if not null), then the loop graph until
-  // every work item of the active jobs has started; no tail, no host wait.
-  // The paths still alive stay in the pool.  Returns the eager iteration count
-  // in *eager and the iteration counter before the launches in *it0, for
-  // finish_pipelined() once the stream has passed them.
+  // wait_slot < 0 or the job has already finished), records `between` (if not
+  // null), then the loop graph until every work item of the active jobs has
+  // started; no tail, no host wait.  The paths still alive stay in the pool.
+  // Returns the iteration counter before the launches in *it0 and the number
+  // of loop launches in *loops, for finish_pipelined() once the stream has
+  // passed them.
   int launch_pipelined(int wait_slot, unsigned long long max_iter, cudaEvent_t between, unsigned long long* it0,
-                       unsigned long long* eager);
-  void finish_pipelined(unsigned long long it0, unsigned long long eager);
+                       int* loops);
+  void finish_pipelined(unsigned long long it0, int loops);
   // More work items for a job already in the table (a progressive render that
   // continues the same accumulation while its earlier paths are in flight).
   int add_items(int slot, unsigned long long items);
@@ -97,7 +98,7 @@ class Engine {
  private:
   int one_iteration(bool counting);
   int capture_graph();
-  int capture_loop_graph();
+  int capture_loop_graph(int p0);
   void extend_and_connect(const Sched& sc, const PathBuf& b, int cur);
   void drop_graph();
   cudaEvent_t next_event();
@@ -130,8 +131,9 @@ class Engine {
   HostStatus* d_status_ = nullptr;
   // two iterations (parity 0 then 1) captured once
   cudaGraphExec_t graph_ = nullptr;
-  // a render call: while (device condition) { two iterations }, then the tail
-  cudaGraphExec_t loop_graph_ = nullptr;
+  // a render call: while (device condition) { two iterations }, then the tail;
+  // one graph per parity of the loop's first iteration
+  cudaGraphExec_t loop_graph_[2] = {nullptr, nullptr};
   // fork / join of the parallel extend and connect branches during capture
   cudaStream_t side_ = nullptr;
   cudaEvent_t fork_ = nullptr, join_ = nullptr;

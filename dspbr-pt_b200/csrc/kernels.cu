@@ -458,6 +458,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
     const unsigned int live = b.counts[cur ^ 1];
     hs->live_paths = live;
     hs->nactive = uint32_t(n);
+    hs->next_cur = regen_ran ? uint32_t(cur ^ 1) : 0u;
     __threadfence_system();
     hs->iteration = it;
     unsigned long long now;
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
       }
       const bool go = left > 1 && !stop;
       ctl->iters_left = left ? left - 1 : 0;
-      if (mode != kLoopDrain && !tail) {  // whole pairs, no tail
+      if (mode == kLoopUntilDone && !tail) {  // whole pairs, no tail
         if (lh.first) cudaGraphSetConditional(lh.second, 1u);
         else cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
       } else {
@@ -497,7 +498,7 @@ __global__ void __launch_bounds__(kMaxJobs) k_commit(Sched sc, PathBuf b, int cu
         } else {
           cudaGraphSetConditional(lh.loop, go ? 1u : 0u);
         }
-        if (!go) cudaGraphSetConditional(lh.tail, 1u);
+        if (!go && mode != kLoopUntilStarted) cudaGraphSetConditional(lh.tail, 1u);
       }
     }
   }

@@ -58,6 +58,8 @@ struct HostStatus {
   unsigned long long iteration;     // iterations committed so far
   unsigned int live_paths;          // paths queued for the next extend
   unsigned int nactive;
+  unsigned int next_cur;            // parity of the next iteration (0 after a tail drain: both queues empty)
+  unsigned int pad;
   JobStatus job[kMaxJobs];          // by job slot
   unsigned long long stats[8];      // ray counters, stored on request (Engine::read_stats)
 };
@@ -196,16 +198,19 @@ void launch_shade(const Sched& sc, const PathBuf& b, int next, const LaunchCfg& 
 void launch_commit(const Sched& sc, const PathBuf& b, int cur, cudaStream_t st, bool regen_ran = true);
 
 // Device-side loop control of a render call run as one graph.  The loop body
-// is iteration A (parity 0), then iteration B (parity 1) under an IF node.
+// is iteration A, then iteration B of the other parity under an IF node; the
+// loop graph is captured once per parity of A.
 // kLoopDrain: after each iteration k_commit keeps going while iterations
 // remain and either a work item has not started or at least drain_below paths
 // are alive; the commit that stops selects the tail of its parity (an IF node
 // each), which runs every remaining path to its end.
-// kLoopUntilDone / kLoopUntilStarted (pipelined frames): the loop runs whole
-// pairs (A always continues to B, so the next launch starts at parity 0) until
-// job wait_job has finished (every item started, no live path), or until every
-// work item of the active jobs has started; the paths still alive stay in the
-// pool for the next launch.  kLoopUntilDone ends in the tail instead, like
+// kLoopUntilStarted (pipelined frames): stops after the first iteration whose
+// regen placed every work item of the active jobs, at either parity; the paths
+// still alive stay in the pool, and the next launch takes the loop graph that
+// starts at HostStatus::next_cur.
+// kLoopUntilDone (pipelined frames): whole pairs (A always continues to B, so
+// the launch ends at the parity it started at) until job wait_job has finished
+// (every item started, no live path); it ends in the tail instead, like
 // kLoopDrain, once every work item has started and fewer than drain_below
 // paths are alive: the pool is then empty.
 enum { kLoopDrain = 0, kLoopUntilDone = 1, kLoopUntilStarted = 2 };

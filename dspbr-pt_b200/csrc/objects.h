@@ -150,6 +150,7 @@ struct dspbr_ctx {
   // slot and sum buffer.  At most `depth` epochs are in flight: a render call
   // that finds depth - 1 older epochs waits for the oldest before it returns.
   bool pipelined = false;
+  static constexpr int kMaxDepth = 16;
   int depth = 2;
   int slot = 0;
   bool tail_live = false;
@@ -165,6 +166,14 @@ struct dspbr_ctx {
   // its mean and copy are enqueued once the epoch has finished
   float* deferred = nullptr;
   cudaEvent_t ev_between = nullptr;
+  // A pipelined render call returns once its loop launches are enqueued; the
+  // next call that needs the pool's state waits for them (complete_call):
+  // the iteration counter before them, the loop launches, the job slot the
+  // call waited for (-1: none) and its epoch's slot.  Until then tail_live
+  // is assumed.
+  bool call_inflight = false;
+  unsigned long long call_it0 = 0;
+  int call_loops = 0, call_wait = -1, call_slot = 0;
   dspbr::Status st() { return dspbr::Status{&err}; }
 };
 

@@ -190,6 +190,7 @@ SIGNATURES = {
     "dspbr_display_image": (C.c_int, [_V, _F, C.c_int, C.c_int, C.POINTER(Display), _F, C.POINTER(C.c_uint8)]),
     "dspbr_host_free": (C.c_int, [_V, _V]),
     "dspbr_get_diagnostics": (C.c_int, [_V, C.POINTER(Diag)]),
+    "dspbr_get_sample_count": (C.c_int, [_V, C.POINTER(C.c_ulonglong)]),
     "dspbr_get_timeline": (C.c_int, [_V, C.c_uint32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                      C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "dspbr_set_wave_paths": (C.c_int, [_V, C.c_uint32]),

@@ -393,8 +393,8 @@ class PathtracingViewport:
 
     def _set_pipelining(self, v):
         depth = 2 if v is True else int(v)
-        if v is not False and depth not in (0, 1, 2, 3):
-            raise ValueError(f"pipelinedFrames: {v!r} is not a bool, 2 or 3")
+        if v is not False and not 0 <= depth <= 16:
+            raise ValueError(f"pipelinedFrames: {v!r} is not a bool or 2..16")
         on = v is not False and depth >= 2
         if on:
             self.ctx.check(self.ctx.lib.dspbr_set_pipeline_depth(self.ctx.h, depth))
@@ -488,7 +488,9 @@ class PathtracingViewport:
             raise RuntimeError("Cannot start rendering without a scene.")
         self.running = True
         target = 1 if sampleLimit < 0 else int(sampleLimit)
-        done = self.diagnostics["sample_count"]
+        count = C.c_ulonglong(0)
+        self.ctx.check(self.ctx.lib.dspbr_get_sample_count(self.ctx.h, C.byref(count)))
+        done = int(count.value)
         while self.running and done < target:
             n = target - done if frames_per_call is None else min(frames_per_call, target - done)
             self.ctx.check(self.ctx.lib.dspbr_render(self.ctx.h, n))

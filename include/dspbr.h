@@ -247,20 +247,25 @@ int dspbr_read_wait(dspbr_ctx* ctx);
 /* Pipelined frames (off by default).  The reference renders one frame per
  * requestAnimationFrame and presents it (renderer.ts:512-565, 595-714); here
  * the frames of consecutive accumulations overlap on the device.  With it on,
- * dspbr_render returns once every sample of its frames has started: the last
- * paths stay in the path pool and finish during the next dspbr_render, which
- * first completes the previous accumulation.  A reset (setCamera, setSettings,
+ * dspbr_render enqueues the render loop until every sample of its frames has
+ * started and returns without waiting for it: the host prepares the next
+ * frame while the device runs, the last paths stay in the path pool and
+ * finish during the next dspbr_render, which first completes the previous
+ * accumulation.  A device error of the loop is reported by the next call
+ * that waits for it (render, reads, diagnostics).  A reset (setCamera, setSettings,
  * resetAccumulation) starts the new accumulation in a second sum buffer while
  * the old one finishes.  dspbr_read_accum_async of an accumulation still in
  * flight is enqueued when its paths finish (during the next render, or in
  * dspbr_read_wait); dspbr_read_accum, the display reads and every other call
  * finish all paths first.  Images are the same as with it off. */
 int dspbr_set_pipelining(dspbr_ctx* ctx, int enable);
-/* Accumulations in flight with pipelined frames: 2 (default) or 3.  With 3 a
- * render call that finds two earlier accumulations with paths in the pool
- * waits only for the oldest: a caller that takes frame k's image while frame
- * k+2 renders (a render-ahead queue of two frames, dspbr_read_wait_ready)
- * keeps the pool fuller.  Images are the same. */
+/* Accumulations in flight with pipelined frames: 2 (default) to 16.  A
+ * render call that finds depth - 1 earlier accumulations with paths in the
+ * pool waits only for the oldest: a caller that takes frame k's image while
+ * frame k + depth - 1 renders (a render-ahead queue, dspbr_read_wait_ready)
+ * keeps the pool fuller, and each call runs fewer, fuller iterations.  Each
+ * accumulation in flight holds a sum buffer (32 bytes per pixel).  Images are
+ * the same. */
 int dspbr_set_pipeline_depth(dspbr_ctx* ctx, int depth);
 /* Waits for the device-to-host copies enqueued so far (reads of
  * accumulations that have finished) and returns in *in_flight the number of
@@ -306,6 +311,11 @@ int dspbr_display_image(dspbr_ctx* ctx, const float* rgba, int width, int height
 int dspbr_host_alloc(dspbr_ctx* ctx, size_t bytes, void** out);
 int dspbr_host_free(dspbr_ctx* ctx, void* ptr);
 int dspbr_get_diagnostics(dspbr_ctx* ctx, dspbr_diag* diag);
+/* Samples per pixel of the current accumulation handed to render calls so
+ * far (diag.sample_count), read without waiting for the device: the
+ * progressive loop's counter (renderer.ts frameCount), which lets a
+ * pipelined render call's loop run while the caller prepares the next one. */
+int dspbr_get_sample_count(dspbr_ctx* ctx, unsigned long long* count);
 /* The context's GPU (diagnostics.backend's counterpart, renderer.ts:79-110):
  * name, SM count, compute capability, device memory; keys per-GPU caches
  * such as the autotuner's. */

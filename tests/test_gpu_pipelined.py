@@ -36,7 +36,7 @@ def _cam(k):
 
 
 @pytest.mark.parametrize("pool", [0, 4000])
-@pytest.mark.parametrize("mode", [True, 3])
+@pytest.mark.parametrize("mode", [True, 3, 16])
 def test_camera_per_frame_with_async_reads(scene, pool, mode):
     """The interactive loop: per frame setCamera, start(1), then the previous
     frame's readWait and this frame's readAccumulationAsync."""
@@ -116,30 +116,33 @@ def test_pipelined_frames_equal_single_frames_of_a_fresh_viewport(scene):
 
 
 @pytest.mark.parametrize("pool", [0, 4000])
-def test_render_ahead_queue_of_two_frames(scene, pool):
-    """Three accumulations in flight: per frame setCamera, start(1),
-    readWaitReady() (frame k-2's copy is complete) and this frame's
-    readAccumulationAsync; each image equals the frame rendered alone."""
+@pytest.mark.parametrize("depth", [3, 8, 16])
+def test_render_ahead_queue(scene, pool, depth):
+    """`depth` accumulations in flight: per frame setCamera, start(1),
+    readWaitReady() (frame k - depth + 1's copy is complete) and this frame's
+    readAccumulationAsync; each image equals the frame rendered alone.  The
+    render calls stop at either iteration parity, so the frames cover both."""
+    n = depth + 5
     ref = []
     f = _viewport(scene, False, pool=pool)
-    for k in range(7):
-        f.setCamera(_cam(k))
+    for k in range(n):
+        f.setCamera(_cam(k % 7))
         f.start(1)
         ref.append(f.readAccumulation())
     f.dispose()
-    v = _viewport(scene, 3, pool=pool)
-    bufs = [v.allocReadbackBuffer() for _ in range(7)]
-    for k in range(7):
-        v.setCamera(_cam(k))
+    v = _viewport(scene, depth, pool=pool)
+    bufs = [v.allocReadbackBuffer() for _ in range(n)]
+    for k in range(n):
+        v.setCamera(_cam(k % 7))
         v.start(1)
         in_flight = v.readWaitReady()
-        assert 0 <= in_flight <= 2
-        if k >= 2:  # frame k-2 has finished and its copy is on the host
-            np.testing.assert_allclose(bufs[k - 2], ref[k - 2], **TOL)
+        assert 0 <= in_flight <= depth - 1
+        if k >= depth - 1:  # frame k - depth + 1 has finished and its copy is on the host
+            np.testing.assert_allclose(bufs[k - depth + 1], ref[k - depth + 1], **TOL)
         v.readAccumulationAsync(bufs[k])
     v.readWait()
     d = v.diagnostics
-    assert d["rays_primary"] == 7 * 96 * 64 and d["traversal_aborted"] == 0
+    assert d["rays_primary"] == n * 96 * 64 and d["traversal_aborted"] == 0
     v.dispose()
-    for k in range(7):
+    for k in range(n):
         np.testing.assert_allclose(bufs[k], ref[k], **TOL)
