@@ -147,10 +147,18 @@ static int free_slot(const dspbr_ctx* c) {
   }
 }
 
+// A deferred read of a finished epoch, enqueued after the next loop launch.
+struct LateRead {
+  const double4* sums;
+  uint64_t samples;
+  float* dst;
+};
+
 // The older epochs that have finished leave the flight list, oldest first:
-// their deferred reads are enqueued (after `after` when given) and their sum
-// buffers become spares.
-static int retire_finished(dspbr_ctx* c, cudaEvent_t after) {
+// their deferred reads are enqueued (after `after` when given; with `late`,
+// collected there for the caller to enqueue) and their sum buffers become
+// spares (taken again only by a reset, after the caller's reads).
+static int retire_finished(dspbr_ctx* c, cudaEvent_t after, std::vector<LateRead>* late = nullptr) {
   Engine& E = *c->eng;
   for (size_t i = 0; i < c->older.size();) {
     auto& o = c->older[i];
@@ -158,7 +166,9 @@ static int retire_finished(dspbr_ctx* c, cudaEvent_t after) {
       ++i;
       continue;
     }
-    if (o.deferred) {
+    if (o.deferred && late) {
+      late->push_back(LateRead{o.sums->p, o.samples, o.deferred});
+    } else if (o.deferred) {
       int rc = issue_read(c, o.sums->p, o.samples, o.deferred, after);
       if (rc) return rc;
     }
@@ -172,7 +182,7 @@ static int retire_finished(dspbr_ctx* c, cudaEvent_t after) {
 // over its results: the parity the pool's queues are at, the epochs that
 // finished (their deferred reads enqueued, their sums spare), whether the
 // call's epoch still has paths in the pool, and the call's device time.
-static int complete_call(dspbr_ctx* c) {
+static int complete_call(dspbr_ctx* c, std::vector<LateRead>* late = nullptr) {
   if (!c->call_inflight) return DSPBR_OK;
   c->call_inflight = false;
   Status s = c->st();
@@ -182,7 +192,7 @@ static int complete_call(dspbr_ctx* c) {
   E.finish_pipelined(c->call_it0, c->call_loops);
   if (c->call_wait >= 0 && !E.job_done(c->call_wait))
     return s.fail(DSPBR_ERR_DEVICE_FAULT, "render: earlier frame not finished by the render loop");
-  int rc = retire_finished(c, nullptr);
+  int rc = retire_finished(c, nullptr, late);
   if (rc) return rc;
   // a reset since the call has moved its epoch to the older ones
   if (c->slot == c->call_slot && c->tail_live) c->tail_live = !E.job_done(c->slot);
@@ -467,6 +477,7 @@ int dspbr_destroy(dspbr_ctx* c) {
   if (c->mean_stream) cudaStreamDestroy(c->mean_stream);
   if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   if (c->ev_between) cudaEventDestroy(c->ev_between);
+  if (c->ev_retired) cudaEventDestroy(c->ev_retired);
   c->eng.reset();
   if (c->stage) cudaFreeHost(c->stage);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
@@ -1036,10 +1047,11 @@ static int enqueue_frames(dspbr_ctx* c, int frames, bool async) {
 // The call returns once the loop launches are enqueued, with this epoch's
 // last paths possibly still in the pool; the next call that needs the pool's
 // state waits for them (complete_call).
+static int render_pipelined_launch(dspbr_ctx* c, int frames, std::vector<LateRead>& late);
+
 static int render_pipelined(dspbr_ctx* c, int frames) {
   Status s = c->st();
   int rc = settle_worker(c);
-  if (!rc) rc = complete_call(c);
   if (rc) return rc;
   if (frames <= 0) return s.fail(DSPBR_ERR_INVALID, "render: frames must be positive");
   if (!c->scene) return s.fail(DSPBR_ERR_STATE, "render: no scene set");
@@ -1047,6 +1059,24 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
     return s.fail(DSPBR_ERR_STATE, "render: the scene's materials use textures; call dspbr_scene_set_textures");
   if (!c->has_camera) return s.fail(DSPBR_ERR_STATE, "render: no camera set");
   if (c->width <= 0 || !c->accum.p) return s.fail(DSPBR_ERR_STATE, "render: resize() was not called");
+  // the reads of the epochs the last call finished are enqueued after this
+  // call's loop launches (their means wait for ev_retired, recorded before
+  // them): the device goes on to the loop first
+  std::vector<LateRead> late;
+  rc = complete_call(c, &late);
+  if (!rc && !late.empty()) rc = s.cuda(cudaEventRecord(c->ev_retired, c->stream), "event");
+  if (!rc) rc = render_pipelined_launch(c, frames, late);
+  // the reads the launch did not enqueue (an error, or a flush before it)
+  for (const LateRead& r : late) {
+    int rc2 = issue_read(c, r.sums, r.samples, r.dst, c->ev_retired);
+    if (!rc) rc = rc2;
+  }
+  return rc;
+}
+
+static int render_pipelined_launch(dspbr_ctx* c, int frames, std::vector<LateRead>& late) {
+  Status s = c->st();
+  int rc = DSPBR_OK;
   // a read of this epoch waits for the samples rendered so far, not these
   if (c->deferred && (rc = flush_pipeline(c))) return rc;
   TRY_CUDA(s, cudaSetDevice(c->device), "cudaSetDevice");
@@ -1087,6 +1117,9 @@ static int render_pipelined(dspbr_ctx* c, int frames) {
   unsigned long long it0 = 0;
   int loops = 0;
   rc = E.launch_pipelined(wait, max_iter, read_oldest ? c->ev_between : nullptr, &it0, &loops);
+  for (const LateRead& r : late)
+    if (!rc) rc = issue_read(c, r.sums, r.samples, r.dst, c->ev_retired);
+  late.clear();
   if (!rc && read_oldest) {
     // the oldest epoch is complete at ev_between: its image is copied while
     // this epoch's iterations run
@@ -1115,6 +1148,8 @@ int dspbr_set_pipelining(dspbr_ctx* c, int enable) {
   Status s = c->st();
   if (enable && !c->ev_between)
     TRY_CUDA(s, cudaEventCreateWithFlags(&c->ev_between, cudaEventDisableTiming), "event");
+  if (enable && !c->ev_retired)
+    TRY_CUDA(s, cudaEventCreateWithFlags(&c->ev_retired, cudaEventDisableTiming), "event");
   c->pipelined = enable != 0;
   return DSPBR_OK;
 }

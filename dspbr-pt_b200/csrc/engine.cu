@@ -452,7 +452,8 @@ int Engine::run_loop(int slot, unsigned long long max_iter) {
 int Engine::launch_pipelined(int wait_slot, unsigned long long max_iter, cudaEvent_t between,
                              unsigned long long* it0, int* loops) {
   Status s{err_};
-  TRY_CUDA(s, cudaStreamSynchronize(stream_), "render");  // the status below is current
+  // the caller has waited for every earlier loop launch (a pipelined call is
+  // completed before the next one): the status below is current
   *it0 = h_status_->iteration;
   *loops = 0;
   // the loop starts at the parity the last iteration left: kLoopUntilDone

@@ -166,6 +166,7 @@ struct dspbr_ctx {
   // its mean and copy are enqueued once the epoch has finished
   float* deferred = nullptr;
   cudaEvent_t ev_between = nullptr;
+  cudaEvent_t ev_retired = nullptr;  // a render call's start: the epochs retired before it are complete
   // A pipelined render call returns once its loop launches are enqueued; the
   // next call that needs the pool's state waits for them (complete_call):
   // the iteration counter before them, the loop launches, the job slot the
