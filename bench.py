@@ -857,28 +857,36 @@ def run_gpu_arm(args):
         rays = (d4["rays_primary"] + d4["rays_extension"] + d4["rays_shadow"]) - \
                (d3["rays_primary"] + d3["rays_extension"] + d3["rays_shadow"])
         value = reduce_sum(dist, float(rays)) / reduce_max(dist, t1 - t0) / 1e6
-        return value, parts / steps
+        iters = (d4["extend_launches"] - d3["extend_launches"]) / steps  # render-loop iterations per step
+        return value, parts / steps, iters
 
     e2e_run(True)  # untimed: the second buffer's first use
-    e2e_serial, parts_serial = e2e_run(False)
-    e2e_copy, parts_copy = e2e_run(True)
+    e2e_serial, parts_serial, _ = e2e_run(False)
+    e2e_copy, parts_copy, _ = e2e_run(True)
     # pipelined frames: step k+1's samples start while step k's last paths
     # finish; step k's image is copied as soon as they have
     v.setSettings({"pipelinedFrames": True})
     e2e_run(True)  # untimed: the second sum buffer's first use
-    e2e_two, parts_two = e2e_run(True)
+    e2e_two, parts_two, _ = e2e_run(True)
     v.setSettings({"pipelinedFrames": 3})
     e2e_run(True, ahead=True)  # untimed: the third sum buffer's first use
-    e2e_three, parts_three = e2e_run(True, ahead=True)
+    e2e_three, parts_three, iters_three = e2e_run(True, ahead=True)
     # the headline: AHEAD accumulations in flight; each render call runs one
     # iteration over the new frame's camera rays and the earlier frames' last
     # paths, and returns while it runs
     v.setSettings({"pipelinedFrames": AHEAD})
     e2e_run(True, ahead=True, steps=2 * AHEAD)  # untimed: every sum buffer's first use
-    e2e_value, parts = e2e_run(True, ahead=True, steps=e2e_steps)
+    e2e_value, parts, iters_ahead = e2e_run(True, ahead=True, steps=e2e_steps)
+    # device clock between the commits of the loop's last iterations (the
+    # steady state: each holds a new frame and the earlier frames' last paths)
+    tla = v.timeline(64)
+    full = tla[1:, 2] >= 0.5 * tla[:, 2].max() if len(tla) > 1 else np.zeros(0, bool)
+    iter_ms = float(np.median(np.diff(tla[:, 1])[full])) if full.any() else None
     v.setSettings({"pipelinedFrames": False})
     e2e_parts = {"set_camera_ms": 1e3 * parts[0], "render_1_frame_ms": 1e3 * parts[1],
                  "read_wait_ready_and_enqueue_ms": 1e3 * parts[2],
+                 "loop_iterations_per_step": iters_ahead,
+                 "loop_iteration_ms_median": iter_ms,
                  "frames": f"pipelined, {AHEAD} accumulations in flight (viewport setting pipelinedFrames: "
                            f"{AHEAD}): a step's render enqueues one render-loop launch that runs until its "
                            "samples have started and returns without waiting for it; the next step's render "
@@ -888,7 +896,8 @@ def run_gpu_arm(args):
                              "finished and runs beside later renders; each step first waits for the copies "
                              "of the frames that have finished (readWaitReady), the last step for every image",
                  "frames_three_in_flight": {"value": e2e_three, "steps": part_steps,
-                                            "render_1_frame_ms": 1e3 * parts_three[1]},
+                                            "render_1_frame_ms": 1e3 * parts_three[1],
+                                            "loop_iterations_per_step": iters_three},
                  "frames_two_in_flight": {"value": e2e_two, "steps": part_steps,
                                           "render_1_frame_ms": 1e3 * parts_two[1],
                                           "read_wait_and_enqueue_ms": 1e3 * parts_two[2],
