@@ -4,6 +4,8 @@ the device.  Every image must equal
 the image of the same calls without pipelining (FP64 pixel sums in another
 order: allclose 1e-6), whatever mix of camera changes, progressive renders,
 asynchronous and synchronous reads, display reads and resizes comes."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -67,7 +69,7 @@ def test_progressive_and_mixed_calls(scene):
     an accumulation in flight followed by more frames of it, a synchronous
     read, a display read, a resize and a reset with nothing rendered."""
     res = {}
-    for pipelined in (False, True, 3):
+    for pipelined in (False, True, 3, 16):
         v = _viewport(scene, pipelined)
         got = []
         v.setCamera(_cam(0))
@@ -92,9 +94,46 @@ def test_progressive_and_mixed_calls(scene):
         assert v.diagnostics["sample_count"] == 1
         res[pipelined] = got
         v.dispose()
-    for mode in (True, 3):
+    for mode in (True, 3, 16):
         for a, b in zip(res[False], res[mode]):
             np.testing.assert_allclose(b, a, **TOL)
+
+
+def _sample_count(v):
+    n = C.c_ulonglong(0)
+    v.ctx.check(v.ctx.lib.dspbr_get_sample_count(v.ctx.h, C.byref(n)))
+    return n.value
+
+
+def test_calls_while_a_render_loop_runs(scene):
+    """A pipelined render call returns while its loop runs: the counter read
+    without waiting, diagnostics (which wait for the loop), a settings change
+    (a reset), a progressive continuation and a synchronous read right after
+    it give what the same calls give without pipelining."""
+    res = {}
+    for pipelined in (False, 16):
+        v = _viewport(scene, pipelined)
+        got = []
+        v.setCamera(_cam(0))
+        v.start(1)
+        assert _sample_count(v) == 1
+        d = v.diagnostics
+        assert d["sample_count"] == 1 and d["last_render_ms"] > 0.0
+        v.start(3)  # continues the accumulation in flight
+        assert _sample_count(v) == 3
+        v.setSettings({"maxBounces": 5})  # a reset while the loop runs
+        assert _sample_count(v) == 0
+        v.start(1)
+        v.setCamera(_cam(4))
+        v.start(2)
+        got.append(v.readAccumulation())
+        d = v.diagnostics
+        assert d["sample_count"] == 2 and d["traversal_aborted"] == 0
+        got.append(d["rays_primary"])
+        res[pipelined] = got
+        v.dispose()
+    np.testing.assert_allclose(res[16][0], res[False][0], **TOL)
+    assert res[16][1] == res[False][1]
 
 
 def test_pipelined_frames_equal_single_frames_of_a_fresh_viewport(scene):
